@@ -1,0 +1,156 @@
+/*
+ * ipole_b200.h -- C-ABI of the B200 (sm_100a) ray pipeline of ipole.
+ *
+ * The library replaces ipole's per-pixel OpenMP loop (src/main.c:536-615 and
+ * :640-777, each iteration calling get_pixel, src/main.c:822-883) with GPU
+ * kernels: backward geodesic integration in Kerr FMKS coordinates
+ * (src/model_geodesics.c:38-171, src/geodesics.c:9-70), the iharm grid gather
+ * (src/grid.c:15-44, model/iharm/model.c:420-593), the plasma tetrad
+ * (src/model_tetrads.c:35-127), thermal synchrotron coefficients
+ * (src/model_radiation.c:145-332, src/symphony/maxwell_juettner_fits.c) and
+ * the polarized transfer step (src/ipolarray.c:59-628).
+ *
+ * Conventions: every call is synchronous unless it says otherwise, the
+ * caller owns every host buffer, functions return IPG_OK or an IPG_E_* code
+ * and never call exit().  Arrays are plain C arrays; no framework types cross
+ * this boundary.  One context per host thread.
+ */
+#ifndef IPOLE_B200_H
+#define IPOLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the CLI maps them to the reference's exit codes) ---- */
+#define IPG_OK 0
+#define IPG_E_ARG 1       /* invalid argument */
+#define IPG_E_CUDA 2      /* CUDA runtime error or no device */
+#define IPG_E_MAXNSTEP 3  /* a geodesic hit maxnstep (reference: exit(-10), src/main.c:841-845) */
+#define IPG_E_NAN 4       /* NaN in the image (reference: exit(-1), src/main.c:905-908) */
+#define IPG_E_TIMEOUT 5   /* a device-side step budget ran out */
+#define IPG_E_NOMEM 6     /* device or trajectory-pool memory exhausted */
+#define IPG_E_IO 7        /* file read/write error */
+#define IPG_E_STATE 8     /* call order error (e.g. tracing before a model upload) */
+#define IPG_E_FORMAT 9    /* unsupported dump content (metric, schema) */
+
+/* ---- grid / coordinate description (coordinates.h:25-33, grid.h:6) ----
+ * FMKS ("funky" modified Kerr-Schild) only, metric == METRIC_FMKS. */
+typedef struct ipg_grid {
+  int n1, n2, n3;                 /* physical zones (ghost zones excluded) */
+  double startx[4], stopx[4], dx[4];
+  double cstartx[4], cstopx[4];   /* coordinate-system limits (step control) */
+  double a, hslope;               /* spin, MKS hslope */
+  double poly_xt, poly_alpha, mks_smooth, poly_norm;
+  double Rin, Rout, Rh;           /* Rh = 1 + sqrt(1 - a^2) */
+  double rmin_geo, rmax_geo;      /* radiating region in r */
+  double th_beg;                  /* radiating region cut around the poles */
+  double sigma_cut;               /* emission cut: ne = 0 where sigma > sigma_cut */
+  double sigma_cut_high;          /* model key sigma_cut_high (<= 0: off), only decides sigma == sigma_cut */
+  double L_unit;                  /* GM/c^2 in cm */
+} ipg_grid;
+
+/* Field order of ipg_upload_iharm: primitives U1..3, B1..3 (native FMKS
+ * components as in the dump), then the derived cgs fields of
+ * init_physical_quantities (model/iharm/model.c:610-717). */
+enum {
+  IPG_F_U1 = 0, IPG_F_U2, IPG_F_U3, IPG_F_B1, IPG_F_B2, IPG_F_B3,
+  IPG_F_NE, IPG_F_THETAE, IPG_F_B, IPG_F_SIGMA, IPG_NFIELD
+};
+
+/* ---- camera + run parameters of one image (main.c:125-168, par.h) ---- */
+typedef struct ipg_camera {
+  double Xcam[4];                 /* native_coord(rcam, thetacam, phicam) */
+  double Econ[4][4], Ecov[4][4];  /* make_camera_tetrad(Xcam) (or the old centering) */
+  double fovx, fovy;              /* camera FOV: DX / rcam, DY / rcam */
+  double rotcam;                  /* radians */
+  double xoff, yoff;              /* pixel offsets (par keys xoff, yoff) */
+  double freq;                    /* freqcgs * HPL / (ME CL^2) */
+  double freqcgs;
+  double eps;                     /* geodesic accuracy (par key eps) */
+  int nx, ny;                     /* params.nx, params.ny (image size, not the padded internal size) */
+  int maxnstep;
+  int only_unpolarized;           /* -unpol */
+  int emission_type;              /* 4 (Dexter thermal, default) or 1 (Pandya thermal) */
+  int stokes_floors;
+  int target_nturns;              /* -1: off */
+  int subring_dtheta;
+  int counterjet;                 /* isolate_counterjet: 0, 1 or 2 */
+} ipg_camera;
+
+/* ---- per-ray result, the outputs of get_pixel (main.c:822-883) ---- */
+typedef struct ipg_pixel_out {
+  double I_unpol;     /* *Intensity  (invariant, before the nu^3 of save_pixel) */
+  double tau;         /* *Tau */
+  double tauF;        /* *tauF */
+  double I, Q, U, V;  /* project_N outputs (before nu^3 and the qu_conv sign) */
+  int32_t nstep;      /* geodesic steps */
+  int32_t flag;       /* oddflag bits: 1 tetrad, 2 tauF, 4 NaN N, 8 NaN Ucov, 16 singular gcov */
+} ipg_pixel_out;
+
+typedef struct ipg_ctx ipg_ctx;
+
+/* Create a context on CUDA device `device`.  The trajectory pool is sized
+ * from free device memory unless pool_bytes > 0. */
+int ipg_create(ipg_ctx **ctx, int device, size_t pool_bytes);
+void ipg_destroy(ipg_ctx *ctx);
+const char *ipg_strerror(int code);
+/* Text of the last error recorded on the context (CUDA message, pixel id). */
+const char *ipg_last_error(const ipg_ctx *ctx);
+
+/* Upload one iharm FMKS model: grid constants plus IPG_NFIELD ghost-padded
+ * fields, each (n1+2)*(n2+2)*(n3+2) doubles indexed [i][j][k], k fastest,
+ * exactly the arrays model/iharm/model.c keeps in data[0] (p[U1..B3], ne,
+ * thetae, b, sigma).  Replaces the model's static field storage as the source
+ * of get_model_fourv / get_model_ne / get_model_thetae / get_model_b /
+ * get_model_sigma point queries. */
+int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *grid, const double *const fields[IPG_NFIELD]);
+
+/* Trace n pixels (ij[2*m] = i, ij[2*m+1] = j) and return get_pixel's
+ * outputs for each.  Host buffers; the call copies in, runs, copies out.
+ * Returns IPG_E_MAXNSTEP if any ray hit maxnstep (its out[].nstep is
+ * maxnstep-1); the other rays are still filled in. */
+int ipg_trace_pixels(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *ij, size_t n, ipg_pixel_out *out);
+
+/* Same, on device-resident buffers (d_ij: int32[2n], d_out: ipg_pixel_out[n]),
+ * enqueued on `stream` (a cudaStream_t, 0 = legacy default) and
+ * synchronised before return.  No host<->device copies. */
+int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n,
+                            ipg_pixel_out *d_out, void *stream);
+
+/* Kernel statistics of the last trace call: total ray-steps of the geodesic
+ * pass, number of kernel launches, and the device time (ms, CUDA events) of
+ * the geodesic and transfer kernels. */
+typedef struct ipg_stats {
+  uint64_t ray_steps;
+  uint64_t radiating_steps;
+  int32_t launches;
+  int32_t waves;
+  double geodesic_ms;
+  double transfer_ms;
+} ipg_stats;
+int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
+
+/* ---- host-side helpers mirroring the reference's setup code ---- */
+
+/* Camera setup of main.c:125-168 and init_XK's tetrad (model_geodesics.c:
+ * 178-190): native_coord/root_find (coordinates.c:375-442), FOV from
+ * fov (muas) or dx/dy, make_camera_tetrad (model_tetrads.c:143-193) or the
+ * old centering.  Fills cam->Xcam/Econ/Ecov/fovx/fovy/freq/freqcgs and
+ * returns the intensity-to-Jy `scale` and DX, DY (GM/c^2) through pointers. */
+int ipg_camera_setup(const ipg_grid *grid, double rcam, double thetacam_deg, double phicam_deg,
+                     double rotcam_deg, double fovx_muas, double fovy_muas, double dx_rg, double dy_rg,
+                     double dsource_pc, int nx, int ny, double freqcgs, int old_centering,
+                     ipg_camera *cam, double *scale, double *DX, double *DY);
+
+/* Peak FP64 FMA throughput of the device in TFLOP/s (2 flops per FMA),
+ * measured with a register-resident FMA loop for `ms` milliseconds. */
+int ipg_measure_fp64_peak(int device, double ms, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IPOLE_B200_H */

@@ -1,0 +1,128 @@
+/*
+ * ipole_host.h -- host-side C API that mirrors the reference program around
+ * the ray pipeline: parameters (src/par.h, src/par.c), the iharm fluid model
+ * set-up (model/iharm/model.c), the fast-light image driver with adaptive
+ * refinement (src/main.c:506-811) and the image writer (src/io.c:140-273).
+ *
+ * All functions are plain C, return IPG_OK / IPG_E_* and never exit().
+ */
+#ifndef IPOLE_HOST_H
+#define IPOLE_HOST_H
+
+#include "ipole_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IPG_STRLEN 2048
+
+/* Params (src/par.h:14-73) plus the iharm model keys
+ * (model/iharm/model.c:130-167) and the radiation keys
+ * (src/model_radiation.c:77-96). */
+typedef struct ipg_params {
+  double rcam, thetacam, phicam, rotcam;
+  double dx, dy;
+  double fovx_dsource, fovy_dsource;
+  int nx, ny;
+  double dsource;
+  double freqcgs;
+  int old_centering;
+  double eps;
+  int maxnstep;
+  int add_ppm, qu_conv, quench_output, only_unpolarized, perform_check;
+  int emission_type, stokes_floors, isolate_counterjet;
+  char dump[IPG_STRLEN];
+  char outf[IPG_STRLEN];
+  int target_nturns, subring_dtheta;
+  int nx_min, ny_min;
+  double refine_abs, refine_rel, refine_cut;
+  int nearest_neighbor;
+  double xoff, yoff;
+  double img_cadence, restart_int;
+  int trace, trace_stride, trace_i, trace_j;
+  char trace_outf[IPG_STRLEN];
+  int histo, histo_polar;
+  char histo_outf[IPG_STRLEN];
+  /* iharm model keys */
+  double MBH_solar, M_unit, target_mdot;
+  double tp_over_te, trat_small, trat_large, sigma_cut, sigma_cut_high, beta_crit;
+  double cooling_dynamical_times;
+  double rmax_geo, rmin_geo;
+  int reverse_field;
+  double polar_cut;
+  int dump_min, dump_max, dump_skip;
+  /* radiation keys (thermal path ignores the non-thermal ones) */
+  double model_kappa, powerlaw_gamma_cut, powerlaw_gamma_min, powerlaw_gamma_max, powerlaw_p, powerlaw_eta;
+  int variable_kappa;
+  double variable_kappa_min, variable_kappa_interp_start, variable_kappa_max;
+  int bremss, bremss_type;
+} ipg_params;
+
+/* Defaults of load_par_from_argv (src/par.c:48-100) and the model/radiation
+ * statics. */
+void ipg_params_default(ipg_params *p);
+/* try_set_parameter chain (src/par.c:139-210): sets any matching key; unknown
+ * keys are ignored, as in the reference. */
+void ipg_params_set(ipg_params *p, const char *word, const char *value);
+/* load_par (src/par.c:213-232): returns IPG_E_IO if the file cannot be opened. */
+int ipg_params_load_file(ipg_params *p, const char *fname);
+/* load_par_from_argv (src/par.c:43-136): -par, --k=v, --k v, bare --flag,
+ * -unpol, -quench, -check.  Returns IPG_E_ARG for histogram requests (the
+ * reference exits 42) or a missing -par file name. */
+int ipg_params_from_argv(ipg_params *p, int argc, char **argv);
+
+/* The iharm model after init_model (model/iharm/model.c:295-389). */
+typedef struct ipg_iharm_model {
+  ipg_grid grid;
+  double *fields[IPG_NFIELD];  /* ghost-padded, [i][j][k], k fastest */
+  double M_unit, L_unit, T_unit, RHO_unit, U_unit, B_unit, Te_unit, MBH;
+  double Mdot_dump, MdotEdd_dump, Ladv_dump, t, DTd;
+  int electrons;
+  double gam, game, gamp;
+  void *fluid_header;          /* copy of the dump's /header group (for /fluid_header) */
+} ipg_iharm_model;
+
+/* init_model: read the dump named in p->dump (IPGC container holding the
+ * iharm v1 schema), build ghost zones and derived fields.  Returns
+ * IPG_E_IO / IPG_E_FORMAT on a bad dump (reference: exit(-1) / exit(-3)). */
+int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m);
+void ipg_iharm_free(ipg_iharm_model *m);
+
+/* A rendered image, internal size nx x ny (params.nx + 1 when refining an
+ * even size, main.c:107-123), arrays as in main.c:184-197. */
+typedef struct ipg_image {
+  size_t nx, ny;           /* internal (memory) size */
+  double *image;           /* [nx*ny] unpolarized I nu^3 */
+  double *imageS;          /* [nx*ny*5] I, Q, U, V (nu^3, qu_conv sign), tauF; NULL if unpolarized */
+  double *taus;            /* [nx*ny] */
+  int *interp_flag;        /* [nx*ny] 1 where refinement interpolated */
+  double scale;            /* intensity -> Jy per pixel */
+  double Xcam[4];
+  double fovx, fovy;
+  ipg_camera cam;
+  int32_t *oddflag;        /* [nx*ny] oddflag of traced pixels */
+  int32_t *nstep;          /* [nx*ny] steps of traced pixels, 0 if interpolated */
+  size_t traced;           /* pixels traced */
+} ipg_image;
+
+/* Fast-light image of main.c:506-792: base image at nx_min, then the
+ * refinement levels, each level traced with one ipg_trace_pixels call.
+ * Progress lines go to `log` (stderr in the CLI) when non-NULL. */
+int ipg_render_image(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, ipg_image *img, void *log);
+void ipg_image_free(ipg_image *img);
+
+/* print_image_stats (src/main.c:1001-1042) to `log` (a FILE*), same lines;
+ * the "Ftot" line format is kept verbatim for scripts that scrape it. */
+void ipg_print_image_stats(const ipg_image *img, const ipg_params *p, void *log);
+/* Totals of print_image_stats: Ftot, Ftot_unpol, Qtot, Utot, Vtot (Jy). */
+void ipg_image_totals(const ipg_image *img, const ipg_params *p, double tot[5]);
+
+/* dump() (src/io.c:229-273) with write_header (:140-191) and the iharm
+ * output_hdf5 (model/iharm/model.c:1254-1301), as an IPGC container. */
+int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p, const ipg_iharm_model *m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IPOLE_HOST_H */

@@ -1,0 +1,480 @@
+/* Fast-light image driver (src/main.c:98-123, 184-197, 506-811): base image at
+ * nx_min, adaptive refinement levels, save_pixel / lininterp bookkeeping,
+ * image statistics and the image writer (src/io.c:140-273 with the iharm
+ * output_hdf5, model/iharm/model.c:1254-1301).  Every level's pixels are
+ * traced with one ipg_trace_pixels call. */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../ipg_constants.h"
+#include "ipgc.h"
+#include "ipole_host.h"
+
+#define NIMG 5
+#define IPG_VERSION_STRING "ipole-b200-1"
+
+void ipg_image_free(ipg_image *img)
+{
+  free(img->image);
+  free(img->imageS);
+  free(img->taus);
+  free(img->interp_flag);
+  free(img->oddflag);
+  free(img->nstep);
+  memset(img, 0, sizeof(*img));
+}
+
+/* save_pixel, src/main.c:885-910 */
+static int save_pixel(ipg_image *img, const ipg_params *p, size_t i, size_t j, const ipg_pixel_out *o)
+{
+  const size_t ny = img->ny;
+  double f3 = pow(p->freqcgs, 3);
+  img->image[i * ny + j] = o->I_unpol * f3;
+  img->taus[i * ny + j] = o->tau;
+  img->oddflag[i * ny + j] = o->flag;
+  img->nstep[i * ny + j] = o->nstep;
+  if (!p->only_unpolarized) {
+    double *s = img->imageS + (i * ny + j) * NIMG;
+    s[0] = o->I * f3;
+    if (p->qu_conv == 0) {
+      s[1] = -o->Q * f3;
+      s[2] = -o->U * f3;
+    } else {
+      s[1] = o->Q * f3;
+      s[2] = o->U * f3;
+    }
+    s[3] = o->V * f3;
+    s[4] = o->tauF;
+    if (isnan(s[0])) {
+      fprintf(stderr, "NaN in image! Exiting.\n");
+      return IPG_E_NAN;
+    }
+  }
+  return IPG_OK;
+}
+
+/* save_pixelTransfer, src/main.c:912-939 */
+static int copy_pixel(ipg_image *img, int unpol, size_t io, size_t jo, size_t in, size_t jn)
+{
+  const size_t ny = img->ny;
+  img->image[in * ny + jn] = img->image[io * ny + jo];
+  if (!unpol) {
+    img->taus[in * ny + jn] = img->taus[io * ny + jo];
+    for (int c = 0; c < NIMG; c++) img->imageS[(in * ny + jn) * NIMG + c] = img->imageS[(io * ny + jo) * NIMG + c];
+    if (isnan(img->imageS[(io * ny + jo) * NIMG])) return IPG_E_NAN;
+  }
+  return IPG_OK;
+}
+
+/* lininterp2, src/main.c:941-968 */
+static int lininterp2(ipg_image *img, int unpol, size_t i1, size_t j1, size_t i2, size_t j2, size_t in, size_t jn)
+{
+  const size_t ny = img->ny;
+  img->image[in * ny + jn] = .5 * (img->image[i1 * ny + j1] + img->image[i2 * ny + j2]);
+  img->taus[in * ny + jn] = .5 * (img->taus[i1 * ny + j1] + img->taus[i2 * ny + j2]);
+  if (!unpol) {
+    for (int c = 0; c < NIMG; c++)
+      img->imageS[(in * ny + jn) * NIMG + c] =
+          .5 * (img->imageS[(i1 * ny + j1) * NIMG + c] + img->imageS[(i2 * ny + j2) * NIMG + c]);
+    if (isnan(img->imageS[(i1 * ny + j1) * NIMG]) || isnan(img->imageS[(i2 * ny + j2) * NIMG])) return IPG_E_NAN;
+  }
+  return IPG_OK;
+}
+
+/* lininterp4, src/main.c:971-999 */
+static int lininterp4(ipg_image *img, int unpol, size_t i1, size_t j1, size_t i2, size_t j2, size_t i3, size_t j3,
+                      size_t i4, size_t j4, size_t in, size_t jn)
+{
+  const size_t ny = img->ny;
+  img->image[in * ny + jn] = .25 * (img->image[i1 * ny + j1] + img->image[i2 * ny + j2] + img->image[i3 * ny + j3] +
+                                    img->image[i4 * ny + j4]);
+  img->taus[in * ny + jn] =
+      .25 * (img->taus[i1 * ny + j1] + img->taus[i2 * ny + j2] + img->taus[i3 * ny + j3] + img->taus[i4 * ny + j4]);
+  if (!unpol) {
+    for (int c = 0; c < NIMG; c++)
+      img->imageS[(in * ny + jn) * NIMG + c] =
+          .25 * (img->imageS[(i1 * ny + j1) * NIMG + c] + img->imageS[(i2 * ny + j2) * NIMG + c] +
+                 img->imageS[(i3 * ny + j3) * NIMG + c] + img->imageS[(i4 * ny + j4) * NIMG + c]);
+    if (isnan(img->imageS[(i1 * ny + j1) * NIMG]) || isnan(img->imageS[(i2 * ny + j2) * NIMG]) ||
+        isnan(img->imageS[(i3 * ny + j3) * NIMG]) || isnan(img->imageS[(i4 * ny + j4) * NIMG]))
+      return IPG_E_NAN;
+  }
+  return IPG_OK;
+}
+
+static void report_oddities(const ipg_params *p, const int32_t *ij, const ipg_pixel_out *o, size_t n, FILE *log)
+{
+  if (!log) return;
+  for (size_t m = 0; m < n; m++) {
+    if (o[m].flag != 0 || (!p->only_unpolarized && o[m].I < -1.e-10)) {
+      fprintf(log, "\nOddity in pixel %d %d (flag %d):\n", ij[2 * m], ij[2 * m + 1], o[m].flag);
+      fprintf(log, "nstep: %d\n", o[m].nstep);
+      fprintf(log, "Final Stokes parameters: [%g %g %g %g]\n", o[m].I, o[m].Q, o[m].U, o[m].V);
+    }
+  }
+}
+
+static int trace_list(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *ij, size_t n, ipg_pixel_out *out, FILE *log)
+{
+  int rc = ipg_trace_pixels(ctx, cam, ij, n, out);
+  if (rc == IPG_E_MAXNSTEP) {
+    for (size_t m = 0; m < n; m++)
+      if (out[m].nstep >= cam->maxnstep - 1) {
+        if (log) fprintf(log, "\nMaxNStep exceeded in pixel %d %d!\n", ij[2 * m], ij[2 * m + 1]);
+        break;
+      }
+  } else if (rc != IPG_OK && log) {
+    fprintf(log, "trace failed: %s (%s)\n", ipg_strerror(rc), ipg_last_error(ctx));
+  }
+  return rc;
+}
+
+int ipg_render_image(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, ipg_image *img, void *logp)
+{
+  FILE *log = (FILE *)logp;
+  memset(img, 0, sizeof(*img));
+  if (p->perform_check) {
+    if (log) fprintf(log, "-check (check/recheck output) is not supported by this build\n");
+    return IPG_E_ARG;
+  }
+  if (p->nx_min < 0) {
+    p->nx_min = p->nx;
+    p->ny_min = p->ny;
+  }
+  int refine_level = (int)(log2((double)((p->nx - p->nx % 2) / (p->nx_min - p->nx_min % 2))) + 1);
+  size_t nx, ny, nxmin, nymin;
+  if (refine_level > 1 && p->nx % 2 == 0) {
+    nx = p->nx + 1;
+    nxmin = p->nx_min + 1;
+  } else {
+    nx = p->nx;
+    nxmin = p->nx_min;
+  }
+  if (refine_level > 1 && p->ny % 2 == 0) {
+    ny = p->ny + 1;
+    nymin = p->ny_min + 1;
+  } else {
+    ny = p->ny;
+    nymin = p->ny_min;
+  }
+  if (nxmin < 2 || nymin < 2 || nx < 2 || ny < 2) {
+    if (log) fprintf(log, "image sizes below 2 pixels are not supported\n");
+    return IPG_E_ARG;
+  }
+
+  /* camera, main.c:125-168 */
+  ipg_camera *cam = &img->cam;
+  double scale, DX, DY;
+  int rc = ipg_camera_setup(&m->grid, p->rcam, p->thetacam, p->phicam, p->rotcam, p->fovx_dsource, p->fovy_dsource,
+                            p->dx, p->dy, p->dsource, p->nx, p->ny, p->freqcgs, p->old_centering, cam, &scale, &DX, &DY);
+  if (rc) return rc;
+  double fov_to_d = p->dsource * IPG_PC / m->grid.L_unit / IPG_MUAS_PER_RAD;
+  if (p->fovx_dsource != 0.0) {
+  } else if (p->dx != 0.0) {
+    p->fovx_dsource = p->dx / fov_to_d;
+    p->fovy_dsource = p->dy / fov_to_d;
+  } else {
+    p->fovx_dsource = 160.;
+    p->fovy_dsource = 160.;
+  }
+  p->rotcam *= M_PI / 180.;
+  p->dsource *= IPG_PC;
+  p->dx = DX;
+  p->dy = DY;
+  cam->xoff = p->xoff;
+  cam->yoff = p->yoff;
+  cam->eps = p->eps;
+  cam->maxnstep = p->maxnstep;
+  cam->only_unpolarized = p->only_unpolarized;
+  cam->emission_type = p->emission_type;
+  cam->stokes_floors = p->stokes_floors;
+  cam->target_nturns = p->target_nturns;
+  cam->subring_dtheta = p->subring_dtheta;
+  cam->counterjet = p->isolate_counterjet;
+  img->scale = scale;
+  memcpy(img->Xcam, cam->Xcam, sizeof(img->Xcam));
+  img->fovx = cam->fovx;
+  img->fovy = cam->fovy;
+  if (log) {
+    fprintf(log, "Xcam[] = %e %e %e %e\n", cam->Xcam[0], cam->Xcam[1], cam->Xcam[2], cam->Xcam[3]);
+    fprintf(log, "intensity [cgs] to flux per pixel [Jy] conversion: %g\n", scale);
+    fprintf(log, "Dsource: %g [cm]\n", p->dsource);
+    fprintf(log, "Dsource: %g [kpc]\n", p->dsource / (1.e3 * IPG_PC));
+    fprintf(log, "FOVx, FOVy: %g %g [GM/c^2]\n", DX, DY);
+    fprintf(log, "FOVx, FOVy: %g %g [rad]\n", DX * m->grid.L_unit / p->dsource, DY * m->grid.L_unit / p->dsource);
+    fprintf(log, "FOVx, FOVy: %g %g [muas]\n", DX * m->grid.L_unit / p->dsource * IPG_MUAS_PER_RAD,
+            DY * m->grid.L_unit / p->dsource * IPG_MUAS_PER_RAD);
+    if (refine_level > 1) {
+      fprintf(log, "Resolution: %dx%d, refined up to %dx%d (%d levels)\n", p->nx_min, p->ny_min, p->nx, p->ny,
+              refine_level);
+      fprintf(log,
+              "Refinement when relative error is >%g%% or absolute error is >%g%% of estimated total flux, for pixel "
+              "brightness > %f%% of average\n",
+              p->refine_rel * 100, p->refine_abs * 100, p->refine_cut * 100);
+    } else {
+      fprintf(log, "Resolution: %dx%d\n", p->nx, p->ny);
+    }
+  }
+
+  img->nx = nx;
+  img->ny = ny;
+  img->image = (double *)calloc(nx * ny, sizeof(double));
+  img->taus = (double *)calloc(nx * ny, sizeof(double));
+  img->interp_flag = (int *)calloc(nx * ny, sizeof(int));
+  img->oddflag = (int32_t *)calloc(nx * ny, sizeof(int32_t));
+  img->nstep = (int32_t *)calloc(nx * ny, sizeof(int32_t));
+  if (!p->only_unpolarized) img->imageS = (double *)calloc(nx * ny * NIMG, sizeof(double));
+  int32_t *ij = (int32_t *)malloc(2 * nx * ny * sizeof(int32_t));
+  ipg_pixel_out *out = (ipg_pixel_out *)malloc(nx * ny * sizeof(ipg_pixel_out));
+  if (!img->image || !img->taus || !img->interp_flag || !ij || !out || (!p->only_unpolarized && !img->imageS)) {
+    free(ij);
+    free(out);
+    return IPG_E_NOMEM;
+  }
+
+  /* base image, main.c:535-615 */
+  size_t sx = (nx - 1) / (nxmin - 1);
+  size_t sy = (ny - 1) / (nymin - 1);
+  double *prelim = refine_level > 1 ? (double *)calloc(nxmin * nymin, sizeof(double)) : NULL;
+  size_t n = 0;
+  for (size_t i = 0; i < nx; i += sx)
+    for (size_t j = 0; j < ny; j += sy) {
+      ij[2 * n] = (int32_t)i;
+      ij[2 * n + 1] = (int32_t)j;
+      n++;
+    }
+  rc = trace_list(ctx, cam, ij, n, out, log);
+  if (rc) goto done;
+  report_oddities(p, ij, out, n, log);
+  for (size_t q = 0; q < n; q++) {
+    size_t i = (size_t)ij[2 * q], j = (size_t)ij[2 * q + 1];
+    rc = save_pixel(img, p, i, j, &out[q]);
+    if (rc) goto done;
+    img->interp_flag[i * ny + j] = 0;
+    if (refine_level > 1) {
+      double Intensity = out[q].I_unpol;
+      size_t loc = i / sy * nymin + j / sx;
+      if (i % (nx - 1) != 0 && j % (ny - 1) != 0) prelim[loc] = Intensity * sx * sx;
+      else if ((i == 0 && j % (ny - 1) != 0) || (i % (nx - 1) != 0 && j == 0))
+        prelim[loc] = Intensity * (sx / 2 + 1) * sx;
+      else if (i % (nx - 1) != 0 || j % (ny - 1) != 0) prelim[loc] = Intensity * (sx / 2) * sx;
+      else if (i == 0 && j == 0) prelim[loc] = Intensity * (sx / 2 + 1) * (sx / 2 + 1);
+      else if (i == 0 || j == 0) prelim[loc] = Intensity * (sx / 2 + 1) * sx / 2;
+      else prelim[loc] = Intensity * (sx * sx) / 4;
+    }
+  }
+  img->traced = n;
+
+  double Iavg = 0;
+  if (refine_level > 1) {
+    double interp_tot = 0;
+    for (size_t q = 0; q < nxmin * nymin; q++) interp_tot += prelim[q];
+    Iavg = interp_tot * pow(p->freqcgs, 3) / (nx * ny);
+  }
+
+  /* refinement levels, main.c:635-792 */
+  for (int lvl = 1; lvl < refine_level; lvl++) {
+    size_t nsx = sx / pow(2, lvl);
+    size_t nsy = sy / pow(2, lvl);
+    size_t psx = nsx * 2, psy = nsy * 2;
+    if (log) fprintf(log, "Refining level %d of %d, spacing %zu,%zu\n", lvl + 1, refine_level, nsx, nsy);
+    n = 0;
+    for (size_t i = 0; i < nx; i += nsx)
+      for (size_t j = 0; j < ny; j += nsy) {
+        if (i % psx == 0 && j % psy == 0) continue;
+        double I1, I2, I3, err_abs, err_rel;
+        int trace;
+        if (i % psx == 0) {
+          I1 = img->image[i * ny + j - nsy];
+          I2 = img->image[i * ny + j + nsy];
+          err_abs = (I2 - I1) / 2 / Iavg;
+          err_rel = (I2 - I1) / 2 / I1;
+        } else if (j % psy == 0) {
+          I1 = img->image[(i - nsx) * ny + j];
+          I2 = img->image[(i + nsx) * ny + j];
+          err_abs = (I2 - I1) / 2 / Iavg;
+          err_rel = (I2 - I1) / 2 / I1;
+        } else {
+          I1 = img->image[(i - nsx) * ny + j - nsy];
+          I2 = img->image[(i + nsx) * ny + j - nsy];
+          I3 = img->image[(i - nsx) * ny + j + nsy];
+          err_abs = ((I2 + I3) / 2 - I1) / Iavg;
+          err_rel = (I2 + I3) / (2 * I1) - 1.;
+        }
+        trace = (fabs(err_abs) > p->refine_abs && fabs(err_rel) > p->refine_rel) && fabs(I1) > p->refine_cut;
+        if (trace) {
+          ij[2 * n] = (int32_t)i;
+          ij[2 * n + 1] = (int32_t)j;
+          n++;
+          img->interp_flag[i * ny + j] = 0;
+          continue;
+        }
+        img->interp_flag[i * ny + j] = 1;
+        int unpol = p->only_unpolarized;
+        if (i % psx == 0) {
+          rc = p->nearest_neighbor ? copy_pixel(img, unpol, i, j - nsy, i, j)
+                                   : lininterp2(img, unpol, i, j - nsy, i, j + nsy, i, j);
+        } else if (j % psy == 0) {
+          rc = p->nearest_neighbor ? copy_pixel(img, unpol, i - nsx, j, i, j)
+                                   : lininterp2(img, unpol, i - nsx, j, i + nsx, j, i, j);
+        } else {
+          rc = p->nearest_neighbor
+                   ? copy_pixel(img, unpol, i - nsx, j - nsy, i, j)
+                   : lininterp4(img, unpol, i - nsx, j - nsy, i + nsx, j - nsy, i - nsx, j + nsy, i + nsx, j + nsy, i,
+                                j);
+        }
+        if (rc) {
+          if (log) fprintf(log, "NaN in image! Exiting.\n");
+          goto done;
+        }
+      }
+    if (n) {
+      rc = trace_list(ctx, cam, ij, n, out, log);
+      if (rc) goto done;
+      report_oddities(p, ij, out, n, log);
+      for (size_t q = 0; q < n; q++) {
+        rc = save_pixel(img, p, (size_t)ij[2 * q], (size_t)ij[2 * q + 1], &out[q]);
+        if (rc) goto done;
+      }
+      img->traced += n;
+    }
+    size_t total_interpolated = 0;
+    for (size_t q = 0; q < nx * ny; q++) total_interpolated += img->interp_flag[q];
+    size_t nxl = p->nx / nsx, nyl = p->ny / nsy;
+    if (log)
+      fprintf(log, "\n%zu of %zu (%f%%) of computed pixels at %zux%zu were interpolated\n\n", total_interpolated,
+              nxl * nyl, ((double)total_interpolated) / (nxl * nyl) * 100, nxl, nyl);
+  }
+done:
+  free(prelim);
+  free(ij);
+  free(out);
+  return rc;
+}
+
+void ipg_image_totals(const ipg_image *img, const ipg_params *p, double tot[5])
+{
+  double Ftot = 0., Ftot_unpol = 0., Qtot = 0., Utot = 0., Vtot = 0.;
+  const size_t ny = img->ny;
+  for (size_t i = 0; i < (size_t)p->nx; i++)
+    for (size_t j = 0; j < (size_t)p->ny; j++) {
+      Ftot_unpol += img->image[i * ny + j] * img->scale;
+      if (!p->only_unpolarized) {
+        Ftot += img->imageS[(i * ny + j) * NIMG + 0] * img->scale;
+        Qtot += img->imageS[(i * ny + j) * NIMG + 1] * img->scale;
+        Utot += img->imageS[(i * ny + j) * NIMG + 2] * img->scale;
+        Vtot += img->imageS[(i * ny + j) * NIMG + 3] * img->scale;
+      }
+    }
+  tot[0] = Ftot;
+  tot[1] = Ftot_unpol;
+  tot[2] = Qtot;
+  tot[3] = Utot;
+  tot[4] = Vtot;
+}
+
+/* src/main.c:1001-1042 */
+void ipg_print_image_stats(const ipg_image *img, const ipg_params *p, void *logp)
+{
+  FILE *log = (FILE *)logp;
+  if (!log) return;
+  double Imax = 0.0, Iavg = 0.0;
+  size_t imax = 0, jmax = 0;
+  const size_t ny = img->ny;
+  double t[5];
+  ipg_image_totals(img, p, t);
+  if (!p->only_unpolarized)
+    for (size_t i = 0; i < (size_t)p->nx; i++)
+      for (size_t j = 0; j < (size_t)p->ny; j++) {
+        double v = img->imageS[(i * ny + j) * NIMG + 0];
+        Iavg += v;
+        if (v > Imax) {
+          imax = i;
+          jmax = j;
+          Imax = v;
+        }
+      }
+  fprintf(log, "\nscale = %e\n", img->scale);
+  fprintf(log, "imax=%zu jmax=%zu Imax=%g Iavg=%g\n", imax, jmax, Imax, Iavg / (p->nx * p->ny));
+  fprintf(log, "freq: %g Ftot: %g Jy (%g Jy unpol xfer) scale=%g\n", p->freqcgs, t[0], t[1], img->scale);
+  fprintf(log, "nuLnu = %g erg/s\n", 4. * M_PI * t[0] * p->dsource * p->dsource * IPG_JY * p->freqcgs);
+  double LPfrac = 100. * sqrt(t[2] * t[2] + t[3] * t[3]) / t[0];
+  double CPfrac = 100. * t[4] / t[0];
+  fprintf(log, "I,Q,U,V [Jy]: %g %g %g %g\n", t[0], t[2], t[3], t[4]);
+  fprintf(log, "LP,CP [%%]: %g %g\n", LPfrac, CPfrac);
+}
+
+/* dump (src/io.c:229-273) + write_header (:140-191) + output_hdf5
+ * (model/iharm/model.c:1254-1301) */
+int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p, const ipg_iharm_model *m)
+{
+  ipgc_file f = {0};
+  ipgc_put_str(&f, "/@githash", "b200", 20);
+  ipgc_put_group(&f, "/header");
+  ipgc_put_str(&f, "/header/version", IPG_VERSION_STRING, 20);
+  ipgc_put_str(&f, "/header/githash", "b200", 20);
+  ipgc_put_f64(&f, "/header/freqcgs", p->freqcgs);
+  ipgc_put_f64(&f, "/header/scale", img->scale);
+  ipgc_put_f64(&f, "/header/dsource", p->dsource);
+  ipgc_put_str(&f, "/header/evpa_0", p->qu_conv == 0 ? "N" : "W", 2);
+  ipgc_put_group(&f, "/header/camera");
+  ipgc_put_i32(&f, "/header/camera/nx", p->nx);
+  ipgc_put_i32(&f, "/header/camera/ny", p->ny);
+  ipgc_put_f64(&f, "/header/camera/dx", p->dx);
+  ipgc_put_f64(&f, "/header/camera/dy", p->dy);
+  ipgc_put_f64(&f, "/header/camera/fovx_dsource", p->fovx_dsource);
+  ipgc_put_f64(&f, "/header/camera/fovy_dsource", p->fovy_dsource);
+  ipgc_put_f64(&f, "/header/camera/rcam", p->rcam);
+  ipgc_put_f64(&f, "/header/camera/thetacam", p->thetacam);
+  ipgc_put_f64(&f, "/header/camera/phicam", p->phicam);
+  ipgc_put_f64(&f, "/header/camera/rotcam", p->rotcam);
+  ipgc_put_f64(&f, "/header/camera/fovx", img->fovx);
+  ipgc_put_f64(&f, "/header/camera/fovy", img->fovy);
+  ipgc_put_f64(&f, "/header/camera/xoff", p->xoff);
+  ipgc_put_f64(&f, "/header/camera/yoff", p->yoff);
+  uint64_t d4 = 4;
+  ipgc_put_array_f64(&f, "/header/camera/x", 1, &d4, img->Xcam);
+  if (m) {
+    if (m->fluid_header) ipgc_copy_subtree((const ipgc_file *)m->fluid_header, "", &f, "/fluid_header");
+    ipgc_put_f64(&f, "/Mdot", m->Mdot_dump);
+    ipgc_put_f64(&f, "/MdotEdd", m->MdotEdd_dump);
+    ipgc_put_f64(&f, "/Ladv", m->Ladv_dump);
+    ipgc_put_f64(&f, "/header/t", m->t);
+    ipgc_put_f64(&f, "/header/sigma_cut", p->sigma_cut);
+    ipgc_put_group(&f, "/header/electrons");
+    ipgc_put_f64(&f, "/header/electrons/rlow", p->trat_small);
+    ipgc_put_f64(&f, "/header/electrons/rhigh", p->trat_large);
+    ipgc_put_f64(&f, "/header/electrons/beta_crit", p->beta_crit);
+    ipgc_put_i32(&f, "/header/electrons/type", m->electrons);
+    ipgc_put_i32(&f, "/header/field_config", p->reverse_field);
+    ipgc_put_group(&f, "/header/units");
+    ipgc_put_f64(&f, "/header/units/L_unit", m->L_unit);
+    ipgc_put_f64(&f, "/header/units/M_unit", m->M_unit);
+    ipgc_put_f64(&f, "/header/units/T_unit", m->T_unit);
+    ipgc_put_f64(&f, "/header/units/Thetae_unit", m->Te_unit);
+  }
+  double t[5];
+  ipg_image_totals(img, p, t);
+  ipgc_put_f64(&f, "/Ftot_unpol", t[1]);
+  if (!p->only_unpolarized) ipgc_put_f64(&f, "/Ftot", t[0]);
+  ipgc_put_f64(&f, "/nuLnu", 4. * M_PI * t[0] * p->dsource * p->dsource * IPG_JY * p->freqcgs);
+  ipgc_put_f64(&f, "/nuLnu_unpol", 4. * M_PI * t[1] * p->dsource * p->dsource * IPG_JY * p->freqcgs);
+  size_t nx = (size_t)p->nx, ny = (size_t)p->ny;
+  double *buf = (double *)malloc(nx * ny * NIMG * sizeof(double));
+  uint64_t d2[2] = {nx, ny}, d3[3] = {nx, ny, NIMG};
+  for (size_t i = 0; i < nx; i++) memcpy(buf + i * ny, img->image + i * img->ny, ny * sizeof(double));
+  ipgc_put_array_f64(&f, "/unpol", 2, d2, buf);
+  for (size_t i = 0; i < nx; i++) memcpy(buf + i * ny, img->taus + i * img->ny, ny * sizeof(double));
+  ipgc_put_array_f64(&f, "/tau", 2, d2, buf);
+  if (!p->only_unpolarized) {
+    for (size_t i = 0; i < nx; i++)
+      memcpy(buf + i * ny * NIMG, img->imageS + i * img->ny * NIMG, ny * NIMG * sizeof(double));
+    ipgc_put_array_f64(&f, "/pol", 3, d3, buf);
+  }
+  free(buf);
+  int rc = ipgc_write(fname, &f) == 0 ? IPG_OK : IPG_E_IO;
+  ipgc_free(&f);
+  return rc;
+}

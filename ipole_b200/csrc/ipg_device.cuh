@@ -1,0 +1,992 @@
+/*
+ * Device-side physics of the ray pipeline (sm_100a, FP64).
+ *
+ * Each function restates the reference routine it cites.  The arithmetic is
+ * regrouped for the GPU where the regrouping changes results only at the
+ * rounding level (the finite-difference connection amplifies every rounding
+ * of the metric by 1/(2 DEL) = 5e6, so the reference's own noise floor in the
+ * connection is ~1e-9 relative; the regroupings here stay far below that):
+ *
+ *   - the metric and its derivatives use the sparsity of the FMKS Jacobian
+ *     and of the Kerr-Schild metric (g02 = g23 = 0) instead of 4^4 loops;
+ *   - the five metric evaluations of one finite-difference connection share
+ *     their transcendentals (exp, sin/cos of 2 pi X2, sin/cos theta) through
+ *     exact argument differences and short Taylor polynomials;
+ *   - the connection is contracted with the wavevector before it is formed
+ *     (Gamma^k_ij K^i K^j and Gamma^i_kl K^l), never stored as 64 numbers;
+ *   - g^{mu nu} is the closed-form inverse of the FMKS Kerr-Schild metric;
+ *   - the coherency tensor N is kept Hermitian (16 reals instead of 32), and
+ *     evolve_N updates it by the 2x2 tetrad block that the step changes.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "ipg_constants.h"
+
+#define IPG_DEL 1.e-7            /* finite-difference step, src/geometry.c:91 */
+#define IPG_CUT_SMALL_TAU 1e-5   /* src/ipolarray.c:34 */
+#define IPG_CUT_PREVENT_NAN 1e-80 /* src/ipolarray.c:37 */
+#define IPG_STEP_DOUBLES 16
+#define IPG_CHUNK_STEPS 32
+
+/* ray status */
+#define IPG_RAY_OK 0
+#define IPG_RAY_MAXNSTEP 1
+#define IPG_RAY_POOL_FULL 2
+
+struct DevGrid {
+  int n1, n2, n3;
+  int alpha_int;            /* poly_alpha - 1 as an integer exponent, or -1 */
+  double startx[4], stopx[4], dx[4], cstartx[4], cstopx[4];
+  double a, hslope, poly_xt, poly_alpha, mks_smooth, poly_norm;
+  double Rh, rmin_geo, rmax_geo, th_beg, sigma_cut;
+  double sigma_eq_factor;   /* ne factor when sigma == sigma_cut exactly */
+  double L_unit;
+  double dlfac;             /* L_unit * HPL / (ME CL^2), src/model_geodesics.c:94 */
+  long long sj, si;         /* cell strides (k fastest) */
+};
+
+struct DevCam {
+  double Xcam[4];
+  double Econ[4][4], Ecov[4][4];
+  double fovx, fovy;
+  double crot, srot;        /* cos, sin of rotcam */
+  double cproj, sproj;      /* cos, sin of -2 rotcam (project_N) */
+  double xoff, yoff;
+  double freq;
+  double eps;
+  int nx, ny, maxnstep;
+  int unpol, emission_type, stokes_floors, target_nturns, subring_dtheta, counterjet;
+};
+
+/* Defined here: the header is included by exactly one translation unit. */
+__constant__ DevGrid c_grid;
+__constant__ DevCam c_cam;
+
+/* --------------------------------------------------------------------- */
+/* small helpers                                                           */
+/* --------------------------------------------------------------------- */
+__device__ __forceinline__ double ipow_int(double q, int n)
+{
+  double r = 1.0, b = q;
+  while (n > 0) {
+    if (n & 1) r *= b;
+    b *= b;
+    n >>= 1;
+  }
+  return r;
+}
+
+/* q^(alpha-1) of the FMKS polar map */
+__device__ __forceinline__ double fmks_pow_am1(double q)
+{
+  const DevGrid &G = c_grid;
+  return (G.alpha_int >= 0) ? ipow_int(q, G.alpha_int) : pow(q, G.poly_alpha - 1.);
+}
+
+/* exp(d) and sin/cos(d) for |d| < 1e-5 (Taylor; exact to rounding) */
+__device__ __forceinline__ double expm_small(double d) { return d * (1. + d * (0.5 + d * (1. / 6.))); }
+__device__ __forceinline__ void sincos_small(double d, double *s, double *c)
+{
+  double d2 = d * d;
+  *s = d * (1. - d2 * (1. / 6.));
+  *c = 1. - 0.5 * d2;
+}
+
+/* --------------------------------------------------------------------- */
+/* FMKS metric (src/coordinates.c:46-97, 175-239, 263-305)                 */
+/* --------------------------------------------------------------------- */
+struct Met {  /* symmetric; g02 = g23 = 0 in FMKS */
+  double g00, g01, g03, g11, g12, g13, g22, g33;
+};
+
+/* X2-dependent parts of theta(X1,X2) and its Jacobian */
+struct X2P {
+  double S2, C2, y, P, P1;  /* sin 2piX2, cos 2piX2, 2X2-1, q^alpha, q^(alpha-1), q = y/xt */
+};
+
+__device__ __forceinline__ void x2_parts_from(double X2, double S2, double C2, X2P *o)
+{
+  const DevGrid &G = c_grid;
+  o->S2 = S2;
+  o->C2 = C2;
+  o->y = 2. * X2 - 1.;
+  double q = o->y / G.poly_xt;
+  o->P1 = fmks_pow_am1(q);
+  o->P = o->P1 * q;
+}
+
+/* theta, dtheta/dX1 (J21) and dtheta/dX2 (J22) from the parts;
+ * E = exp(mks_smooth (startx1 - X1)) */
+__device__ __forceinline__ void theta_jac(double X2, double E, const X2P &p, double *th, double *J21, double *J22)
+{
+  const DevGrid &G = c_grid;
+  const double omh = 1. - G.hslope;
+  double poly = 1. + p.P / (G.poly_alpha + 1.);
+  double thG = IPG_PI * X2 + (omh * 0.5) * p.S2;
+  double thJ = G.poly_norm * p.y * poly + 0.5 * IPG_PI;
+  *th = thG + E * (thJ - thG);
+  *J21 = -E * G.mks_smooth * (IPG_PI * 0.5 - IPG_PI * X2 + G.poly_norm * p.y * poly - 0.5 * omh * p.S2);
+  *J22 = IPG_PI + omh * IPG_PI * p.C2 +
+         E * (-IPG_PI + 2. * G.poly_norm * poly +
+              (2. * G.poly_alpha * G.poly_norm * p.y * p.P1) / ((1. + G.poly_alpha) * G.poly_xt) - omh * IPG_PI * p.C2);
+}
+
+/* g_{mu nu} of FMKS at (r, theta) with Jacobian J21, J22 (J11 = r) */
+__device__ __forceinline__ Met met_from(double r, double sth, double cth, double J21, double J22)
+{
+  const double a = c_grid.a;
+  double s2 = sth * sth;
+  double rho2 = r * r + a * a * cth * cth;
+  double t = 2. * r / rho2;
+  double G00 = -1. + t, G01 = t, G03 = -a * s2 * t, G11 = 1. + t, G13 = -a * s2 * (1. + t);
+  double G22 = rho2, G33 = s2 * (rho2 + a * a * s2 * (1. + t));
+  Met m;
+  m.g00 = G00;
+  m.g01 = G01 * r;
+  m.g03 = G03;
+  m.g11 = G11 * r * r + G22 * J21 * J21;
+  m.g12 = G22 * J21 * J22;
+  m.g13 = G13 * r;
+  m.g22 = G22 * J22 * J22;
+  m.g33 = G33;
+  return m;
+}
+
+/* Closed-form g^{mu nu} of FMKS Kerr-Schild (the reference inverts gcov by LU,
+ * src/geometry.c:54-64, 252-287; both agree to rounding). */
+struct Gcon {
+  double u00, u01, u02, u11, u12, u13, u22, u23, u33;  /* g^03 = 0 */
+};
+
+__device__ __forceinline__ Gcon gcon_from(double r, double sth, double cth, double J21, double J22)
+{
+  const double a = c_grid.a;
+  double s2 = sth * sth;
+  double rho2 = r * r + a * a * cth * cth;
+  double irho2 = 1. / rho2;
+  double ir = 1. / r;
+  double iJ22 = 1. / J22;
+  double Delta = r * r - 2. * r + a * a;
+  double Gtt = -(1. + 2. * r * irho2), Gtr = 2. * r * irho2, Grr = Delta * irho2, Grp = a * irho2;
+  double Gthth = irho2, Gpp = irho2 / s2;
+  double M21 = -J21 * ir * iJ22; /* dX2/dr */
+  Gcon u;
+  u.u00 = Gtt;
+  u.u01 = Gtr * ir;
+  u.u02 = M21 * Gtr;
+  u.u11 = ir * ir * Grr;
+  u.u12 = ir * M21 * Grr;
+  u.u13 = ir * Grp;
+  u.u22 = M21 * M21 * Grr + iJ22 * iJ22 * Gthth;
+  u.u23 = M21 * Grp;
+  u.u33 = Gpp;
+  return u;
+}
+
+__device__ __forceinline__ void lower(const Met &g, const double v[4], double o[4])
+{
+  o[0] = g.g00 * v[0] + g.g01 * v[1] + g.g03 * v[3];
+  o[1] = g.g01 * v[0] + g.g11 * v[1] + g.g12 * v[2] + g.g13 * v[3];
+  o[2] = g.g12 * v[1] + g.g22 * v[2];
+  o[3] = g.g03 * v[0] + g.g13 * v[1] + g.g33 * v[3];
+}
+
+__device__ __forceinline__ void raise(const Gcon &u, const double v[4], double o[4])
+{
+  o[0] = u.u00 * v[0] + u.u01 * v[1] + u.u02 * v[2];
+  o[1] = u.u01 * v[0] + u.u11 * v[1] + u.u12 * v[2] + u.u13 * v[3];
+  o[2] = u.u02 * v[0] + u.u12 * v[1] + u.u22 * v[2] + u.u23 * v[3];
+  o[3] = u.u13 * v[1] + u.u23 * v[2] + u.u33 * v[3];
+}
+
+/* Everything of one point evaluation of the metric */
+struct PointGeo {
+  double r, th, sth, cth, J21, J22;
+  Met g;
+};
+
+__device__ __forceinline__ void point_geo(double X1, double X2, PointGeo *pg)
+{
+  const DevGrid &G = c_grid;
+  double r = exp(X1);
+  double E = exp(G.mks_smooth * (G.startx[1] - X1));
+  double S2, C2;
+  sincospi(2. * X2, &S2, &C2);
+  X2P p;
+  x2_parts_from(X2, S2, C2, &p);
+  theta_jac(X2, E, p, &pg->th, &pg->J21, &pg->J22);
+  sincos(pg->th, &pg->sth, &pg->cth);
+  pg->r = r;
+  pg->g = met_from(r, pg->sth, pg->cth, pg->J21, pg->J22);
+}
+
+/* --------------------------------------------------------------------- */
+/* Finite-difference connection (src/geometry.c:93-144)                    */
+/* --------------------------------------------------------------------- */
+/* d_d g_{mu nu} for d = 1, 2 (the metric does not depend on X0, X3, so the
+ * reference's differences in those directions are exactly zero). */
+struct Conn {
+  Met D1, D2;   /* partial_1 g, partial_2 g */
+  Gcon gu;      /* g^{mu nu} at X */
+  double r;     /* r at X */
+};
+
+__device__ __forceinline__ Met met_diff(const Met &h, const Met &l, double inv)
+{
+  Met d;
+  d.g00 = (h.g00 - l.g00) * inv;
+  d.g01 = (h.g01 - l.g01) * inv;
+  d.g03 = (h.g03 - l.g03) * inv;
+  d.g11 = (h.g11 - l.g11) * inv;
+  d.g12 = (h.g12 - l.g12) * inv;
+  d.g13 = (h.g13 - l.g13) * inv;
+  d.g22 = (h.g22 - l.g22) * inv;
+  d.g33 = (h.g33 - l.g33) * inv;
+  return d;
+}
+
+__device__ void fd_connection(double X1, double X2, Conn *cn)
+{
+  const DevGrid &G = c_grid;
+  const double sm = G.mks_smooth;
+  /* center */
+  double r = exp(X1);
+  double E = exp(sm * (G.startx[1] - X1));
+  double S2, C2;
+  sincospi(2. * X2, &S2, &C2);
+  X2P p0;
+  x2_parts_from(X2, S2, C2, &p0);
+  double th0, J21, J22;
+  theta_jac(X2, E, p0, &th0, &J21, &J22);
+  double s0, c0;
+  sincos(th0, &s0, &c0);
+  cn->gu = gcon_from(r, s0, c0, J21, J22);
+  cn->r = r;
+
+  /* X1 +- DEL: r and E by exact offsets, theta by its exact difference */
+  {
+    double Xh = X1 + IPG_DEL, Xl = X1 - IPG_DEL;
+    double dh = Xh - X1, dl = Xl - X1; /* exact */
+    double rh = r + r * expm_small(dh), rl = r + r * expm_small(dl);
+    double Eh = E + E * expm_small(-sm * dh), El = E + E * expm_small(-sm * dl);
+    double thh, J21h, J22h, thl, J21l, J22l;
+    theta_jac(X2, Eh, p0, &thh, &J21h, &J22h);
+    theta_jac(X2, El, p0, &thl, &J21l, &J22l);
+    double sd, cd, sh, ch, sl, cl;
+    sincos_small(thh - th0, &sd, &cd);
+    sh = s0 * cd + c0 * sd;
+    ch = c0 * cd - s0 * sd;
+    sincos_small(thl - th0, &sd, &cd);
+    sl = s0 * cd + c0 * sd;
+    cl = c0 * cd - s0 * sd;
+    Met gh = met_from(rh, sh, ch, J21h, J22h);
+    Met gl = met_from(rl, sl, cl, J21l, J22l);
+    cn->D1 = met_diff(gh, gl, 1. / (Xh - Xl));
+  }
+  /* X2 +- DEL */
+  {
+    double Xh = X2 + IPG_DEL, Xl = X2 - IPG_DEL;
+    double dh = Xh - X2, dl = Xl - X2; /* exact */
+    double sd, cd;
+    sincos_small(2. * IPG_PI * dh, &sd, &cd);
+    X2P ph, pl;
+    x2_parts_from(Xh, S2 * cd + C2 * sd, C2 * cd - S2 * sd, &ph);
+    sincos_small(2. * IPG_PI * dl, &sd, &cd);
+    x2_parts_from(Xl, S2 * cd + C2 * sd, C2 * cd - S2 * sd, &pl);
+    double thh, J21h, J22h, thl, J21l, J22l;
+    theta_jac(Xh, E, ph, &thh, &J21h, &J22h);
+    theta_jac(Xl, E, pl, &thl, &J21l, &J22l);
+    double sh, ch, sl, cl;
+    sincos_small(thh - th0, &sd, &cd);
+    sh = s0 * cd + c0 * sd;
+    ch = c0 * cd - s0 * sd;
+    sincos_small(thl - th0, &sd, &cd);
+    sl = s0 * cd + c0 * sd;
+    cl = c0 * cd - s0 * sd;
+    Met gh = met_from(r, sh, ch, J21h, J22h);
+    Met gl = met_from(r, sl, cl, J21l, J22l);
+    cn->D2 = met_diff(gh, gl, 1. / (Xh - Xl));
+  }
+}
+
+/* v = (partial_d g) K */
+__device__ __forceinline__ void dg_dot(const Met &D, const double K[4], double v[4])
+{
+  v[0] = D.g00 * K[0] + D.g01 * K[1] + D.g03 * K[3];
+  v[1] = D.g01 * K[0] + D.g11 * K[1] + D.g12 * K[2] + D.g13 * K[3];
+  v[2] = D.g12 * K[1] + D.g22 * K[2];
+  v[3] = D.g03 * K[0] + D.g13 * K[1] + D.g33 * K[3];
+}
+
+/* Gamma^k_ij K^i K^j (the contraction of push_photon, src/geodesics.c:19-49) */
+__device__ __forceinline__ void geo_accel(const Conn &cn, const double K[4], double acc[4])
+{
+  double v1[4], v2[4], T[4];
+  dg_dot(cn.D1, K, v1);
+  dg_dot(cn.D2, K, v2);
+  double kv1 = K[0] * v1[0] + K[1] * v1[1] + K[2] * v1[2] + K[3] * v1[3];
+  double kv2 = K[0] * v2[0] + K[1] * v2[1] + K[2] * v2[2] + K[3] * v2[3];
+#pragma unroll
+  for (int m = 0; m < 4; m++) T[m] = K[1] * v1[m] + K[2] * v2[m];
+  T[1] -= 0.5 * kv1;
+  T[2] -= 0.5 * kv2;
+  raise(cn.gu, T, acc);
+}
+
+/* A^i_k = Gamma^i_kl K^l (the contraction of push_polar, src/ipolarray.c:253-289) */
+__device__ __forceinline__ void transport_matrix(const Conn &cn, const double K[4], double A[4][4])
+{
+  double v1[4], v2[4], B[4][4];
+  dg_dot(cn.D1, K, v1);
+  dg_dot(cn.D2, K, v2);
+  const Met &D1 = cn.D1, &D2 = cn.D2;
+  /* B[m][k] = 1/2 (K1 d1 g_km + K2 d2 g_km + delta_k1 v1_m + delta_k2 v2_m - delta_m1 v1_k - delta_m2 v2_k) */
+  double d[4][4];
+  d[0][0] = K[1] * D1.g00 + K[2] * D2.g00;
+  d[0][1] = K[1] * D1.g01 + K[2] * D2.g01;
+  d[0][2] = 0.;
+  d[0][3] = K[1] * D1.g03 + K[2] * D2.g03;
+  d[1][1] = K[1] * D1.g11 + K[2] * D2.g11;
+  d[1][2] = K[1] * D1.g12 + K[2] * D2.g12;
+  d[1][3] = K[1] * D1.g13 + K[2] * D2.g13;
+  d[2][2] = K[1] * D1.g22 + K[2] * D2.g22;
+  d[2][3] = 0.;
+  d[3][3] = K[1] * D1.g33 + K[2] * D2.g33;
+  d[1][0] = d[0][1];
+  d[2][0] = d[0][2];
+  d[3][0] = d[0][3];
+  d[2][1] = d[1][2];
+  d[3][1] = d[1][3];
+  d[3][2] = d[2][3];
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      double b = d[k][m];
+      if (k == 1) b += v1[m];
+      if (k == 2) b += v2[m];
+      if (m == 1) b -= v1[k];
+      if (m == 2) b -= v2[k];
+      B[m][k] = 0.5 * b;
+    }
+  const Gcon &u = cn.gu;
+  double gu[4][4] = {{u.u00, u.u01, u.u02, 0.},
+                     {u.u01, u.u11, u.u12, u.u13},
+                     {u.u02, u.u12, u.u22, u.u23},
+                     {0., u.u13, u.u23, u.u33}};
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) A[i][k] = gu[i][0] * B[0][k] + gu[i][1] * B[1][k] + gu[i][2] * B[2][k] + gu[i][3] * B[3][k];
+}
+
+/* --------------------------------------------------------------------- */
+/* Hermitian coherency tensor N = R + i S (R symmetric, S antisymmetric)   */
+/* --------------------------------------------------------------------- */
+struct HermN {
+  double r00, r01, r02, r03, r11, r12, r13, r22, r23, r33;  /* symmetric real part */
+  double s01, s02, s03, s12, s13, s23;                      /* antisymmetric imaginary part, s_ij = Im N^ij (i<j) */
+};
+
+__device__ __forceinline__ void hn_zero(HermN *n)
+{
+  n->r00 = n->r01 = n->r02 = n->r03 = n->r11 = n->r12 = n->r13 = n->r22 = n->r23 = n->r33 = 0.;
+  n->s01 = n->s02 = n->s03 = n->s12 = n->s13 = n->s23 = 0.;
+}
+
+__device__ __forceinline__ void hn_unpack(const HermN &n, double R[4][4], double S[4][4])
+{
+  R[0][0] = n.r00; R[0][1] = n.r01; R[0][2] = n.r02; R[0][3] = n.r03;
+  R[1][0] = n.r01; R[1][1] = n.r11; R[1][2] = n.r12; R[1][3] = n.r13;
+  R[2][0] = n.r02; R[2][1] = n.r12; R[2][2] = n.r22; R[2][3] = n.r23;
+  R[3][0] = n.r03; R[3][1] = n.r13; R[3][2] = n.r23; R[3][3] = n.r33;
+  S[0][0] = 0.; S[0][1] = n.s01; S[0][2] = n.s02; S[0][3] = n.s03;
+  S[1][0] = -n.s01; S[1][1] = 0.; S[1][2] = n.s12; S[1][3] = n.s13;
+  S[2][0] = -n.s02; S[2][1] = -n.s12; S[2][2] = 0.; S[2][3] = n.s23;
+  S[3][0] = -n.s03; S[3][1] = -n.s13; S[3][2] = -n.s23; S[3][3] = 0.;
+}
+
+/* out = base - dl (A M + M A^T), M Hermitian (push_polar, src/ipolarray.c:277-287) */
+__device__ __forceinline__ void hn_push(const HermN &base, const HermN &Mh, const double A[4][4], double dl, HermN *out)
+{
+  double R[4][4], S[4][4], AR[4][4], AS[4][4];
+  hn_unpack(Mh, R, S);
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      AR[i][j] = A[i][0] * R[0][j] + A[i][1] * R[1][j] + A[i][2] * R[2][j] + A[i][3] * R[3][j];
+      AS[i][j] = A[i][0] * S[0][j] + A[i][1] * S[1][j] + A[i][2] * S[2][j] + A[i][3] * S[3][j];
+    }
+  out->r00 = base.r00 - dl * (AR[0][0] + AR[0][0]);
+  out->r01 = base.r01 - dl * (AR[0][1] + AR[1][0]);
+  out->r02 = base.r02 - dl * (AR[0][2] + AR[2][0]);
+  out->r03 = base.r03 - dl * (AR[0][3] + AR[3][0]);
+  out->r11 = base.r11 - dl * (AR[1][1] + AR[1][1]);
+  out->r12 = base.r12 - dl * (AR[1][2] + AR[2][1]);
+  out->r13 = base.r13 - dl * (AR[1][3] + AR[3][1]);
+  out->r22 = base.r22 - dl * (AR[2][2] + AR[2][2]);
+  out->r23 = base.r23 - dl * (AR[2][3] + AR[3][2]);
+  out->r33 = base.r33 - dl * (AR[3][3] + AR[3][3]);
+  out->s01 = base.s01 - dl * (AS[0][1] - AS[1][0]);
+  out->s02 = base.s02 - dl * (AS[0][2] - AS[2][0]);
+  out->s03 = base.s03 - dl * (AS[0][3] - AS[3][0]);
+  out->s12 = base.s12 - dl * (AS[1][2] - AS[2][1]);
+  out->s13 = base.s13 - dl * (AS[1][3] - AS[3][1]);
+  out->s23 = base.s23 - dl * (AS[2][3] - AS[3][2]);
+}
+
+/* Stokes parameters of N in a tetrad with covariant rows e1 = Ecov[1],
+ * e2 = Ecov[2] (complex_coord_to_tetrad_rank2 + tensor_to_stokes,
+ * src/ipolarray.c:684-728); also returns the block entries. */
+__device__ __forceinline__ void hn_stokes(const HermN &n, const double e1[4], const double e2[4], double *T11,
+                                          double *T22, double *T12r, double *T21i)
+{
+  double R[4][4], S[4][4];
+  hn_unpack(n, R, S);
+  double Re1[4], Re2[4], Se1[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    Re1[k] = R[k][0] * e1[0] + R[k][1] * e1[1] + R[k][2] * e1[2] + R[k][3] * e1[3];
+    Re2[k] = R[k][0] * e2[0] + R[k][1] * e2[1] + R[k][2] * e2[2] + R[k][3] * e2[3];
+    Se1[k] = S[k][0] * e1[0] + S[k][1] * e1[1] + S[k][2] * e1[2] + S[k][3] * e1[3];
+  }
+  *T11 = e1[0] * Re1[0] + e1[1] * Re1[1] + e1[2] * Re1[2] + e1[3] * Re1[3];
+  *T22 = e2[0] * Re2[0] + e2[1] * Re2[1] + e2[2] * Re2[2] + e2[3] * Re2[3];
+  *T12r = e1[0] * Re2[0] + e1[1] * Re2[1] + e1[2] * Re2[2] + e1[3] * Re2[3];
+  /* Im T21 = e2 . S . e1 */
+  *T21i = e2[0] * Se1[0] + e2[1] * Se1[1] + e2[2] * Se1[2] + e2[3] * Se1[3];
+}
+
+/* --------------------------------------------------------------------- */
+/* Modified Bessel functions K0, K1, K2 (the reference calls GSL's
+ * gsl_sf_bessel_Kn, src/symphony/maxwell_juettner_fits.c:227-228,263-264,376)
+ * x <= 2: ascending series (Abramowitz & Stegun 9.6.11); x > 2: Temme's
+ * method / Steed's continued fraction CF2; K2 = K0 + (2/x) K1.  Values that
+ * underflow return 0. */
+/* --------------------------------------------------------------------- */
+__device__ void bessel_k012(double x, double *k0, double *k1, double *k2)
+{
+  if (x <= 2.0) {
+    const double EG = 0.57721566490153286061;
+    double y = 0.25 * x * x;
+    double lg = log(0.5 * x);
+    double t = 1.0, i0 = 1.0, sum0 = 0.0, hk = 0.0;
+    double u = 1.0, i1s = 1.0;
+    double psi1 = -EG, psi2 = 1.0 - EG;
+    double sum1 = psi1 + psi2;
+    for (int k = 1; k < 60; k++) {
+      double dk = (double)k;
+      t *= y / (dk * dk);
+      hk += 1.0 / dk;
+      i0 += t;
+      sum0 += t * hk;
+      u *= y / (dk * (dk + 1.));
+      psi1 += 1.0 / dk;
+      psi2 += 1.0 / (dk + 1.);
+      i1s += u;
+      sum1 += u * (psi1 + psi2);
+      if (t < 1e-18 * i0 && u < 1e-18 * i1s) break;
+    }
+    *k0 = -(lg + EG) * i0 + sum0;
+    *k1 = 1.0 / x + lg * (0.5 * x * i1s) - 0.25 * x * sum1;
+    *k2 = *k0 + 2.0 / x * *k1;
+    return;
+  }
+  const double a1 = 0.25;
+  double b = 2.0 * (1.0 + x);
+  double d = 1.0 / b;
+  double delh = d, h = d;
+  double q1 = 0.0, q2 = 1.0;
+  double q = a1, c = a1;
+  double a = -a1;
+  double s = 1.0 + q * delh;
+  for (int i = 2; i < 10000; i++) {
+    a -= 2.0 * (i - 1);
+    c = -a * c / i;
+    double qnew = (q1 - b * q2) / a;
+    q1 = q2;
+    q2 = qnew;
+    q += c * qnew;
+    b += 2.0;
+    d = 1.0 / (b + a * d);
+    delh = (b * d - 1.0) * delh;
+    h += delh;
+    double dels = q * delh;
+    s += dels;
+    if (fabs(dels / s) < 1.0e-17) break;
+  }
+  h = a1 * h;
+  double k0s = sqrt(IPG_PI / (2.0 * x)) / s;
+  double k1s = k0s * (x + 0.5 - h) / x;
+  double ex = exp(-x);
+  *k0 = k0s * ex;
+  *k1 = k1s * ex;
+  *k2 = (k0s + 2.0 / x * k1s) * ex;
+}
+
+/* --------------------------------------------------------------------- */
+/* Model point evaluation: grid gather + four-vectors                     */
+/* (src/grid.c:15-44, 216-334; model/iharm/model.c:420-593)               */
+/* --------------------------------------------------------------------- */
+struct ModelPt {
+  PointGeo geo;
+  Gcon gu;
+  double Ucon[4], Ucov[4], Bcon[4], Bcov[4];
+  double ne, thetae, bmag;
+  int in_domain;
+};
+
+__device__ __forceinline__ void model_point(const double *__restrict__ fields, double X1, double X2, double X3,
+                                            const PointGeo &pg, ModelPt *mp)
+{
+  const DevGrid &G = c_grid;
+  mp->geo = pg;
+  mp->gu = gcon_from(mp->geo.r, mp->geo.sth, mp->geo.cth, mp->geo.J21, mp->geo.J22);
+  const Met &g = mp->geo.g;
+  mp->in_domain = !(X1 < G.startx[1] || X1 >= G.stopx[1] || X2 < G.startx[2] || X2 >= G.stopx[2]);
+  if (!mp->in_domain) {
+    double u0 = -1. / sqrt(-mp->gu.u00);
+    mp->Ucov[0] = u0;
+    mp->Ucov[1] = mp->Ucov[2] = mp->Ucov[3] = 0.;
+    mp->Ucon[0] = u0 * mp->gu.u00;
+    mp->Ucon[1] = u0 * mp->gu.u01;
+    mp->Ucon[2] = u0 * mp->gu.u02;
+    mp->Ucon[3] = 0.;
+    for (int m = 0; m < 4; m++) mp->Bcon[m] = mp->Bcov[m] = 0.;
+    mp->ne = mp->thetae = mp->bmag = 0.;
+    return;
+  }
+  /* Xtoijk_ghost, src/grid.c:216-283 */
+  double phi = fmod(X3, G.cstopx[3]);
+  if (phi < 0.0) phi = G.cstopx[3] + phi;
+  int i = (int)((X1 - G.startx[1]) / G.dx[1] - 0.5 + 1000) - 1000;
+  int j = (int)((X2 - G.startx[2]) / G.dx[2] - 0.5 + 1000) - 1000;
+  int k = (int)((phi - G.startx[3]) / G.dx[3] - 0.5 + 1000) - 1000;
+  i = max(-1, min(i, G.n1 - 1));
+  j = max(-1, min(j, G.n2 - 1));
+  k = max(-1, min(k, G.n3 - 1));
+  double d1 = (X1 - ((i + 0.5) * G.dx[1] + G.startx[1])) / G.dx[1];
+  double d2 = (X2 - ((j + 0.5) * G.dx[2] + G.startx[2])) / G.dx[2];
+  double d3 = (phi - ((k + 0.5) * G.dx[3] + G.startx[3])) / G.dx[3];
+  d1 = fmin(fmax(d1, 0.), 1.);
+  d2 = fmin(fmax(d2, 0.), 1.);
+  d3 = fmin(fmax(d3, 0.), 1.);
+  i += 1;
+  j += 1;
+  k += 1;
+  /* interp_scalar, src/grid.c:15-44, for all 10 fields at once */
+  double b1 = 1. - d1, b2 = 1. - d2, b3 = 1. - d3;
+  double w[8] = {b1 * b2 * b3, b1 * b2 * d3, b1 * d2 * b3, b1 * d2 * d3,
+                 d1 * b2 * b3, d1 * b2 * d3, d1 * d2 * b3, d1 * d2 * d3};
+  long long c0 = ((long long)i * G.si + (long long)j * G.sj + k);
+  long long cs[4] = {c0, c0 + G.sj, c0 + G.si, c0 + G.si + G.sj};
+  double acc[10];
+#pragma unroll
+  for (int f = 0; f < 10; f++) acc[f] = 0.;
+#pragma unroll
+  for (int cc = 0; cc < 4; cc++) {
+    const double2 *p = reinterpret_cast<const double2 *>(fields + cs[cc] * 10);
+    /* two adjacent cells in k: 20 contiguous doubles */
+#pragma unroll
+    for (int h = 0; h < 10; h++) {
+      double2 v = __ldg(p + h);
+      int f0 = (2 * h) % 10, kk = (2 * h) / 10;
+      double wt = w[2 * cc + kk];
+      acc[f0] += wt * v.x;
+      acc[f0 + 1] += wt * v.y;
+    }
+  }
+  double V1 = acc[0], V2 = acc[1], V3 = acc[2];
+  double Bp1 = acc[3], Bp2 = acc[4], Bp3 = acc[5];
+  double ne = acc[6], th_e = acc[7], bm = acc[8], sig = acc[9];
+  /* get_model_fourv, model/iharm/model.c:455-492 */
+  double VdotV = g.g11 * V1 * V1 + g.g12 * V1 * V2 + g.g13 * V1 * V3 + g.g12 * V2 * V1 + g.g22 * V2 * V2 +
+                 g.g13 * V3 * V1 + g.g33 * V3 * V3;
+  double Vfac = sqrt(-1. / mp->gu.u00 * (1. + fabs(VdotV)));
+  mp->Ucon[0] = -Vfac * mp->gu.u00;
+  mp->Ucon[1] = V1 - Vfac * mp->gu.u01;
+  mp->Ucon[2] = V2 - Vfac * mp->gu.u02;
+  mp->Ucon[3] = V3; /* g^03 = 0 */
+  lower(g, mp->Ucon, mp->Ucov);
+  mp->Bcon[0] = Bp1 * mp->Ucov[1] + Bp2 * mp->Ucov[2] + Bp3 * mp->Ucov[3];
+  double iu0 = 1. / mp->Ucon[0];
+  mp->Bcon[1] = (Bp1 + mp->Ucon[1] * mp->Bcon[0]) * iu0;
+  mp->Bcon[2] = (Bp2 + mp->Ucon[2] * mp->Bcon[0]) * iu0;
+  mp->Bcon[3] = (Bp3 + mp->Ucon[3] * mp->Bcon[0]) * iu0;
+  lower(g, mp->Bcon, mp->Bcov);
+  /* get_model_ne with the geodesic sigma cut, model/iharm/model.c:567-593 */
+  if (sig > G.sigma_cut) ne = 0.;
+  else if (!(sig < G.sigma_cut)) ne = ne * G.sigma_eq_factor;
+  mp->ne = ne;
+  mp->thetae = th_e;
+  mp->bmag = bm;
+}
+
+/* --------------------------------------------------------------------- */
+/* Radiation coefficients (src/model_radiation.c:145-332, src/radiation.c) */
+/* --------------------------------------------------------------------- */
+/* src/radiation.c:14-23 */
+__device__ __forceinline__ double Bnu_inv(double nu, double Thetae)
+{
+  double x = IPG_HPL * nu / (IPG_ME * IPG_CL * IPG_CL * Thetae);
+  if (x < 2.e-3)
+    return ((2. * IPG_HPL / (IPG_CL * IPG_CL)) / (x / 24. * (24. + x * (12. + x * (4. + x)))));
+  return ((2. * IPG_HPL / (IPG_CL * IPG_CL)) / (exp(x) - 1.));
+}
+
+struct Jar {
+  double jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV;
+};
+
+/* Faraday rotativities rho_Q (Dexter 2016), rho_V (Shcherbakov 2008), both
+ * times nu (src/symphony/maxwell_juettner_fits.c:207-284) */
+__device__ __forceinline__ void rho_QV(double Ne, double nu, double Thetae, double B, double theta, double k0,
+                                       double k1, double k2, int want_q, double *rQ, double *rV)
+{
+  const double pi = 3.1415926535897932384;
+  double omega0 = IPG_EE * B / (IPG_ME * IPG_CL);
+  double wp2 = 4. * pi * Ne * (IPG_EE * IPG_EE) / IPG_ME;
+  double sth, cth;
+  sincos(theta, &sth, &cth);
+  double x = Thetae * sqrt(sqrt(2.) * sth * (1.e3 * omega0 / (2. * pi * nu)));
+  double tpn = 2. * pi * nu;
+  if (want_q) {
+    double lx = log(x);
+    double e472 = exp(-x / 47.2);
+    double extraterm = (.011 * e472 - 0.011767707320949831 * pi * 1.e4 *
+                                          pow((x + 1.e-16), (-8. / 3.))) *
+                       (0.5 + 0.5 * tanh((lx - 4.78749174278204599425) / 0.1));
+    double jffunc = 2.011 * exp(-pow(x, 1.035) / 4.7) - cos(x / 2.) * exp(-pow(x, 1.2) / 2.73) - .011 * e472 + extraterm;
+    double k_ratio = (k2 > 0) ? k1 / k2 : 1;
+    double tpn2 = tpn * tpn;
+    double eps11m22 = jffunc * wp2 * (omega0 * omega0) / (tpn2 * tpn2) * (k_ratio + 6. * Thetae) * (sth * sth);
+    *rQ = tpn / (2. * IPG_CL) * eps11m22 * nu;
+  }
+  double k_ratio = (k2 > 0) ? k0 / k2 : 1;
+  double shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
+  double eps12 = wp2 * omega0 / (tpn * tpn * tpn) * (k_ratio * shgmfunc) * cth;
+  *rV = tpn / IPG_CL * eps12 * nu;
+}
+
+/* Coefficients at one point for both calls the reference makes there:
+ * pol = 0 (get_jkinv: Leung j_I / nu^2, Kirchhoff a_I) into (*ju, *ku) and
+ * pol = 1 (jar_calc) into *jr.  src/model_radiation.c:145-332 with
+ * emission_type 4 (Dexter) or 1 (Pandya); U components are zero. */
+__device__ void jar_both(const ModelPt &mp, const double K[4], int want_pol, int emission_type, double *ju,
+                         double *ku, Jar *jr)
+{
+  const double pi = IPG_PI;
+  Jar z = {0., 0., 0., 0., 0., 0., 0., 0., 0., 0., 0.};
+  *jr = z;
+  *ju = 0.;
+  *ku = 0.;
+  double Ne = mp.ne;
+  if (Ne <= 0.) return;
+  /* get_fluid_nu, src/radiation.c:26-44 */
+  double kdu = K[0] * mp.Ucov[0] + K[1] * mp.Ucov[1] + K[2] * mp.Ucov[2] + K[3] * mp.Ucov[3];
+  double nu = -kdu * IPG_ME * IPG_CL * IPG_CL / IPG_HPL;
+  double nusq = nu * nu;
+  /* get_bk_angle, src/radiation.c:47-72 */
+  double theta;
+  {
+    double Bm = sqrt(fabs(mp.Bcon[0] * mp.Bcov[0] + mp.Bcon[1] * mp.Bcov[1] + mp.Bcon[2] * mp.Bcov[2] +
+                          mp.Bcon[3] * mp.Bcov[3]));
+    if (Bm == 0.) {
+      theta = pi / 2.;
+    } else {
+      double kk = fabs(kdu);
+      double mu = (K[0] * mp.Bcov[0] + K[1] * mp.Bcov[1] + K[2] * mp.Bcov[2] + K[3] * mp.Bcov[3]) / (kk * Bm);
+      if (fabs(mu) > 1.) mu /= fabs(mu);
+      theta = acos(mu);
+    }
+  }
+  double Thetae = mp.thetae, B = mp.bmag;
+  double k0, k1, k2;
+  bessel_k012(1. / Thetae, &k0, &k1, &k2);
+  if (theta <= 0.0 || theta >= pi) {
+    if (want_pol) {
+      double rq;
+      rho_QV(Ne, nu, Thetae, B, theta, k0, k1, k2, 0, &rq, &jr->rV);
+    }
+    return;
+  }
+  double sth = sin(theta);
+  double Bnuinv = Bnu_inv(nu, Thetae);
+  /* pol = 0: Leung fit, src/symphony/maxwell_juettner_fits.c:368-395 */
+  {
+    double K2 = fmax(k2, IPG_SMALL);
+    double nuc = IPG_EE * B / (2. * pi * IPG_ME * IPG_CL);
+    double nus = (2. / 9.) * nuc * Thetae * Thetae * sth;
+    double j = 0.;
+    if (!(nu > 1.e12 * nus)) {
+      double x = nu / nus;
+      double cx = cbrt(x);
+      double f = sqrt(x) + 1.8877486253633868 * sqrt(cx); /* 2^(11/12) x^(1/6) */
+      f = f * f;
+      j = (1.4142135623730951 * pi * IPG_EE * IPG_EE * Ne * nus / (3. * IPG_CL * K2)) * f * exp(-cx);
+    }
+    *ju = j / nusq;
+    *ku = (Bnuinv > 0) ? *ju / Bnuinv : 0.;
+  }
+  if (!want_pol) return;
+  /* pol = 1 */
+  double jI, jQ, jV;
+  if (emission_type == 1) {
+    /* Pandya+ 2016, src/symphony/maxwell_juettner_fits.c:27-129 */
+    double nu_c = IPG_EE * B / (2. * pi * IPG_ME * IPG_CL);
+    double nu_s = (2. / 9.) * nu_c * sth * Thetae * Thetae;
+    double X = nu / nu_s;
+    double prefactor = (Ne * (IPG_EE * IPG_EE) * nu_c) / IPG_CL;
+    double cX = cbrt(X);
+    double eX = exp(-cX);
+    double sX = sqrt(X), X16 = sqrt(cX);
+    double t1 = 1.4142135623730951 * pi / 27. * sth;
+    double tI = sX + 1.8877486253633868 * X16;
+    jI = prefactor * t1 * (tI * tI) * eX;
+    double te = pow(Thetae, 24. / 25.);
+    double tq = (7. * te + 35.) / (10. * te + 75.);
+    double tQ = sX + tq * 1.8877486253633868 * X16;
+    jQ = prefactor * t1 * (tQ * tQ) * eX;
+    double v1 = (37. - 87. * sin(theta - 28. / 25.)) / (100. * (Thetae + 1.));
+    double v2 = pow(1. + (pow(Thetae, 3. / 5.) / 25. + 7. / 10.) * pow(X, 9. / 25.), 5. / 3.);
+    jV = prefactor * v1 * v2 * eX;
+  } else {
+    /* Dexter 2016, src/symphony/maxwell_juettner_fits.c:287-356 */
+    double nus = 3.0 * IPG_EE * B * sth / 4.0 / pi / IPG_ME / IPG_CL * Thetae * Thetae + 1.0;
+    double x = nu / nus;
+    double cx = cbrt(x), icx = 1. / cx;
+    double ex = exp(-1.8899 * cx);
+    double pre = Ne * IPG_EE * IPG_EE * nu / 2. / 1.7320508075688772 / IPG_CL / Thetae / Thetae;
+    double II = 2.5651 * (1 + 1.92 * icx + 0.9977 * icx * icx) * ex;
+    double IQ = 2.5651 * (1 + 0.93193 * icx + 0.499873 * icx * icx) * ex;
+    double IV = (1.81384 / x + 3.42319 * icx * icx + 0.0292545 * rsqrt(x) + 2.03773 * icx) * ex;
+    jI = pre * II;
+    jQ = pre * IQ;
+    jV = 2. * Ne * IPG_EE * IPG_EE * nu / tan(theta) / 3. / 1.7320508075688772 / IPG_CL / Thetae / Thetae / Thetae * IV;
+  }
+  jI /= nusq;
+  jQ /= nusq;
+  jV /= nusq;
+  double jU = -0. / nusq;
+  double jP = sqrt(jQ * jQ + jU * jU + jV * jV);
+  if (jI < jP / 0.99) {
+    double pf = jI / jP * 0.99;
+    jQ *= pf;
+    jU *= pf;
+    jV *= pf;
+  }
+  jr->jI = jI;
+  jr->jQ = jQ;
+  jr->jU = jU;
+  jr->jV = jV;
+  if (Bnuinv > 0) {
+    jr->aI = jI / Bnuinv;
+    jr->aQ = jQ / Bnuinv;
+    jr->aU = jU / Bnuinv;
+    jr->aV = jV / Bnuinv;
+  }
+  rho_QV(Ne, nu, Thetae, B, theta, k0, k1, k2, 1, &jr->rQ, &jr->rV);
+  jr->rU = 0.;
+}
+
+/* --------------------------------------------------------------------- */
+/* Transfer steps (src/ipolarray.c:332-628)                               */
+/* --------------------------------------------------------------------- */
+/* src/ipolarray.c:607-628 */
+__device__ __forceinline__ double approximate_solve(double Ii, double ji, double ki, double jf, double kf, double dl,
+                                                    double *tau)
+{
+  double javg = (ji + jf) / 2.;
+  double kavg = (ki + kf) / 2.;
+  double dtau = dl * kavg;
+  *tau += dtau;
+  if (dtau < 1.e-3) return Ii + (javg - Ii * kavg) * dl * (1. - (dtau / 2.) * (1. - dtau / 3.));
+  double efac = exp(-dtau);
+  return Ii * efac + (javg / kavg) * (1. - efac);
+}
+
+/* Faraday rotation over x (src/ipolarray.c:390-408) */
+__device__ __forceinline__ void faraday(double rQ, double rU, double rV, double x, double *SQ, double *SU, double *SV)
+{
+  double SQ0 = *SQ, SU0 = *SU, SV0 = *SV;
+  double rho2 = rQ * rQ + rU * rU + rV * rV;
+  if (rho2 > IPG_CUT_PREVENT_NAN) {
+    double rho = sqrt(rho2);
+    double rdS = rQ * SQ0 + rU * SU0 + rV * SV0;
+    double s, c;
+    sincos(rho * x, &s, &c);
+    double sh = sin(0.5 * rho * x);
+    double f = 2. * rdS / rho2 * sh * sh;
+    double ir = s / rho;
+    *SQ = SQ0 * c + rQ * f + (rU * SV0 - rV * SU0) * ir;
+    *SU = SU0 * c + rU * f + (rV * SQ0 - rQ * SV0) * ir;
+    *SV = SV0 * c + rV * f + (rQ * SU0 - rU * SQ0) * ir;
+  } else {
+    *SQ = SQ0 + (-rV * SU0 + rU * SV0) * x;
+    *SU = SU0 + (rV * SQ0 - rQ * SV0) * x;
+    *SV = SV0 + (-rU * SQ0 + rQ * SU0) * x;
+  }
+}
+
+/* Absorption/emission full step (src/ipolarray.c:410-500) */
+__device__ __forceinline__ void absorb_emit(const Jar &c, double x, double *SI, double *SQ, double *SU, double *SV)
+{
+  double SI1 = *SI, SQ1 = *SQ, SU1 = *SU, SV1 = *SV;
+  double aI = c.aI, aQ = c.aQ, aU = c.aU, aV = c.aV, jI = c.jI, jQ = c.jQ, jU = c.jU, jV = c.jV;
+  double aP2 = aQ * aQ + aU * aU + aV * aV;
+  if (aP2 > IPG_CUT_PREVENT_NAN) {
+    double aP = sqrt(aP2);
+    double tauP = aP * x;
+    double tauI = aI * x;
+    double ads0 = aQ * SQ1 + aU * SU1 + aV * SV1;
+    double adj = aQ * jQ + aU * jU + aV * jV;
+    double efacm = exp(-tauI + tauP);
+    double efacp = exp(-tauI - tauP);
+    double efac = exp(-tauI);
+    double i2aP = 1. / (2. * aP), i2aP2 = 1. / (2. * aP2), iaP2 = 1. / aP2;
+    double SI2 = efacm * (SI1 / 2. - ads0 * i2aP) + efacp * (SI1 / 2. + ads0 * i2aP);
+    double cm = (-SI1 * aP + ads0) * i2aP2, cp = (SI1 * aP + ads0) * i2aP2;
+    double SQ2 = efacm * aQ * cm + efacp * aQ * cp + efac * (SQ1 - ads0 * aQ * iaP2);
+    double SU2 = efacm * aU * cm + efacp * aU * cp + efac * (SU1 - ads0 * aU * iaP2);
+    double SV2 = efacm * aV * cm + efacp * aV * cp + efac * (SV1 - ads0 * aV * iaP2);
+    double afacm = 1. - efacm, afac = 1. - efac, afacp = 1. - efacp;
+    if (tauI - tauP <= IPG_CUT_SMALL_TAU) {
+      double e = tauI - tauP;
+      afacm = e * (1. - (e / 2.) * (1. - e / 3.));
+      if (tauI <= IPG_CUT_SMALL_TAU) {
+        e = tauI;
+        afac = e * (1. - (e / 2.) * (1. - e / 3.));
+        if (tauI + tauP <= IPG_CUT_SMALL_TAU) {
+          e = tauI + tauP;
+          afacp = e * (1. - (e / 2.) * (1. - e / 3.));
+        }
+      }
+    }
+    double iaI = 1. / aI;
+    double adjP = adj / (aI * aP2);
+    SQ2 += afac * (jQ * iaI - aQ * adjP);
+    SU2 += afac * (jU * iaI - aU * adjP);
+    SV2 += afac * (jV * iaI - aV * adjP);
+    double m1 = (aP * jI - adj) / (2. * aP * (aI - aP));
+    double m2 = (-aP * jI + adj) / (2. * aP2 * (aI - aP));
+    SI2 += afacm * m1;
+    SQ2 += afacm * aQ * m2;
+    SU2 += afacm * aU * m2;
+    SV2 += afacm * aV * m2;
+    double p1 = (aP * jI + adj) / (2. * aP * (aI + aP));
+    double p2 = (aP * jI + adj) / (2. * aP2 * (aI + aP));
+    SI2 += afacp * p1;
+    SQ2 += afacp * aQ * p2;
+    SU2 += afacp * aU * p2;
+    SV2 += afacp * aV * p2;
+    *SI = SI2;
+    *SQ = SQ2;
+    *SU = SU2;
+    *SV = SV2;
+  } else {
+    double tf = 0;
+    *SI = approximate_solve(SI1, jI, aI, jI, aI, x, &tf);
+    *SQ = approximate_solve(SQ1, jQ, aI, jQ, aI, x, &tf);
+    *SU = approximate_solve(SU1, jU, aI, jU, aI, x, &tf);
+    *SV = approximate_solve(SV1, jV, aI, jV, aI, x, &tf);
+  }
+}
+
+/* --------------------------------------------------------------------- */
+/* Plasma tetrad (src/model_tetrads.c:35-127, src/tetrads.c:40-115)        */
+/* --------------------------------------------------------------------- */
+__device__ __forceinline__ double qform(const Met &g, const double a[4], const double b[4])
+{
+  double gb[4];
+  lower(g, b, gb);
+  return a[0] * gb[0] + a[1] * gb[1] + a[2] * gb[2] + a[3] * gb[3];
+}
+
+__device__ __forceinline__ void t_normalize(const Met &g, double v[4])
+{
+  double n = sqrt(fabs(qform(g, v, v)));
+  double in = 1. / n;
+  v[0] *= in;
+  v[1] *= in;
+  v[2] *= in;
+  v[3] *= in;
+}
+
+__device__ __forceinline__ void t_project_out(const Met &g, double a[4], const double b[4])
+{
+  double bsq = qform(g, b, b);
+  double adb = qform(g, a, b);
+  double f = adb / bsq;
+  a[0] -= b[0] * f;
+  a[1] -= b[1] * f;
+  a[2] -= b[2] * f;
+  a[3] -= b[3] * f;
+}
+
+__device__ __forceinline__ void t_trial(double E[4], int defdir, const double t[4])
+{
+  double norm = fabs(t[1]) + fabs(t[2]) + fabs(t[3]);
+  for (int k = 0; k < 4; k++) E[k] = (norm <= IPG_SMALL) ? (double)(k == defdir) : t[k];
+}
+
+__device__ __forceinline__ double det4(const double E[4][4])
+{
+  double s0 = E[0][0] * E[1][1] - E[1][0] * E[0][1];
+  double s1 = E[0][0] * E[1][2] - E[1][0] * E[0][2];
+  double s2 = E[0][0] * E[1][3] - E[1][0] * E[0][3];
+  double s3 = E[0][1] * E[1][2] - E[1][1] * E[0][2];
+  double s4 = E[0][1] * E[1][3] - E[1][1] * E[0][3];
+  double s5 = E[0][2] * E[1][3] - E[1][2] * E[0][3];
+  double c5 = E[2][2] * E[3][3] - E[3][2] * E[2][3];
+  double c4 = E[2][1] * E[3][3] - E[3][1] * E[2][3];
+  double c3 = E[2][1] * E[3][2] - E[3][1] * E[2][2];
+  double c2 = E[2][0] * E[3][3] - E[3][0] * E[2][3];
+  double c1 = E[2][0] * E[3][2] - E[3][0] * E[2][2];
+  double c0 = E[2][0] * E[3][1] - E[3][0] * E[2][1];
+  return s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+}
+
+/* Econ[a][mu] rows; returns oddflag bits 1 / 16.  Only Ecov rows 1 and 2
+ * and Econ rows 1 and 2 are consumed downstream. */
+__device__ int plasma_tetrad(const double Ucon[4], const double Kcon[4], const double Bcon[4], const Met &g,
+                             const PointGeo &pg, double Econ[4][4], double Ecov1[4], double Ecov2[4])
+{
+  const double ones[4] = {1., 1., 1., 1.};
+  t_trial(Econ[0], 0, Ucon);
+  t_trial(Econ[1], 3, ones);
+  t_trial(Econ[2], 2, Bcon);
+  t_trial(Econ[3], 3, Kcon);
+  t_normalize(g, Econ[0]);
+  t_project_out(g, Econ[3], Econ[0]);
+  t_project_out(g, Econ[3], Econ[0]);
+  t_normalize(g, Econ[3]);
+  t_project_out(g, Econ[2], Econ[0]);
+  t_project_out(g, Econ[2], Econ[3]);
+  t_project_out(g, Econ[2], Econ[0]);
+  t_project_out(g, Econ[2], Econ[3]);
+  t_normalize(g, Econ[2]);
+  t_project_out(g, Econ[1], Econ[0]);
+  t_project_out(g, Econ[1], Econ[2]);
+  t_project_out(g, Econ[1], Econ[3]);
+  t_project_out(g, Econ[1], Econ[0]);
+  t_project_out(g, Econ[1], Econ[2]);
+  t_project_out(g, Econ[1], Econ[3]);
+  t_normalize(g, Econ[1]);
+  /* check_handedness: sqrt|det g| * det(Econ); det g = -(rho^2 sin(th) r J22)^2 */
+  const double a = c_grid.a;
+  double rho2 = pg.r * pg.r + a * a * pg.cth * pg.cth;
+  double gdet = fabs(rho2 * pg.sth * pg.r * pg.J22);
+  double dot = gdet * det4(Econ);
+  int flag = 0;
+  if (fabs(fabs(dot) - 1.) > 1.e-10) flag |= 1;
+  if (dot < 0.)
+    for (int k = 0; k < 4; k++) Econ[1][k] *= -1.;
+  lower(g, Econ[1], Ecov1);
+  lower(g, Econ[2], Ecov2);
+  return flag;
+}

@@ -1,0 +1,803 @@
+/*
+ * Kernels and C-ABI core of the ray pipeline.
+ *
+ * Two kernels per batch of pixels (one thread per ray):
+ *   k_geodesic  camera -> source: init_XK + trace_geodesic/push_photon with
+ *               stepsize control and the stop tests; writes each ray's
+ *               trajectory into a device pool of 32-step chunks
+ *               (src/model_geodesics.c:38-212, src/geodesics.c:9-70);
+ *   k_transfer  source -> camera over the stored trajectory: parallel
+ *               transport, model point queries, synchrotron coefficients,
+ *               unpolarized and polarized transfer steps, camera projection
+ *               (src/ipolarray.c:59-628).
+ * A trajectory step is 16 doubles (128 B, sector aligned):
+ *   [X1 X2 X3 dl | K0 K1 K2 K3 | Xh1 Xh2 nturns - | Kh0 Kh1 Kh2 Kh3]
+ * (X0 and Xh3 never enter the fast-light computation and are not kept).
+ * Chunks are linked backwards (chunk_prev) so the transfer pass walks each
+ * ray from its last step to the camera.  Rays that do not fit into the pool
+ * are deferred to the next wave; every loop is bounded by maxnstep.
+ */
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "ipg_device.cuh"
+#include "ipole_b200.h"
+
+struct RayRec {
+  int last_chunk;
+  int nstep;
+  int status;
+  int pad;
+};
+
+enum { CNT_POOL = 0, CNT_STEPS = 1, CNT_RAD = 2, CNT_DEFER = 3, CNT_N = 4 };
+
+/* ===================================================================== */
+/* geodesic pass                                                          */
+/* ===================================================================== */
+
+/* src/model_geodesics.c:267-293 */
+__device__ __forceinline__ double stepsize(const double X[4], const double K[4], double eps)
+{
+  const DevGrid &G = c_grid;
+  const double SS = IPG_SMALL * IPG_SMALL;
+  double deh = fmin(fabs(X[1] - G.cstartx[1]), 0.1);
+  double dlx1 = eps * (10 * deh) / (fabs(K[1]) + SS);
+  double cut = 0.02;
+  double lx2 = G.cstopx[2] - G.cstartx[2];
+  double dpole = fmin(fabs(X[2] / lx2), fabs((G.cstopx[2] - X[2]) / lx2));
+  double d2fac = (dpole < cut) ? dpole / 3 : fmin(cut / 3 + (dpole - cut) * 10., 1.);
+  double dlx2 = eps * d2fac / (fabs(K[2]) + SS);
+  double dlx3 = eps / (fabs(K[3]) + SS);
+  double idlx1 = 1. / (fabs(dlx1) + SS);
+  double idlx2 = 1. / (fabs(dlx2) + SS);
+  double idlx3 = 1. / (fabs(dlx3) + SS);
+  return 1. / (idlx1 + idlx2 + idlx3);
+}
+
+/* theta of bl_coord (src/coordinates.c:75-81), for the sub-ring counter */
+__device__ __forceinline__ double bl_theta(double X1, double X2)
+{
+  const DevGrid &G = c_grid;
+  double E = exp(G.mks_smooth * (G.startx[1] - X1));
+  double S2, C2;
+  sincospi(2. * X2, &S2, &C2);
+  X2P p;
+  x2_parts_from(X2, S2, C2, &p);
+  double th, j1, j2;
+  theta_jac(X2, E, p, &th, &j1, &j2);
+  return th;
+}
+
+__device__ __forceinline__ double *step_ptr(double *pool, int chunk, int slot)
+{
+  return pool + ((size_t)chunk * IPG_CHUNK_STEPS + slot) * IPG_STEP_DOUBLES;
+}
+
+__device__ __forceinline__ void store_step(double *p, const double X[4], const double K[4], const double Xh[4],
+                                           const double Kh[4], double dl, double nturns)
+{
+  double2 *q = reinterpret_cast<double2 *>(p);
+  q[0] = make_double2(X[1], X[2]);
+  q[1] = make_double2(X[3], dl);
+  q[2] = make_double2(K[0], K[1]);
+  q[3] = make_double2(K[2], K[3]);
+  q[4] = make_double2(Xh[1], Xh[2]);
+  q[5] = make_double2(nturns, 0.);
+  q[6] = make_double2(Kh[0], Kh[1]);
+  q[7] = make_double2(Kh[2], Kh[3]);
+}
+
+/* init_XK, src/model_geodesics.c:178-212, and Kcon *= freq (src/main.c:837).
+ * Explicit round-to-nearest operations keep this block free of FMA
+ * contraction so the initial wavevector matches the reference's bits. */
+__device__ __forceinline__ void init_ray(int i, int j, double X[4], double K[4])
+{
+  const DevCam &C = c_cam;
+  double dxoff = __dadd_rn(__ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn((double)i, 0.5), C.xoff), -0.01), (double)C.nx), -0.5);
+  double dyoff = __dadd_rn(__ddiv_rn(__dadd_rn(__dadd_rn((double)j, 0.5), C.yoff), (double)C.ny), -0.5);
+  double kt1 = __dmul_rn(__dsub_rn(__dmul_rn(dxoff, C.crot), __dmul_rn(dyoff, C.srot)), C.fovx);
+  double kt2 = __dmul_rn(__dadd_rn(__dmul_rn(dxoff, C.srot), __dmul_rn(dyoff, C.crot)), C.fovy);
+  double kt3 = 1.;
+  /* null_normalize, src/geometry.c:190-201 */
+  double inorm = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(kt1, kt1), __dmul_rn(kt2, kt2)), __dmul_rn(kt3, kt3)));
+  double f = __ddiv_rn(1., inorm);
+  double kt[4] = {1., __dmul_rn(kt1, f), __dmul_rn(kt2, f), __dmul_rn(kt3, f)};
+  /* tetrad_to_coordinate, src/tetrads.c:22-33 */
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    double s = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(C.Econ[0][l], kt[0]), __dmul_rn(C.Econ[1][l], kt[1])),
+                                   __dmul_rn(C.Econ[2][l], kt[2])),
+                         __dmul_rn(C.Econ[3][l], kt[3]));
+    K[l] = __dmul_rn(s, C.freq);
+    X[l] = C.Xcam[l];
+  }
+}
+
+__global__ void __launch_bounds__(128) k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list,
+                                                  int n_list, double *__restrict__ pool, int *__restrict__ chunk_prev,
+                                                  long long n_chunks, unsigned long long *__restrict__ counters,
+                                                  RayRec *__restrict__ rays, int32_t *__restrict__ deferred)
+{
+  const DevGrid &G = c_grid;
+  const DevCam &C = c_cam;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_list; t += gridDim.x * blockDim.x) {
+    int ray = list ? list[t] : t;
+    double X[4], K[4], Xh[4], Kh[4];
+    init_ray(ij[2 * ray], ij[2 * ray + 1], X, K);
+    Xh[0] = X[0]; Xh[1] = X[1]; Xh[2] = X[2]; Xh[3] = X[3];
+    Kh[0] = K[0]; Kh[1] = K[1]; Kh[2] = K[2]; Kh[3] = K[3];
+    RayRec rec = {-1, 0, IPG_RAY_OK, 0};
+    long long c = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
+    if (c >= n_chunks) {
+      rec.status = IPG_RAY_POOL_FULL;
+      rays[ray] = rec;
+      deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = ray;
+      continue;
+    }
+    int chunk = (int)c;
+    chunk_prev[chunk] = -1;
+    store_step(step_ptr(pool, chunk, 0), X, K, Xh, Kh, 0., 0.);
+
+    /* sub-ring bookkeeping, src/model_geodesics.c:58-68,129-165 */
+    const int track = C.target_nturns >= 0;
+    int passed = (C.Xcam[2] < 0.5) ? 1 : ((C.Xcam[2] > 0.5) ? -1 : 0);
+    int nturns = 0;
+    double X1m1 = X[1], X2m1 = X[2], X1m2 = X[1], X2m2 = X[2]; /* steps n-1, n-2 */
+    int nstep = 0;
+    while (true) {
+      /* stop_backward_integration, src/model_geodesics.c:218-254 */
+      double r = exp(X[1]);
+      if ((r > G.rmax_geo && K[1] < 0.) || r < (G.Rh + 0.0001)) break;
+      if (!(nstep < C.maxnstep - 1)) break;
+      nstep++;
+      double dl = stepsize(X, K, C.eps);
+      double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
+      /* push_photon(X, Kcon, -dl, Xhalf, Kconhalf), src/geodesics.c:9-70 */
+      double h = -dl;
+      Conn cn;
+      double acc[4];
+      fd_connection(X[1], X[2], &cn);
+      geo_accel(cn, K, acc);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        Kh[k] = K[k] - 0.5 * h * acc[k];
+        Xh[k] = X[k] + 0.5 * h * K[k];
+      }
+      fd_connection(Xh[1], Xh[2], &cn);
+      geo_accel(cn, Kh, acc);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        K[k] = K[k] - h * acc[k];
+        X[k] = X[k] + h * Kh[k];
+      }
+      if (track) {
+        if (passed != 0) {
+          if (passed > 0) {
+            if (X[2] > 0.5) passed = 0;
+          } else {
+            if (X[2] < 0.5) passed = 0;
+          }
+        } else if (nstep > 3) {
+          if (C.subring_dtheta == 1) {
+            double dX2a = X2m1 - X2m2, dX2b = X[2] - X2m1;
+            if (dX2a * dX2b < 0) nturns++;
+          } else {
+            double ra = exp(X1m2), rb = exp(X1m1), rc = exp(X[1]);
+            double za = ra * cos(bl_theta(X1m2, X2m2)), zb = rb * cos(bl_theta(X1m1, X2m1));
+            double zc = rc * cos(bl_theta(X[1], X[2]));
+            if ((zb - za) * (zc - zb) < 0) nturns++;
+          }
+        }
+        X1m2 = X1m1; X2m2 = X2m1; X1m1 = X[1]; X2m1 = X[2];
+      }
+      int slot = nstep % IPG_CHUNK_STEPS;
+      if (slot == 0) {
+        long long nc = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
+        if (nc >= n_chunks) {
+          rec.status = IPG_RAY_POOL_FULL;
+          break;
+        }
+        chunk_prev[(int)nc] = chunk;
+        chunk = (int)nc;
+      }
+      store_step(step_ptr(pool, chunk, slot), X, K, Xh, Kh, dl_cgs, (double)nturns);
+    }
+    if (rec.status == IPG_RAY_OK && nstep >= C.maxnstep - 1) rec.status = IPG_RAY_MAXNSTEP;
+    rec.last_chunk = chunk;
+    rec.nstep = nstep;
+    rays[ray] = rec;
+    if (rec.status == IPG_RAY_POOL_FULL) {
+      deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = ray;
+    } else {
+      atomicAdd(&counters[CNT_STEPS], (unsigned long long)nstep);
+    }
+  }
+}
+
+/* ===================================================================== */
+/* transfer pass                                                          */
+/* ===================================================================== */
+struct TStep {
+  double X1, X2, X3, dl, K[4], Xh1, Xh2, nturns, Kh[4];
+};
+
+__device__ __forceinline__ void load_step(const double *p, TStep *s)
+{
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+  double2 a = __ldg(q + 0), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+  double2 e = __ldg(q + 4), f = __ldg(q + 5), g = __ldg(q + 6), h = __ldg(q + 7);
+  s->X1 = a.x; s->X2 = a.y; s->X3 = b.x; s->dl = b.y;
+  s->K[0] = c.x; s->K[1] = c.y; s->K[2] = d.x; s->K[3] = d.y;
+  s->Xh1 = e.x; s->Xh2 = e.y; s->nturns = f.x;
+  s->Kh[0] = g.x; s->Kh[1] = g.y; s->Kh[2] = h.x; s->Kh[3] = h.y;
+}
+
+/* radiating_region, model/iharm/model.c:2093-2098 */
+__device__ __forceinline__ int radiating(const PointGeo &pg)
+{
+  const DevGrid &G = c_grid;
+  return (pg.r > G.rmin_geo && pg.r < G.rmax_geo && pg.th > G.th_beg && pg.th < (IPG_PI - G.th_beg));
+}
+
+__device__ __forceinline__ void model_point_geo(const double *__restrict__ fields, double X1, double X2, double X3,
+                                                const PointGeo &pg, ModelPt *mp);
+
+/* evolve_N (src/ipolarray.c:332-575) on the Hermitian N; returns oddflag bits */
+__device__ int evolve_N(const ModelPt &mp, const double Kf[4], double dlam, const Jar &jar_in, int zero_emission,
+                        HermN *N, double *tauF)
+{
+  Jar c = jar_in;
+  if (zero_emission) c.jI = c.jQ = c.jU = c.jV = 0.;
+  double Bcon[4] = {mp.Bcon[0], mp.Bcon[1], mp.Bcon[2], mp.Bcon[3]};
+  double bsq = Bcon[0] * mp.Bcov[0] + Bcon[1] * mp.Bcov[1] + Bcon[2] * mp.Bcov[2] + Bcon[3] * mp.Bcov[3];
+  if (bsq <= 0.) {
+    Bcon[0] = 0.; Bcon[1] = 1.; Bcon[2] = 1.; Bcon[3] = 1.;
+  }
+  double Econ[4][4], e1[4], e2[4];
+  int flag = plasma_tetrad(mp.Ucon, Kf, Bcon, mp.geo.g, mp.geo, Econ, e1, e2);
+  double T11, T22, T12r, T21i;
+  hn_stokes(*N, e1, e2, &T11, &T22, &T12r, &T21i);
+  double SI = (T11 + T22) / 2, SQ = (T11 - T22) / 2, SU = T12r, SV = T21i;
+  faraday(c.rQ, c.rU, c.rV, dlam * 0.5, &SQ, &SU, &SV);
+  absorb_emit(c, dlam, &SI, &SQ, &SU, &SV);
+  faraday(c.rQ, c.rU, c.rV, dlam * 0.5, &SQ, &SU, &SV);
+  *tauF += dlam * fabs(c.rV);
+  if (c_cam.stokes_floors) {
+    if (SI < 0) {
+      SI = SQ = SU = SV = 0;
+    } else {
+      double pf = sqrt(SQ * SQ + SU * SU + SV * SV) / SI;
+      if (pf > 1.) {
+        SQ /= pf;
+        SU /= pf;
+        SV /= pf;
+      }
+    }
+  }
+  /* N += Econ^T (new block - old block) Econ (stokes_to_tensor +
+   * complex_tetrad_to_coord_rank2, src/ipolarray.c:673-682, 730-748) */
+  double d11 = (SI + SQ) - T11, d22 = (SI - SQ) - T22, dr12 = SU - T12r, di21 = SV - T21i;
+  const double *a = Econ[1], *b = Econ[2];
+#define DR(i, j) (a[i] * a[j] * d11 + b[i] * b[j] * d22 + (a[i] * b[j] + b[i] * a[j]) * dr12)
+#define DS(i, j) ((b[i] * a[j] - a[i] * b[j]) * di21)
+  N->r00 += DR(0, 0); N->r01 += DR(0, 1); N->r02 += DR(0, 2); N->r03 += DR(0, 3);
+  N->r11 += DR(1, 1); N->r12 += DR(1, 2); N->r13 += DR(1, 3);
+  N->r22 += DR(2, 2); N->r23 += DR(2, 3); N->r33 += DR(3, 3);
+  N->s01 += DS(0, 1); N->s02 += DS(0, 2); N->s03 += DS(0, 3);
+  N->s12 += DS(1, 2); N->s13 += DS(1, 3); N->s23 += DS(2, 3);
+#undef DR
+#undef DS
+  if (*tauF > 1.e100 || *tauF < -1.e100 || isnan(*tauF)) flag |= 2;
+  if (isnan(N->r00) || isnan(SI)) flag |= 4;
+  if (isnan(mp.Ucov[0])) flag |= 8;
+  return flag;
+}
+
+__global__ void __launch_bounds__(128) k_transfer(const int32_t *__restrict__ list, int n_list,
+                                                  const double *__restrict__ pool, const int *__restrict__ chunk_prev,
+                                                  const RayRec *__restrict__ rays, const double *__restrict__ fields,
+                                                  ipg_pixel_out *__restrict__ out,
+                                                  unsigned long long *__restrict__ counters)
+{
+  const DevGrid &G = c_grid;
+  const DevCam &C = c_cam;
+  const int unpol = C.unpol;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_list; t += gridDim.x * blockDim.x) {
+    int ray = list ? list[t] : t;
+    RayRec rec = rays[ray];
+    if (rec.status == IPG_RAY_POOL_FULL) continue;
+    ipg_pixel_out o;
+    o.I_unpol = o.tau = o.tauF = o.I = o.Q = o.U = o.V = 0.;
+    o.nstep = rec.nstep;
+    o.flag = 0;
+    if (rec.status == IPG_RAY_MAXNSTEP) {
+      out[ray] = o;
+      continue;
+    }
+    int nsteps = rec.nstep;
+    int chunk = rec.last_chunk;
+    TStep ti, tf;
+    load_step(step_ptr(const_cast<double *>(pool), chunk, nsteps % IPG_CHUNK_STEPS), &ti);
+
+    double Intensity = 0., Tau = 0., tauF = 0., js, ks;
+    HermN N;
+    hn_zero(&N);
+    int flag = 0;
+    unsigned long long nrad = 0;
+    {
+      /* get_jkinv at the far end of the ray, src/ipolarray.c:74 */
+      PointGeo pg;
+      point_geo(ti.X1, ti.X2, &pg);
+      ModelPt mp;
+      model_point_geo(fields, ti.X1, ti.X2, ti.X3, pg, &mp);
+      Jar jdummy;
+      jar_both(mp, ti.K, 0, C.emission_type, &js, &ks, &jdummy);
+    }
+    for (int n = nsteps; n > 0; --n) {
+      int s = n - 1;
+      if (s % IPG_CHUNK_STEPS == IPG_CHUNK_STEPS - 1) chunk = chunk_prev[chunk];
+      load_step(step_ptr(const_cast<double *>(pool), chunk, s % IPG_CHUNK_STEPS), &tf);
+
+      if (!unpol) {
+        /* push_polar twice, src/ipolarray.c:85-89 */
+        double dlfull = ti.dl / G.dlfac;
+        double dlhalf = (0.5 * ti.dl) / G.dlfac;
+        Conn cn;
+        double A[4][4];
+        HermN Nh;
+        fd_connection(ti.X1, ti.X2, &cn);
+        transport_matrix(cn, ti.K, A);
+        hn_push(N, N, A, dlhalf, &Nh);
+        fd_connection(ti.Xh1, ti.Xh2, &cn);
+        transport_matrix(cn, ti.Kh, A);
+        HermN Nn;
+        hn_push(N, Nh, A, dlfull, &Nn);
+        N = Nn;
+      }
+
+      PointGeo pg;
+      point_geo(tf.X1, tf.X2, &pg);
+      if (radiating(pg)) {
+        nrad++;
+        int zero_emission = 0;
+        if (C.target_nturns >= 0 && (int)ti.nturns != C.target_nturns) zero_emission = 1;
+        if (C.counterjet == 1) {
+          if (tf.X2 < (G.cstopx[2] - G.cstartx[2]) / 2) zero_emission = 1;
+        } else if (C.counterjet == 2) {
+          if (tf.X2 > (G.cstopx[2] - G.cstartx[2]) / 2) zero_emission = 1;
+        }
+        ModelPt mp;
+        model_point_geo(fields, tf.X1, tf.X2, tf.X3, pg, &mp);
+        double jf, kf;
+        Jar jar;
+        jar_both(mp, tf.K, !unpol, C.emission_type, &jf, &kf, &jar);
+        double ji = js, ki = ks;
+        js = jf;
+        ks = kf;
+        if (zero_emission) Intensity = approximate_solve(Intensity, 0, ki, 0, kf, ti.dl, &Tau);
+        else Intensity = approximate_solve(Intensity, ji, ki, jf, kf, ti.dl, &Tau);
+        if (!unpol) flag |= evolve_N(mp, tf.K, ti.dl, jar, zero_emission, &N, &tauF);
+      }
+      ti = tf;
+    }
+    o.I_unpol = Intensity;
+    o.tau = Tau;
+    o.tauF = tauF;
+    if (!unpol) {
+      /* project_N, src/ipolarray.c:578-598 */
+      double T11, T22, T12r, T21i;
+      hn_stokes(N, C.Ecov[1], C.Ecov[2], &T11, &T22, &T12r, &T21i);
+      double Q = (T11 - T22) / 2, U = T12r;
+      o.I = (T11 + T22) / 2;
+      o.Q = Q * C.cproj - U * C.sproj;
+      o.U = Q * C.sproj + U * C.cproj;
+      o.V = T21i;
+    }
+    o.flag = flag;
+    out[ray] = o;
+    atomicAdd(&counters[CNT_RAD], nrad);
+  }
+}
+
+__device__ __forceinline__ void model_point_geo(const double *__restrict__ fields, double X1, double X2, double X3,
+                                                const PointGeo &pg, ModelPt *mp)
+{
+  model_point(fields, X1, X2, X3, pg, mp);
+}
+
+/* ===================================================================== */
+/* FP64 peak probe                                                        */
+/* ===================================================================== */
+__global__ void k_fma_peak(double *out, int iters, double seed)
+{
+  double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+         a7 = a0 + 7;
+  const double m = 0.999999, c = 1e-7;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+      a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+    }
+  }
+  double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 12345.678) out[0] = s;
+}
+
+/* ===================================================================== */
+/* context + C-ABI                                                        */
+/* ===================================================================== */
+struct ipg_ctx {
+  int device;
+  cudaStream_t stream;
+  cudaEvent_t ev[4];
+  double *d_fields;
+  size_t ncell;
+  int have_model;
+  DevGrid dg;
+  double *d_pool;
+  int *d_chunk_prev;
+  long long n_chunks;
+  size_t pool_bytes_req;
+  unsigned long long *d_cnt;
+  RayRec *d_rays;
+  int32_t *d_list[2];
+  int32_t *d_ij;
+  ipg_pixel_out *d_out;
+  size_t cap;
+  int n_sm;
+  ipg_stats stats;
+  char err[512];
+};
+
+static int cuda_fail(ipg_ctx *ctx, cudaError_t e, const char *where)
+{
+  if (ctx) snprintf(ctx->err, sizeof(ctx->err), "%s: %s", where, cudaGetErrorString(e));
+  return IPG_E_CUDA;
+}
+#define CK(call)                                                      \
+  do {                                                                \
+    cudaError_t e_ = (call);                                          \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);          \
+  } while (0)
+
+extern "C" const char *ipg_strerror(int code)
+{
+  switch (code) {
+    case IPG_OK: return "ok";
+    case IPG_E_ARG: return "invalid argument";
+    case IPG_E_CUDA: return "CUDA error";
+    case IPG_E_MAXNSTEP: return "MaxNStep exceeded";
+    case IPG_E_NAN: return "NaN in image";
+    case IPG_E_TIMEOUT: return "device step budget exhausted";
+    case IPG_E_NOMEM: return "out of device memory";
+    case IPG_E_IO: return "I/O error";
+    case IPG_E_STATE: return "invalid call order";
+    case IPG_E_FORMAT: return "unsupported dump format";
+  }
+  return "unknown error";
+}
+
+extern "C" const char *ipg_last_error(const ipg_ctx *ctx) { return ctx ? ctx->err : "no context"; }
+
+extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
+{
+  if (!out) return IPG_E_ARG;
+  *out = NULL;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return IPG_E_CUDA;
+  if (device < 0 || device >= ndev) return IPG_E_ARG;
+  ipg_ctx *ctx = (ipg_ctx *)calloc(1, sizeof(ipg_ctx));
+  ctx->device = device;
+  ctx->pool_bytes_req = pool_bytes;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  for (int i = 0; e == cudaSuccess && i < 4; i++) e = cudaEventCreate(&ctx->ev[i]);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_cnt, CNT_N * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    free(ctx);
+    return IPG_E_CUDA;
+  }
+  *out = ctx;
+  return IPG_OK;
+}
+
+extern "C" void ipg_destroy(ipg_ctx *ctx)
+{
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaFree(ctx->d_fields);
+  cudaFree(ctx->d_pool);
+  cudaFree(ctx->d_chunk_prev);
+  cudaFree(ctx->d_cnt);
+  cudaFree(ctx->d_rays);
+  cudaFree(ctx->d_list[0]);
+  cudaFree(ctx->d_list[1]);
+  cudaFree(ctx->d_ij);
+  cudaFree(ctx->d_out);
+  for (int i = 0; i < 4; i++) cudaEventDestroy(ctx->ev[i]);
+  cudaStreamDestroy(ctx->stream);
+  free(ctx);
+}
+
+extern "C" int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *g, const double *const fields[IPG_NFIELD])
+{
+  if (!ctx || !g || !fields || g->n1 <= 0 || g->n2 <= 0 || g->n3 <= 0) return IPG_E_ARG;
+  for (int f = 0; f < IPG_NFIELD; f++)
+    if (!fields[f]) return IPG_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  size_t ncell = (size_t)(g->n1 + 2) * (g->n2 + 2) * (g->n3 + 2);
+  /* cell-major (AoS) layout: the 10 fields of a zone are 80 contiguous bytes
+   * and the k+1 neighbour follows, so one trilinear gather reads 4 runs of
+   * 160 B instead of 80 scattered words. */
+  std::vector<double> aos(ncell * IPG_NFIELD);
+  for (size_t c = 0; c < ncell; c++)
+    for (int f = 0; f < IPG_NFIELD; f++) aos[c * IPG_NFIELD + f] = fields[f][c];
+  if (ctx->d_fields && ctx->ncell != ncell) {
+    cudaFree(ctx->d_fields);
+    ctx->d_fields = NULL;
+  }
+  if (!ctx->d_fields) CK(cudaMalloc(&ctx->d_fields, ncell * IPG_NFIELD * sizeof(double)));
+  CK(cudaMemcpy(ctx->d_fields, aos.data(), ncell * IPG_NFIELD * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->ncell = ncell;
+  DevGrid &d = ctx->dg;
+  memset(&d, 0, sizeof(d));
+  d.n1 = g->n1;
+  d.n2 = g->n2;
+  d.n3 = g->n3;
+  for (int i = 0; i < 4; i++) {
+    d.startx[i] = g->startx[i];
+    d.stopx[i] = g->stopx[i];
+    d.dx[i] = g->dx[i];
+    d.cstartx[i] = g->cstartx[i];
+    d.cstopx[i] = g->cstopx[i];
+  }
+  d.a = g->a;
+  d.hslope = g->hslope;
+  d.poly_xt = g->poly_xt;
+  d.poly_alpha = g->poly_alpha;
+  d.mks_smooth = g->mks_smooth;
+  d.poly_norm = g->poly_norm;
+  d.Rh = g->Rh;
+  d.rmin_geo = g->rmin_geo;
+  d.rmax_geo = g->rmax_geo;
+  d.th_beg = g->th_beg;
+  d.sigma_cut = g->sigma_cut;
+  d.sigma_eq_factor = (g->sigma_cut_high > 0 && g->sigma_cut_high > g->sigma_cut) ? 1. : 0.;
+  d.L_unit = g->L_unit;
+  d.dlfac = g->L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
+  d.sj = g->n3 + 2;
+  d.si = (long long)(g->n2 + 2) * (g->n3 + 2);
+  double am1 = g->poly_alpha - 1.;
+  d.alpha_int = (am1 >= 0 && am1 <= 64 && am1 == (double)(int)am1) ? (int)am1 : -1;
+  ctx->have_model = 1;
+  return IPG_OK;
+}
+
+static int ensure_pool(ipg_ctx *ctx)
+{
+  if (ctx->d_pool) return IPG_OK;
+  size_t freeb = 0, totalb = 0;
+  CK(cudaMemGetInfo(&freeb, &totalb));
+  size_t want = ctx->pool_bytes_req ? ctx->pool_bytes_req : (size_t)(0.6 * (double)freeb);
+  size_t chunk_bytes = (size_t)IPG_CHUNK_STEPS * IPG_STEP_DOUBLES * sizeof(double) + sizeof(int);
+  long long n = (long long)(want / chunk_bytes);
+  if (n > 0x7fffffffLL) n = 0x7fffffffLL;
+  if (n < 16) return IPG_E_NOMEM;
+  CK(cudaMalloc(&ctx->d_pool, (size_t)n * IPG_CHUNK_STEPS * IPG_STEP_DOUBLES * sizeof(double)));
+  CK(cudaMalloc(&ctx->d_chunk_prev, (size_t)n * sizeof(int)));
+  ctx->n_chunks = n;
+  return IPG_OK;
+}
+
+static int ensure_cap(ipg_ctx *ctx, size_t n)
+{
+  if (n <= ctx->cap) return IPG_OK;
+  cudaFree(ctx->d_rays);
+  cudaFree(ctx->d_list[0]);
+  cudaFree(ctx->d_list[1]);
+  cudaFree(ctx->d_ij);
+  cudaFree(ctx->d_out);
+  ctx->cap = 0;
+  CK(cudaMalloc(&ctx->d_rays, n * sizeof(RayRec)));
+  CK(cudaMalloc(&ctx->d_list[0], n * sizeof(int32_t)));
+  CK(cudaMalloc(&ctx->d_list[1], n * sizeof(int32_t)));
+  CK(cudaMalloc(&ctx->d_ij, 2 * n * sizeof(int32_t)));
+  CK(cudaMalloc(&ctx->d_out, n * sizeof(ipg_pixel_out)));
+  ctx->cap = n;
+  return IPG_OK;
+}
+
+static void make_devcam(const ipg_camera *c, DevCam *d)
+{
+  memset(d, 0, sizeof(*d));
+  for (int i = 0; i < 4; i++) {
+    d->Xcam[i] = c->Xcam[i];
+    for (int j = 0; j < 4; j++) {
+      d->Econ[i][j] = c->Econ[i][j];
+      d->Ecov[i][j] = c->Ecov[i][j];
+    }
+  }
+  d->fovx = c->fovx;
+  d->fovy = c->fovy;
+  d->crot = cos(c->rotcam);
+  d->srot = sin(c->rotcam);
+  double rc = c->rotcam * -2.;
+  d->cproj = cos(rc);
+  d->sproj = sin(rc);
+  d->xoff = c->xoff;
+  d->yoff = c->yoff;
+  d->freq = c->freq;
+  d->eps = c->eps;
+  d->nx = c->nx;
+  d->ny = c->ny;
+  d->maxnstep = c->maxnstep;
+  d->unpol = c->only_unpolarized;
+  d->emission_type = c->emission_type;
+  d->stokes_floors = c->stokes_floors;
+  d->target_nturns = c->target_nturns;
+  d->subring_dtheta = c->subring_dtheta;
+  d->counterjet = c->counterjet;
+}
+
+static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n)
+{
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  size_t full = (size_t)ctx->n_sm * per_sm;
+  size_t need = (n + threads - 1) / threads;
+  return (int)(need < full ? need : full);
+}
+
+/* device-resident core: d_ij/d_out on the device, enqueued on ctx->stream */
+static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n, ipg_pixel_out *d_out)
+{
+  if (!ctx->have_model) return IPG_E_STATE;
+  if (cam->emission_type != 4 && cam->emission_type != 1) {
+    snprintf(ctx->err, sizeof(ctx->err), "emission_type %d not supported (thermal types 1 and 4 only)",
+             cam->emission_type);
+    return IPG_E_ARG;
+  }
+  if (cam->maxnstep < 2 || cam->nx <= 0 || cam->ny <= 0) return IPG_E_ARG;
+  int rc = ensure_pool(ctx);
+  if (rc) return rc;
+  rc = ensure_cap(ctx, n);
+  if (rc) return rc;
+  DevCam dc;
+  make_devcam(cam, &dc);
+  CK(cudaMemcpyToSymbolAsync(c_grid, &ctx->dg, sizeof(DevGrid), 0, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyToSymbolAsync(c_cam, &dc, sizeof(DevCam), 0, cudaMemcpyHostToDevice, ctx->stream));
+  memset(&ctx->stats, 0, sizeof(ctx->stats));
+  const int threads = 128;
+  const int32_t *list = NULL; /* identity on the first wave */
+  size_t pending = n;
+  int cur = 0;
+  float gms = 0.f, tms = 0.f;
+  while (pending > 0) {
+    CK(cudaMemsetAsync(ctx->d_cnt, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
+    int gb = grid_blocks(ctx, (const void *)k_geodesic, threads, pending);
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    k_geodesic<<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)pending, ctx->d_pool, ctx->d_chunk_prev,
+                                                 ctx->n_chunks, ctx->d_cnt, ctx->d_rays, ctx->d_list[cur ^ 1]);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    int tb = grid_blocks(ctx, (const void *)k_transfer, threads, pending);
+    k_transfer<<<tb, threads, 0, ctx->stream>>>(list, (int)pending, ctx->d_pool, ctx->d_chunk_prev, ctx->d_rays,
+                                                 ctx->d_fields, d_out, ctx->d_cnt);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    unsigned long long cnt[CNT_N];
+    CK(cudaMemcpyAsync(cnt, ctx->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+    gms += a;
+    tms += b;
+    ctx->stats.ray_steps += cnt[CNT_STEPS];
+    ctx->stats.radiating_steps += cnt[CNT_RAD];
+    ctx->stats.launches += 2;
+    ctx->stats.waves += 1;
+    size_t deferred = (size_t)cnt[CNT_DEFER];
+    if (deferred == pending) {
+      snprintf(ctx->err, sizeof(ctx->err), "trajectory pool (%lld chunks) too small for a single ray",
+               (long long)ctx->n_chunks);
+      return IPG_E_NOMEM;
+    }
+    pending = deferred;
+    cur ^= 1;
+    list = ctx->d_list[cur];
+  }
+  ctx->stats.geodesic_ms = gms;
+  ctx->stats.transfer_ms = tms;
+  return IPG_OK;
+}
+
+extern "C" int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n,
+                                       ipg_pixel_out *d_out, void *stream)
+{
+  if (!ctx || !cam || (n && (!d_ij || !d_out))) return IPG_E_ARG;
+  if (n == 0) return IPG_OK;
+  if (n > 0x7fffffff) return IPG_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (stream) CK(cudaStreamSynchronize((cudaStream_t)stream));
+  int rc = trace_core(ctx, cam, d_ij, n, d_out);
+  if (rc) return rc;
+  /* MAXNSTEP check on the device results */
+  std::vector<RayRec> recs(n);
+  CK(cudaMemcpy(recs.data(), ctx->d_rays, n * sizeof(RayRec), cudaMemcpyDeviceToHost));
+  for (size_t m = 0; m < n; m++)
+    if (recs[m].status == IPG_RAY_MAXNSTEP) {
+      snprintf(ctx->err, sizeof(ctx->err), "MaxNStep exceeded in ray %zu", m);
+      return IPG_E_MAXNSTEP;
+    }
+  return IPG_OK;
+}
+
+extern "C" int ipg_trace_pixels(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *ij, size_t n, ipg_pixel_out *out)
+{
+  if (!ctx || !cam || (n && (!ij || !out))) return IPG_E_ARG;
+  if (n == 0) return IPG_OK;
+  if (n > 0x7fffffff) return IPG_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  int rc = ensure_cap(ctx, n);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(ctx->d_ij, ij, 2 * n * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+  rc = trace_core(ctx, cam, ctx->d_ij, n, ctx->d_out);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(out, ctx->d_out, n * sizeof(ipg_pixel_out), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (size_t m = 0; m < n; m++)
+    if (out[m].nstep >= cam->maxnstep - 1) {
+      snprintf(ctx->err, sizeof(ctx->err), "MaxNStep exceeded in pixel %d %d", ij[2 * m], ij[2 * m + 1]);
+      return IPG_E_MAXNSTEP;
+    }
+  return IPG_OK;
+}
+
+extern "C" int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats)
+{
+  if (!ctx || !stats) return IPG_E_ARG;
+  *stats = ctx->stats;
+  return IPG_OK;
+}
+
+extern "C" int ipg_measure_fp64_peak(int device, double ms, double *tflops)
+{
+  ipg_ctx *ctx = NULL;
+  if (!tflops) return IPG_E_ARG;
+  CK(cudaSetDevice(device));
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  double *d = NULL;
+  CK(cudaMalloc(&d, sizeof(double)));
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  const int threads = 256, blocks = nsm * 8;
+  int iters = 256;
+  float t = 0;
+  for (int rep = 0; rep < 12; rep++) {
+    CK(cudaEventRecord(a));
+    k_fma_peak<<<blocks, threads>>>(d, iters, 1.0);
+    CK(cudaEventRecord(b));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(&t, a, b));
+    if (t > ms) break;
+    if (t < ms / 4) iters *= 2;
+  }
+  double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+  *tflops = flops / (t * 1e-3) / 1e12;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(d);
+  return IPG_OK;
+}
