@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the ipole ray pipeline on B200.
+
+Workload (the headline configuration): a seeded synthetic iharm FMKS dump of
+288x128x128 zones (seed 1), imaged at 400x400 pixels, full polarization,
+230 GHz, thetacam 163 deg, R_high 160 / R_low 1, MBH 6.5e9 Msun, D 16.8 Mpc,
+160 muas field of view, M_unit chosen so that the total flux is ~0.6 Jy.
+One *step* is one complete 400^2 image (every pixel traced, no refinement).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` = images/s with the pixel list and outputs resident in device memory
+(ipg_trace_pixels_device), `e2e` = images/s through the host image driver
+(ipg_render_image: host pixel lists, host output arrays, copies in the timed
+region).  Under torchrun each rank renders its own image (weak scaling, no
+collective on the data path); time is the max over ranks.  The reference arm
+runs the reference ipole built from its sources (oracle/_ref/ipole, the
+makefile's -O3 flags, OpenMP on every host core) on a bounded 64^2 sample of
+the same workload and scales it to a 400^2 image.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "IQUV 400² images/s & ray-steps/s, 1 B200: plain FP64 vs mixed+batched+adjoint"
+DUMP = dict(n1=288, n2=128, n3=128, seed=1)
+SMALL_DUMP = dict(n1=128, n2=64, n3=64, seed=1)
+NX = NY = 400
+M_UNIT = 3.0e27
+BASE_ARGS = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
+             "--fov=160", "--trat_large=160", "--trat_small=1"]
+CPU_SAMPLE = 64  # reference / oracle sample image size (pixels per side)
+# Executed FP64 flops per ray-step of each kernel (2 per DFMA, 1 per DADD/DMUL),
+# from ncu instruction counts on the small case (profiles/fp64_flops_per_step.md).
+FLOPS_PER_STEP = {"geodesic": None, "transfer": None}
+
+
+def data_dir():
+    d = os.environ.get("IPG_BENCH_DATA", os.path.join(tempfile.gettempdir(), "ipole_b200_bench"))
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def ensure_dump(spec, tag=""):
+    from ipole_b200 import synthdump
+    path = os.path.join(data_dir(), f"dump_{spec['n1']}x{spec['n2']}x{spec['n3']}_s{spec['seed']}{tag}.ipgc")
+    if not os.path.exists(path):
+        tmp = path + f".tmp{os.getpid()}"
+        synthdump.write_iharm_dump(tmp, spec["n1"], spec["n2"], spec["n3"], seed=spec["seed"])
+        os.replace(tmp, path)
+    return path
+
+
+def workload_args(dump, nx, ny, m_unit):
+    return [f"--dump={dump}", *BASE_ARGS, f"--M_unit={m_unit:g}", f"--nx={nx}", f"--ny={ny}"]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_reference_sample(dump, m_unit, n=CPU_SAMPLE, threads=None):
+    """Time the reference binary (or, without it, the C restatement) on an
+    n x n image of the workload; returns dict with seconds per 400^2 image."""
+    threads = threads or os.cpu_count()
+    from oracle import oracle as orc
+    if orc.have_reference_binary():
+        out = os.path.join(data_dir(), f"ref_sample_{os.getpid()}.ipgc")
+        rc, err = orc.run_reference([*workload_args(dump, n, n, m_unit), f"--outfile={out}"], binary=orc.REF_BIN,
+                                    threads=threads)
+        if rc != 0:
+            raise RuntimeError("reference run failed: " + err[-500:])
+        m = re.search(r"Total wallclock time: ([0-9.eE+-]+) s \(([0-9.eE+-]+) s\)", err)
+        render_s = float(m.group(1)) - float(m.group(2))
+        ftot = float(re.search(r"Ftot: ([0-9.eE+-]+) Jy", err).group(1))
+        kind = "reference"
+    else:
+        import ipole_b200 as ip
+        p = ip.Params.from_args(workload_args(dump, n, n, m_unit))
+        mdl = ip.Model.load(p)
+        o = orc.Oracle(mdl.grid, [mdl.field(q) for q in range(10)])
+        cam = o.camera(p.rcam, p.thetacam, p.phicam, p.rotcam, p.fovx_dsource, p.dsource, n, n, p.freqcgs)
+        ij = [(i, j) for i in range(n) for j in range(n)]
+        t0 = time.perf_counter()
+        o.trace(cam, ij, threads=threads)
+        render_s = time.perf_counter() - t0
+        ftot = None
+        kind = "port"
+    per_image = render_s * (NX * NY) / (n * n)
+    return {"seconds_per_image": per_image, "render_s": render_s, "kind": kind, "cores": threads,
+            "sample": f"{n}x{n} image of the same workload ({n * n} rays), scaled by pixel count to 400x400",
+            "Ftot_sample": ftot}
+
+
+def run_reference_arm(args):
+    rank, world, _ = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
+    if rank != 0:
+        return 0
+    dump = ensure_dump(DUMP)
+    times = []
+    for s in range(args.warmup + args.steps):
+        r = cpu_reference_sample(dump, args.m_unit)
+        if s >= args.warmup:
+            times.append(r)
+    per = statistics.mean(t["seconds_per_image"] for t in times)
+    v = 1.0 / per
+    line = {"metric": METRIC, "value": v, "unit": "images/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "iharm FMKS 288x128x128 seed 1, 400x400 IQUV, 230 GHz, thetacam 163, "
+                                   "R_high 160", "M_unit": args.m_unit},
+            "cpu_baseline": {"value": v, "unit": "images/s", "cores": times[0]["cores"], "kind": times[0]["kind"],
+                             "sample": times[0]["sample"]},
+            "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import ipole_b200 as ip
+    rank, world, local = dist_setup()
+    torch.cuda.set_device(local)
+    spec = SMALL_DUMP if args.small else DUMP
+    nx = ny = args.size
+    dump = ensure_dump(spec, tag=f"_r{rank}" if world > 1 else "")
+    p = ip.Params.from_args(workload_args(dump, nx, ny, args.m_unit))
+    model = ip.Model.load(p)
+    ctx = ip.Context(local, pool_bytes=int(args.pool_gb * (1 << 30)))
+    ctx.upload(model)
+    cam = ip.camera_for(p, model.grid)
+    ij = np.array([(i, j) for i in range(nx) for j in range(ny)], dtype=np.int32)
+    n = len(ij)
+    d_ij = torch.from_numpy(ij).cuda()
+    d_out = torch.empty(n * ip.PIXEL_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream())
+
+    for _ in range(args.warmup):
+        ctx.trace_device(cam, d_ij.data_ptr(), n, d_out.data_ptr())
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = rad = launches = 0
+    geo_ms = xfer_ms = 0.0
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.trace_device(cam, d_ij.data_ptr(), n, d_out.data_ptr())
+        s = ctx.stats()
+        steps += s["ray_steps"]
+        rad += s["radiating_steps"]
+        launches += s["launches"]
+        geo_ms += s["geodesic_ms"]
+        xfer_ms += s["transfer_ms"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world)
+    total_steps = sum_over_ranks(float(steps), world)
+    value = world * args.steps / (ms_max / 1e3)
+    out = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=ip.PIXEL_DTYPE)
+    f3 = p.freqcgs ** 3
+    ftot = float(out["I"].sum() * f3 * cam._scale)
+
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": value, "ms_per_step": ms_max / args.steps,
+                              "geodesic_ms": geo_ms / args.steps, "transfer_ms": xfer_ms / args.steps,
+                              "ray_steps_per_image": steps / args.steps, "Ftot_Jy": ftot, "clocks": clk,
+                              "lib": os.environ.get("IPOLE_B200_LIB", "default")}))
+        ctx.close()
+        return 0
+    # e2e: the host image driver, host buffers, copies inside the timed region
+    ctx.render(p, model)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        ctx.render(p, model)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
+    e2e = {"value": world * args.steps / (e2e_ms / 1e3), "unit": "images/s", "h2d_bytes_per_step": int(ij.nbytes),
+           "d2h_bytes_per_step": int(n * ip.PIXEL_DTYPE.itemsize), "api": "ipg_render_image (host driver)"}
+
+    peak = ip.fp64_peak_tflops(local, 300.0)
+    dom = "transfer" if xfer_ms >= geo_ms else "geodesic"
+    kms = xfer_ms if dom == "transfer" else geo_ms
+    fps = FLOPS_PER_STEP[dom]
+    achieved = (fps * steps / (kms / 1e3) / 1e12) if fps else None
+    roofline = {"bound": "fp64", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "peak_source": "measured in this run: FP64 FMA loop (ipg_measure_fp64_peak); MEASURED_PEAKS.json "
+                               "has no FP64 figure",
+                "flops_per_ray_step": fps, "kernel_ms_per_image": kms / args.steps,
+                "geodesic_ms_per_image": geo_ms / args.steps, "transfer_ms_per_image": xfer_ms / args.steps}
+    line = {"metric": METRIC, "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": ("iharm FMKS 288x128x128 seed 1" if not args.small else
+                                    "iharm FMKS 128x64x64 seed 1") + f", {nx}x{ny} IQUV, 230 GHz, thetacam 163, "
+                                                                     "R_high 160, plain FP64",
+                       "M_unit": args.m_unit, "parallelism": f"replicas x{world} (one image per GPU)",
+                       "l2": "inputs larger than L2: 392 MB field array + trajectory pool writes per step"},
+            "ray_steps_per_s": total_steps / (ms_max / 1e3), "ray_steps_per_image": steps / args.steps,
+            "radiating_fraction": rad / max(steps, 1), "Ftot_Jy": ftot, "e2e": e2e, "roofline": roofline,
+            "clocks": clk, "gpu_launches": launches}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cb = cpu_reference_sample(dump, args.m_unit)
+            line["cpu_baseline"] = {"value": 1.0 / cb["seconds_per_image"], "unit": "images/s", "cores": cb["cores"],
+                                    "kind": cb["kind"], "sample": cb["sample"],
+                                    "ray_steps_per_s": (steps / args.steps) / cb["seconds_per_image"]}
+        except Exception as ex:  # reported, not fatal
+            line["cpu_baseline"] = {"value": None, "unit": "images/s", "error": str(ex)[:300]}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--m-unit", dest="m_unit", type=float, default=M_UNIT)
+    ap.add_argument("--size", type=int, default=NX, help="image side in pixels (400 for the headline)")
+    ap.add_argument("--small", action="store_true", help="128x64x64 dump (profiling case)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e / CPU / peak legs)")
+    ap.add_argument("--pool-gb", dest="pool_gb", type=float, default=0.0,
+                    help="trajectory pool size in GiB (0: 60%% of free device memory)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

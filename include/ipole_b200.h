@@ -134,6 +134,10 @@ typedef struct ipg_stats {
 } ipg_stats;
 int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 
+/* The context's CUDA stream (a cudaStream_t), on which every kernel of the
+ * context is launched; lets a caller bracket calls with its own events. */
+int ipg_get_stream(const ipg_ctx *ctx, void **stream);
+
 /* ---- host-side helpers mirroring the reference's setup code ---- */
 
 /* Camera setup of main.c:125-168 and init_XK's tetrad (model_geodesics.c:

@@ -110,6 +110,14 @@ typedef struct ipg_image {
  * refinement levels, each level traced with one ipg_trace_pixels call.
  * Progress lines go to `log` (stderr in the CLI) when non-NULL. */
 int ipg_render_image(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, ipg_image *img, void *log);
+
+/* The same driver with the per-level tracing supplied by the caller: the
+ * tracer fills out[0..n) for the pixel list ij (get_pixel semantics) and
+ * returns IPG_OK or an IPG_E_* code.  ipg_render_image passes
+ * ipg_trace_pixels on its context. */
+typedef int (*ipg_tracer_fn)(void *user, const ipg_camera *cam, const int32_t *ij, size_t n, ipg_pixel_out *out);
+int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const ipg_iharm_model *m, ipg_image *img,
+                          void *log);
 void ipg_image_free(ipg_image *img);
 
 /* print_image_stats (src/main.c:1001-1042) to `log` (a FILE*), same lines;

@@ -123,6 +123,9 @@ class _Image(C.Structure):
                 ("oddflag", C.POINTER(C.c_int32)), ("nstep", C.POINTER(C.c_int32)), ("traced", C.c_size_t)]
 
 
+TRACER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(Camera), C.POINTER(C.c_int32), C.c_size_t,
+                        C.POINTER(PixelOut))
+
 _lib = None
 
 
@@ -131,7 +134,9 @@ def lib():
     global _lib
     if _lib is not None:
         return _lib
-    path = _build.LIB
+    # IPOLE_B200_LIB selects another build of the library (code-generation
+    # variants made with build.build(defines=..., out_dir=...))
+    path = os.environ.get("IPOLE_B200_LIB") or _build.LIB
     if not os.path.exists(path):
         _build.build()
     L = C.CDLL(path)
@@ -147,6 +152,7 @@ def lib():
     L.ipg_trace_pixels_device.argtypes = [C.c_void_p, C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p,
                                           C.c_void_p]
     L.ipg_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+    L.ipg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.ipg_camera_setup.argtypes = [C.POINTER(Grid)] + [C.c_double] * 9 + [C.c_int, C.c_int, C.c_double, C.c_int,
                                                                           C.POINTER(Camera), C.POINTER(C.c_double),
                                                                           C.POINTER(C.c_double),
@@ -162,6 +168,8 @@ def lib():
     L.ipg_iharm_free.argtypes = [C.POINTER(_Model)]
     L.ipg_iharm_free.restype = None
     L.ipg_render_image.argtypes = [C.c_void_p, C.POINTER(_Params), C.POINTER(_Model), C.POINTER(_Image), C.c_void_p]
+    L.ipg_render_image_with.argtypes = [TRACER_FN, C.c_void_p, C.POINTER(_Params), C.POINTER(_Model),
+                                        C.POINTER(_Image), C.c_void_p]
     L.ipg_image_free.argtypes = [C.POINTER(_Image)]
     L.ipg_image_free.restype = None
     L.ipg_image_totals.argtypes = [C.POINTER(_Image), C.POINTER(_Params), C.POINTER(C.c_double)]
@@ -351,6 +359,12 @@ class Context:
         _check(lib().ipg_trace_pixels_device(self._h, C.byref(cam), C.c_void_p(d_ij_ptr), n, C.c_void_p(d_out_ptr),
                                              C.c_void_p(stream)), self._h)
 
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer handle."""
+        s = C.c_void_p()
+        _check(lib().ipg_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def stats(self) -> dict:
         s = Stats()
         _check(lib().ipg_get_stats(self._h, C.byref(s)))
@@ -369,6 +383,38 @@ class Context:
         finally:
             L.ipg_image_free(C.byref(im))
         return img
+
+
+def render_with(tracer, params: Params, model: Model) -> Image:
+    """The host image driver (ipg_render_image_with) with a Python tracer:
+    ``tracer(cam, ij)`` gets the Camera and an (n, 2) int32 pixel list and
+    returns an (n,) PIXEL_DTYPE array (get_pixel outputs)."""
+    err = []
+
+    def cb(user, cam_p, ij_p, n, out_p):
+        try:
+            ij = np.ctypeslib.as_array(ij_p, shape=(2 * n,)).reshape(n, 2).copy()
+            res = np.asarray(tracer(cam_p.contents, ij), dtype=PIXEL_DTYPE)
+            C.memmove(out_p, res.ctypes.data, n * PIXEL_DTYPE.itemsize)
+            return IPG_E_MAXNSTEP if np.any(res["nstep"] >= cam_p.contents.maxnstep - 1) else IPG_OK
+        except Exception as e:  # surfaced after the call
+            err.append(e)
+            return IPG_E_ARG
+
+    fn = TRACER_FN(cb)
+    p = params.copy()
+    im = _Image()
+    L = lib()
+    rc = L.ipg_render_image_with(fn, None, C.byref(p._p), C.byref(model._m), C.byref(im), None)
+    try:
+        if err:
+            raise err[0]
+        _check(rc)
+        img = Image(im, params)
+        img.params_after = p
+    finally:
+        L.ipg_image_free(C.byref(im))
+    return img
 
 
 def trace_pixels(ctx: Context, cam: Camera, ij) -> np.ndarray:

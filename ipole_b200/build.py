@@ -65,30 +65,37 @@ def _run(cmd, log):
     return r.stdout + r.stderr
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, defines=(), out_dir: str | None = None) -> str:
     """Compile the kernels and host library (and the CLI) if sources changed.
-    Returns the path of libipole_b200.so."""
+    Returns the path of libipole_b200.so.  ``defines`` (e.g.
+    ["IPG_XFER_MINB=2"]) and ``out_dir`` build a variant library elsewhere
+    (no CLI) for code-generation experiments."""
     log = sys.stderr if verbose else None
-    os.makedirs(BUILD, exist_ok=True)
+    bdir = out_dir or BUILD
+    lib = os.path.join(bdir, "libipole_b200.so")
+    os.makedirs(bdir, exist_ok=True)
     os.makedirs(BIN, exist_ok=True)
     deps = _sources()
-    if force or _stale(LIB, deps) or _stale(CLI, deps + [LIB]):
+    if force or out_dir or _stale(lib, deps) or _stale(CLI, deps + [lib]):
         objs = []
-        ko = os.path.join(BUILD, "ipg_kernels.o")
-        out = _run([_nvcc(), *NVCC_FLAGS, "-I", INC, "-c", os.path.join(CSRC, "ipg_kernels.cu"), "-o", ko], log)
-        with open(os.path.join(BUILD, "ptxas.txt"), "w") as f:
+        ko = os.path.join(bdir, "ipg_kernels.o")
+        dflags = [f"-D{d}" for d in defines]
+        out = _run([_nvcc(), *NVCC_FLAGS, *dflags, "-I", INC, "-c", os.path.join(CSRC, "ipg_kernels.cu"), "-o", ko],
+                   log)
+        with open(os.path.join(bdir, "ptxas.txt"), "w") as f:
             f.write(out)
         objs.append(ko)
         for s in HOST_SRC:
-            o = os.path.join(BUILD, s[:-2] + ".o")
+            o = os.path.join(bdir, s[:-2] + ".o")
             _run([_cc(), *CC_FLAGS, "-I", INC, "-c", os.path.join(HOST, s), "-o", o], log)
             objs.append(o)
-        tmp = LIB + ".tmp"
+        tmp = lib + ".tmp"
         _run([_nvcc(), "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-lm"], log)
-        os.replace(tmp, LIB)
-        _run([_cc(), *CC_FLAGS, "-I", INC, os.path.join(HOST, "main.c"), "-o", CLI, "-L", BUILD,
-              "-lipole_b200", "-Wl,-rpath,$ORIGIN/../_build", "-lm"], log)
-    return LIB
+        os.replace(tmp, lib)
+        if not out_dir:
+            _run([_cc(), *CC_FLAGS, "-I", INC, os.path.join(HOST, "main.c"), "-o", CLI, "-L", BUILD,
+                  "-lipole_b200", "-Wl,-rpath,$ORIGIN/../_build", "-lm"], log)
+    return lib
 
 
 if __name__ == "__main__":

@@ -116,9 +116,20 @@ static void report_oddities(const ipg_params *p, const int32_t *ij, const ipg_pi
   }
 }
 
-static int trace_list(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *ij, size_t n, ipg_pixel_out *out, FILE *log)
+typedef struct {
+  ipg_tracer_fn fn;
+  void *user;
+} tracer_t;
+
+static int ctx_tracer(void *user, const ipg_camera *cam, const int32_t *ij, size_t n, ipg_pixel_out *out)
 {
-  int rc = ipg_trace_pixels(ctx, cam, ij, n, out);
+  return ipg_trace_pixels((ipg_ctx *)user, cam, ij, n, out);
+}
+
+static int trace_list(const tracer_t *tr, const ipg_camera *cam, const int32_t *ij, size_t n, ipg_pixel_out *out,
+                      FILE *log)
+{
+  int rc = tr->fn(tr->user, cam, ij, n, out);
   if (rc == IPG_E_MAXNSTEP) {
     for (size_t m = 0; m < n; m++)
       if (out[m].nstep >= cam->maxnstep - 1) {
@@ -126,14 +137,23 @@ static int trace_list(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *ij, si
         break;
       }
   } else if (rc != IPG_OK && log) {
-    fprintf(log, "trace failed: %s (%s)\n", ipg_strerror(rc), ipg_last_error(ctx));
+    fprintf(log, "trace failed: %s\n", ipg_strerror(rc));
   }
   return rc;
 }
 
 int ipg_render_image(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, ipg_image *img, void *logp)
 {
+  if (!ctx) return IPG_E_ARG;
+  return ipg_render_image_with(ctx_tracer, ctx, p, m, img, logp);
+}
+
+int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const ipg_iharm_model *m, ipg_image *img,
+                          void *logp)
+{
   FILE *log = (FILE *)logp;
+  if (!tracer || !p || !m || !img) return IPG_E_ARG;
+  tracer_t tr = {tracer, user};
   memset(img, 0, sizeof(*img));
   if (p->perform_check) {
     if (log) fprintf(log, "-check (check/recheck output) is not supported by this build\n");
@@ -245,7 +265,7 @@ int ipg_render_image(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, ipg_
       ij[2 * n + 1] = (int32_t)j;
       n++;
     }
-  rc = trace_list(ctx, cam, ij, n, out, log);
+  rc = trace_list(&tr, cam, ij, n, out, log);
   if (rc) goto done;
   report_oddities(p, ij, out, n, log);
   for (size_t q = 0; q < n; q++) {
@@ -331,7 +351,7 @@ int ipg_render_image(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, ipg_
         }
       }
     if (n) {
-      rc = trace_list(ctx, cam, ij, n, out, log);
+      rc = trace_list(&tr, cam, ij, n, out, log);
       if (rc) goto done;
       report_oddities(p, ij, out, n, log);
       for (size_t q = 0; q < n; q++) {

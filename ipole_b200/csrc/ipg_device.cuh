@@ -29,8 +29,27 @@
 #define IPG_DEL 1.e-7            /* finite-difference step, src/geometry.c:91 */
 #define IPG_CUT_SMALL_TAU 1e-5   /* src/ipolarray.c:34 */
 #define IPG_CUT_PREVENT_NAN 1e-80 /* src/ipolarray.c:37 */
-#define IPG_STEP_DOUBLES 16
+/* trajectory record: 16 doubles of geodesic state, then the transport
+ * matrices A^i_k = Gamma^i_kl K^l at (X_n, K_n) and at (Xh_n, Kh_n) that
+ * the polarized transfer step needs (16 doubles each) */
+#define IPG_TRAJ_DOUBLES 16
+#define IPG_STEP_DOUBLES 48
 #define IPG_CHUNK_STEPS 32
+
+/* Code-generation knobs (build-time): minimum resident blocks per SM of the
+ * two kernels (register budget) and whether the large device functions are
+ * kept out of line (smaller code, fewer instruction-cache misses). */
+#ifndef IPG_GEO_MINB
+#define IPG_GEO_MINB 1
+#endif
+#ifndef IPG_XFER_MINB
+#define IPG_XFER_MINB 1
+#endif
+#ifdef IPG_NOINLINE_HEAVY
+#define IPG_HEAVY __device__ __noinline__
+#else
+#define IPG_HEAVY __device__
+#endif
 
 /* ray status */
 #define IPG_RAY_OK 0
@@ -249,7 +268,7 @@ __device__ __forceinline__ Met met_diff(const Met &h, const Met &l, double inv)
   return d;
 }
 
-__device__ void fd_connection(double X1, double X2, Conn *cn)
+IPG_HEAVY void fd_connection(double X1, double X2, Conn *cn)
 {
   const DevGrid &G = c_grid;
   const double sm = G.mks_smooth;
@@ -463,70 +482,63 @@ __device__ __forceinline__ void hn_stokes(const HermN &n, const double e1[4], co
 }
 
 /* --------------------------------------------------------------------- */
-/* Modified Bessel functions K0, K1, K2 (the reference calls GSL's
- * gsl_sf_bessel_Kn, src/symphony/maxwell_juettner_fits.c:227-228,263-264,376)
- * x <= 2: ascending series (Abramowitz & Stegun 9.6.11); x > 2: Temme's
- * method / Steed's continued fraction CF2; K2 = K0 + (2/x) K1.  Values that
- * underflow return 0. */
+/* Modified Bessel functions K0, K1, K2 of the thermal fits (the reference
+ * calls GSL's gsl_sf_bessel_Kn, src/symphony/maxwell_juettner_fits.c:
+ * 227-228,263-264,376).  x <= 2: ascending series (Abramowitz & Stegun
+ * 9.6.10-11) as Horner polynomials in y = x^2/4 with exact coefficients;
+ * x > 2: Chebyshev expansions of K_n(x) sqrt(x) e^x (coefficients from
+ * gen_bessel_coeffs.py); K2 = K0 + (2/x) K1.  Relative error <= 2e-15 where
+ * the result is a normal number; values that underflow are returned as 0. */
 /* --------------------------------------------------------------------- */
-__device__ void bessel_k012(double x, double *k0, double *k1, double *k2)
+#include "ipg_bessel_coeffs.h"
+
+template <int N>
+__device__ __forceinline__ double horner(const double (&c)[N], double y)
+{
+  double r = c[N - 1];
+#pragma unroll
+  for (int k = N - 2; k >= 0; k--) r = fma(r, y, c[k]);
+  return r;
+}
+
+template <int N>
+__device__ __forceinline__ double clenshaw(const double (&c)[N], double s)
+{
+  double b1 = 0., b2 = 0., s2 = 2. * s;
+#pragma unroll
+  for (int k = N - 1; k >= 1; k--) {
+    double t = fma(s2, b1, c[k] - b2);
+    b2 = b1;
+    b1 = t;
+  }
+  return fma(s, b1, c[0] - b2);
+}
+
+IPG_HEAVY void bessel_k012(double x, double *k0, double *k1, double *k2)
 {
   if (x <= 2.0) {
     const double EG = 0.57721566490153286061;
     double y = 0.25 * x * x;
     double lg = log(0.5 * x);
-    double t = 1.0, i0 = 1.0, sum0 = 0.0, hk = 0.0;
-    double u = 1.0, i1s = 1.0;
-    double psi1 = -EG, psi2 = 1.0 - EG;
-    double sum1 = psi1 + psi2;
-    for (int k = 1; k < 60; k++) {
-      double dk = (double)k;
-      t *= y / (dk * dk);
-      hk += 1.0 / dk;
-      i0 += t;
-      sum0 += t * hk;
-      u *= y / (dk * (dk + 1.));
-      psi1 += 1.0 / dk;
-      psi2 += 1.0 / (dk + 1.);
-      i1s += u;
-      sum1 += u * (psi1 + psi2);
-      if (t < 1e-18 * i0 && u < 1e-18 * i1s) break;
-    }
-    *k0 = -(lg + EG) * i0 + sum0;
-    *k1 = 1.0 / x + lg * (0.5 * x * i1s) - 0.25 * x * sum1;
+    *k0 = -(lg + EG) * horner(kI0, y) + horner(kK0R, y);
+    *k1 = 1.0 / x + lg * (0.5 * x * horner(kI1, y)) - 0.25 * x * horner(kK1R, y);
     *k2 = *k0 + 2.0 / x * *k1;
     return;
   }
-  const double a1 = 0.25;
-  double b = 2.0 * (1.0 + x);
-  double d = 1.0 / b;
-  double delh = d, h = d;
-  double q1 = 0.0, q2 = 1.0;
-  double q = a1, c = a1;
-  double a = -a1;
-  double s = 1.0 + q * delh;
-  for (int i = 2; i < 10000; i++) {
-    a -= 2.0 * (i - 1);
-    c = -a * c / i;
-    double qnew = (q1 - b * q2) / a;
-    q1 = q2;
-    q2 = qnew;
-    q += c * qnew;
-    b += 2.0;
-    d = 1.0 / (b + a * d);
-    delh = (b * d - 1.0) * delh;
-    h += delh;
-    double dels = q * delh;
-    s += dels;
-    if (fabs(dels / s) < 1.0e-17) break;
+  double f0, f1;
+  if (x <= 8.0) {
+    double s = (16. / x - 5.) * (1. / 3.);
+    f0 = clenshaw(kK0M, s);
+    f1 = clenshaw(kK1M, s);
+  } else {
+    double s = 16. / x - 1.;
+    f0 = clenshaw(kK0F, s);
+    f1 = clenshaw(kK1F, s);
   }
-  h = a1 * h;
-  double k0s = sqrt(IPG_PI / (2.0 * x)) / s;
-  double k1s = k0s * (x + 0.5 - h) / x;
-  double ex = exp(-x);
-  *k0 = k0s * ex;
-  *k1 = k1s * ex;
-  *k2 = (k0s + 2.0 / x * k1s) * ex;
+  double pre = exp(-x) * rsqrt(x);
+  *k0 = f0 * pre;
+  *k1 = f1 * pre;
+  *k2 = (f0 + 2. / x * f1) * pre;
 }
 
 /* --------------------------------------------------------------------- */
@@ -677,7 +689,7 @@ __device__ __forceinline__ void rho_QV(double Ne, double nu, double Thetae, doub
  * pol = 0 (get_jkinv: Leung j_I / nu^2, Kirchhoff a_I) into (*ju, *ku) and
  * pol = 1 (jar_calc) into *jr.  src/model_radiation.c:145-332 with
  * emission_type 4 (Dexter) or 1 (Pandya); U components are zero. */
-__device__ void jar_both(const ModelPt &mp, const double K[4], int want_pol, int emission_type, double *ju,
+IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int emission_type, double *ju,
                          double *ku, Jar *jr)
 {
   const double pi = IPG_PI;
@@ -953,7 +965,7 @@ __device__ __forceinline__ double det4(const double E[4][4])
 
 /* Econ[a][mu] rows; returns oddflag bits 1 / 16.  Only Ecov rows 1 and 2
  * and Econ rows 1 and 2 are consumed downstream. */
-__device__ int plasma_tetrad(const double Ucon[4], const double Kcon[4], const double Bcon[4], const Met &g,
+IPG_HEAVY int plasma_tetrad(const double Ucon[4], const double Kcon[4], const double Bcon[4], const Met &g,
                              const PointGeo &pg, double Econ[4][4], double Ecov1[4], double Ecov2[4])
 {
   const double ones[4] = {1., 1., 1., 1.};

@@ -79,6 +79,36 @@ __device__ __forceinline__ double *step_ptr(double *pool, int chunk, int slot)
   return pool + ((size_t)chunk * IPG_CHUNK_STEPS + slot) * IPG_STEP_DOUBLES;
 }
 
+__device__ __forceinline__ void store_A(double *p, const double A[4][4])
+{
+  double2 *q = reinterpret_cast<double2 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    q[2 * i] = make_double2(A[i][0], A[i][1]);
+    q[2 * i + 1] = make_double2(A[i][2], A[i][3]);
+  }
+}
+
+__device__ __forceinline__ void load_A(const double *p, double A[4][4])
+{
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double2 a = __ldg(q + 2 * i), b = __ldg(q + 2 * i + 1);
+    A[i][0] = a.x;
+    A[i][1] = a.y;
+    A[i][2] = b.x;
+    A[i][3] = b.y;
+  }
+}
+
+/* Gamma^k_ij K^i K^j = A^k_i K^i */
+__device__ __forceinline__ void accel_from_A(const double A[4][4], const double K[4], double acc[4])
+{
+#pragma unroll
+  for (int k = 0; k < 4; k++) acc[k] = A[k][0] * K[0] + A[k][1] * K[1] + A[k][2] * K[2] + A[k][3] * K[3];
+}
+
 __device__ __forceinline__ void store_step(double *p, const double X[4], const double K[4], const double Xh[4],
                                            const double Kh[4], double dl, double nturns)
 {
@@ -119,7 +149,7 @@ __device__ __forceinline__ void init_ray(int i, int j, double X[4], double K[4])
   }
 }
 
-__global__ void __launch_bounds__(128) k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list,
+__global__ void __launch_bounds__(128, IPG_GEO_MINB) k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list,
                                                   int n_list, double *__restrict__ pool, int *__restrict__ chunk_prev,
                                                   long long n_chunks, unsigned long long *__restrict__ counters,
                                                   RayRec *__restrict__ rays, int32_t *__restrict__ deferred)
@@ -142,7 +172,9 @@ __global__ void __launch_bounds__(128) k_geodesic(const int32_t *__restrict__ ij
     }
     int chunk = (int)c;
     chunk_prev[chunk] = -1;
-    store_step(step_ptr(pool, chunk, 0), X, K, Xh, Kh, 0., 0.);
+    double *prev = step_ptr(pool, chunk, 0);
+    store_step(prev, X, K, Xh, Kh, 0., 0.);
+    const int pol = !C.unpol;
 
     /* sub-ring bookkeeping, src/model_geodesics.c:58-68,129-165 */
     const int track = C.target_nturns >= 0;
@@ -161,16 +193,28 @@ __global__ void __launch_bounds__(128) k_geodesic(const int32_t *__restrict__ ij
       /* push_photon(X, Kcon, -dl, Xhalf, Kconhalf), src/geodesics.c:9-70 */
       double h = -dl;
       Conn cn;
-      double acc[4];
+      double acc[4], A[4][4];
       fd_connection(X[1], X[2], &cn);
-      geo_accel(cn, K, acc);
+      if (pol) {
+        /* the transfer pass needs Gamma(X_n) K_n for step n: keep it */
+        transport_matrix(cn, K, A);
+        store_A(prev + IPG_TRAJ_DOUBLES, A);
+        accel_from_A(A, K, acc);
+      } else {
+        geo_accel(cn, K, acc);
+      }
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         Kh[k] = K[k] - 0.5 * h * acc[k];
         Xh[k] = X[k] + 0.5 * h * K[k];
       }
       fd_connection(Xh[1], Xh[2], &cn);
-      geo_accel(cn, Kh, acc);
+      if (pol) {
+        transport_matrix(cn, Kh, A);
+        accel_from_A(A, Kh, acc);
+      } else {
+        geo_accel(cn, Kh, acc);
+      }
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         K[k] = K[k] - h * acc[k];
@@ -206,9 +250,19 @@ __global__ void __launch_bounds__(128) k_geodesic(const int32_t *__restrict__ ij
         chunk_prev[(int)nc] = chunk;
         chunk = (int)nc;
       }
-      store_step(step_ptr(pool, chunk, slot), X, K, Xh, Kh, dl_cgs, (double)nturns);
+      prev = step_ptr(pool, chunk, slot);
+      store_step(prev, X, K, Xh, Kh, dl_cgs, (double)nturns);
+      if (pol) store_A(prev + 2 * IPG_TRAJ_DOUBLES, A); /* Gamma(Xh_n) Kh_n */
     }
     if (rec.status == IPG_RAY_OK && nstep >= C.maxnstep - 1) rec.status = IPG_RAY_MAXNSTEP;
+    if (rec.status == IPG_RAY_OK && pol && nstep > 0) {
+      /* the last point is where the walk back starts: its Gamma(X) K too */
+      Conn cn;
+      double A[4][4];
+      fd_connection(X[1], X[2], &cn);
+      transport_matrix(cn, K, A);
+      store_A(prev + IPG_TRAJ_DOUBLES, A);
+    }
     rec.last_chunk = chunk;
     rec.nstep = nstep;
     rays[ray] = rec;
@@ -249,7 +303,7 @@ __device__ __forceinline__ void model_point_geo(const double *__restrict__ field
                                                 const PointGeo &pg, ModelPt *mp);
 
 /* evolve_N (src/ipolarray.c:332-575) on the Hermitian N; returns oddflag bits */
-__device__ int evolve_N(const ModelPt &mp, const double Kf[4], double dlam, const Jar &jar_in, int zero_emission,
+IPG_HEAVY int evolve_N(const ModelPt &mp, const double Kf[4], double dlam, const Jar &jar_in, int zero_emission,
                         HermN *N, double *tauF)
 {
   Jar c = jar_in;
@@ -299,7 +353,7 @@ __device__ int evolve_N(const ModelPt &mp, const double Kf[4], double dlam, cons
   return flag;
 }
 
-__global__ void __launch_bounds__(128) k_transfer(const int32_t *__restrict__ list, int n_list,
+__global__ void __launch_bounds__(128, IPG_XFER_MINB) k_transfer(const int32_t *__restrict__ list, int n_list,
                                                   const double *__restrict__ pool, const int *__restrict__ chunk_prev,
                                                   const RayRec *__restrict__ rays, const double *__restrict__ fields,
                                                   ipg_pixel_out *__restrict__ out,
@@ -323,7 +377,8 @@ __global__ void __launch_bounds__(128) k_transfer(const int32_t *__restrict__ li
     int nsteps = rec.nstep;
     int chunk = rec.last_chunk;
     TStep ti, tf;
-    load_step(step_ptr(const_cast<double *>(pool), chunk, nsteps % IPG_CHUNK_STEPS), &ti);
+    const double *rec_i = step_ptr(const_cast<double *>(pool), chunk, nsteps % IPG_CHUNK_STEPS);
+    load_step(rec_i, &ti);
 
     double Intensity = 0., Tau = 0., tauF = 0., js, ks;
     HermN N;
@@ -342,21 +397,19 @@ __global__ void __launch_bounds__(128) k_transfer(const int32_t *__restrict__ li
     for (int n = nsteps; n > 0; --n) {
       int s = n - 1;
       if (s % IPG_CHUNK_STEPS == IPG_CHUNK_STEPS - 1) chunk = chunk_prev[chunk];
-      load_step(step_ptr(const_cast<double *>(pool), chunk, s % IPG_CHUNK_STEPS), &tf);
+      const double *rec_f = step_ptr(const_cast<double *>(pool), chunk, s % IPG_CHUNK_STEPS);
+      load_step(rec_f, &tf);
 
       if (!unpol) {
-        /* push_polar twice, src/ipolarray.c:85-89 */
+        /* push_polar twice, src/ipolarray.c:85-89, with the transport
+         * matrices the geodesic pass stored for this step */
         double dlfull = ti.dl / G.dlfac;
         double dlhalf = (0.5 * ti.dl) / G.dlfac;
-        Conn cn;
         double A[4][4];
-        HermN Nh;
-        fd_connection(ti.X1, ti.X2, &cn);
-        transport_matrix(cn, ti.K, A);
+        HermN Nh, Nn;
+        load_A(rec_i + IPG_TRAJ_DOUBLES, A);
         hn_push(N, N, A, dlhalf, &Nh);
-        fd_connection(ti.Xh1, ti.Xh2, &cn);
-        transport_matrix(cn, ti.Kh, A);
-        HermN Nn;
+        load_A(rec_i + 2 * IPG_TRAJ_DOUBLES, A);
         hn_push(N, Nh, A, dlfull, &Nn);
         N = Nn;
       }
@@ -385,6 +438,7 @@ __global__ void __launch_bounds__(128) k_transfer(const int32_t *__restrict__ li
         if (!unpol) flag |= evolve_N(mp, tf.K, ti.dl, jar, zero_emission, &N, &tauF);
       }
       ti = tf;
+      rec_i = rec_f;
     }
     o.I_unpol = Intensity;
     o.tau = Tau;
@@ -677,20 +731,43 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
   CK(cudaMemcpyToSymbolAsync(c_cam, &dc, sizeof(DevCam), 0, cudaMemcpyHostToDevice, ctx->stream));
   memset(&ctx->stats, 0, sizeof(ctx->stats));
   const int threads = 128;
+  /* Waves: every pending ray starts; rays that find the pool full are
+   * deferred to the next wave, after the finished ones have been transferred
+   * and the pool recycled.  A wave that finishes no ray (too many rays
+   * sharing a small pool) is retried with half as many rays; the rest of the
+   * pending list is carried over unchanged. */
   const int32_t *list = NULL; /* identity on the first wave */
-  size_t pending = n;
+  size_t pending = n, wave = n;
   int cur = 0;
   float gms = 0.f, tms = 0.f;
   while (pending > 0) {
+    size_t run = pending < wave ? pending : wave;
+    size_t carry = pending - run;
     CK(cudaMemsetAsync(ctx->d_cnt, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
-    int gb = grid_blocks(ctx, (const void *)k_geodesic, threads, pending);
+    if (carry) {
+      /* pending rays beyond this wave go first into the next list */
+      if (list) {
+        CK(cudaMemcpyAsync(ctx->d_list[cur ^ 1], list + run, carry * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+      } else {
+        std::vector<int32_t> ids(carry);
+        for (size_t q = 0; q < carry; q++) ids[q] = (int32_t)(run + q);
+        CK(cudaMemcpyAsync(ctx->d_list[cur ^ 1], ids.data(), carry * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+      }
+      unsigned long long c0 = carry;
+      CK(cudaMemcpyAsync(ctx->d_cnt + CNT_DEFER, &c0, sizeof(c0), cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
+    int gb = grid_blocks(ctx, (const void *)k_geodesic, threads, run);
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    k_geodesic<<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)pending, ctx->d_pool, ctx->d_chunk_prev,
+    k_geodesic<<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, ctx->d_pool, ctx->d_chunk_prev,
                                                  ctx->n_chunks, ctx->d_cnt, ctx->d_rays, ctx->d_list[cur ^ 1]);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    int tb = grid_blocks(ctx, (const void *)k_transfer, threads, pending);
-    k_transfer<<<tb, threads, 0, ctx->stream>>>(list, (int)pending, ctx->d_pool, ctx->d_chunk_prev, ctx->d_rays,
+    int tb = grid_blocks(ctx, (const void *)k_transfer, threads, run);
+    k_transfer<<<tb, threads, 0, ctx->stream>>>(list, (int)run, ctx->d_pool, ctx->d_chunk_prev, ctx->d_rays,
                                                  ctx->d_fields, d_out, ctx->d_cnt);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
@@ -708,9 +785,12 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
     ctx->stats.waves += 1;
     size_t deferred = (size_t)cnt[CNT_DEFER];
     if (deferred == pending) {
-      snprintf(ctx->err, sizeof(ctx->err), "trajectory pool (%lld chunks) too small for a single ray",
-               (long long)ctx->n_chunks);
-      return IPG_E_NOMEM;
+      if (run == 1) {
+        snprintf(ctx->err, sizeof(ctx->err), "trajectory pool (%lld chunks) too small for a single ray",
+                 (long long)ctx->n_chunks);
+        return IPG_E_NOMEM;
+      }
+      wave = run / 2;
     }
     pending = deferred;
     cur ^= 1;
@@ -767,6 +847,13 @@ extern "C" int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats)
 {
   if (!ctx || !stats) return IPG_E_ARG;
   *stats = ctx->stats;
+  return IPG_OK;
+}
+
+extern "C" int ipg_get_stream(const ipg_ctx *ctx, void **stream)
+{
+  if (!ctx || !stream) return IPG_E_ARG;
+  *stream = (void *)ctx->stream;
   return IPG_OK;
 }
 

@@ -76,7 +76,7 @@ def write(path: str, entries: Dict[str, Value], strlen: Dict[str, int] | None = 
                 f.write(struct.pack("<BBQ", STR, 0, len(data)))
                 f.write(data)
                 continue
-            a = np.ascontiguousarray(v, dtype="<f8" if kind == F64 else "<i4")
+            a = np.array(v, dtype="<f8" if kind == F64 else "<i4", order="C")  # keeps rank 0 for scalars
             f.write(struct.pack("<BB", kind, a.ndim))
             for d in a.shape:
                 f.write(struct.pack("<Q", d))

@@ -21,9 +21,9 @@ Physical content (all in code units, GM = c = 1):
   * sub-Keplerian rotation utilde^3 = 1/(r^1.5 + a) with a slow radial inflow
     utilde^1 = -0.1 r^-1.5, plus 1% seeded Gaussian noise on each component;
   * B^i = *F^{it} from a vector potential: one poloidal loop A_phi ~ (rho -
-    0.2 rho_max)_+ scaled to plasma beta ~ 100 at the pressure maximum, plus a
+    0.05 rho_max)_+ scaled so that max(P_gas) / max(P_mag) = 10, plus a
     weak vertical background field so that |b| > 0 in every zone (the
-    reference's electron model divides by b^2).
+    reference's electron model divides by b^2) and sigma > 1 in the funnel.
 
 The construction is deterministic for a given (shape, seed) through numpy's
 PCG64 generator.
@@ -40,6 +40,7 @@ from . import ipgc
 FMKS_DEFAULTS = dict(a=0.9375, hslope=0.3, poly_xt=0.82, poly_alpha=14.0,
                      mks_smooth=0.5, Rin=1.2, Rout=50.0)
 GAM = 13.0 / 9.0
+BETA_NORM = 10.0  # max(P_gas) / max(P_mag) of the poloidal loop
 
 
 def fmks_theta(X1, X2, startx1, p):
@@ -87,14 +88,17 @@ def make_iharm_dump(n1: int, n2: int, n3: int, seed: int = 1, **geom) -> dict:
     q = 1.0 - ((R - rc) / w) ** 2 - (z / (h * np.maximum(R, 1e-3))) ** 2
     rho_t = np.where(q > 0, np.maximum(q, 0.0) ** (1.0 / (GAM - 1.0)), 0.0)
     u_t = K * rho_t ** GAM
+    # hot, geometrically thick inflow from the torus to the horizon
+    rho_i = 0.2 * (r / 6.0) ** -1.0 * np.exp(-np.cos(th) ** 2 / (2 * 0.3 ** 2))
+    u_i = rho_i * 0.8 / r
     rho_atm = 1e-4 * r ** -1.5
     u_atm = 0.05 / r * rho_atm
-    rho2 = rho_t + rho_atm
-    u2 = u_t + u_atm
+    rho2 = rho_t + rho_i + rho_atm
+    u2 = u_t + u_i + u_atm
 
     # magnetic field from A_phi: one loop + weak vertical background
-    rho_max = rho_t.max()
-    A = np.maximum(rho_t - 0.2 * rho_max, 0.0)
+    rho_max = (rho_t + rho_i).max()
+    A = np.maximum(rho_t + rho_i - 0.05 * rho_max, 0.0)
     sig = r * r + a * a * np.cos(th) ** 2
     gdet = sig * np.sin(th) * r * fmks_dthdx2(X1g, X2g, startx1, p)
     dAdx1, dAdx2 = np.gradient(A, dx1, dx2)
@@ -104,16 +108,16 @@ def make_iharm_dump(n1: int, n2: int, n3: int, seed: int = 1, **geom) -> dict:
     dbdx1, dbdx2 = np.gradient(Ab, dx1, dx2)
     B1b = dbdx2 / gdet
     B2b = -dbdx1 / gdet
-    # scale the loop to beta ~ 100 at the pressure maximum, using the
-    # orthonormal-frame magnitude b^2 ~ g_11 B1^2 + g_22 B2^2 (KS, FMKS Jacobian)
-    imax = np.unravel_index(np.argmax(u_t), u_t.shape)
+    # scale the loop so that max(P_gas) / max(P_mag) = 100 over the grid (the
+    # usual GRMHD normalisation), with b^2 ~ g_11 B1^2 + g_22 B2^2; the
+    # background field has b^2 ~ 2e-4 (it sets sigma > 1 in the polar funnel)
     g11 = (1.0 + 2.0 * r / sig) * r * r
     g22 = sig * fmks_dthdx2(X1g, X2g, startx1, p) ** 2
     bsq_loop = g11 * B1l ** 2 + g22 * B2l ** 2
-    P = (GAM - 1.0) * u_t[imax]
-    loop_scale = math.sqrt(P / (0.5 * 100.0) / max(bsq_loop[imax], 1e-300))
+    P = (GAM - 1.0) * u2.max()
+    loop_scale = math.sqrt(P / (0.5 * BETA_NORM) / max(float(bsq_loop.max()), 1e-300))
     bsq_bg = g11 * B1b ** 2 + g22 * B2b ** 2
-    bg_scale = math.sqrt(2e-4 / max(bsq_bg[imax], 1e-300))
+    bg_scale = math.sqrt(2e-4 / max(float(np.median(bsq_bg)), 1e-300))
     B1 = loop_scale * B1l + bg_scale * B1b
     B2 = loop_scale * B2l + bg_scale * B2b
 

@@ -1,0 +1,103 @@
+"""Shared helpers of the test-suite: golden fixtures, dumps, comparisons."""
+from __future__ import annotations
+
+import glob
+import json
+import os
+
+import numpy as np
+
+import ipole_b200 as ip
+from ipole_b200 import synthdump
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+
+
+def golden_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_golden(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    arrs = {k: z[k] for k in z.files if k != "meta"}
+    return meta, arrs
+
+
+class DumpCache:
+    def __init__(self, root):
+        self.root = root
+        self.paths = {}
+
+    def get(self, meta):
+        key = meta["dump"]
+        if key not in self.paths:
+            n1, n2, n3, seed = meta["dump_shape_seed"]
+            path = os.path.join(self.root, f"dump_{key}.ipgc")
+            h = synthdump.write_iharm_dump(path, n1, n2, n3, seed=seed)
+            assert h == meta["dump_sha256"], "regenerated synthetic dump differs from the golden one"
+            self.paths[key] = path
+        return self.paths[key]
+
+
+def params_for(meta, dump_path, extra=()):
+    return ip.Params.from_args([f"--dump={dump_path}", *meta["args"], *extra])
+
+
+def oracle_tracer(orc, threads=8):
+    """Adapter: the CPU oracle as the tracer of ipg_render_image_with."""
+    from oracle.oracle import OrcCamera
+
+    def tracer(cam, ij):
+        oc = OrcCamera()
+        for k, _ in OrcCamera._fields_:
+            if k in ("Econ", "Ecov", "Xcam"):
+                continue
+            setattr(oc, k, getattr(cam, k))
+        oc.Xcam = (type(oc.Xcam))(*cam.Xcam)
+        for a in range(4):
+            for b in range(4):
+                oc.Econ[a][b] = cam.Econ[a][b]
+                oc.Ecov[a][b] = cam.Ecov[a][b]
+        o = orc.trace(oc, ij, threads=threads)
+        res = np.zeros(len(ij), dtype=ip.PIXEL_DTYPE)
+        for q, k in enumerate(["I_unpol", "tau", "tauF", "I", "Q", "U", "V"]):
+            res[k] = o[:, q]
+        res["nstep"] = o[:, 7]
+        res["flag"] = o[:, 8]
+        return res
+    return tracer
+
+
+def image_errors(img, arrs):
+    """Errors of a rendered image against golden arrays (relative to totals
+    of I; per-pixel where I > 1e-6 max)."""
+    e = {}
+    u, ug = img.unpol, arrs["unpol"]
+    e["Ftot_unpol"] = abs(u.sum() / ug.sum() - 1)
+    m = ug > 1e-6 * ug.max()
+    e["pix_unpol_max"] = float(np.max(np.abs(u[m] / ug[m] - 1)))
+    e["pix_unpol_frac_1e-6"] = float(np.mean(np.abs(u[m] / ug[m] - 1) > 1e-6))
+    if "pol" in arrs:
+        p, pg = img.pol, arrs["pol"]
+        I = pg[..., 0]
+        Itot = I.sum()
+        e["Ftot"] = abs(p[..., 0].sum() / Itot - 1)
+        for c, n in ((1, "Q"), (2, "U"), (3, "V")):
+            e["tot" + n] = abs(p[..., c].sum() - pg[..., c].sum()) / abs(Itot)
+        m = I > 1e-6 * I.max()
+        rel = np.abs(p[..., 0][m] / I[m] - 1)
+        e["pix_I_max"] = float(rel.max())
+        e["pix_I_frac_1e-6"] = float(np.mean(rel > 1e-6))
+        e["pix_QUV_over_I_max"] = float(np.max(np.abs(p[..., 1:4][m] - pg[..., 1:4][m]) / I[m][:, None]))
+        # polarization fractions and flux-weighted EVPA of the whole image
+        def fr(x):
+            Q, U, V, It = x[..., 1].sum(), x[..., 2].sum(), x[..., 3].sum(), x[..., 0].sum()
+            return np.hypot(Q, U) / It, V / It, 0.5 * np.arctan2(U, Q)
+        lp, cp, ev = fr(p)
+        lpg, cpg, evg = fr(pg)
+        e["LP_abs"] = float(abs(lp - lpg))
+        e["CP_abs"] = float(abs(cp - cpg))
+        e["EVPA_deg"] = float(abs(np.degrees(ev - evg)))
+    return e

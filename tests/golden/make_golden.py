@@ -1,0 +1,114 @@
+"""Generate the golden images used by the parity tests.
+
+Each case runs the reference ipole itself (oracle/_ref/ipole_nofma: the
+reference sources built with -O2 -ffp-contract=off, see oracle/Makefile) on a
+seeded synthetic iharm FMKS dump and stores its image arrays in
+tests/golden/<case>.npz together with the command-line arguments and the
+sha256 of the dump's primitives (the dump is regenerated on demand from its
+seed, so the tests check the hash before comparing).
+
+    python tests/golden/make_golden.py [case ...]
+
+Needs the reference build (``make -C oracle ref``), i.e. the reference tree.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from ipole_b200 import ipgc, synthdump  # noqa: E402
+
+# dump name -> (n1, n2, n3, seed)
+DUMPS = {"c1": (128, 64, 64, 1)}
+
+BASE = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
+        "--fov=160", "--trat_large=20", "--trat_small=1"]
+
+# case -> (dump, extra args).  Sizes are small so the reference finishes in seconds.
+CASES = {
+    "c1_thin_32": ("c1", ["--M_unit=1e25", "--nx=32", "--ny=32"]),
+    "c1_bright_32": ("c1", ["--M_unit=3e27", "--nx=32", "--ny=32"]),
+    "c1_thick_24": ("c1", ["--M_unit=9e28", "--nx=24", "--ny=24"]),
+    "c1_faraday_24": ("c1", ["--M_unit=3e27", "--trat_large=160", "--nx=24", "--ny=24"]),
+    "c1_pandya_24": ("c1", ["--M_unit=3e27", "--emission_type=1", "--nx=24", "--ny=24"]),
+    "c1_unpol_24": ("c1", ["--M_unit=3e27", "-unpol", "--nx=24", "--ny=24"]),
+    "c1_refine_32": ("c1", ["--M_unit=3e27", "--nx=32", "--ny=32", "--nx_min=8", "--ny_min=8",
+                            "--refine_abs=2e-2", "--refine_rel=1e-2"]),
+    "c1_refine_odd_33": ("c1", ["--M_unit=3e27", "--nx=33", "--ny=33", "--nx_min=9", "--ny_min=9"]),
+    "c1_incl17_rot_24": ("c1", ["--M_unit=3e27", "--thetacam=17", "--rotcam=30", "--qu_conv=1", "--nx=24",
+                                "--ny=24"]),
+    "c1_subring1_16": ("c1", ["--M_unit=3e27", "--target_nturns=1", "--nx=16", "--ny=16"]),
+    "c1_counterjet_16": ("c1", ["--M_unit=3e27", "--counterjet=1", "--nx=16", "--ny=16"]),
+    "c1_xoff_floors_16": ("c1", ["--M_unit=3e27", "--xoff=0.3", "--yoff=-0.2", "--stokes_floors=1",
+                                 "--eps=0.02", "--nx=16", "--ny=20"]),
+}
+
+
+def dump_path(name: str, tmpdir: str) -> tuple[str, str]:
+    n1, n2, n3, seed = DUMPS[name]
+    path = os.path.join(tmpdir, f"dump_{name}.ipgc")
+    h = synthdump.write_iharm_dump(path, n1, n2, n3, seed=seed)
+    return path, h
+
+
+def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
+    dname, extra = CASES[case]
+    dpath, dhash = dumps[dname]
+    out = os.path.join(tmpdir, f"{case}.ipgc")
+    args = [f"--dump={dpath}", *BASE, *extra, f"--outfile={out}"]
+    r = subprocess.run([binary, *args], capture_output=True, text=True, env=dict(os.environ, OMP_NUM_THREADS="8"))
+    if r.returncode != 0:
+        raise RuntimeError(f"{case}: reference exited {r.returncode}\n{r.stderr[-2000:]}")
+    img = ipgc.read(out)
+    rec = {"unpol": img["/unpol"], "tau": img["/tau"]}
+    if "/pol" in img:
+        rec["pol"] = img["/pol"]
+    # the reference's own noise floor: its makefile build (FMA contraction)
+    # against this -ffp-contract=off build, in the metrics the tests use
+    floor = None
+    fma = os.path.join(os.path.dirname(binary), "ipole")
+    if os.path.exists(fma):
+        out2 = os.path.join(tmpdir, f"{case}_fma.ipgc")
+        r = subprocess.run([fma, *args[:-1], f"--outfile={out2}"], capture_output=True, text=True,
+                           env=dict(os.environ, OMP_NUM_THREADS="8"))
+        if r.returncode == 0:
+            from tests.common import image_errors
+            other = ipgc.read(out2)
+
+            class _Img:
+                unpol = other["/unpol"]
+                pol = other.get("/pol")
+            floor = image_errors(_Img, rec)
+    meta = {"case": case, "dump": dname, "dump_shape_seed": DUMPS[dname], "dump_sha256": dhash,
+            "args": [*BASE, *extra], "Ftot_unpol": float(img["/Ftot_unpol"]),
+            "Ftot": float(img["/Ftot"]) if "/Ftot" in img else None, "scale": float(img["/header/scale"]),
+            "generator": "oracle/_ref/ipole_nofma (reference sources, -O2 -ffp-contract=off)",
+            "fma_floor": floor}
+    np.savez_compressed(os.path.join(HERE, f"{case}.npz"), meta=json.dumps(meta), **rec)
+    print(case, "Ftot", meta["Ftot"], "Ftot_unpol", meta["Ftot_unpol"])
+
+
+def main(cases):
+    binary = os.path.join(ROOT, "oracle", "_ref", "ipole_nofma")
+    if not os.path.exists(binary):
+        raise SystemExit("build the reference first: make -C oracle ref")
+    with tempfile.TemporaryDirectory() as td:
+        dumps = {}
+        for c in cases:
+            d = CASES[c][0]
+            if d not in dumps:
+                dumps[d] = dump_path(d, td)
+            make_case(c, binary, td, dumps)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or list(CASES))
