@@ -38,13 +38,13 @@ METRIC = "IQUV 400² images/s & ray-steps/s, 1 B200: plain FP64 vs mixed+batched
 DUMP = dict(n1=288, n2=128, n3=128, seed=1)
 SMALL_DUMP = dict(n1=128, n2=64, n3=64, seed=1)
 NX = NY = 400
-M_UNIT = 3.0e27
+M_UNIT = 7.5e27
 BASE_ARGS = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
              "--fov=160", "--trat_large=160", "--trat_small=1"]
 CPU_SAMPLE = 64  # reference / oracle sample image size (pixels per side)
 # Executed FP64 flops per ray-step of each kernel (2 per DFMA, 1 per DADD/DMUL),
 # from ncu instruction counts on the small case (profiles/fp64_flops_per_step.md).
-FLOPS_PER_STEP = {"geodesic": None, "transfer": None}
+FLOPS_PER_STEP = {"geodesic": None, "coeffs": None, "transfer": None}
 
 
 def data_dir():
@@ -226,7 +226,8 @@ def run_ours(args):
     spec = SMALL_DUMP if args.small else DUMP
     nx = ny = args.size
     dump = ensure_dump(spec, tag=f"_r{rank}" if world > 1 else "")
-    p = ip.Params.from_args(workload_args(dump, nx, ny, args.m_unit))
+    extra = [f"--eps={args.eps}"] if args.eps else []
+    p = ip.Params.from_args(workload_args(dump, nx, ny, args.m_unit) + extra)
     model = ip.Model.load(p)
     ctx = ip.Context(local, pool_bytes=int(args.pool_gb * (1 << 30)))
     ctx.upload(model)
@@ -245,7 +246,7 @@ def run_ours(args):
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     steps = rad = launches = 0
-    geo_ms = xfer_ms = 0.0
+    kms = {"geodesic": 0.0, "coeffs": 0.0, "transfer": 0.0}
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
@@ -254,8 +255,8 @@ def run_ours(args):
         steps += s["ray_steps"]
         rad += s["radiating_steps"]
         launches += s["launches"]
-        geo_ms += s["geodesic_ms"]
-        xfer_ms += s["transfer_ms"]
+        for k in kms:
+            kms[k] += s[f"{k}_ms"]
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
@@ -271,7 +272,7 @@ def run_ours(args):
     if args.quick:
         if rank == 0:
             print(json.dumps({"quick": True, "value": value, "ms_per_step": ms_max / args.steps,
-                              "geodesic_ms": geo_ms / args.steps, "transfer_ms": xfer_ms / args.steps,
+                              **{f"{k}_ms": v / args.steps for k, v in kms.items()},
                               "ray_steps_per_image": steps / args.steps, "Ftot_Jy": ftot, "clocks": clk,
                               "lib": os.environ.get("IPOLE_B200_LIB", "default")}))
         ctx.close()
@@ -292,16 +293,15 @@ def run_ours(args):
            "d2h_bytes_per_step": int(n * ip.PIXEL_DTYPE.itemsize), "api": "ipg_render_image (host driver)"}
 
     peak = ip.fp64_peak_tflops(local, 300.0)
-    dom = "transfer" if xfer_ms >= geo_ms else "geodesic"
-    kms = xfer_ms if dom == "transfer" else geo_ms
+    dom = max(kms, key=kms.get)
     fps = FLOPS_PER_STEP[dom]
-    achieved = (fps * steps / (kms / 1e3) / 1e12) if fps else None
+    achieved = (fps * steps / (kms[dom] / 1e3) / 1e12) if fps else None
     roofline = {"bound": "fp64", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": None,
                 "peak_source": "measured in this run: FP64 FMA loop (ipg_measure_fp64_peak); MEASURED_PEAKS.json "
                                "has no FP64 figure",
-                "flops_per_ray_step": fps, "kernel_ms_per_image": kms / args.steps,
-                "geodesic_ms_per_image": geo_ms / args.steps, "transfer_ms_per_image": xfer_ms / args.steps}
+                "flops_per_ray_step": fps, "kernel_ms_per_image": kms[dom] / args.steps,
+                **{f"{k}_ms_per_image": v / args.steps for k, v in kms.items()}}
     line = {"metric": METRIC, "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -341,6 +341,8 @@ def main():
     ap.add_argument("--small", action="store_true", help="128x64x64 dump (profiling case)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e / CPU / peak legs)")
+    ap.add_argument("--eps", type=float, default=0.0,
+                    help="geodesic step parameter for profiling cases (0: the workload's 0.01)")
     ap.add_argument("--pool-gb", dest="pool_gb", type=float, default=0.0,
                     help="trajectory pool size in GiB (0: 60%% of free device memory)")
     args = ap.parse_args()

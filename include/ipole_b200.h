@@ -122,8 +122,9 @@ int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *
                             ipg_pixel_out *d_out, void *stream);
 
 /* Kernel statistics of the last trace call: total ray-steps of the geodesic
- * pass, number of kernel launches, and the device time (ms, CUDA events) of
- * the geodesic and transfer kernels. */
+ * pass, steps inside the radiating region, number of kernel launches and
+ * pool waves, and the device time (ms, CUDA events) of the geodesic,
+ * coefficient and transfer kernels. */
 typedef struct ipg_stats {
   uint64_t ray_steps;
   uint64_t radiating_steps;
@@ -131,6 +132,7 @@ typedef struct ipg_stats {
   int32_t waves;
   double geodesic_ms;
   double transfer_ms;
+  double coeffs_ms;
 } ipg_stats;
 int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 

@@ -29,21 +29,47 @@
 #define IPG_DEL 1.e-7            /* finite-difference step, src/geometry.c:91 */
 #define IPG_CUT_SMALL_TAU 1e-5   /* src/ipolarray.c:34 */
 #define IPG_CUT_PREVENT_NAN 1e-80 /* src/ipolarray.c:37 */
-/* trajectory record: 16 doubles of geodesic state, then the transport
- * matrices A^i_k = Gamma^i_kl K^l at (X_n, K_n) and at (Xh_n, Kh_n) that
- * the polarized transfer step needs (16 doubles each) */
-#define IPG_TRAJ_DOUBLES 16
-#define IPG_STEP_DOUBLES 48
+/* Trajectory record of one step, 64 doubles (512 B):
+ *   [ 0..15]  A1 = Gamma^i_kl K^l at (X_n, K_n)        written by k_geodesic
+ *   [16..31]  A2 = Gamma^i_kl K^l at (Xh_n, Kh_n)      written by k_geodesic
+ *   [32..47]  geodesic state (REC_X1 ...)               written by k_geodesic,
+ *   [32..63]  replaced in place by the coefficient block of k_coeffs
+ *             (REC_FLAGS ...); dl and nturns keep their slots. */
+#define IPG_STEP_DOUBLES 64
 #define IPG_CHUNK_STEPS 32
+#define REC_A1 0
+#define REC_A2 16
+#define REC_X1 32
+#define REC_X2 33
+#define REC_X3 34
+#define REC_DL 35
+#define REC_K 36
+#define REC_XH1 40
+#define REC_XH2 41
+#define REC_NTURNS 42
+#define REC_KH 44
+#define REC_FLAGS 32 /* bit 0 radiating, bit 1 counterjet cut, bits 2.. oddflag of the point */
+#define REC_JU 33    /* unpolarized j_I / nu^2 and alpha_I (get_jkinv) */
+#define REC_KU 34
+#define REC_JI 36    /* jar_calc: jI jQ jV aI aQ aV (U components are zero) */
+#define REC_RQ 43    /* rho_Q, rho_V */
+#define REC_RV 44
+#define REC_E1COV 48 /* plasma tetrad rows 1, 2: covariant, then contravariant */
+#define REC_E2COV 52
+#define REC_E1CON 56
+#define REC_E2CON 60
 
 /* Code-generation knobs (build-time): minimum resident blocks per SM of the
- * two kernels (register budget) and whether the large device functions are
+ * kernels (register budget) and whether the large device functions are
  * kept out of line (smaller code, fewer instruction-cache misses). */
 #ifndef IPG_GEO_MINB
 #define IPG_GEO_MINB 1
 #endif
 #ifndef IPG_XFER_MINB
 #define IPG_XFER_MINB 1
+#endif
+#ifndef IPG_COEF_MINB
+#define IPG_COEF_MINB 1
 #endif
 #ifdef IPG_NOINLINE_HEAVY
 #define IPG_HEAVY __device__ __noinline__
@@ -655,10 +681,11 @@ struct Jar {
   double jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV;
 };
 
-/* Faraday rotativities rho_Q (Dexter 2016), rho_V (Shcherbakov 2008), both
- * times nu (src/symphony/maxwell_juettner_fits.c:207-284) */
+/* Faraday rotativities rho_Q (Dexter 2016), rho_V (Shcherbakov 2008, or
+ * Dexter's g(X) when dexter_v and K2 > 0), both times nu
+ * (src/symphony/maxwell_juettner_fits.c:207-284) */
 __device__ __forceinline__ void rho_QV(double Ne, double nu, double Thetae, double B, double theta, double k0,
-                                       double k1, double k2, int want_q, double *rQ, double *rV)
+                                       double k1, double k2, int want_q, int dexter_v, double *rQ, double *rV)
 {
   const double pi = 3.1415926535897932384;
   double omega0 = IPG_EE * B / (IPG_ME * IPG_CL);
@@ -679,9 +706,16 @@ __device__ __forceinline__ void rho_QV(double Ne, double nu, double Thetae, doub
     double eps11m22 = jffunc * wp2 * (omega0 * omega0) / (tpn2 * tpn2) * (k_ratio + 6. * Thetae) * (sth * sth);
     *rQ = tpn / (2. * IPG_CL) * eps11m22 * nu;
   }
-  double k_ratio = (k2 > 0) ? k0 / k2 : 1;
-  double shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
-  double eps12 = wp2 * omega0 / (tpn * tpn * tpn) * (k_ratio * shgmfunc) * cth;
+  double fit_factor;
+  if (dexter_v && k2 > 0) {
+    double shgmfunc = 0.43793091 * log(1. + 0.00185777 * pow(x, 1.50316886));
+    fit_factor = (k0 - shgmfunc) / k2;
+  } else {
+    double k_ratio = (k2 > 0) ? k0 / k2 : 1;
+    double shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
+    fit_factor = k_ratio * shgmfunc;
+  }
+  double eps12 = wp2 * omega0 / (tpn * tpn * tpn) * fit_factor * cth;
   *rV = tpn / IPG_CL * eps12 * nu;
 }
 
@@ -721,9 +755,11 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
   double k0, k1, k2;
   bessel_k012(1. / Thetae, &k0, &k1, &k2);
   if (theta <= 0.0 || theta >= pi) {
+    /* only rho_V; the reference still has dexter_fit = 1 set for the Dexter
+     * emission type here (src/model_radiation.c:202-207, 212-221) */
     if (want_pol) {
       double rq;
-      rho_QV(Ne, nu, Thetae, B, theta, k0, k1, k2, 0, &rq, &jr->rV);
+      rho_QV(Ne, nu, Thetae, B, theta, k0, k1, k2, 0, emission_type == 4, &rq, &jr->rV);
     }
     return;
   }
@@ -802,7 +838,7 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
     jr->aU = jU / Bnuinv;
     jr->aV = jV / Bnuinv;
   }
-  rho_QV(Ne, nu, Thetae, B, theta, k0, k1, k2, 1, &jr->rQ, &jr->rV);
+  rho_QV(Ne, nu, Thetae, B, theta, k0, k1, k2, 1, 0, &jr->rQ, &jr->rV);
   jr->rU = 0.;
 }
 

@@ -1,28 +1,39 @@
 /*
  * Kernels and C-ABI core of the ray pipeline.
  *
- * Two kernels per batch of pixels (one thread per ray):
- *   k_geodesic  camera -> source: init_XK + trace_geodesic/push_photon with
- *               stepsize control and the stop tests; writes each ray's
- *               trajectory into a device pool of 32-step chunks
- *               (src/model_geodesics.c:38-212, src/geodesics.c:9-70);
- *   k_transfer  source -> camera over the stored trajectory: parallel
- *               transport, model point queries, synchrotron coefficients,
- *               unpolarized and polarized transfer steps, camera projection
- *               (src/ipolarray.c:59-628).
- * A trajectory step is 16 doubles (128 B, sector aligned):
- *   [X1 X2 X3 dl | K0 K1 K2 K3 | Xh1 Xh2 nturns - | Kh0 Kh1 Kh2 Kh3]
- * (X0 and Xh3 never enter the fast-light computation and are not kept).
- * Chunks are linked backwards (chunk_prev) so the transfer pass walks each
- * ray from its last step to the camera.  Rays that do not fit into the pool
- * are deferred to the next wave; every loop is bounded by maxnstep.
+ * get_pixel (src/main.c:822-883) runs as three kernels per batch of pixels:
+ *
+ *   k_geodesic  one lane per ray, camera -> source: init_XK, trace_geodesic /
+ *               push_photon with step control and the stop tests
+ *               (src/model_geodesics.c:38-293, src/geodesics.c:9-70).  Each
+ *               step goes to a record of the trajectory pool together with
+ *               the two transport matrices Gamma^i_kl K^l that the polarized
+ *               transfer needs there (they come out of the same connection
+ *               evaluations).
+ *   k_coeffs    one thread per stored step, fully parallel: radiating-region
+ *               test, model point query (grid gather, four-vectors), the
+ *               synchrotron coefficients of get_jkinv and jar_calc and the
+ *               plasma tetrad (model/iharm/model.c:420-593,
+ *               src/model_radiation.c:145-332, src/model_tetrads.c:35-127).
+ *               None of these depend on the radiation field, so they leave
+ *               the sequential loop; the coefficient block replaces the
+ *               geodesic state of the record in place.
+ *   k_transfer  one lane per ray, source -> camera over the records: parallel
+ *               transport of N, the unpolarized and polarized transfer steps
+ *               and the camera projection (src/ipolarray.c:59-628).
+ *
+ * The two sequential kernels take rays from a per-wave queue (one atomic per
+ * ray), so lanes stay busy until the queue drains.  Records are chained in
+ * chunks of 32 steps (chunk_prev, walked backwards by the transfer) and
+ * tagged with their ray and first step (chunk_meta, read by k_coeffs).  Rays
+ * that do not fit into the pool are deferred to the next wave.  Every loop is
+ * bounded by maxnstep.
  */
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
-#include <string>
 #include <vector>
 
 #include "ipg_device.cuh"
@@ -35,10 +46,10 @@ struct RayRec {
   int pad;
 };
 
-enum { CNT_POOL = 0, CNT_STEPS = 1, CNT_RAD = 2, CNT_DEFER = 3, CNT_N = 4 };
+enum { CNT_POOL = 0, CNT_STEPS = 1, CNT_RAD = 2, CNT_DEFER = 3, CNT_NEXT_G = 4, CNT_NEXT_T = 5, CNT_N = 6 };
 
 /* ===================================================================== */
-/* geodesic pass                                                          */
+/* helpers                                                                */
 /* ===================================================================== */
 
 /* src/model_geodesics.c:267-293 */
@@ -79,27 +90,33 @@ __device__ __forceinline__ double *step_ptr(double *pool, int chunk, int slot)
   return pool + ((size_t)chunk * IPG_CHUNK_STEPS + slot) * IPG_STEP_DOUBLES;
 }
 
-__device__ __forceinline__ void store_A(double *p, const double A[4][4])
+__device__ __forceinline__ void store4(double *p, double a, double b, double c, double d)
 {
   double2 *q = reinterpret_cast<double2 *>(p);
+  q[0] = make_double2(a, b);
+  q[1] = make_double2(c, d);
+}
+
+__device__ __forceinline__ void load4(const double *p, double v[4])
+{
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+  double2 a = q[0], b = q[1];
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+
+__device__ __forceinline__ void store_A(double *p, const double A[4][4])
+{
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    q[2 * i] = make_double2(A[i][0], A[i][1]);
-    q[2 * i + 1] = make_double2(A[i][2], A[i][3]);
-  }
+  for (int i = 0; i < 4; i++) store4(p + 4 * i, A[i][0], A[i][1], A[i][2], A[i][3]);
 }
 
 __device__ __forceinline__ void load_A(const double *p, double A[4][4])
 {
-  const double2 *q = reinterpret_cast<const double2 *>(p);
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    double2 a = __ldg(q + 2 * i), b = __ldg(q + 2 * i + 1);
-    A[i][0] = a.x;
-    A[i][1] = a.y;
-    A[i][2] = b.x;
-    A[i][3] = b.y;
-  }
+  for (int i = 0; i < 4; i++) load4(p + 4 * i, A[i]);
 }
 
 /* Gamma^k_ij K^i K^j = A^k_i K^i */
@@ -109,18 +126,15 @@ __device__ __forceinline__ void accel_from_A(const double A[4][4], const double 
   for (int k = 0; k < 4; k++) acc[k] = A[k][0] * K[0] + A[k][1] * K[1] + A[k][2] * K[2] + A[k][3] * K[3];
 }
 
-__device__ __forceinline__ void store_step(double *p, const double X[4], const double K[4], const double Xh[4],
-                                           const double Kh[4], double dl, double nturns)
+/* Geodesic state of a record.  X0 and Xh3 never enter the fast-light
+ * computation and are not kept. */
+__device__ __forceinline__ void store_geo(double *p, const double X[4], const double K[4], const double Xh[4],
+                                          const double Kh[4], double dl, double nturns)
 {
-  double2 *q = reinterpret_cast<double2 *>(p);
-  q[0] = make_double2(X[1], X[2]);
-  q[1] = make_double2(X[3], dl);
-  q[2] = make_double2(K[0], K[1]);
-  q[3] = make_double2(K[2], K[3]);
-  q[4] = make_double2(Xh[1], Xh[2]);
-  q[5] = make_double2(nturns, 0.);
-  q[6] = make_double2(Kh[0], Kh[1]);
-  q[7] = make_double2(Kh[2], Kh[3]);
+  store4(p + REC_X1, X[1], X[2], X[3], dl);
+  store4(p + REC_K, K[0], K[1], K[2], K[3]);
+  store4(p + REC_XH1, Xh[1], Xh[2], nturns, 0.);
+  store4(p + REC_KH, Kh[0], Kh[1], Kh[2], Kh[3]);
 }
 
 /* init_XK, src/model_geodesics.c:178-212, and Kcon *= freq (src/main.c:837).
@@ -149,149 +163,6 @@ __device__ __forceinline__ void init_ray(int i, int j, double X[4], double K[4])
   }
 }
 
-__global__ void __launch_bounds__(128, IPG_GEO_MINB) k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list,
-                                                  int n_list, double *__restrict__ pool, int *__restrict__ chunk_prev,
-                                                  long long n_chunks, unsigned long long *__restrict__ counters,
-                                                  RayRec *__restrict__ rays, int32_t *__restrict__ deferred)
-{
-  const DevGrid &G = c_grid;
-  const DevCam &C = c_cam;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_list; t += gridDim.x * blockDim.x) {
-    int ray = list ? list[t] : t;
-    double X[4], K[4], Xh[4], Kh[4];
-    init_ray(ij[2 * ray], ij[2 * ray + 1], X, K);
-    Xh[0] = X[0]; Xh[1] = X[1]; Xh[2] = X[2]; Xh[3] = X[3];
-    Kh[0] = K[0]; Kh[1] = K[1]; Kh[2] = K[2]; Kh[3] = K[3];
-    RayRec rec = {-1, 0, IPG_RAY_OK, 0};
-    long long c = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
-    if (c >= n_chunks) {
-      rec.status = IPG_RAY_POOL_FULL;
-      rays[ray] = rec;
-      deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = ray;
-      continue;
-    }
-    int chunk = (int)c;
-    chunk_prev[chunk] = -1;
-    double *prev = step_ptr(pool, chunk, 0);
-    store_step(prev, X, K, Xh, Kh, 0., 0.);
-    const int pol = !C.unpol;
-
-    /* sub-ring bookkeeping, src/model_geodesics.c:58-68,129-165 */
-    const int track = C.target_nturns >= 0;
-    int passed = (C.Xcam[2] < 0.5) ? 1 : ((C.Xcam[2] > 0.5) ? -1 : 0);
-    int nturns = 0;
-    double X1m1 = X[1], X2m1 = X[2], X1m2 = X[1], X2m2 = X[2]; /* steps n-1, n-2 */
-    int nstep = 0;
-    while (true) {
-      /* stop_backward_integration, src/model_geodesics.c:218-254 */
-      double r = exp(X[1]);
-      if ((r > G.rmax_geo && K[1] < 0.) || r < (G.Rh + 0.0001)) break;
-      if (!(nstep < C.maxnstep - 1)) break;
-      nstep++;
-      double dl = stepsize(X, K, C.eps);
-      double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
-      /* push_photon(X, Kcon, -dl, Xhalf, Kconhalf), src/geodesics.c:9-70 */
-      double h = -dl;
-      Conn cn;
-      double acc[4], A[4][4];
-      fd_connection(X[1], X[2], &cn);
-      if (pol) {
-        /* the transfer pass needs Gamma(X_n) K_n for step n: keep it */
-        transport_matrix(cn, K, A);
-        store_A(prev + IPG_TRAJ_DOUBLES, A);
-        accel_from_A(A, K, acc);
-      } else {
-        geo_accel(cn, K, acc);
-      }
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        Kh[k] = K[k] - 0.5 * h * acc[k];
-        Xh[k] = X[k] + 0.5 * h * K[k];
-      }
-      fd_connection(Xh[1], Xh[2], &cn);
-      if (pol) {
-        transport_matrix(cn, Kh, A);
-        accel_from_A(A, Kh, acc);
-      } else {
-        geo_accel(cn, Kh, acc);
-      }
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        K[k] = K[k] - h * acc[k];
-        X[k] = X[k] + h * Kh[k];
-      }
-      if (track) {
-        if (passed != 0) {
-          if (passed > 0) {
-            if (X[2] > 0.5) passed = 0;
-          } else {
-            if (X[2] < 0.5) passed = 0;
-          }
-        } else if (nstep > 3) {
-          if (C.subring_dtheta == 1) {
-            double dX2a = X2m1 - X2m2, dX2b = X[2] - X2m1;
-            if (dX2a * dX2b < 0) nturns++;
-          } else {
-            double ra = exp(X1m2), rb = exp(X1m1), rc = exp(X[1]);
-            double za = ra * cos(bl_theta(X1m2, X2m2)), zb = rb * cos(bl_theta(X1m1, X2m1));
-            double zc = rc * cos(bl_theta(X[1], X[2]));
-            if ((zb - za) * (zc - zb) < 0) nturns++;
-          }
-        }
-        X1m2 = X1m1; X2m2 = X2m1; X1m1 = X[1]; X2m1 = X[2];
-      }
-      int slot = nstep % IPG_CHUNK_STEPS;
-      if (slot == 0) {
-        long long nc = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
-        if (nc >= n_chunks) {
-          rec.status = IPG_RAY_POOL_FULL;
-          break;
-        }
-        chunk_prev[(int)nc] = chunk;
-        chunk = (int)nc;
-      }
-      prev = step_ptr(pool, chunk, slot);
-      store_step(prev, X, K, Xh, Kh, dl_cgs, (double)nturns);
-      if (pol) store_A(prev + 2 * IPG_TRAJ_DOUBLES, A); /* Gamma(Xh_n) Kh_n */
-    }
-    if (rec.status == IPG_RAY_OK && nstep >= C.maxnstep - 1) rec.status = IPG_RAY_MAXNSTEP;
-    if (rec.status == IPG_RAY_OK && pol && nstep > 0) {
-      /* the last point is where the walk back starts: its Gamma(X) K too */
-      Conn cn;
-      double A[4][4];
-      fd_connection(X[1], X[2], &cn);
-      transport_matrix(cn, K, A);
-      store_A(prev + IPG_TRAJ_DOUBLES, A);
-    }
-    rec.last_chunk = chunk;
-    rec.nstep = nstep;
-    rays[ray] = rec;
-    if (rec.status == IPG_RAY_POOL_FULL) {
-      deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = ray;
-    } else {
-      atomicAdd(&counters[CNT_STEPS], (unsigned long long)nstep);
-    }
-  }
-}
-
-/* ===================================================================== */
-/* transfer pass                                                          */
-/* ===================================================================== */
-struct TStep {
-  double X1, X2, X3, dl, K[4], Xh1, Xh2, nturns, Kh[4];
-};
-
-__device__ __forceinline__ void load_step(const double *p, TStep *s)
-{
-  const double2 *q = reinterpret_cast<const double2 *>(p);
-  double2 a = __ldg(q + 0), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
-  double2 e = __ldg(q + 4), f = __ldg(q + 5), g = __ldg(q + 6), h = __ldg(q + 7);
-  s->X1 = a.x; s->X2 = a.y; s->X3 = b.x; s->dl = b.y;
-  s->K[0] = c.x; s->K[1] = c.y; s->K[2] = d.x; s->K[3] = d.y;
-  s->Xh1 = e.x; s->Xh2 = e.y; s->nturns = f.x;
-  s->Kh[0] = g.x; s->Kh[1] = g.y; s->Kh[2] = h.x; s->Kh[3] = h.y;
-}
-
 /* radiating_region, model/iharm/model.c:2093-2098 */
 __device__ __forceinline__ int radiating(const PointGeo &pg)
 {
@@ -299,22 +170,271 @@ __device__ __forceinline__ int radiating(const PointGeo &pg)
   return (pg.r > G.rmin_geo && pg.r < G.rmax_geo && pg.th > G.th_beg && pg.th < (IPG_PI - G.th_beg));
 }
 
-__device__ __forceinline__ void model_point_geo(const double *__restrict__ fields, double X1, double X2, double X3,
-                                                const PointGeo &pg, ModelPt *mp);
+/* ===================================================================== */
+/* k_geodesic                                                             */
+/* ===================================================================== */
+struct GeoLane {
+  double X[4], K[4], Xh[4], Kh[4];
+  double X1m1, X2m1, X1m2, X2m2; /* sub-ring bookkeeping: X1, X2 of steps n-1, n-2 */
+  double *prev;                  /* record of the last stored step */
+  int ray, nstep, chunk, passed, nturns;
+};
 
-/* evolve_N (src/ipolarray.c:332-575) on the Hermitian N; returns oddflag bits */
-IPG_HEAVY int evolve_N(const ModelPt &mp, const double Kf[4], double dlam, const Jar &jar_in, int zero_emission,
-                        HermN *N, double *tauF)
+/* Take the next ray from the wave's queue and store its camera point as
+ * step 0; rays that find the pool full are deferred.  False when the queue
+ * is empty. */
+__device__ __forceinline__ bool geo_fetch(GeoLane &L, const int32_t *__restrict__ ij, const int32_t *__restrict__ list,
+                                          int n_list, double *__restrict__ pool, int *__restrict__ chunk_prev,
+                                          int2 *__restrict__ chunk_meta, long long n_chunks,
+                                          unsigned long long *__restrict__ counters, RayRec *__restrict__ rays,
+                                          int32_t *__restrict__ deferred)
 {
-  Jar c = jar_in;
-  if (zero_emission) c.jI = c.jQ = c.jU = c.jV = 0.;
-  double Bcon[4] = {mp.Bcon[0], mp.Bcon[1], mp.Bcon[2], mp.Bcon[3]};
-  double bsq = Bcon[0] * mp.Bcov[0] + Bcon[1] * mp.Bcov[1] + Bcon[2] * mp.Bcov[2] + Bcon[3] * mp.Bcov[3];
-  if (bsq <= 0.) {
-    Bcon[0] = 0.; Bcon[1] = 1.; Bcon[2] = 1.; Bcon[3] = 1.;
+  const DevCam &C = c_cam;
+  while (true) {
+    unsigned long long t = atomicAdd(&counters[CNT_NEXT_G], 1ULL);
+    if (t >= (unsigned long long)n_list) return false;
+    int ray = list ? list[t] : (int)t;
+    long long c = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
+    if (c >= n_chunks) {
+      RayRec rec = {-1, 0, IPG_RAY_POOL_FULL, 0};
+      rays[ray] = rec;
+      deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = ray;
+      continue;
+    }
+    L.ray = ray;
+    init_ray(ij[2 * ray], ij[2 * ray + 1], L.X, L.K);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      L.Xh[k] = L.X[k];
+      L.Kh[k] = L.K[k];
+    }
+    L.chunk = (int)c;
+    chunk_prev[L.chunk] = -1;
+    chunk_meta[L.chunk] = make_int2(ray, 0);
+    L.prev = step_ptr(pool, L.chunk, 0);
+    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, 0., 0.);
+    L.nstep = 0;
+    L.passed = (C.Xcam[2] < 0.5) ? 1 : ((C.Xcam[2] > 0.5) ? -1 : 0);
+    L.nturns = 0;
+    L.X1m1 = L.X1m2 = L.X[1];
+    L.X2m1 = L.X2m2 = L.X[2];
+    return true;
   }
-  double Econ[4][4], e1[4], e2[4];
-  int flag = plasma_tetrad(mp.Ucon, Kf, Bcon, mp.geo.g, mp.geo, Econ, e1, e2);
+}
+
+__global__ void __launch_bounds__(128, IPG_GEO_MINB)
+    k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list,
+               double *__restrict__ pool, int *__restrict__ chunk_prev, int2 *__restrict__ chunk_meta,
+               long long n_chunks, unsigned long long *__restrict__ counters, RayRec *__restrict__ rays,
+               int32_t *__restrict__ deferred)
+{
+  const DevGrid &G = c_grid;
+  const DevCam &C = c_cam;
+  const int pol = !C.unpol;
+  const int track = C.target_nturns >= 0;
+  GeoLane L;
+  bool has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+  while (__any_sync(0xffffffffu, has)) {
+    if (!has) continue;
+    /* stop_backward_integration, src/model_geodesics.c:218-254, and the
+     * step limit of trace_geodesic's loop (:71) */
+    double r = exp(L.X[1]);
+    if ((r > G.rmax_geo && L.K[1] < 0.) || r < (G.Rh + 0.0001) || !(L.nstep < C.maxnstep - 1)) {
+      RayRec rec = {L.chunk, L.nstep, (L.nstep >= C.maxnstep - 1) ? IPG_RAY_MAXNSTEP : IPG_RAY_OK, 0};
+      if (rec.status == IPG_RAY_OK && pol && L.nstep > 0) {
+        /* the walk back starts at the last point: its Gamma(X) K too */
+        Conn cn;
+        double A[4][4];
+        fd_connection(L.X[1], L.X[2], &cn);
+        transport_matrix(cn, L.K, A);
+        store_A(L.prev + REC_A1, A);
+      }
+      rays[L.ray] = rec;
+      atomicAdd(&counters[CNT_STEPS], (unsigned long long)L.nstep);
+      has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+      continue;
+    }
+    L.nstep++;
+    double dl = stepsize(L.X, L.K, C.eps);
+    double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
+    /* push_photon(X, Kcon, -dl, Xhalf, Kconhalf), src/geodesics.c:9-70 */
+    double h = -dl;
+    Conn cn;
+    double acc[4], A[4][4];
+    fd_connection(L.X[1], L.X[2], &cn);
+    if (pol) {
+      /* the transfer needs Gamma(X_n) K_n for the step that ends at n */
+      transport_matrix(cn, L.K, A);
+      store_A(L.prev + REC_A1, A);
+      accel_from_A(A, L.K, acc);
+    } else {
+      geo_accel(cn, L.K, acc);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      L.Kh[k] = L.K[k] - 0.5 * h * acc[k];
+      L.Xh[k] = L.X[k] + 0.5 * h * L.K[k];
+    }
+    fd_connection(L.Xh[1], L.Xh[2], &cn);
+    if (pol) {
+      transport_matrix(cn, L.Kh, A);
+      accel_from_A(A, L.Kh, acc);
+    } else {
+      geo_accel(cn, L.Kh, acc);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      L.K[k] = L.K[k] - h * acc[k];
+      L.X[k] = L.X[k] + h * L.Kh[k];
+    }
+    if (track) {
+      /* sub-ring counter, src/model_geodesics.c:129-165 */
+      if (L.passed != 0) {
+        if (L.passed > 0) {
+          if (L.X[2] > 0.5) L.passed = 0;
+        } else {
+          if (L.X[2] < 0.5) L.passed = 0;
+        }
+      } else if (L.nstep > 3) {
+        if (C.subring_dtheta == 1) {
+          double dX2a = L.X2m1 - L.X2m2, dX2b = L.X[2] - L.X2m1;
+          if (dX2a * dX2b < 0) L.nturns++;
+        } else {
+          double ra = exp(L.X1m2), rb = exp(L.X1m1), rc = exp(L.X[1]);
+          double za = ra * cos(bl_theta(L.X1m2, L.X2m2)), zb = rb * cos(bl_theta(L.X1m1, L.X2m1));
+          double zc = rc * cos(bl_theta(L.X[1], L.X[2]));
+          if ((zb - za) * (zc - zb) < 0) L.nturns++;
+        }
+      }
+      L.X1m2 = L.X1m1;
+      L.X2m2 = L.X2m1;
+      L.X1m1 = L.X[1];
+      L.X2m1 = L.X[2];
+    }
+    int slot = L.nstep % IPG_CHUNK_STEPS;
+    if (slot == 0) {
+      long long nc = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
+      if (nc >= n_chunks) {
+        RayRec rec = {L.chunk, L.nstep, IPG_RAY_POOL_FULL, 0};
+        rays[L.ray] = rec;
+        deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = L.ray;
+        has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+        continue;
+      }
+      chunk_prev[(int)nc] = L.chunk;
+      chunk_meta[(int)nc] = make_int2(L.ray, L.nstep);
+      L.chunk = (int)nc;
+    }
+    L.prev = step_ptr(pool, L.chunk, slot);
+    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
+    if (pol) store_A(L.prev + REC_A2, A); /* Gamma(Xh_n) Kh_n */
+  }
+}
+
+/* ===================================================================== */
+/* k_coeffs                                                               */
+/* ===================================================================== */
+/* One thread per stored step s of a finished ray: everything the transfer
+ * step ending at s needs that does not depend on the radiation field.  The
+ * record's geodesic block is overwritten by the coefficient block; dl and
+ * nturns keep their slots. */
+__global__ void __launch_bounds__(128, IPG_COEF_MINB)
+    k_coeffs(double *__restrict__ pool, const int2 *__restrict__ chunk_meta,
+             const unsigned long long *__restrict__ counters, long long n_chunks,
+             const RayRec *__restrict__ rays, const double *__restrict__ fields)
+{
+  const DevGrid &G = c_grid;
+  const DevCam &C = c_cam;
+  const int pol = !C.unpol;
+  long long used = (long long)counters[CNT_POOL];
+  if (used > n_chunks) used = n_chunks;
+  const long long total = used * IPG_CHUNK_STEPS;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int c = (int)(t / IPG_CHUNK_STEPS), slot = (int)(t % IPG_CHUNK_STEPS);
+    int2 meta = chunk_meta[c];
+    RayRec rec = rays[meta.x];
+    int s = meta.y + slot;
+    if (rec.status != IPG_RAY_OK || s > rec.nstep) continue;
+    double *p = step_ptr(pool, c, slot);
+    double X1 = p[REC_X1], X2 = p[REC_X2], X3 = p[REC_X3];
+    double K[4];
+    load4(p + REC_K, K);
+    PointGeo pg;
+    point_geo(X1, X2, &pg);
+    int flags = radiating(pg) ? 1 : 0;
+    /* isolate_counterjet, src/ipolarray.c:128-136 */
+    if (C.counterjet == 1) {
+      if (X2 < (G.cstopx[2] - G.cstartx[2]) / 2) flags |= 2;
+    } else if (C.counterjet == 2) {
+      if (X2 > (G.cstopx[2] - G.cstartx[2]) / 2) flags |= 2;
+    }
+    double ju = 0., ku = 0.;
+    Jar jar = {0., 0., 0., 0., 0., 0., 0., 0., 0., 0., 0.};
+    double e1[4] = {0., 0., 0., 0.}, e2[4] = {0., 0., 0., 0.}, Econ[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) Econ[1][q] = Econ[2][q] = 0.;
+    /* get_jkinv at every radiating point and at the far end of the ray
+     * (src/ipolarray.c:74,143); jar_calc and the tetrad of evolve_N
+     * (src/ipolarray.c:357-384) at radiating points */
+    if ((flags & 1) || s == rec.nstep) {
+      ModelPt mp;
+      model_point(fields, X1, X2, X3, pg, &mp);
+      int want_pol = pol && (flags & 1);
+      jar_both(mp, K, want_pol, C.emission_type, &ju, &ku, &jar);
+      if (want_pol) {
+        double Bcon[4] = {mp.Bcon[0], mp.Bcon[1], mp.Bcon[2], mp.Bcon[3]};
+        double bsq = Bcon[0] * mp.Bcov[0] + Bcon[1] * mp.Bcov[1] + Bcon[2] * mp.Bcov[2] + Bcon[3] * mp.Bcov[3];
+        if (bsq <= 0.) {
+          Bcon[0] = 0.;
+          Bcon[1] = 1.;
+          Bcon[2] = 1.;
+          Bcon[3] = 1.;
+        }
+        int tf = plasma_tetrad(mp.Ucon, K, Bcon, mp.geo.g, mp.geo, Econ, e1, e2);
+        if (isnan(mp.Ucov[0])) tf |= 8;
+        flags |= tf << 2;
+      }
+    }
+    p[REC_FLAGS] = (double)flags;
+    p[REC_JU] = ju;
+    p[REC_KU] = ku;
+    store4(p + REC_JI, jar.jI, jar.jQ, jar.jV, jar.aI);
+    p[REC_JI + 4] = jar.aQ;
+    p[REC_JI + 5] = jar.aV;
+    p[REC_RQ] = jar.rQ;
+    p[REC_RV] = jar.rV;
+    store4(p + REC_E1COV, e1[0], e1[1], e1[2], e1[3]);
+    store4(p + REC_E2COV, e2[0], e2[1], e2[2], e2[3]);
+    store4(p + REC_E1CON, Econ[1][0], Econ[1][1], Econ[1][2], Econ[1][3]);
+    store4(p + REC_E2CON, Econ[2][0], Econ[2][1], Econ[2][2], Econ[2][3]);
+  }
+}
+
+/* ===================================================================== */
+/* k_transfer                                                             */
+/* ===================================================================== */
+/* evolve_N (src/ipolarray.c:332-575) from a coefficient block: N to Stokes
+ * in the plasma tetrad, Faraday half step, absorption/emission, Faraday half
+ * step, back to N.  Returns the tauF / NaN oddflag bits. */
+__device__ __forceinline__ int evolve_N_rec(const double *__restrict__ p, double dlam, int zero_emission, HermN *N,
+                                            double *tauF)
+{
+  double e1[4], e2[4], v[4];
+  load4(p + REC_E1COV, e1);
+  load4(p + REC_E2COV, e2);
+  Jar c;
+  load4(p + REC_JI, v);
+  c.jI = v[0];
+  c.jQ = v[1];
+  c.jV = v[2];
+  c.aI = v[3];
+  c.aQ = p[REC_JI + 4];
+  c.aV = p[REC_JI + 5];
+  c.rQ = p[REC_RQ];
+  c.rV = p[REC_RV];
+  c.jU = c.aU = c.rU = 0.;
+  if (zero_emission) c.jI = c.jQ = c.jU = c.jV = 0.;
   double T11, T22, T12r, T21i;
   hn_stokes(*N, e1, e2, &T11, &T22, &T12r, &T21i);
   double SI = (T11 + T22) / 2, SQ = (T11 - T22) / 2, SU = T12r, SV = T21i;
@@ -336,8 +456,10 @@ IPG_HEAVY int evolve_N(const ModelPt &mp, const double Kf[4], double dlam, const
   }
   /* N += Econ^T (new block - old block) Econ (stokes_to_tensor +
    * complex_tetrad_to_coord_rank2, src/ipolarray.c:673-682, 730-748) */
+  double a[4], b[4];
+  load4(p + REC_E1CON, a);
+  load4(p + REC_E2CON, b);
   double d11 = (SI + SQ) - T11, d22 = (SI - SQ) - T22, dr12 = SU - T12r, di21 = SV - T21i;
-  const double *a = Econ[1], *b = Econ[2];
 #define DR(i, j) (a[i] * a[j] * d11 + b[i] * b[j] * d22 + (a[i] * b[j] + b[i] * a[j]) * dr12)
 #define DS(i, j) ((b[i] * a[j] - a[i] * b[j]) * di21)
   N->r00 += DR(0, 0); N->r01 += DR(0, 1); N->r02 += DR(0, 2); N->r03 += DR(0, 3);
@@ -347,122 +469,125 @@ IPG_HEAVY int evolve_N(const ModelPt &mp, const double Kf[4], double dlam, const
   N->s12 += DS(1, 2); N->s13 += DS(1, 3); N->s23 += DS(2, 3);
 #undef DR
 #undef DS
+  int flag = 0;
   if (*tauF > 1.e100 || *tauF < -1.e100 || isnan(*tauF)) flag |= 2;
   if (isnan(N->r00) || isnan(SI)) flag |= 4;
-  if (isnan(mp.Ucov[0])) flag |= 8;
   return flag;
 }
 
-__global__ void __launch_bounds__(128, IPG_XFER_MINB) k_transfer(const int32_t *__restrict__ list, int n_list,
-                                                  const double *__restrict__ pool, const int *__restrict__ chunk_prev,
-                                                  const RayRec *__restrict__ rays, const double *__restrict__ fields,
-                                                  ipg_pixel_out *__restrict__ out,
-                                                  unsigned long long *__restrict__ counters)
+struct XferLane {
+  HermN N;
+  const double *rec_i;
+  double I, tau, tauF, js, ks;
+  int ray, n, chunk, flag, nrad;
+};
+
+/* Take the next ray whose trajectory is complete; rays that hit maxnstep get
+ * an all-zero result, deferred rays are left for their next wave. */
+__device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restrict__ list, int n_list,
+                                           const double *__restrict__ pool, const RayRec *__restrict__ rays,
+                                           ipg_pixel_out *__restrict__ out, unsigned long long *__restrict__ counters)
+{
+  while (true) {
+    unsigned long long t = atomicAdd(&counters[CNT_NEXT_T], 1ULL);
+    if (t >= (unsigned long long)n_list) return false;
+    int ray = list ? list[t] : (int)t;
+    RayRec rec = rays[ray];
+    if (rec.status == IPG_RAY_POOL_FULL) continue;
+    if (rec.status == IPG_RAY_MAXNSTEP) {
+      ipg_pixel_out o;
+      o.I_unpol = o.tau = o.tauF = o.I = o.Q = o.U = o.V = 0.;
+      o.nstep = rec.nstep;
+      o.flag = 0;
+      out[ray] = o;
+      continue;
+    }
+    L.ray = ray;
+    L.n = rec.nstep;
+    L.chunk = rec.last_chunk;
+    L.rec_i = step_ptr(const_cast<double *>(pool), L.chunk, L.n % IPG_CHUNK_STEPS);
+    /* get_jkinv at the far end of the ray, src/ipolarray.c:74 */
+    L.js = L.rec_i[REC_JU];
+    L.ks = L.rec_i[REC_KU];
+    L.I = L.tau = L.tauF = 0.;
+    hn_zero(&L.N);
+    L.flag = 0;
+    L.nrad = 0;
+    return true;
+  }
+}
+
+__global__ void __launch_bounds__(128, IPG_XFER_MINB)
+    k_transfer(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
+               const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays, ipg_pixel_out *__restrict__ out,
+               unsigned long long *__restrict__ counters)
 {
   const DevGrid &G = c_grid;
   const DevCam &C = c_cam;
   const int unpol = C.unpol;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_list; t += gridDim.x * blockDim.x) {
-    int ray = list ? list[t] : t;
-    RayRec rec = rays[ray];
-    if (rec.status == IPG_RAY_POOL_FULL) continue;
-    ipg_pixel_out o;
-    o.I_unpol = o.tau = o.tauF = o.I = o.Q = o.U = o.V = 0.;
-    o.nstep = rec.nstep;
-    o.flag = 0;
-    if (rec.status == IPG_RAY_MAXNSTEP) {
-      out[ray] = o;
+  XferLane L;
+  bool has = xfer_fetch(L, list, n_list, pool, rays, out, counters);
+  while (__any_sync(0xffffffffu, has)) {
+    if (!has) continue;
+    if (L.n == 0) {
+      ipg_pixel_out o;
+      o.I_unpol = L.I;
+      o.tau = L.tau;
+      o.tauF = L.tauF;
+      o.I = o.Q = o.U = o.V = 0.;
+      if (!unpol) {
+        /* project_N, src/ipolarray.c:578-598 */
+        double T11, T22, T12r, T21i;
+        hn_stokes(L.N, C.Ecov[1], C.Ecov[2], &T11, &T22, &T12r, &T21i);
+        double Q = (T11 - T22) / 2, U = T12r;
+        o.I = (T11 + T22) / 2;
+        o.Q = Q * C.cproj - U * C.sproj;
+        o.U = Q * C.sproj + U * C.cproj;
+        o.V = T21i;
+      }
+      o.nstep = rays[L.ray].nstep;
+      o.flag = L.flag;
+      out[L.ray] = o;
+      atomicAdd(&counters[CNT_RAD], (unsigned long long)L.nrad);
+      has = xfer_fetch(L, list, n_list, pool, rays, out, counters);
       continue;
     }
-    int nsteps = rec.nstep;
-    int chunk = rec.last_chunk;
-    TStep ti, tf;
-    const double *rec_i = step_ptr(const_cast<double *>(pool), chunk, nsteps % IPG_CHUNK_STEPS);
-    load_step(rec_i, &ti);
-
-    double Intensity = 0., Tau = 0., tauF = 0., js, ks;
-    HermN N;
-    hn_zero(&N);
-    int flag = 0;
-    unsigned long long nrad = 0;
-    {
-      /* get_jkinv at the far end of the ray, src/ipolarray.c:74 */
-      PointGeo pg;
-      point_geo(ti.X1, ti.X2, &pg);
-      ModelPt mp;
-      model_point_geo(fields, ti.X1, ti.X2, ti.X3, pg, &mp);
-      Jar jdummy;
-      jar_both(mp, ti.K, 0, C.emission_type, &js, &ks, &jdummy);
-    }
-    for (int n = nsteps; n > 0; --n) {
-      int s = n - 1;
-      if (s % IPG_CHUNK_STEPS == IPG_CHUNK_STEPS - 1) chunk = chunk_prev[chunk];
-      const double *rec_f = step_ptr(const_cast<double *>(pool), chunk, s % IPG_CHUNK_STEPS);
-      load_step(rec_f, &tf);
-
-      if (!unpol) {
-        /* push_polar twice, src/ipolarray.c:85-89, with the transport
-         * matrices the geodesic pass stored for this step */
-        double dlfull = ti.dl / G.dlfac;
-        double dlhalf = (0.5 * ti.dl) / G.dlfac;
-        double A[4][4];
-        HermN Nh, Nn;
-        load_A(rec_i + IPG_TRAJ_DOUBLES, A);
-        hn_push(N, N, A, dlhalf, &Nh);
-        load_A(rec_i + 2 * IPG_TRAJ_DOUBLES, A);
-        hn_push(N, Nh, A, dlfull, &Nn);
-        N = Nn;
-      }
-
-      PointGeo pg;
-      point_geo(tf.X1, tf.X2, &pg);
-      if (radiating(pg)) {
-        nrad++;
-        int zero_emission = 0;
-        if (C.target_nturns >= 0 && (int)ti.nturns != C.target_nturns) zero_emission = 1;
-        if (C.counterjet == 1) {
-          if (tf.X2 < (G.cstopx[2] - G.cstartx[2]) / 2) zero_emission = 1;
-        } else if (C.counterjet == 2) {
-          if (tf.X2 > (G.cstopx[2] - G.cstartx[2]) / 2) zero_emission = 1;
-        }
-        ModelPt mp;
-        model_point_geo(fields, tf.X1, tf.X2, tf.X3, pg, &mp);
-        double jf, kf;
-        Jar jar;
-        jar_both(mp, tf.K, !unpol, C.emission_type, &jf, &kf, &jar);
-        double ji = js, ki = ks;
-        js = jf;
-        ks = kf;
-        if (zero_emission) Intensity = approximate_solve(Intensity, 0, ki, 0, kf, ti.dl, &Tau);
-        else Intensity = approximate_solve(Intensity, ji, ki, jf, kf, ti.dl, &Tau);
-        if (!unpol) flag |= evolve_N(mp, tf.K, ti.dl, jar, zero_emission, &N, &tauF);
-      }
-      ti = tf;
-      rec_i = rec_f;
-    }
-    o.I_unpol = Intensity;
-    o.tau = Tau;
-    o.tauF = tauF;
+    /* step n -> n-1 of integrate_emission's loop, src/ipolarray.c:78-244 */
+    int s = L.n - 1;
+    if (s % IPG_CHUNK_STEPS == IPG_CHUNK_STEPS - 1) L.chunk = chunk_prev[L.chunk];
+    const double *rec_f = step_ptr(const_cast<double *>(pool), L.chunk, s % IPG_CHUNK_STEPS);
+    double dl = L.rec_i[REC_DL];
     if (!unpol) {
-      /* project_N, src/ipolarray.c:578-598 */
-      double T11, T22, T12r, T21i;
-      hn_stokes(N, C.Ecov[1], C.Ecov[2], &T11, &T22, &T12r, &T21i);
-      double Q = (T11 - T22) / 2, U = T12r;
-      o.I = (T11 + T22) / 2;
-      o.Q = Q * C.cproj - U * C.sproj;
-      o.U = Q * C.sproj + U * C.cproj;
-      o.V = T21i;
+      /* push_polar twice, src/ipolarray.c:85-89 */
+      double dlfull = dl / G.dlfac;
+      double dlhalf = (0.5 * dl) / G.dlfac;
+      double A[4][4];
+      HermN Nh, Nn;
+      load_A(L.rec_i + REC_A1, A);
+      hn_push(L.N, L.N, A, dlhalf, &Nh);
+      load_A(L.rec_i + REC_A2, A);
+      hn_push(L.N, Nh, A, dlfull, &Nn);
+      L.N = Nn;
     }
-    o.flag = flag;
-    out[ray] = o;
-    atomicAdd(&counters[CNT_RAD], nrad);
+    int flags = (int)rec_f[REC_FLAGS];
+    if (flags & 1) {
+      L.nrad++;
+      int zero_emission = (flags & 2) ? 1 : 0;
+      if (C.target_nturns >= 0 && (int)L.rec_i[REC_NTURNS] != C.target_nturns) zero_emission = 1;
+      double ji = L.js, ki = L.ks;
+      double jf = rec_f[REC_JU], kf = rec_f[REC_KU];
+      L.js = jf;
+      L.ks = kf;
+      if (zero_emission) L.I = approximate_solve(L.I, 0, ki, 0, kf, dl, &L.tau);
+      else L.I = approximate_solve(L.I, ji, ki, jf, kf, dl, &L.tau);
+      if (!unpol) {
+        L.flag |= flags >> 2;
+        L.flag |= evolve_N_rec(rec_f, dl, zero_emission, &L.N, &L.tauF);
+      }
+    }
+    L.rec_i = rec_f;
+    L.n--;
   }
-}
-
-__device__ __forceinline__ void model_point_geo(const double *__restrict__ fields, double X1, double X2, double X3,
-                                                const PointGeo &pg, ModelPt *mp)
-{
-  model_point(fields, X1, X2, X3, pg, mp);
 }
 
 /* ===================================================================== */
@@ -497,6 +622,7 @@ struct ipg_ctx {
   DevGrid dg;
   double *d_pool;
   int *d_chunk_prev;
+  int2 *d_chunk_meta;
   long long n_chunks;
   size_t pool_bytes_req;
   unsigned long long *d_cnt;
@@ -515,10 +641,10 @@ static int cuda_fail(ipg_ctx *ctx, cudaError_t e, const char *where)
   if (ctx) snprintf(ctx->err, sizeof(ctx->err), "%s: %s", where, cudaGetErrorString(e));
   return IPG_E_CUDA;
 }
-#define CK(call)                                                      \
-  do {                                                                \
-    cudaError_t e_ = (call);                                          \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);          \
+#define CK(call)                                             \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
   } while (0)
 
 extern "C" const char *ipg_strerror(int code)
@@ -570,6 +696,7 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   cudaFree(ctx->d_fields);
   cudaFree(ctx->d_pool);
   cudaFree(ctx->d_chunk_prev);
+  cudaFree(ctx->d_chunk_meta);
   cudaFree(ctx->d_cnt);
   cudaFree(ctx->d_rays);
   cudaFree(ctx->d_list[0]);
@@ -635,18 +762,22 @@ extern "C" int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *g, const double *c
   return IPG_OK;
 }
 
+/* The trajectory pool: 70% of the free device memory unless the caller asked
+ * for a size.  One 400x400 image of a 288x128x128 dump stores ~2.1e8 steps
+ * (108 GB at 512 B a step) and so fits in one wave on a 180 GB device. */
 static int ensure_pool(ipg_ctx *ctx)
 {
   if (ctx->d_pool) return IPG_OK;
   size_t freeb = 0, totalb = 0;
   CK(cudaMemGetInfo(&freeb, &totalb));
-  size_t want = ctx->pool_bytes_req ? ctx->pool_bytes_req : (size_t)(0.6 * (double)freeb);
-  size_t chunk_bytes = (size_t)IPG_CHUNK_STEPS * IPG_STEP_DOUBLES * sizeof(double) + sizeof(int);
+  size_t want = ctx->pool_bytes_req ? ctx->pool_bytes_req : (size_t)(0.7 * (double)freeb);
+  size_t chunk_bytes = (size_t)IPG_CHUNK_STEPS * IPG_STEP_DOUBLES * sizeof(double) + sizeof(int) + sizeof(int2);
   long long n = (long long)(want / chunk_bytes);
   if (n > 0x7fffffffLL) n = 0x7fffffffLL;
   if (n < 16) return IPG_E_NOMEM;
   CK(cudaMalloc(&ctx->d_pool, (size_t)n * IPG_CHUNK_STEPS * IPG_STEP_DOUBLES * sizeof(double)));
   CK(cudaMalloc(&ctx->d_chunk_prev, (size_t)n * sizeof(int)));
+  CK(cudaMalloc(&ctx->d_chunk_meta, (size_t)n * sizeof(int2)));
   ctx->n_chunks = n;
   return IPG_OK;
 }
@@ -701,6 +832,8 @@ static void make_devcam(const ipg_camera *c, DevCam *d)
   d->counterjet = c->counterjet;
 }
 
+/* persistent grid: the resident blocks of the kernel on every SM, no more
+ * than the work needs */
 static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n)
 {
   int per_sm = 1;
@@ -708,6 +841,7 @@ static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n)
   if (per_sm < 1) per_sm = 1;
   size_t full = (size_t)ctx->n_sm * per_sm;
   size_t need = (n + threads - 1) / threads;
+  if (need < 1) need = 1;
   return (int)(need < full ? need : full);
 }
 
@@ -739,7 +873,7 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
   const int32_t *list = NULL; /* identity on the first wave */
   size_t pending = n, wave = n;
   int cur = 0;
-  float gms = 0.f, tms = 0.f;
+  float gms = 0.f, cms = 0.f, tms = 0.f;
   while (pending > 0) {
     size_t run = pending < wave ? pending : wave;
     size_t carry = pending - run;
@@ -763,25 +897,33 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
     int gb = grid_blocks(ctx, (const void *)k_geodesic, threads, run);
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     k_geodesic<<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, ctx->d_pool, ctx->d_chunk_prev,
-                                                 ctx->n_chunks, ctx->d_cnt, ctx->d_rays, ctx->d_list[cur ^ 1]);
+                                                 ctx->d_chunk_meta, ctx->n_chunks, ctx->d_cnt, ctx->d_rays,
+                                                 ctx->d_list[cur ^ 1]);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    int tb = grid_blocks(ctx, (const void *)k_transfer, threads, run);
-    k_transfer<<<tb, threads, 0, ctx->stream>>>(list, (int)run, ctx->d_pool, ctx->d_chunk_prev, ctx->d_rays,
-                                                 ctx->d_fields, d_out, ctx->d_cnt);
+    int cb = grid_blocks(ctx, (const void *)k_coeffs, threads, (size_t)ctx->n_chunks * IPG_CHUNK_STEPS);
+    k_coeffs<<<cb, threads, 0, ctx->stream>>>(ctx->d_pool, ctx->d_chunk_meta, ctx->d_cnt, ctx->n_chunks,
+                                               ctx->d_rays, ctx->d_fields);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    int tb = grid_blocks(ctx, (const void *)k_transfer, threads, run);
+    k_transfer<<<tb, threads, 0, ctx->stream>>>(list, (int)run, ctx->d_pool, ctx->d_chunk_prev, ctx->d_rays, d_out,
+                                                 ctx->d_cnt);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     unsigned long long cnt[CNT_N];
     CK(cudaMemcpyAsync(cnt, ctx->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    float a = 0, b = 0;
+    float a = 0, b = 0, c = 0;
     cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
     cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
     gms += a;
-    tms += b;
+    cms += b;
+    tms += c;
     ctx->stats.ray_steps += cnt[CNT_STEPS];
     ctx->stats.radiating_steps += cnt[CNT_RAD];
-    ctx->stats.launches += 2;
+    ctx->stats.launches += 3;
     ctx->stats.waves += 1;
     size_t deferred = (size_t)cnt[CNT_DEFER];
     if (deferred == pending) {
@@ -797,6 +939,7 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
     list = ctx->d_list[cur];
   }
   ctx->stats.geodesic_ms = gms;
+  ctx->stats.coeffs_ms = cms;
   ctx->stats.transfer_ms = tms;
   return IPG_OK;
 }

@@ -694,16 +694,23 @@ static double rho_Q(const fitp *p)
   return 2. * S_PI * p->nu / (2. * S_CL) * eps11m22;
 }
 
-static double rho_V(const fitp *p)
+static double rho_V(const fitp *p, int dexter)
 {
   double omega0 = S_EE * p->B / (S_ME * S_CL);
   double wp2 = 4. * S_PI * p->Ne * pow(S_EE, 2.) / S_ME;
   double x = p->Thetae * sqrt(sqrt(2.) * sin(p->theta) * (1.e3 * omega0 / (2. * S_PI * p->nu)));
   double k0 = gsl_sf_bessel_Kn(0, 1. / p->Thetae);
   double k2 = gsl_sf_bessel_Kn(2, 1. / p->Thetae);
-  double shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
-  double k_ratio = (k2 > 0) ? k0 / k2 : 1;
-  double fit_factor = k_ratio * shgmfunc;
+  double fit_factor;
+  if (dexter && k2 > 0) {
+    /* Dexter (2016) g(X), src/symphony/maxwell_juettner_fits.c:269-272 */
+    double shgmfunc = 0.43793091 * log(1. + 0.00185777 * pow(x, 1.50316886));
+    fit_factor = (k0 - shgmfunc) / k2;
+  } else {
+    double shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
+    double k_ratio = (k2 > 0) ? k0 / k2 : 1;
+    fit_factor = k_ratio * shgmfunc;
+  }
   double eps12 = wp2 * omega0 / pow((2. * S_PI * p->nu), 3.) * fit_factor * cos(p->theta);
   return 2. * S_PI * p->nu / S_CL * eps12;
 }
@@ -730,7 +737,10 @@ static void jar_calc_dist(const orc_model *m, int dist, int pol, const double X[
     *jI = 0.0; *jQ = 0.0; *jU = 0.0; *jV = 0.0;
     *aI = 0.0; *aQ = 0.0; *aU = 0.0; *aV = 0.0;
     *rQ = 0.0; *rU = 0.0;
-    *rV = pol ? rho_V(&p) * nu : 0.0;
+    /* the reference leaves paramsM.dexter_fit = 1 on this early return for
+     * the Dexter emission type (src/model_radiation.c:202-207, 212-221), so
+     * its rho_V takes Dexter's g(X) here, Shcherbakov's elsewhere */
+    *rV = pol ? rho_V(&p, dist == 4) * nu : 0.0;
     return;
   }
   if (!pol) {
@@ -771,7 +781,7 @@ static void jar_calc_dist(const orc_model *m, int dist, int pol, const double X[
   }
   *rQ = rho_Q(&p) * nu;
   *rU = 0. * nu;
-  *rV = rho_V(&p) * nu;
+  *rV = rho_V(&p, 0) * nu;
 }
 
 static void get_jkinv(const orc_model *m, const orc_camera *c, const double X[NDIM], const double K[NDIM], double *j,
