@@ -121,6 +121,45 @@ int ipg_trace_pixels(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *ij, siz
 int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n,
                             ipg_pixel_out *d_out, void *stream);
 
+/* Trace n pixels without allocating any device memory.  This entry point has
+ * no counterpart in the reference.
+ *
+ * It is for callers that cannot call cudaMalloc: applications that give the
+ * library a fixed share of device memory through their own allocator or pool
+ * and treat any allocation made behind their back as a budget violation, and
+ * latency-sensitive pipelines in which cudaMalloc/cudaFree, which can
+ * synchronise the whole device, would stall their other streams.  Everything
+ * the call needs beyond its inputs and outputs lives in one statically sized
+ * scratch array per device (IPG_NOALLOC_SCRATCH_BYTES, 26.5 MiB) that every
+ * process loading the library holds on each GPU it uses until it exits.
+ *
+ * Inputs and outputs, all on the current device: d_fields holds the model in
+ * the library's layout, cell-major with the IPG_NFIELD fields of a zone
+ * contiguous: d_fields[((i*(n2+2) + j)*(n3+2) + k)*IPG_NFIELD + f] for the
+ * ghost-padded zone (i, j, k) and field f; d_ij is int32[2n], d_out is
+ * ipg_pixel_out[n].  grid and cam are host structs as for the other calls.
+ * Work is enqueued on `stream` (a cudaStream_t, 0 = legacy default stream),
+ * which is synchronised before the call returns.
+ *
+ * Limits: n <= IPG_NOALLOC_MAX_RAYS and cam->maxnstep <= IPG_NOALLOC_MAX_STEPS,
+ * otherwise IPG_E_ARG.  The scratch holds IPG_NOALLOC_MAX_STEPS trajectory
+ * steps at a time, so a batch runs in as many waves as it needs and is much
+ * slower than ipg_trace_pixels_device.  Returns IPG_E_MAXNSTEP like
+ * ipg_trace_pixels_device.
+ *
+ * The first call on a device sets the call up: it looks up the device address
+ * of the scratch array, which may load the library's device code, so make
+ * that first call before any stream capture begins.  All calls share the
+ * scratch array and the kernels' constant parameters, which keep what the last
+ * call wrote: calls whose work overlaps on the GPU (from other streams or host
+ * threads, or a context's ipg_trace_pixels* calls) race and give wrong
+ * results, so serialise them. */
+#define IPG_NOALLOC_MAX_RAYS 65536
+#define IPG_NOALLOC_MAX_STEPS 51200
+#define IPG_NOALLOC_SCRATCH_BYTES 27806720
+int ipg_trace_pixels_noalloc(const ipg_grid *grid, const double *d_fields, const ipg_camera *cam,
+                             const int32_t *d_ij, size_t n, ipg_pixel_out *d_out, void *stream);
+
 /* Kernel statistics of the last trace call: total ray-steps of the geodesic
  * pass, steps inside the radiating region, number of kernel launches and
  * pool waves, and the device time (ms, CUDA events) of the geodesic,

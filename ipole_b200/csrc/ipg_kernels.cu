@@ -1031,3 +1031,204 @@ extern "C" int ipg_measure_fp64_peak(int device, double ms, double *tflops)
   cudaFree(d);
   return IPG_OK;
 }
+
+/* ===================================================================== */
+/* tracing without device allocation                                      */
+/* ===================================================================== */
+/* ipg_trace_pixels_noalloc serves callers that cannot call cudaMalloc (a host
+ * application that owns the device-memory budget through its own allocator,
+ * or a pipeline that cannot afford the device-wide synchronisation of
+ * cudaMalloc/cudaFree).  It runs the same three kernels as a context, with
+ * every scratch buffer carved out of one file-scope device array of fixed
+ * size instead of memory allocated at run time. */
+#include <mutex>
+
+#define NA_CHUNKS (IPG_NOALLOC_MAX_STEPS / IPG_CHUNK_STEPS)
+#define NA_OFF_CNT ((size_t)0)
+#define NA_OFF_RAYS ((size_t)256)
+#define NA_OFF_LIST0 (NA_OFF_RAYS + (size_t)IPG_NOALLOC_MAX_RAYS * sizeof(RayRec))
+#define NA_OFF_LIST1 (NA_OFF_LIST0 + (size_t)IPG_NOALLOC_MAX_RAYS * sizeof(int32_t))
+#define NA_OFF_PREV (NA_OFF_LIST1 + (size_t)IPG_NOALLOC_MAX_RAYS * sizeof(int32_t))
+#define NA_OFF_META (NA_OFF_PREV + (size_t)NA_CHUNKS * sizeof(int))
+#define NA_OFF_POOL (NA_OFF_META + (size_t)NA_CHUNKS * sizeof(int2))
+#define NA_BYTES (NA_OFF_POOL + (size_t)NA_CHUNKS * IPG_CHUNK_STEPS * IPG_STEP_DOUBLES * sizeof(double))
+#define NA_MAX_DEVICES 64
+#define NA_CNT_MAXN CNT_N /* extra counter after the wave counters: rays that hit maxnstep */
+
+static_assert(NA_BYTES == IPG_NOALLOC_SCRATCH_BYTES, "scratch layout and its published size disagree");
+static_assert(NA_OFF_LIST0 % 256 == 0 && NA_OFF_LIST1 % 256 == 0 && NA_OFF_PREV % 256 == 0 &&
+                  NA_OFF_META % 256 == 0 && NA_OFF_POOL % 256 == 0,
+              "scratch sections must stay 256-byte aligned");
+static_assert((CNT_N + 1) * sizeof(unsigned long long) <= NA_OFF_RAYS, "counters overflow their section");
+static_assert(IPG_NOALLOC_MAX_STEPS % IPG_CHUNK_STEPS == 0, "the step limit must be whole chunks");
+
+/* The scratch array.  In host code this name only stands in for the symbol;
+ * its device address comes from cudaGetSymbolAddress, once per device. */
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+static std::mutex g_na_mutex;
+static unsigned char *g_na_base[NA_MAX_DEVICES];
+static int g_na_nsm[NA_MAX_DEVICES];
+
+/* Set-up, once per device with that device current: the device address of
+ * the scratch array and the SM count. */
+static int na_setup(int dev, unsigned char **base, int *n_sm)
+{
+  if (dev < 0 || dev >= NA_MAX_DEVICES) return IPG_E_ARG;
+  std::lock_guard<std::mutex> lock(g_na_mutex);
+  if (!g_na_base[dev]) {
+    unsigned char *ptr = NULL;
+    if (cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return IPG_E_CUDA;
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1)
+      return IPG_E_CUDA;
+    g_na_nsm[dev] = nsm;
+    g_na_base[dev] = ptr;
+  }
+  *base = g_na_base[dev];
+  *n_sm = g_na_nsm[dev];
+  return IPG_OK;
+}
+
+__global__ void k_na_iota(int32_t *list, int n, int first)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) list[t] = first + t;
+}
+
+__global__ void k_na_count_maxnstep(const RayRec *__restrict__ rays, int n, unsigned long long *count)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n && rays[t].status == IPG_RAY_MAXNSTEP) atomicAdd(count, 1ULL);
+}
+
+static int na_blocks(int n_sm, const void *kernel, int threads, size_t n)
+{
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  size_t full = (size_t)n_sm * per_sm;
+  size_t need = (n + threads - 1) / threads;
+  if (need < 1) need = 1;
+  return (int)(need < full ? need : full);
+}
+
+#define NA_CK(call)                                \
+  do {                                             \
+    if ((call) != cudaSuccess) return IPG_E_CUDA;  \
+  } while (0)
+
+extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_fields, const ipg_camera *cam,
+                                        const int32_t *d_ij, size_t n, ipg_pixel_out *d_out, void *stream_)
+{
+  if (!g || !d_fields || !cam || (n && (!d_ij || !d_out))) return IPG_E_ARG;
+  if (n > IPG_NOALLOC_MAX_RAYS || cam->maxnstep > IPG_NOALLOC_MAX_STEPS) return IPG_E_ARG;
+  if (g->n1 <= 0 || g->n2 <= 0 || g->n3 <= 0) return IPG_E_ARG;
+  if (cam->emission_type != 4 && cam->emission_type != 1) return IPG_E_ARG;
+  if (cam->maxnstep < 2 || cam->nx <= 0 || cam->ny <= 0) return IPG_E_ARG;
+  if (n == 0) return IPG_OK;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  int dev = 0;
+  NA_CK(cudaGetDevice(&dev));
+  unsigned char *base = NULL;
+  int n_sm = 0;
+  int rc = na_setup(dev, &base, &n_sm);
+  if (rc) return rc;
+  unsigned long long *cnt_d = (unsigned long long *)(base + NA_OFF_CNT);
+  RayRec *rays = (RayRec *)(base + NA_OFF_RAYS);
+  int32_t *lists[2] = {(int32_t *)(base + NA_OFF_LIST0), (int32_t *)(base + NA_OFF_LIST1)};
+  int *chunk_prev = (int *)(base + NA_OFF_PREV);
+  int2 *chunk_meta = (int2 *)(base + NA_OFF_META);
+  double *pool = (double *)(base + NA_OFF_POOL);
+  const long long n_chunks = NA_CHUNKS;
+
+  /* grid constants as ipg_upload_iharm derives them */
+  DevGrid d;
+  memset(&d, 0, sizeof(d));
+  d.n1 = g->n1;
+  d.n2 = g->n2;
+  d.n3 = g->n3;
+  for (int i = 0; i < 4; i++) {
+    d.startx[i] = g->startx[i];
+    d.stopx[i] = g->stopx[i];
+    d.dx[i] = g->dx[i];
+    d.cstartx[i] = g->cstartx[i];
+    d.cstopx[i] = g->cstopx[i];
+  }
+  d.a = g->a;
+  d.hslope = g->hslope;
+  d.poly_xt = g->poly_xt;
+  d.poly_alpha = g->poly_alpha;
+  d.mks_smooth = g->mks_smooth;
+  d.poly_norm = g->poly_norm;
+  d.Rh = g->Rh;
+  d.rmin_geo = g->rmin_geo;
+  d.rmax_geo = g->rmax_geo;
+  d.th_beg = g->th_beg;
+  d.sigma_cut = g->sigma_cut;
+  d.sigma_eq_factor = (g->sigma_cut_high > 0 && g->sigma_cut_high > g->sigma_cut) ? 1. : 0.;
+  d.L_unit = g->L_unit;
+  d.dlfac = g->L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
+  d.sj = g->n3 + 2;
+  d.si = (long long)(g->n2 + 2) * (g->n3 + 2);
+  double am1 = g->poly_alpha - 1.;
+  d.alpha_int = (am1 >= 0 && am1 <= 64 && am1 == (double)(int)am1) ? (int)am1 : -1;
+  DevCam dc;
+  make_devcam(cam, &dc);
+  NA_CK(cudaMemcpyToSymbolAsync(c_grid, &d, sizeof(DevGrid), 0, cudaMemcpyHostToDevice, stream));
+  NA_CK(cudaMemcpyToSymbolAsync(c_cam, &dc, sizeof(DevCam), 0, cudaMemcpyHostToDevice, stream));
+
+  /* the wave loop of a context's trace, on the scratch buffers; the
+   * counters are the only scratch that must start at zero, and they are
+   * cleared before every wave */
+  const int threads = 128;
+  const int32_t *list = NULL;
+  size_t pending = n, wave = n;
+  int cur = 0;
+  while (pending > 0) {
+    size_t run = pending < wave ? pending : wave;
+    size_t carry = pending - run;
+    NA_CK(cudaMemsetAsync(cnt_d, 0, sizeof(unsigned long long) * (CNT_N + 1), stream));
+    if (carry) {
+      if (list) {
+        NA_CK(cudaMemcpyAsync(lists[cur ^ 1], list + run, carry * sizeof(int32_t), cudaMemcpyDeviceToDevice, stream));
+      } else {
+        k_na_iota<<<(int)((carry + 255) / 256), 256, 0, stream>>>(lists[cur ^ 1], (int)carry, (int)run);
+        NA_CK(cudaGetLastError());
+      }
+      unsigned long long c0 = carry;
+      NA_CK(cudaMemcpyAsync(cnt_d + CNT_DEFER, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
+      NA_CK(cudaStreamSynchronize(stream));
+    }
+    int gb = na_blocks(n_sm, (const void *)k_geodesic, threads, run);
+    k_geodesic<<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta, n_chunks, cnt_d, rays,
+                                           lists[cur ^ 1]);
+    NA_CK(cudaGetLastError());
+    int cb = na_blocks(n_sm, (const void *)k_coeffs, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
+    k_coeffs<<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
+    NA_CK(cudaGetLastError());
+    int tb = na_blocks(n_sm, (const void *)k_transfer, threads, run);
+    k_transfer<<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev, rays, d_out, cnt_d);
+    NA_CK(cudaGetLastError());
+    unsigned long long cnt[CNT_N];
+    NA_CK(cudaMemcpyAsync(cnt, cnt_d, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
+    NA_CK(cudaStreamSynchronize(stream));
+    size_t deferred = (size_t)cnt[CNT_DEFER];
+    if (deferred == pending) {
+      /* no ray finished: fewer rays share the scratch next time; a single
+       * ray always fits because maxnstep <= IPG_NOALLOC_MAX_STEPS */
+      if (run == 1) return IPG_E_NOMEM;
+      wave = run / 2;
+    }
+    pending = deferred;
+    cur ^= 1;
+    list = lists[cur];
+  }
+  /* every ray's record now holds its final status */
+  k_na_count_maxnstep<<<(int)((n + 255) / 256), 256, 0, stream>>>(rays, (int)n, cnt_d + NA_CNT_MAXN);
+  NA_CK(cudaGetLastError());
+  unsigned long long n_maxn = 0;
+  NA_CK(cudaMemcpyAsync(&n_maxn, cnt_d + NA_CNT_MAXN, sizeof(n_maxn), cudaMemcpyDeviceToHost, stream));
+  NA_CK(cudaStreamSynchronize(stream));
+  return n_maxn ? IPG_E_MAXNSTEP : IPG_OK;
+}
