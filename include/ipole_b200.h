@@ -162,8 +162,10 @@ int ipg_trace_pixels_noalloc(const ipg_grid *grid, const double *d_fields, const
 
 /* Kernel statistics of the last trace call: total ray-steps of the geodesic
  * pass, steps inside the radiating region, number of kernel launches and
- * pool waves, and the device time (ms, CUDA events) of the geodesic,
- * coefficient and transfer kernels. */
+ * pool waves, the device time (ms, CUDA events) of the geodesic, coefficient
+ * and transfer kernels, summed over the batches of a wave (batches run
+ * concurrently, so these can add up to more than the call), the time of the
+ * ray-length prediction, and the device time of the whole call. */
 typedef struct ipg_stats {
   uint64_t ray_steps;
   uint64_t radiating_steps;
@@ -172,6 +174,8 @@ typedef struct ipg_stats {
   double geodesic_ms;
   double transfer_ms;
   double coeffs_ms;
+  double predict_ms;
+  double wall_ms;
 } ipg_stats;
 int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 

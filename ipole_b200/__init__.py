@@ -74,7 +74,7 @@ assert PIXEL_DTYPE.itemsize == C.sizeof(PixelOut)
 class Stats(C.Structure):
     _fields_ = [("ray_steps", C.c_uint64), ("radiating_steps", C.c_uint64), ("launches", C.c_int32),
                 ("waves", C.c_int32), ("geodesic_ms", C.c_double), ("transfer_ms", C.c_double),
-                ("coeffs_ms", C.c_double)]
+                ("coeffs_ms", C.c_double), ("predict_ms", C.c_double), ("wall_ms", C.c_double)]
 
 
 class _Params(C.Structure):

@@ -176,8 +176,10 @@ __device__ __forceinline__ int radiating(const PointGeo &pg)
 struct GeoLane {
   double X[4], K[4], Xh[4], Kh[4];
   double X1m1, X2m1, X1m2, X2m2; /* sub-ring bookkeeping: X1, X2 of steps n-1, n-2 */
+  double h;                      /* -dl of the step in progress */
   double *prev;                  /* record of the last stored step */
   int ray, nstep, chunk, passed, nturns;
+  int phase;                     /* 0: next is Gamma at X, 1: Gamma at Xhalf */
 };
 
 /* Take the next ray from the wave's queue and store its camera point as
@@ -214,6 +216,8 @@ __device__ __forceinline__ bool geo_fetch(GeoLane &L, const int32_t *__restrict_
     L.prev = step_ptr(pool, L.chunk, 0);
     store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, 0., 0.);
     L.nstep = 0;
+    L.phase = 0;
+    L.h = 0.;
     L.passed = (C.Xcam[2] < 0.5) ? 1 : ((C.Xcam[2] > 0.5) ? -1 : 0);
     L.nturns = 0;
     L.X1m1 = L.X1m2 = L.X[1];
@@ -222,6 +226,39 @@ __device__ __forceinline__ bool geo_fetch(GeoLane &L, const int32_t *__restrict_
   }
 }
 
+/* Sub-ring counter, src/model_geodesics.c:129-165, after step nstep */
+__device__ __forceinline__ void count_turns(GeoLane &L)
+{
+  const DevCam &C = c_cam;
+  if (L.passed != 0) {
+    if (L.passed > 0) {
+      if (L.X[2] > 0.5) L.passed = 0;
+    } else {
+      if (L.X[2] < 0.5) L.passed = 0;
+    }
+  } else if (L.nstep > 3) {
+    if (C.subring_dtheta == 1) {
+      double dX2a = L.X2m1 - L.X2m2, dX2b = L.X[2] - L.X2m1;
+      if (dX2a * dX2b < 0) L.nturns++;
+    } else {
+      double ra = exp(L.X1m2), rb = exp(L.X1m1), rc = exp(L.X[1]);
+      double za = ra * cos(bl_theta(L.X1m2, L.X2m2)), zb = rb * cos(bl_theta(L.X1m1, L.X2m1));
+      double zc = rc * cos(bl_theta(L.X[1], L.X[2]));
+      if ((zb - za) * (zc - zb) < 0) L.nturns++;
+    }
+  }
+  L.X1m2 = L.X1m1;
+  L.X2m2 = L.X2m1;
+  L.X1m1 = L.X[1];
+  L.X2m1 = L.X[2];
+}
+
+/* One loop iteration is one half of push_photon (src/geodesics.c:9-70):
+ * the connection at X (phase 0) or at Xhalf (phase 1).  Lanes of a warp in
+ * different phases still run the connection code together, and the kernel
+ * holds one copy of it, which keeps the loop body small: a lone ray's step
+ * time is set by instruction-fetch and dependency latency, not by the FP64
+ * throughput of the SM. */
 __global__ void __launch_bounds__(128, IPG_GEO_MINB)
     k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list,
                double *__restrict__ pool, int *__restrict__ chunk_prev, int2 *__restrict__ chunk_meta,
@@ -236,81 +273,65 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
   bool has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
-    /* stop_backward_integration, src/model_geodesics.c:218-254, and the
-     * step limit of trace_geodesic's loop (:71) */
-    double r = exp(L.X[1]);
-    if ((r > G.rmax_geo && L.K[1] < 0.) || r < (G.Rh + 0.0001) || !(L.nstep < C.maxnstep - 1)) {
-      RayRec rec = {L.chunk, L.nstep, (L.nstep >= C.maxnstep - 1) ? IPG_RAY_MAXNSTEP : IPG_RAY_OK, 0};
-      if (rec.status == IPG_RAY_OK && pol && L.nstep > 0) {
-        /* the walk back starts at the last point: its Gamma(X) K too */
-        Conn cn;
-        double A[4][4];
-        fd_connection(L.X[1], L.X[2], &cn);
-        transport_matrix(cn, L.K, A);
-        store_A(L.prev + REC_A1, A);
+    const int ph = L.phase;
+    int stop = 0;
+    if (ph == 0) {
+      /* stop_backward_integration, src/model_geodesics.c:218-254, and the
+       * step limit of trace_geodesic's loop (:71) */
+      double r = exp(L.X[1]);
+      if ((r > G.rmax_geo && L.K[1] < 0.) || r < (G.Rh + 0.0001) || !(L.nstep < C.maxnstep - 1)) {
+        int status = (L.nstep >= C.maxnstep - 1) ? IPG_RAY_MAXNSTEP : IPG_RAY_OK;
+        if (status != IPG_RAY_OK || !pol || L.nstep == 0) {
+          RayRec rec = {L.chunk, L.nstep, status, 0};
+          rays[L.ray] = rec;
+          atomicAdd(&counters[CNT_STEPS], (unsigned long long)L.nstep);
+          has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+          continue;
+        }
+        stop = 1; /* the walk back starts at the last point: its Gamma(X) K too */
       }
-      rays[L.ray] = rec;
-      atomicAdd(&counters[CNT_STEPS], (unsigned long long)L.nstep);
-      has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
-      continue;
     }
-    L.nstep++;
-    double dl = stepsize(L.X, L.K, C.eps);
-    double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
-    /* push_photon(X, Kcon, -dl, Xhalf, Kconhalf), src/geodesics.c:9-70 */
-    double h = -dl;
+    double Ke[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) Ke[k] = ph ? L.Kh[k] : L.K[k];
     Conn cn;
     double acc[4], A[4][4];
-    fd_connection(L.X[1], L.X[2], &cn);
+    fd_connection(ph ? L.Xh[1] : L.X[1], ph ? L.Xh[2] : L.X[2], &cn);
     if (pol) {
-      /* the transfer needs Gamma(X_n) K_n for the step that ends at n */
-      transport_matrix(cn, L.K, A);
-      store_A(L.prev + REC_A1, A);
-      accel_from_A(A, L.K, acc);
+      /* the transfer needs Gamma K at X_n and at Xhalf_n for each step */
+      transport_matrix(cn, Ke, A);
+      accel_from_A(A, Ke, acc);
     } else {
-      geo_accel(cn, L.K, acc);
+      geo_accel(cn, Ke, acc);
     }
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      L.Kh[k] = L.K[k] - 0.5 * h * acc[k];
-      L.Xh[k] = L.X[k] + 0.5 * h * L.K[k];
-    }
-    fd_connection(L.Xh[1], L.Xh[2], &cn);
-    if (pol) {
-      transport_matrix(cn, L.Kh, A);
-      accel_from_A(A, L.Kh, acc);
-    } else {
-      geo_accel(cn, L.Kh, acc);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      L.K[k] = L.K[k] - h * acc[k];
-      L.X[k] = L.X[k] + h * L.Kh[k];
-    }
-    if (track) {
-      /* sub-ring counter, src/model_geodesics.c:129-165 */
-      if (L.passed != 0) {
-        if (L.passed > 0) {
-          if (L.X[2] > 0.5) L.passed = 0;
-        } else {
-          if (L.X[2] < 0.5) L.passed = 0;
-        }
-      } else if (L.nstep > 3) {
-        if (C.subring_dtheta == 1) {
-          double dX2a = L.X2m1 - L.X2m2, dX2b = L.X[2] - L.X2m1;
-          if (dX2a * dX2b < 0) L.nturns++;
-        } else {
-          double ra = exp(L.X1m2), rb = exp(L.X1m1), rc = exp(L.X[1]);
-          double za = ra * cos(bl_theta(L.X1m2, L.X2m2)), zb = rb * cos(bl_theta(L.X1m1, L.X2m1));
-          double zc = rc * cos(bl_theta(L.X[1], L.X[2]));
-          if ((zb - za) * (zc - zb) < 0) L.nturns++;
-        }
+    if (ph == 0) {
+      if (pol) store_A(L.prev + REC_A1, A);
+      if (stop) {
+        RayRec rec = {L.chunk, L.nstep, IPG_RAY_OK, 0};
+        rays[L.ray] = rec;
+        atomicAdd(&counters[CNT_STEPS], (unsigned long long)L.nstep);
+        has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+        continue;
       }
-      L.X1m2 = L.X1m1;
-      L.X2m2 = L.X2m1;
-      L.X1m1 = L.X[1];
-      L.X2m1 = L.X[2];
+      L.nstep++;
+      L.h = -stepsize(L.X, L.K, C.eps);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        L.Kh[k] = L.K[k] - 0.5 * L.h * acc[k];
+        L.Xh[k] = L.X[k] + 0.5 * L.h * L.K[k];
+      }
+      L.phase = 1;
+      continue;
     }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      L.K[k] = L.K[k] - L.h * acc[k];
+      L.X[k] = L.X[k] + L.h * L.Kh[k];
+    }
+    L.phase = 0;
+    double dl = -L.h;
+    double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
+    if (track) count_turns(L);
     int slot = L.nstep % IPG_CHUNK_STEPS;
     if (slot == 0) {
       long long nc = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
@@ -328,6 +349,72 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
     L.prev = step_ptr(pool, L.chunk, slot);
     store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
     if (pol) store_A(L.prev + REC_A2, A); /* Gamma(Xh_n) Kh_n */
+  }
+}
+
+
+/* Step count of each ray at a coarser accuracy (eps_scale x eps), without
+ * storing anything: a cheap prediction of the ray lengths, so that the full
+ * trace can start the longest rays first.  pred[t] is the count of list
+ * entry t; a ray whose position turns non-finite, or that passes step_cap,
+ * stops there. */
+__global__ void __launch_bounds__(128, IPG_GEO_MINB)
+    k_geodesic_count(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list, double eps_scale,
+                     int step_cap, int32_t *__restrict__ pred, unsigned long long *__restrict__ counter)
+{
+  const DevGrid &G = c_grid;
+  const DevCam &C = c_cam;
+  const double eps = C.eps * eps_scale;
+  double X[4], K[4], Xh[4], Kh[4], h = 0.;
+  int t = -1, nstep = 0, phase = 0;
+  bool has = false, drained = false;
+  while (true) {
+    if (!has && !drained) {
+      unsigned long long q = atomicAdd(counter, 1ULL);
+      has = q < (unsigned long long)n_list;
+      drained = !has;
+      if (has) {
+        t = (int)q;
+        int ray = list ? list[t] : t;
+        init_ray(ij[2 * ray], ij[2 * ray + 1], X, K);
+        nstep = 0;
+        phase = 0;
+      }
+    }
+    if (!__any_sync(0xffffffffu, has)) break;
+    if (!has) continue;
+    if (phase == 0) {
+      double r = exp(X[1]);
+      if ((r > G.rmax_geo && K[1] < 0.) || r < (G.Rh + 0.0001) || !(nstep < step_cap) || !isfinite(X[1])) {
+        pred[t] = nstep;
+        has = false;
+        continue;
+      }
+    }
+    double Ke[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) Ke[k] = phase ? Kh[k] : K[k];
+    Conn cn;
+    double acc[4];
+    fd_connection(phase ? Xh[1] : X[1], phase ? Xh[2] : X[2], &cn);
+    geo_accel(cn, Ke, acc);
+    if (phase == 0) {
+      nstep++;
+      h = -stepsize(X, K, eps);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        Kh[k] = K[k] - 0.5 * h * acc[k];
+        Xh[k] = X[k] + 0.5 * h * K[k];
+      }
+      phase = 1;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        K[k] = K[k] - h * acc[k];
+        X[k] = X[k] + h * Kh[k];
+      }
+      phase = 0;
+    }
   }
 }
 
@@ -480,12 +567,32 @@ struct XferLane {
   const double *rec_i;
   double I, tau, tauF, js, ks;
   int ray, n, chunk, flag, nrad;
+  int cprev; /* chunk_prev[chunk], loaded on entry to the chunk */
 };
+
+/* Software prefetch of a step record (four 128-byte lines) so that the walk
+ * does not wait on DRAM round trips step after step: a lone ray's step time
+ * is otherwise set by two to three dependent loads (transport matrices of
+ * one record, then flags and coefficients of the next). */
+#ifndef IPG_XFER_PREFETCH
+#define IPG_XFER_PREFETCH 1
+#endif
+__device__ __forceinline__ void prefetch_rec(const double *p)
+{
+#if IPG_XFER_PREFETCH == 1
+#pragma unroll
+  for (int l = 0; l < 4; l++) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + 16 * l));
+#elif IPG_XFER_PREFETCH == 2
+#pragma unroll
+  for (int l = 0; l < 4; l++) asm volatile("prefetch.global.L1 [%0];" ::"l"(p + 16 * l));
+#endif
+}
 
 /* Take the next ray whose trajectory is complete; rays that hit maxnstep get
  * an all-zero result, deferred rays are left for their next wave. */
 __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restrict__ list, int n_list,
-                                           const double *__restrict__ pool, const RayRec *__restrict__ rays,
+                                           const double *__restrict__ pool, const int *__restrict__ chunk_prev,
+                                           const RayRec *__restrict__ rays,
                                            ipg_pixel_out *__restrict__ out, unsigned long long *__restrict__ counters)
 {
   while (true) {
@@ -506,6 +613,9 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
     L.n = rec.nstep;
     L.chunk = rec.last_chunk;
     L.rec_i = step_ptr(const_cast<double *>(pool), L.chunk, L.n % IPG_CHUNK_STEPS);
+    L.cprev = chunk_prev[L.chunk];
+    prefetch_rec(L.rec_i);
+    if (L.n % IPG_CHUNK_STEPS) prefetch_rec(L.rec_i - IPG_STEP_DOUBLES);
     /* get_jkinv at the far end of the ray, src/ipolarray.c:74 */
     L.js = L.rec_i[REC_JU];
     L.ks = L.rec_i[REC_KU];
@@ -526,7 +636,7 @@ __global__ void __launch_bounds__(128, IPG_XFER_MINB)
   const DevCam &C = c_cam;
   const int unpol = C.unpol;
   XferLane L;
-  bool has = xfer_fetch(L, list, n_list, pool, rays, out, counters);
+  bool has = xfer_fetch(L, list, n_list, pool, chunk_prev, rays, out, counters);
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
     if (L.n == 0) {
@@ -549,13 +659,21 @@ __global__ void __launch_bounds__(128, IPG_XFER_MINB)
       o.flag = L.flag;
       out[L.ray] = o;
       atomicAdd(&counters[CNT_RAD], (unsigned long long)L.nrad);
-      has = xfer_fetch(L, list, n_list, pool, rays, out, counters);
+      has = xfer_fetch(L, list, n_list, pool, chunk_prev, rays, out, counters);
       continue;
     }
     /* step n -> n-1 of integrate_emission's loop, src/ipolarray.c:78-244 */
     int s = L.n - 1;
-    if (s % IPG_CHUNK_STEPS == IPG_CHUNK_STEPS - 1) L.chunk = chunk_prev[L.chunk];
+    if (s % IPG_CHUNK_STEPS == IPG_CHUNK_STEPS - 1) {
+      L.chunk = L.cprev;
+      L.cprev = chunk_prev[L.chunk];
+    }
     const double *rec_f = step_ptr(const_cast<double *>(pool), L.chunk, s % IPG_CHUNK_STEPS);
+    /* the record the next iteration reads (step s-1), and the one after */
+    if (s >= 1) {
+      if ((s - 1) % IPG_CHUNK_STEPS != IPG_CHUNK_STEPS - 1) prefetch_rec(rec_f - IPG_STEP_DOUBLES);
+      else if (L.cprev >= 0) prefetch_rec(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
+    }
     double dl = L.rec_i[REC_DL];
     if (!unpol) {
       /* push_polar twice, src/ipolarray.c:85-89 */
@@ -591,6 +709,69 @@ __global__ void __launch_bounds__(128, IPG_XFER_MINB)
 }
 
 /* ===================================================================== */
+/* longest-first order                                                    */
+/* ===================================================================== */
+/* The ray queues hand out rays in list order, and a ray costs its step
+ * count in the sequential kernels, whose time is set by the longest rays
+ * (a lone ray's step takes about as long as one under full load).  Handing
+ * out the longest rays first keeps the kernels from ending on a few long
+ * rays started last (longest-processing-time-first scheduling).  A counting
+ * sort of list positions by a key (predicted step count), descending. */
+#define LEN_BUCKETS 4096
+#define LEN_SCAN_THREADS 1024
+
+__device__ __forceinline__ int len_bucket(int key, int shift)
+{
+  int b = key >> shift;
+  return b < 0 ? 0 : (b < LEN_BUCKETS - 1 ? b : LEN_BUCKETS - 1);
+}
+
+__global__ void k_len_hist(const int32_t *__restrict__ key, int n, int shift, int *hist)
+{
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    atomicAdd(&hist[len_bucket(key[t], shift)], 1);
+}
+
+/* exclusive scan of the counts in descending bucket order, in place: one
+ * block, LEN_SCAN_THREADS threads, LEN_BUCKETS / LEN_SCAN_THREADS buckets each */
+__global__ void __launch_bounds__(LEN_SCAN_THREADS) k_len_scan(int *hist)
+{
+  constexpr int PER = LEN_BUCKETS / LEN_SCAN_THREADS;
+  __shared__ int part[LEN_SCAN_THREADS];
+  int t = threadIdx.x;
+  int c[PER], s = 0;
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    c[q] = hist[LEN_BUCKETS - 1 - (PER * t + q)];
+    s += c[q];
+  }
+  part[t] = s;
+  __syncthreads();
+  for (int off = 1; off < LEN_SCAN_THREADS; off <<= 1) {
+    int v = (t >= off) ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int base = part[t] - s;
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    hist[LEN_BUCKETS - 1 - (PER * t + q)] = base;
+    base += c[q];
+  }
+}
+
+/* sorted[] = the list's rays in descending key order (ties in any order) */
+__global__ void k_len_scatter(const int32_t *__restrict__ list, const int32_t *__restrict__ key, int n, int shift,
+                              int *offs, int32_t *__restrict__ sorted)
+{
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    int pos = atomicAdd(&offs[len_bucket(key[t], shift)], 1);
+    sorted[pos] = list ? list[t] : t;
+  }
+}
+
+/* ===================================================================== */
 /* FP64 peak probe                                                        */
 /* ===================================================================== */
 __global__ void k_fma_peak(double *out, int iters, double seed)
@@ -616,6 +797,9 @@ struct ipg_ctx {
   int device;
   cudaStream_t stream;
   cudaEvent_t ev[4];
+  cudaStream_t bstream[2]; /* the two batches of a split wave */
+  cudaEvent_t bev[2][4];   /* per batch: geodesic, coeffs, transfer boundaries */
+  cudaEvent_t ev_fork, ev_join[2], ev_pred[2];
   double *d_fields;
   size_t ncell;
   int have_model;
@@ -628,6 +812,10 @@ struct ipg_ctx {
   unsigned long long *d_cnt;
   RayRec *d_rays;
   int32_t *d_list[2];
+  int32_t *d_sorted; /* the wave's rays, longest predicted first */
+  int32_t *d_pred;   /* predicted step counts (list positions), also staging */
+  int *d_len_hist;   /* LEN_BUCKETS counters of the sort */
+  int split;         /* 1: split waves into long and short batches */
   int32_t *d_ij;
   ipg_pixel_out *d_out;
   size_t cap;
@@ -679,7 +867,17 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   for (int i = 0; e == cudaSuccess && i < 4; i++) e = cudaEventCreate(&ctx->ev[i]);
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_cnt, CNT_N * sizeof(unsigned long long));
+  for (int b = 0; e == cudaSuccess && b < 2; b++) {
+    e = cudaStreamCreateWithFlags(&ctx->bstream[b], cudaStreamNonBlocking);
+    for (int i = 0; e == cudaSuccess && i < 4; i++) e = cudaEventCreate(&ctx->bev[b][i]);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_join[b]);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_pred[b]);
+  }
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_fork);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_cnt, 3 * CNT_N * sizeof(unsigned long long));
+  ctx->split = 1;
+  if (getenv("IPG_NO_SPLIT")) ctx->split = 0;
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_len_hist, LEN_BUCKETS * sizeof(int));
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) {
     free(ctx);
@@ -701,9 +899,19 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   cudaFree(ctx->d_rays);
   cudaFree(ctx->d_list[0]);
   cudaFree(ctx->d_list[1]);
+  cudaFree(ctx->d_sorted);
+  cudaFree(ctx->d_pred);
+  cudaFree(ctx->d_len_hist);
   cudaFree(ctx->d_ij);
   cudaFree(ctx->d_out);
   for (int i = 0; i < 4; i++) cudaEventDestroy(ctx->ev[i]);
+  for (int b = 0; b < 2; b++) {
+    for (int i = 0; i < 4; i++) cudaEventDestroy(ctx->bev[b][i]);
+    cudaEventDestroy(ctx->ev_join[b]);
+    cudaEventDestroy(ctx->ev_pred[b]);
+    cudaStreamDestroy(ctx->bstream[b]);
+  }
+  cudaEventDestroy(ctx->ev_fork);
   cudaStreamDestroy(ctx->stream);
   free(ctx);
 }
@@ -788,12 +996,16 @@ static int ensure_cap(ipg_ctx *ctx, size_t n)
   cudaFree(ctx->d_rays);
   cudaFree(ctx->d_list[0]);
   cudaFree(ctx->d_list[1]);
+  cudaFree(ctx->d_sorted);
+  cudaFree(ctx->d_pred);
   cudaFree(ctx->d_ij);
   cudaFree(ctx->d_out);
   ctx->cap = 0;
   CK(cudaMalloc(&ctx->d_rays, n * sizeof(RayRec)));
   CK(cudaMalloc(&ctx->d_list[0], n * sizeof(int32_t)));
   CK(cudaMalloc(&ctx->d_list[1], n * sizeof(int32_t)));
+  CK(cudaMalloc(&ctx->d_sorted, n * sizeof(int32_t)));
+  CK(cudaMalloc(&ctx->d_pred, n * sizeof(int32_t)));
   CK(cudaMalloc(&ctx->d_ij, 2 * n * sizeof(int32_t)));
   CK(cudaMalloc(&ctx->d_out, n * sizeof(ipg_pixel_out)));
   ctx->cap = n;
@@ -845,6 +1057,117 @@ static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n)
   return (int)(need < full ? need : full);
 }
 
+/* One batch of a wave: a slice of a ray list, a slice of the trajectory pool
+ * and its own counters, run as geodesic -> coefficients -> transfer on one
+ * stream. */
+struct Batch {
+  const int32_t *list;
+  size_t run;
+  double *pool;
+  int *chunk_prev;
+  int2 *chunk_meta;
+  long long n_chunks;
+  unsigned long long *cnt;
+  int32_t *deferred;
+  cudaStream_t stream;
+  cudaEvent_t *ev;
+};
+
+static int launch_batch(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_pixel_out *d_out)
+{
+  const int threads = 128;
+  CK(cudaEventRecord(b.ev[0], b.stream));
+  int gb = grid_blocks(ctx, (const void *)k_geodesic, threads, b.run);
+  k_geodesic<<<gb, threads, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev, b.chunk_meta, b.n_chunks,
+                                           b.cnt, ctx->d_rays, b.deferred);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(b.ev[1], b.stream));
+  int cb = grid_blocks(ctx, (const void *)k_coeffs, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
+  k_coeffs<<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(b.ev[2], b.stream));
+  int tb = grid_blocks(ctx, (const void *)k_transfer, threads, b.run);
+  k_transfer<<<tb, threads, 0, b.stream>>>(b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(b.ev[3], b.stream));
+  return IPG_OK;
+}
+
+static void add_batch_stats(ipg_ctx *ctx, cudaEvent_t *ev, const unsigned long long *cnt)
+{
+  float a = 0, b = 0, c = 0;
+  cudaEventElapsedTime(&a, ev[0], ev[1]);
+  cudaEventElapsedTime(&b, ev[1], ev[2]);
+  cudaEventElapsedTime(&c, ev[2], ev[3]);
+  ctx->stats.geodesic_ms += a;
+  ctx->stats.coeffs_ms += b;
+  ctx->stats.transfer_ms += c;
+  ctx->stats.ray_steps += cnt[CNT_STEPS];
+  ctx->stats.radiating_steps += cnt[CNT_RAD];
+  ctx->stats.launches += 3;
+}
+
+/* Length prediction and split of a wave (rays run..: the list, or the
+ * identity).  Traces every ray at PRED_EPS_SCALE times the step size without
+ * storing anything, sorts the rays by that step count, longest first, into
+ * ctx->d_sorted, and puts the rays predicted at least PRED_LONG_FACTOR times
+ * the mean into the long batch.  Returns the long batch's size in *n_long
+ * and its predicted share of the steps in *share; *n_long = 0 means: do not
+ * split (the wave is small, nothing is long, or the pool looks too small to
+ * hold the whole wave at once). */
+#define PRED_EPS_SCALE 16.
+#define PRED_LONG_FACTOR 2.
+#define SPLIT_MIN_RAYS 4096
+
+static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, size_t run, const ipg_camera *cam,
+                      size_t *n_long, double *share)
+{
+  *n_long = 0;
+  *share = 0.;
+  const int threads = 128;
+  unsigned long long *cnt = ctx->d_cnt;
+  CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
+  int cap = (int)(cam->maxnstep / PRED_EPS_SCALE) + 1;
+  if (cap > LEN_BUCKETS - 1) cap = LEN_BUCKETS - 1;
+  CK(cudaEventRecord(ctx->ev_pred[0], ctx->stream));
+  int gb = grid_blocks(ctx, (const void *)k_geodesic_count, threads, run);
+  k_geodesic_count<<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, PRED_EPS_SCALE, cap, ctx->d_pred,
+                                                     cnt + CNT_NEXT_G);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(ctx->d_len_hist, 0, LEN_BUCKETS * sizeof(int), ctx->stream));
+  int sb = (int)((run + 255) / 256);
+  if (sb > 4 * ctx->n_sm) sb = 4 * ctx->n_sm;
+  k_len_hist<<<sb, 256, 0, ctx->stream>>>(ctx->d_pred, (int)run, 0, ctx->d_len_hist);
+  CK(cudaGetLastError());
+  std::vector<int> hist(LEN_BUCKETS);
+  CK(cudaMemcpyAsync(hist.data(), ctx->d_len_hist, LEN_BUCKETS * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double total = 0.;
+  for (int b = 0; b < LEN_BUCKETS; b++) total += (double)b * hist[b];
+  if (total <= 0.) return IPG_OK;
+  double mean = total / (double)run;
+  int thr = (int)(PRED_LONG_FACTOR * mean) + 1;
+  size_t nl = 0;
+  double steps_long = 0.;
+  for (int b = LEN_BUCKETS - 1; b >= thr && b >= 0; b--) {
+    nl += (size_t)hist[b];
+    steps_long += (double)b * hist[b];
+  }
+  /* the whole wave should fit: predicted steps scaled back to the real step
+   * size (steps scale as 1/eps), against the pool; rays that do not fit
+   * after all are deferred to the next wave like any other */
+  double need = total * PRED_EPS_SCALE;
+  if (need > (double)ctx->n_chunks * IPG_CHUNK_STEPS) return IPG_OK;
+  if (nl == 0 || nl > run / 2) return IPG_OK;
+  k_len_scan<<<1, LEN_SCAN_THREADS, 0, ctx->stream>>>(ctx->d_len_hist);
+  k_len_scatter<<<sb, 256, 0, ctx->stream>>>(list, ctx->d_pred, (int)run, 0, ctx->d_len_hist, ctx->d_sorted);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev_pred[1], ctx->stream));
+  *n_long = nl;
+  *share = steps_long / total;
+  return IPG_OK;
+}
+
 /* device-resident core: d_ij/d_out on the device, enqueued on ctx->stream */
 static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n, ipg_pixel_out *d_out)
 {
@@ -864,83 +1187,117 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
   CK(cudaMemcpyToSymbolAsync(c_grid, &ctx->dg, sizeof(DevGrid), 0, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyToSymbolAsync(c_cam, &dc, sizeof(DevCam), 0, cudaMemcpyHostToDevice, ctx->stream));
   memset(&ctx->stats, 0, sizeof(ctx->stats));
-  const int threads = 128;
   /* Waves: every pending ray starts; rays that find the pool full are
    * deferred to the next wave, after the finished ones have been transferred
-   * and the pool recycled.  A wave that finishes no ray (too many rays
-   * sharing a small pool) is retried with half as many rays; the rest of the
-   * pending list is carried over unchanged. */
+   * and the pool recycled.  A large wave that fits the pool is split into a
+   * batch of the rays predicted longest and a batch of the rest, run
+   * concurrently on two streams, each longest first: the long rays' walks,
+   * whose step latency bounds the kernels, start at once, and the short
+   * rays' coefficient and transfer work fills the SMs meanwhile.  A wave
+   * that finishes no ray (too many rays sharing a small pool) is retried
+   * unsplit with half as many rays; the rest of the pending list is carried
+   * over unchanged. */
   const int32_t *list = NULL; /* identity on the first wave */
   size_t pending = n, wave = n;
-  int cur = 0;
-  float gms = 0.f, cms = 0.f, tms = 0.f;
+  int cur = 0, split_ok = ctx->split;
   while (pending > 0) {
     size_t run = pending < wave ? pending : wave;
     size_t carry = pending - run;
-    CK(cudaMemsetAsync(ctx->d_cnt, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
-    if (carry) {
-      /* pending rays beyond this wave go first into the next list */
-      if (list) {
-        CK(cudaMemcpyAsync(ctx->d_list[cur ^ 1], list + run, carry * sizeof(int32_t), cudaMemcpyDeviceToDevice,
-                           ctx->stream));
-      } else {
-        std::vector<int32_t> ids(carry);
-        for (size_t q = 0; q < carry; q++) ids[q] = (int32_t)(run + q);
-        CK(cudaMemcpyAsync(ctx->d_list[cur ^ 1], ids.data(), carry * sizeof(int32_t), cudaMemcpyHostToDevice,
-                           ctx->stream));
+    int32_t *next = ctx->d_list[cur ^ 1];
+    size_t n_long = 0, deferred = 0;
+    double share = 0.;
+    if (split_ok && carry == 0 && run >= SPLIT_MIN_RAYS) {
+      rc = plan_split(ctx, d_ij, list, run, cam, &n_long, &share);
+      if (rc) return rc;
+      if (!n_long) split_ok = 0; /* later waves are this wave's leftovers */
+    }
+    if (n_long) {
+      ctx->stats.launches += 4;
+      /* pool shares: the predicted share of steps, with a margin for the
+       * long batch (its rays are the hardest to predict) */
+      double f = share * 1.15 + 0.01;
+      if (f > 0.9) f = 0.9;
+      long long nc0 = (long long)(f * (double)ctx->n_chunks);
+      if (nc0 < 16) nc0 = 16;
+      if (nc0 > ctx->n_chunks - 16) nc0 = ctx->n_chunks - 16;
+      size_t off = (size_t)nc0 * IPG_CHUNK_STEPS * IPG_STEP_DOUBLES;
+      Batch bt[2] = {
+          {ctx->d_sorted, n_long, ctx->d_pool, ctx->d_chunk_prev, ctx->d_chunk_meta, nc0, ctx->d_cnt + CNT_N, next,
+           ctx->bstream[0], ctx->bev[0]},
+          {ctx->d_sorted + n_long, run - n_long, ctx->d_pool + off, ctx->d_chunk_prev + nc0, ctx->d_chunk_meta + nc0,
+           ctx->n_chunks - nc0, ctx->d_cnt + 2 * CNT_N, next + n_long, ctx->bstream[1], ctx->bev[1]}};
+      CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+      for (int b = 0; b < 2; b++) {
+        CK(cudaStreamWaitEvent(bt[b].stream, ctx->ev_fork, 0));
+        CK(cudaMemsetAsync(bt[b].cnt, 0, sizeof(unsigned long long) * CNT_N, bt[b].stream));
+        rc = launch_batch(ctx, bt[b], d_ij, d_out);
+        if (rc) return rc;
+        CK(cudaEventRecord(ctx->ev_join[b], bt[b].stream));
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join[b], 0));
+      }
+      unsigned long long cnt[2 * CNT_N];
+      CK(cudaMemcpyAsync(cnt, ctx->d_cnt + CNT_N, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      float pms = 0.f, wms = 0.f;
+      cudaEventElapsedTime(&pms, ctx->ev_pred[0], ctx->ev_pred[1]);
+      ctx->stats.predict_ms += pms;
+      cudaEventElapsedTime(&wms, ctx->ev_fork, ctx->ev_join[1]);
+      float w0 = 0.f;
+      cudaEventElapsedTime(&w0, ctx->ev_fork, ctx->ev_join[0]);
+      ctx->stats.wall_ms += (wms > w0 ? wms : w0) + pms;
+      for (int b = 0; b < 2; b++) add_batch_stats(ctx, bt[b].ev, cnt + b * CNT_N);
+      ctx->stats.waves += 1;
+      size_t d0 = (size_t)cnt[CNT_DEFER], d1 = (size_t)cnt[CNT_N + CNT_DEFER];
+      if (d1 && d0 != n_long) {
+        /* close the gap between the two batches' deferred rays */
+        CK(cudaMemcpyAsync(ctx->d_pred, next + n_long, d1 * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(next + d0, ctx->d_pred, d1 * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+      }
+      deferred = d0 + d1;
+      if (deferred == pending) split_ok = 0;
+    } else {
+      unsigned long long *cnt_d = ctx->d_cnt;
+      CK(cudaMemsetAsync(cnt_d, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
+      if (carry) {
+        /* pending rays beyond this wave go first into the next list */
+        if (list) {
+          CK(cudaMemcpyAsync(next, list + run, carry * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+        } else {
+          std::vector<int32_t> ids(carry);
+          for (size_t q = 0; q < carry; q++) ids[q] = (int32_t)(run + q);
+          CK(cudaMemcpyAsync(next, ids.data(), carry * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+          CK(cudaStreamSynchronize(ctx->stream));
+        }
+        unsigned long long c0 = carry;
+        CK(cudaMemcpyAsync(cnt_d + CNT_DEFER, &c0, sizeof(c0), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
       }
-      unsigned long long c0 = carry;
-      CK(cudaMemcpyAsync(ctx->d_cnt + CNT_DEFER, &c0, sizeof(c0), cudaMemcpyHostToDevice, ctx->stream));
+      Batch bt = {list, run, ctx->d_pool, ctx->d_chunk_prev, ctx->d_chunk_meta, ctx->n_chunks, cnt_d, next,
+                  ctx->stream, ctx->ev};
+      rc = launch_batch(ctx, bt, d_ij, d_out);
+      if (rc) return rc;
+      unsigned long long cnt[CNT_N];
+      CK(cudaMemcpyAsync(cnt, cnt_d, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
-    }
-    int gb = grid_blocks(ctx, (const void *)k_geodesic, threads, run);
-    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    k_geodesic<<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, ctx->d_pool, ctx->d_chunk_prev,
-                                                 ctx->d_chunk_meta, ctx->n_chunks, ctx->d_cnt, ctx->d_rays,
-                                                 ctx->d_list[cur ^ 1]);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    int cb = grid_blocks(ctx, (const void *)k_coeffs, threads, (size_t)ctx->n_chunks * IPG_CHUNK_STEPS);
-    k_coeffs<<<cb, threads, 0, ctx->stream>>>(ctx->d_pool, ctx->d_chunk_meta, ctx->d_cnt, ctx->n_chunks,
-                                               ctx->d_rays, ctx->d_fields);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    int tb = grid_blocks(ctx, (const void *)k_transfer, threads, run);
-    k_transfer<<<tb, threads, 0, ctx->stream>>>(list, (int)run, ctx->d_pool, ctx->d_chunk_prev, ctx->d_rays, d_out,
-                                                 ctx->d_cnt);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
-    unsigned long long cnt[CNT_N];
-    CK(cudaMemcpyAsync(cnt, ctx->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    float a = 0, b = 0, c = 0;
-    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
-    cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
-    cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
-    gms += a;
-    cms += b;
-    tms += c;
-    ctx->stats.ray_steps += cnt[CNT_STEPS];
-    ctx->stats.radiating_steps += cnt[CNT_RAD];
-    ctx->stats.launches += 3;
-    ctx->stats.waves += 1;
-    size_t deferred = (size_t)cnt[CNT_DEFER];
-    if (deferred == pending) {
-      if (run == 1) {
-        snprintf(ctx->err, sizeof(ctx->err), "trajectory pool (%lld chunks) too small for a single ray",
-                 (long long)ctx->n_chunks);
-        return IPG_E_NOMEM;
+      float wms = 0.f;
+      cudaEventElapsedTime(&wms, ctx->ev[0], ctx->ev[3]);
+      ctx->stats.wall_ms += wms;
+      add_batch_stats(ctx, ctx->ev, cnt);
+      ctx->stats.waves += 1;
+      deferred = (size_t)cnt[CNT_DEFER];
+      if (deferred == pending) {
+        if (run == 1) {
+          snprintf(ctx->err, sizeof(ctx->err), "trajectory pool (%lld chunks) too small for a single ray",
+                   (long long)ctx->n_chunks);
+          return IPG_E_NOMEM;
+        }
+        wave = run / 2;
       }
-      wave = run / 2;
     }
     pending = deferred;
     cur ^= 1;
     list = ctx->d_list[cur];
   }
-  ctx->stats.geodesic_ms = gms;
-  ctx->stats.coeffs_ms = cms;
-  ctx->stats.transfer_ms = tms;
   return IPG_OK;
 }
 
