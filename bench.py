@@ -42,9 +42,12 @@ M_UNIT = 7.5e27
 BASE_ARGS = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
              "--fov=160", "--trat_large=160", "--trat_small=1"]
 CPU_SAMPLE = 64  # reference / oracle sample image size (pixels per side)
-# Executed FP64 flops per ray-step of each kernel (2 per DFMA, 1 per DADD/DMUL),
-# from ncu instruction counts on the small case (profiles/fp64_flops_per_step.md).
-FLOPS_PER_STEP = {"geodesic": None, "coeffs": None, "transfer": None}
+# Work per ray-step of each kernel, from the ncu capture of the small case
+# (profiles/kernels_small_200x200_iharm128.md): FP64 flops (2 per DFMA, 1 per
+# DADD/DMUL) and DRAM bytes read + written.  k_coeffs works per step record
+# (ray-steps + one camera record per ray).
+FLOPS_PER_STEP = {"geodesic": 2275, "coeffs": 2051, "transfer": 1033}
+DRAM_BYTES_PER_STEP = {"geodesic": 377, "coeffs": 415, "transfer": 546}
 
 
 def data_dir():
@@ -247,6 +250,7 @@ def run_ours(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     steps = rad = launches = 0
     kms = {"geodesic": 0.0, "coeffs": 0.0, "transfer": 0.0}
+    pred_ms = wall_ms = 0.0
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
@@ -257,6 +261,8 @@ def run_ours(args):
         launches += s["launches"]
         for k in kms:
             kms[k] += s[f"{k}_ms"]
+        pred_ms += s["predict_ms"]
+        wall_ms += s["wall_ms"]
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
@@ -273,6 +279,7 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"quick": True, "value": value, "ms_per_step": ms_max / args.steps,
                               **{f"{k}_ms": v / args.steps for k, v in kms.items()},
+                              "predict_ms": pred_ms / args.steps, "device_wall_ms": wall_ms / args.steps,
                               "ray_steps_per_image": steps / args.steps, "Ftot_Jy": ftot, "clocks": clk,
                               "lib": os.environ.get("IPOLE_B200_LIB", "default")}))
         ctx.close()
@@ -296,12 +303,20 @@ def run_ours(args):
     dom = max(kms, key=kms.get)
     fps = FLOPS_PER_STEP[dom]
     achieved = (fps * steps / (kms[dom] / 1e3) / 1e12) if fps else None
+    # batches (launches of each kernel) per image: two when the wave was split
+    launches_dom = max(1, round(launches / args.steps / 3)) if pred_ms == 0 else 2
+    traffic = DRAM_BYTES_PER_STEP[dom] * (steps / args.steps) / launches_dom
     roofline = {"bound": "fp64", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "traffic_note": "DRAM bytes per launch: ncu bytes per ray-step of the 200x200 small case "
+                                "times this image's ray-steps per launch",
+                "hbm_GBps_of_dominant": DRAM_BYTES_PER_STEP[dom] * steps / (kms[dom] / 1e3) / 1e9,
                 "peak_source": "measured in this run: FP64 FMA loop (ipg_measure_fp64_peak); MEASURED_PEAKS.json "
                                "has no FP64 figure",
                 "flops_per_ray_step": fps, "kernel_ms_per_image": kms[dom] / args.steps,
-                **{f"{k}_ms_per_image": v / args.steps for k, v in kms.items()}}
+                **{f"{k}_ms_per_image": v / args.steps for k, v in kms.items()},
+                "predict_ms_per_image": pred_ms / args.steps,
+                "note": "per-kernel times are summed over the two concurrent batches of an image"}
     line = {"metric": METRIC, "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
