@@ -522,11 +522,22 @@ __device__ __forceinline__ void hn_stokes(const HermN &n, const double e1[4], co
 /* --------------------------------------------------------------------- */
 #include "ipg_bessel_coeffs.h"
 
+/* Rolled loops keep the code of k_coeffs small (its straight-line code
+ * otherwise outgrows the instruction cache). */
+#ifndef IPG_ROLL_POLY
+#define IPG_ROLL_POLY 1
+#endif
+#if IPG_ROLL_POLY
+#define IPG_POLY_LOOP _Pragma("unroll 1")
+#else
+#define IPG_POLY_LOOP _Pragma("unroll")
+#endif
+
 template <int N>
 __device__ __forceinline__ double horner(const double (&c)[N], double y)
 {
   double r = c[N - 1];
-#pragma unroll
+  IPG_POLY_LOOP
   for (int k = N - 2; k >= 0; k--) r = fma(r, y, c[k]);
   return r;
 }
@@ -535,7 +546,7 @@ template <int N>
 __device__ __forceinline__ double clenshaw(const double (&c)[N], double s)
 {
   double b1 = 0., b2 = 0., s2 = 2. * s;
-#pragma unroll
+  IPG_POLY_LOOP
   for (int k = N - 1; k >= 1; k--) {
     double t = fma(s2, b1, c[k] - b2);
     b2 = b1;
@@ -687,46 +698,54 @@ struct Jar {
 
 /* Faraday rotativities rho_Q (Dexter 2016), rho_V (Shcherbakov 2008, or
  * Dexter's g(X) when dexter_v and K2 > 0), both times nu
- * (src/symphony/maxwell_juettner_fits.c:207-284) */
-__device__ __forceinline__ void rho_QV(double Ne, double nu, double Thetae, double B, double theta, double k0,
-                                       double k1, double k2, int want_q, int dexter_v, double *rQ, double *rV)
+ * (src/symphony/maxwell_juettner_fits.c:207-284).  sth, cth: sin, cos of the
+ * angle between k and B.  Regrouped for the GPU: the three powers of x share
+ * one log(x), and divisions by constants are multiplications by their
+ * reciprocals (last-bit changes only). */
+__device__ __forceinline__ void rho_QV(double Ne, double nu, double Thetae, double B, double sth, double cth,
+                                       double k0, double k1, double k2, int want_q, int dexter_v, double *rQ,
+                                       double *rV)
 {
   const double pi = 3.1415926535897932384;
-  double omega0 = IPG_EE * B / (IPG_ME * IPG_CL);
-  double wp2 = 4. * pi * Ne * (IPG_EE * IPG_EE) / IPG_ME;
-  double sth, cth;
-  sincos(theta, &sth, &cth);
-  double x = Thetae * sqrt(sqrt(2.) * sth * (1.e3 * omega0 / (2. * pi * nu)));
+  double omega0 = (IPG_EE / (IPG_ME * IPG_CL)) * B;
+  double wp2 = (4. * pi * IPG_EE * IPG_EE / IPG_ME) * Ne;
   double tpn = 2. * pi * nu;
+  double itpn = 1. / tpn;
+  double x = Thetae * sqrt(1.4142135623730951 * sth * (1.e3 * omega0 * itpn));
+  double ik2 = (k2 > 0) ? 1. / k2 : 0.;
   if (want_q) {
     double lx = log(x);
-    double e472 = exp(-x / 47.2);
-    double extraterm = (.011 * e472 - 0.011767707320949831 * pi * 1.e4 *
-                                          pow((x + 1.e-16), (-8. / 3.))) *
-                       (0.5 + 0.5 * tanh((lx - 4.78749174278204599425) / 0.1));
-    double jffunc = 2.011 * exp(-pow(x, 1.035) / 4.7) - cos(x / 2.) * exp(-pow(x, 1.2) / 2.73) - .011 * e472 + extraterm;
-    double k_ratio = (k2 > 0) ? k1 / k2 : 1;
-    double tpn2 = tpn * tpn;
-    double eps11m22 = jffunc * wp2 * (omega0 * omega0) / (tpn2 * tpn2) * (k_ratio + 6. * Thetae) * (sth * sth);
-    *rQ = tpn / (2. * IPG_CL) * eps11m22 * nu;
+    double l16 = (x + 1.e-16 == x) ? lx : log(x + 1.e-16);
+    double e472 = exp(x * (-1. / 47.2));
+    double extraterm = (.011 * e472 - 0.011767707320949831 * pi * 1.e4 * exp((-8. / 3.) * l16)) *
+                       (0.5 + 0.5 * tanh((lx - 4.78749174278204599425) * 10.));
+    double jffunc = 2.011 * exp(exp(1.035 * lx) * (-1. / 4.7)) - cos(0.5 * x) * exp(exp(1.2 * lx) * (-1. / 2.73)) -
+                    .011 * e472 + extraterm;
+    double k_ratio = (k2 > 0) ? k1 * ik2 : 1;
+    double itpn2 = itpn * itpn;
+    double eps11m22 = jffunc * wp2 * (omega0 * omega0) * (itpn2 * itpn2) * (k_ratio + 6. * Thetae) * (sth * sth);
+    *rQ = tpn * (0.5 / IPG_CL) * eps11m22 * nu;
   }
   double fit_factor;
   if (dexter_v && k2 > 0) {
     double shgmfunc = 0.43793091 * log(1. + 0.00185777 * pow(x, 1.50316886));
-    fit_factor = (k0 - shgmfunc) / k2;
+    fit_factor = (k0 - shgmfunc) * ik2;
   } else {
-    double k_ratio = (k2 > 0) ? k0 / k2 : 1;
+    double k_ratio = (k2 > 0) ? k0 * ik2 : 1;
     double shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
     fit_factor = k_ratio * shgmfunc;
   }
-  double eps12 = wp2 * omega0 / (tpn * tpn * tpn) * fit_factor * cth;
-  *rV = tpn / IPG_CL * eps12 * nu;
+  double eps12 = wp2 * omega0 * (itpn * itpn * itpn) * fit_factor * cth;
+  *rV = tpn * (1. / IPG_CL) * eps12 * nu;
 }
 
 /* Coefficients at one point for both calls the reference makes there:
  * pol = 0 (get_jkinv: Leung j_I / nu^2, Kirchhoff a_I) into (*ju, *ku) and
  * pol = 1 (jar_calc) into *jr.  src/model_radiation.c:145-332 with
- * emission_type 4 (Dexter) or 1 (Pandya); U components are zero. */
+ * emission_type 4 (Dexter) or 1 (Pandya); U components are zero.
+ * sin and cos of the k-B angle come from its cosine directly
+ * (sin = sqrt((1-mu)(1+mu)), cos = mu) instead of through acos; the angle
+ * itself is formed only where a fit needs it. */
 IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int emission_type, double *ju,
                          double *ku, Jar *jr)
 {
@@ -740,50 +759,60 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
   /* get_fluid_nu, src/radiation.c:26-44 */
   double kdu = K[0] * mp.Ucov[0] + K[1] * mp.Ucov[1] + K[2] * mp.Ucov[2] + K[3] * mp.Ucov[3];
   double nu = -kdu * IPG_ME * IPG_CL * IPG_CL / IPG_HPL;
-  double nusq = nu * nu;
+  double inusq = 1. / (nu * nu);
   /* get_bk_angle, src/radiation.c:47-72 */
-  double theta;
+  double theta = pi / 2., sth, cth;
+  int along = 0; /* theta = 0 or pi: no emission or absorption, only rho_V */
   {
     double Bm = sqrt(fabs(mp.Bcon[0] * mp.Bcov[0] + mp.Bcon[1] * mp.Bcov[1] + mp.Bcon[2] * mp.Bcov[2] +
                           mp.Bcon[3] * mp.Bcov[3]));
     if (Bm == 0.) {
-      theta = pi / 2.;
+      sth = 1.;                    /* sin(pi/2) */
+      cth = 6.123233995736766e-17; /* cos(pi/2) in double */
     } else {
       double kk = fabs(kdu);
       double mu = (K[0] * mp.Bcov[0] + K[1] * mp.Bcov[1] + K[2] * mp.Bcov[2] + K[3] * mp.Bcov[3]) / (kk * Bm);
       if (fabs(mu) > 1.) mu /= fabs(mu);
-      theta = acos(mu);
+      if (mu >= 1. || mu <= -1.) {
+        along = 1;
+        theta = (mu >= 1.) ? 0. : pi;
+        sincos(theta, &sth, &cth);
+      } else {
+        cth = mu;
+        sth = sqrt((1. - mu) * (1. + mu));
+        if (emission_type == 1) theta = acos(mu);
+      }
     }
   }
   double Thetae = mp.thetae, B = mp.bmag;
   double k0, k1, k2;
   bessel_k012(1. / Thetae, &k0, &k1, &k2);
-  if (theta <= 0.0 || theta >= pi) {
+  if (along) {
     /* only rho_V; the reference still has dexter_fit = 1 set for the Dexter
      * emission type here (src/model_radiation.c:202-207, 212-221) */
     if (want_pol) {
       double rq;
-      rho_QV(Ne, nu, Thetae, B, theta, k0, k1, k2, 0, emission_type == 4, &rq, &jr->rV);
+      rho_QV(Ne, nu, Thetae, B, sth, cth, k0, k1, k2, 0, emission_type == 4, &rq, &jr->rV);
     }
     return;
   }
-  double sth = sin(theta);
   double Bnuinv = Bnu_inv(nu, Thetae);
+  double bnu = (Bnuinv > 0) ? 1. / Bnuinv : 0.; /* Kirchhoff: a = j / B_nu-inverse */
+  const double Th2 = Thetae * Thetae;
   /* pol = 0: Leung fit, src/symphony/maxwell_juettner_fits.c:368-395 */
   {
     double K2 = fmax(k2, IPG_SMALL);
-    double nuc = IPG_EE * B / (2. * pi * IPG_ME * IPG_CL);
-    double nus = (2. / 9.) * nuc * Thetae * Thetae * sth;
+    double nus = ((2. / 9.) * IPG_EE / (2. * pi * IPG_ME * IPG_CL)) * B * Th2 * sth;
     double j = 0.;
     if (!(nu > 1.e12 * nus)) {
       double x = nu / nus;
       double cx = cbrt(x);
       double f = sqrt(x) + 1.8877486253633868 * sqrt(cx); /* 2^(11/12) x^(1/6) */
       f = f * f;
-      j = (1.4142135623730951 * pi * IPG_EE * IPG_EE * Ne * nus / (3. * IPG_CL * K2)) * f * exp(-cx);
+      j = ((1.4142135623730951 * pi * IPG_EE * IPG_EE / (3. * IPG_CL)) * Ne * nus / K2) * f * exp(-cx);
     }
-    *ju = j / nusq;
-    *ku = (Bnuinv > 0) ? *ju / Bnuinv : 0.;
+    *ju = j * inusq;
+    *ku = *ju * bnu;
   }
   if (!want_pol) return;
   /* pol = 1 */
@@ -791,7 +820,7 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
   if (emission_type == 1) {
     /* Pandya+ 2016, src/symphony/maxwell_juettner_fits.c:27-129 */
     double nu_c = IPG_EE * B / (2. * pi * IPG_ME * IPG_CL);
-    double nu_s = (2. / 9.) * nu_c * sth * Thetae * Thetae;
+    double nu_s = (2. / 9.) * nu_c * sth * Th2;
     double X = nu / nu_s;
     double prefactor = (Ne * (IPG_EE * IPG_EE) * nu_c) / IPG_CL;
     double cX = cbrt(X);
@@ -809,22 +838,24 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
     jV = prefactor * v1 * v2 * eX;
   } else {
     /* Dexter 2016, src/symphony/maxwell_juettner_fits.c:287-356 */
-    double nus = 3.0 * IPG_EE * B * sth / 4.0 / pi / IPG_ME / IPG_CL * Thetae * Thetae + 1.0;
+    double nus = (3.0 * IPG_EE / (4.0 * pi * IPG_ME * IPG_CL)) * B * sth * Th2 + 1.0;
     double x = nu / nus;
     double cx = cbrt(x), icx = 1. / cx;
+    double icx2 = icx * icx;
     double ex = exp(-1.8899 * cx);
-    double pre = Ne * IPG_EE * IPG_EE * nu / 2. / 1.7320508075688772 / IPG_CL / Thetae / Thetae;
-    double II = 2.5651 * (1 + 1.92 * icx + 0.9977 * icx * icx) * ex;
-    double IQ = 2.5651 * (1 + 0.93193 * icx + 0.499873 * icx * icx) * ex;
-    double IV = (1.81384 / x + 3.42319 * icx * icx + 0.0292545 * rsqrt(x) + 2.03773 * icx) * ex;
+    double iTh2 = 1. / Th2;
+    double pre = (IPG_EE * IPG_EE / (2. * 1.7320508075688772 * IPG_CL)) * Ne * nu * iTh2;
+    double II = 2.5651 * (1 + 1.92 * icx + 0.9977 * icx2) * ex;
+    double IQ = 2.5651 * (1 + 0.93193 * icx + 0.499873 * icx2) * ex;
+    double IV = (1.81384 * (icx2 * icx) + 3.42319 * icx2 + 0.0292545 * rsqrt(x) + 2.03773 * icx) * ex;
     jI = pre * II;
     jQ = pre * IQ;
-    jV = 2. * Ne * IPG_EE * IPG_EE * nu / tan(theta) / 3. / 1.7320508075688772 / IPG_CL / Thetae / Thetae / Thetae * IV;
+    jV = (2. * IPG_EE * IPG_EE / (3. * 1.7320508075688772 * IPG_CL)) * Ne * nu * (cth / sth) * (iTh2 / Thetae) * IV;
   }
-  jI /= nusq;
-  jQ /= nusq;
-  jV /= nusq;
-  double jU = -0. / nusq;
+  jI *= inusq;
+  jQ *= inusq;
+  jV *= inusq;
+  double jU = -0. * inusq;
   double jP = sqrt(jQ * jQ + jU * jU + jV * jV);
   if (jI < jP / 0.99) {
     double pf = jI / jP * 0.99;
@@ -836,13 +867,11 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
   jr->jQ = jQ;
   jr->jU = jU;
   jr->jV = jV;
-  if (Bnuinv > 0) {
-    jr->aI = jI / Bnuinv;
-    jr->aQ = jQ / Bnuinv;
-    jr->aU = jU / Bnuinv;
-    jr->aV = jV / Bnuinv;
-  }
-  rho_QV(Ne, nu, Thetae, B, theta, k0, k1, k2, 1, 0, &jr->rQ, &jr->rV);
+  jr->aI = jI * bnu;
+  jr->aQ = jQ * bnu;
+  jr->aU = jU * bnu;
+  jr->aV = jV * bnu;
+  rho_QV(Ne, nu, Thetae, B, sth, cth, k0, k1, k2, 1, 0, &jr->rQ, &jr->rV);
   jr->rU = 0.;
 }
 
@@ -862,27 +891,42 @@ __device__ __forceinline__ double approximate_solve(double Ii, double ji, double
   return Ii * efac + (javg / kavg) * (1. - efac);
 }
 
-/* Faraday rotation over x (src/ipolarray.c:390-408) */
-__device__ __forceinline__ void faraday(double rQ, double rU, double rV, double x, double *SQ, double *SU, double *SV)
+/* Faraday rotation over x (src/ipolarray.c:390-408 and :502-520).  evolve_N
+ * turns S by the same angle in both of its half steps, so the sines and
+ * cosines are computed once (faraday_rot) and applied twice (faraday_apply);
+ * the small-rho branch is the linear form: c = 1, f = 0, s/rho = x. */
+struct FaradayRot {
+  double c, ir, g; /* cos(rho x), sin(rho x) / rho, 2 sin^2(rho x / 2) / rho^2 */
+};
+
+__device__ __forceinline__ FaradayRot faraday_rot(double rQ, double rU, double rV, double x)
 {
-  double SQ0 = *SQ, SU0 = *SU, SV0 = *SV;
+  FaradayRot R;
   double rho2 = rQ * rQ + rU * rU + rV * rV;
   if (rho2 > IPG_CUT_PREVENT_NAN) {
     double rho = sqrt(rho2);
-    double rdS = rQ * SQ0 + rU * SU0 + rV * SV0;
     double s, c;
     sincos(rho * x, &s, &c);
     double sh = sin(0.5 * rho * x);
-    double f = 2. * rdS / rho2 * sh * sh;
-    double ir = s / rho;
-    *SQ = SQ0 * c + rQ * f + (rU * SV0 - rV * SU0) * ir;
-    *SU = SU0 * c + rU * f + (rV * SQ0 - rQ * SV0) * ir;
-    *SV = SV0 * c + rV * f + (rQ * SU0 - rU * SQ0) * ir;
+    R.c = c;
+    R.ir = s / rho;
+    R.g = 2. * sh * sh / rho2;
   } else {
-    *SQ = SQ0 + (-rV * SU0 + rU * SV0) * x;
-    *SU = SU0 + (rV * SQ0 - rQ * SV0) * x;
-    *SV = SV0 + (-rU * SQ0 + rQ * SU0) * x;
+    R.c = 1.;
+    R.ir = x;
+    R.g = 0.;
   }
+  return R;
+}
+
+__device__ __forceinline__ void faraday_apply(const FaradayRot &R, double rQ, double rU, double rV, double *SQ,
+                                              double *SU, double *SV)
+{
+  double SQ0 = *SQ, SU0 = *SU, SV0 = *SV;
+  double f = (rQ * SQ0 + rU * SU0 + rV * SV0) * R.g;
+  *SQ = SQ0 * R.c + rQ * f + (rU * SV0 - rV * SU0) * R.ir;
+  *SU = SU0 * R.c + rU * f + (rV * SQ0 - rQ * SV0) * R.ir;
+  *SV = SV0 * R.c + rV * f + (rQ * SU0 - rU * SQ0) * R.ir;
 }
 
 /* Absorption/emission full step (src/ipolarray.c:410-500) */
@@ -952,32 +996,35 @@ __device__ __forceinline__ void absorb_emit(const Jar &c, double x, double *SI, 
 /* --------------------------------------------------------------------- */
 /* Plasma tetrad (src/model_tetrads.c:35-127, src/tetrads.c:40-115)        */
 /* --------------------------------------------------------------------- */
-__device__ __forceinline__ double qform(const Met &g, const double a[4], const double b[4])
+/* Gram-Schmidt with the lowered basis vectors kept: once e_b is normalised,
+ * g e_b and e_b.g.e_b are fixed, so each projection of a vector out of e_b is
+ * a 4-term dot product instead of two metric contractions (same arithmetic
+ * as set_Econ_from_trial / project_out / normalize up to rounding order). */
+__device__ __forceinline__ double dot4(const double a[4], const double b[4])
 {
-  double gb[4];
-  lower(g, b, gb);
-  return a[0] * gb[0] + a[1] * gb[1] + a[2] * gb[2] + a[3] * gb[3];
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
 }
 
-__device__ __forceinline__ void t_normalize(const Met &g, double v[4])
+/* normalize (src/tetrads.c:82-98): v /= sqrt|v.g.v|; also returns g v and v.g.v */
+__device__ __forceinline__ void t_normalize(const Met &g, double v[4], double gv[4], double *sq)
 {
-  double n = sqrt(fabs(qform(g, v, v)));
-  double in = 1. / n;
-  v[0] *= in;
-  v[1] *= in;
-  v[2] *= in;
-  v[3] *= in;
+  lower(g, v, gv);
+  double n2 = dot4(v, gv);
+  double in = 1. / sqrt(fabs(n2));
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    v[k] *= in;
+    gv[k] *= in;
+  }
+  *sq = n2 * in * in;
 }
 
-__device__ __forceinline__ void t_project_out(const Met &g, double a[4], const double b[4])
+/* project_out (src/tetrads.c:100-115): a -= b (a.g.b)/(b.g.b), from g b and b.g.b */
+__device__ __forceinline__ void t_project_out(double a[4], const double b[4], const double gb[4], double bsq)
 {
-  double bsq = qform(g, b, b);
-  double adb = qform(g, a, b);
-  double f = adb / bsq;
-  a[0] -= b[0] * f;
-  a[1] -= b[1] * f;
-  a[2] -= b[2] * f;
-  a[3] -= b[3] * f;
+  double f = dot4(a, gb) / bsq;
+#pragma unroll
+  for (int k = 0; k < 4; k++) a[k] -= b[k] * f;
 }
 
 __device__ __forceinline__ void t_trial(double E[4], int defdir, const double t[4])
@@ -1009,26 +1056,27 @@ IPG_HEAVY int plasma_tetrad(const double Ucon[4], const double Kcon[4], const do
                              const PointGeo &pg, double Econ[4][4], double Ecov1[4], double Ecov2[4])
 {
   const double ones[4] = {1., 1., 1., 1.};
+  double g0[4], g1[4], g2[4], g3[4], s0, s1, s2, s3;
   t_trial(Econ[0], 0, Ucon);
   t_trial(Econ[1], 3, ones);
   t_trial(Econ[2], 2, Bcon);
   t_trial(Econ[3], 3, Kcon);
-  t_normalize(g, Econ[0]);
-  t_project_out(g, Econ[3], Econ[0]);
-  t_project_out(g, Econ[3], Econ[0]);
-  t_normalize(g, Econ[3]);
-  t_project_out(g, Econ[2], Econ[0]);
-  t_project_out(g, Econ[2], Econ[3]);
-  t_project_out(g, Econ[2], Econ[0]);
-  t_project_out(g, Econ[2], Econ[3]);
-  t_normalize(g, Econ[2]);
-  t_project_out(g, Econ[1], Econ[0]);
-  t_project_out(g, Econ[1], Econ[2]);
-  t_project_out(g, Econ[1], Econ[3]);
-  t_project_out(g, Econ[1], Econ[0]);
-  t_project_out(g, Econ[1], Econ[2]);
-  t_project_out(g, Econ[1], Econ[3]);
-  t_normalize(g, Econ[1]);
+  t_normalize(g, Econ[0], g0, &s0);
+  t_project_out(Econ[3], Econ[0], g0, s0);
+  t_project_out(Econ[3], Econ[0], g0, s0);
+  t_normalize(g, Econ[3], g3, &s3);
+  t_project_out(Econ[2], Econ[0], g0, s0);
+  t_project_out(Econ[2], Econ[3], g3, s3);
+  t_project_out(Econ[2], Econ[0], g0, s0);
+  t_project_out(Econ[2], Econ[3], g3, s3);
+  t_normalize(g, Econ[2], g2, &s2);
+  t_project_out(Econ[1], Econ[0], g0, s0);
+  t_project_out(Econ[1], Econ[2], g2, s2);
+  t_project_out(Econ[1], Econ[3], g3, s3);
+  t_project_out(Econ[1], Econ[0], g0, s0);
+  t_project_out(Econ[1], Econ[2], g2, s2);
+  t_project_out(Econ[1], Econ[3], g3, s3);
+  t_normalize(g, Econ[1], g1, &s1);
   /* check_handedness: sqrt|det g| * det(Econ); det g = -(rho^2 sin(th) r J22)^2 */
   const double a = c_grid.a;
   double rho2 = pg.r * pg.r + a * a * pg.cth * pg.cth;
@@ -1036,9 +1084,12 @@ IPG_HEAVY int plasma_tetrad(const double Ucon[4], const double Kcon[4], const do
   double dot = gdet * det4(Econ);
   int flag = 0;
   if (fabs(fabs(dot) - 1.) > 1.e-10) flag |= 1;
-  if (dot < 0.)
-    for (int k = 0; k < 4; k++) Econ[1][k] *= -1.;
-  lower(g, Econ[1], Ecov1);
-  lower(g, Econ[2], Ecov2);
+  double sgn = (dot < 0.) ? -1. : 1.;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    Econ[1][k] *= sgn;
+    Ecov1[k] = g1[k] * sgn;
+    Ecov2[k] = g2[k];
+  }
   return flag;
 }

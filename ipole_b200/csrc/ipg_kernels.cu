@@ -525,9 +525,10 @@ __device__ __forceinline__ int evolve_N_rec(const double *__restrict__ p, double
   double T11, T22, T12r, T21i;
   hn_stokes(*N, e1, e2, &T11, &T22, &T12r, &T21i);
   double SI = (T11 + T22) / 2, SQ = (T11 - T22) / 2, SU = T12r, SV = T21i;
-  faraday(c.rQ, c.rU, c.rV, dlam * 0.5, &SQ, &SU, &SV);
+  const FaradayRot R = faraday_rot(c.rQ, c.rU, c.rV, dlam * 0.5);
+  faraday_apply(R, c.rQ, c.rU, c.rV, &SQ, &SU, &SV);
   absorb_emit(c, dlam, &SI, &SQ, &SU, &SV);
-  faraday(c.rQ, c.rU, c.rV, dlam * 0.5, &SQ, &SU, &SV);
+  faraday_apply(R, c.rQ, c.rU, c.rV, &SQ, &SU, &SV);
   *tauF += dlam * fabs(c.rV);
   if (c_cam.stokes_floors) {
     if (SI < 0) {
@@ -1246,6 +1247,14 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
       cudaEventElapsedTime(&w0, ctx->ev_fork, ctx->ev_join[0]);
       ctx->stats.wall_ms += (wms > w0 ? wms : w0) + pms;
       for (int b = 0; b < 2; b++) add_batch_stats(ctx, bt[b].ev, cnt + b * CNT_N);
+#ifdef IPG_DEBUG_TIMING
+      for (int b = 0; b < 2; b++) {
+        float t[4];
+        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&t[i], ctx->ev_fork, bt[b].ev[i]);
+        fprintf(stderr, "batch %d rays %zu chunks %lld: geodesic %.1f-%.1f coeffs -%.1f transfer -%.1f ms\n", b,
+                bt[b].run, bt[b].n_chunks, t[0], t[1], t[2], t[3]);
+      }
+#endif
       ctx->stats.waves += 1;
       size_t d0 = (size_t)cnt[CNT_DEFER], d1 = (size_t)cnt[CNT_N + CNT_DEFER];
       if (d1 && d0 != n_long) {
