@@ -123,6 +123,9 @@ class ClockSampler:
 
 
 def dist_setup():
+    """One process per GPU under torchrun (RANK / LOCAL_RANK / WORLD_SIZE from
+    the environment).  NCCL on GPUs; IPG_DIST_BACKEND=gloo runs the same host
+    logic on CPU processes (tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -131,9 +134,19 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+        backend = os.environ.get("IPG_DIST_BACKEND", "nccl")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return rank, world, local
+
+
+def _dist_device():
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
 
 
 def barrier(world):
@@ -147,7 +160,7 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_dist_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -157,9 +170,15 @@ def sum_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_dist_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def images_per_s(world, steps, ms_max):
+    """Whole-job throughput: every rank renders one image per step (weak
+    scaling); the job takes as long as its slowest rank."""
+    return world * steps / (ms_max / 1e3)
 
 
 def cpu_reference_sample(dump, m_unit, n=CPU_SAMPLE, threads=None):
@@ -270,7 +289,7 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world)
     total_steps = sum_over_ranks(float(steps), world)
-    value = world * args.steps / (ms_max / 1e3)
+    value = images_per_s(world, args.steps, ms_max)
     out = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=ip.PIXEL_DTYPE)
     f3 = p.freqcgs ** 3
     ftot = float(out["I"].sum() * f3 * cam._scale)
@@ -296,7 +315,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
-    e2e = {"value": world * args.steps / (e2e_ms / 1e3), "unit": "images/s", "h2d_bytes_per_step": int(ij.nbytes),
+    e2e = {"value": images_per_s(world, args.steps, e2e_ms), "unit": "images/s", "h2d_bytes_per_step": int(ij.nbytes),
            "d2h_bytes_per_step": int(n * ip.PIXEL_DTYPE.itemsize), "api": "ipg_render_image (host driver)"}
 
     peak = ip.fp64_peak_tflops(local, 300.0)

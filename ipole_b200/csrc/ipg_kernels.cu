@@ -259,7 +259,7 @@ __device__ __forceinline__ void count_turns(GeoLane &L)
  * holds one copy of it, which keeps the loop body small: a lone ray's step
  * time is set by instruction-fetch and dependency latency, not by the FP64
  * throughput of the SM. */
-__global__ void __launch_bounds__(128, IPG_GEO_MINB)
+__global__ void __launch_bounds__(256, IPG_GEO_MINB)
     k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list,
                double *__restrict__ pool, int *__restrict__ chunk_prev, int2 *__restrict__ chunk_meta,
                long long n_chunks, unsigned long long *__restrict__ counters, RayRec *__restrict__ rays,
@@ -628,7 +628,7 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
   }
 }
 
-__global__ void __launch_bounds__(128, IPG_XFER_MINB)
+__global__ void __launch_bounds__(384, IPG_XFER_MINB)
     k_transfer(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
                const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays, ipg_pixel_out *__restrict__ out,
                unsigned long long *__restrict__ counters)
@@ -794,13 +794,15 @@ __global__ void k_fma_peak(double *out, int iters, double seed)
 /* ===================================================================== */
 /* context + C-ABI                                                        */
 /* ===================================================================== */
+#define NB_MAX 3 /* length classes of a split wave */
+
 struct ipg_ctx {
   int device;
   cudaStream_t stream;
   cudaEvent_t ev[4];
-  cudaStream_t bstream[2]; /* the two batches of a split wave */
-  cudaEvent_t bev[2][4];   /* per batch: geodesic, coeffs, transfer boundaries */
-  cudaEvent_t ev_fork, ev_join[2], ev_pred[2];
+  cudaStream_t bstream[NB_MAX]; /* the length classes of a split wave */
+  cudaEvent_t bev[NB_MAX][4];   /* per class: geodesic, coeffs, transfer boundaries */
+  cudaEvent_t ev_fork, ev_join[NB_MAX], ev_pred[2];
   double *d_fields;
   size_t ncell;
   int have_model;
@@ -868,14 +870,21 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   for (int i = 0; e == cudaSuccess && i < 4; i++) e = cudaEventCreate(&ctx->ev[i]);
-  for (int b = 0; e == cudaSuccess && b < 2; b++) {
-    e = cudaStreamCreateWithFlags(&ctx->bstream[b], cudaStreamNonBlocking);
+  /* the longest class gets the highest stream priority: the block scheduler
+   * then places its (SM-filling) blocks before any block of the other
+   * classes takes a slot */
+  int prio_lo = 0, prio_hi = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  for (int b = 0; e == cudaSuccess && b < NB_MAX; b++) {
+    int prio = prio_hi + b;
+    if (prio > prio_lo) prio = prio_lo;
+    e = cudaStreamCreateWithPriority(&ctx->bstream[b], cudaStreamNonBlocking, prio);
     for (int i = 0; e == cudaSuccess && i < 4; i++) e = cudaEventCreate(&ctx->bev[b][i]);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_join[b]);
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_pred[b]);
   }
+  for (int i = 0; e == cudaSuccess && i < 2; i++) e = cudaEventCreate(&ctx->ev_pred[i]);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_fork);
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_cnt, 3 * CNT_N * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_cnt, (NB_MAX + 1) * CNT_N * sizeof(unsigned long long));
   ctx->split = 1;
   if (getenv("IPG_NO_SPLIT")) ctx->split = 0;
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_len_hist, LEN_BUCKETS * sizeof(int));
@@ -906,12 +915,12 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   cudaFree(ctx->d_ij);
   cudaFree(ctx->d_out);
   for (int i = 0; i < 4; i++) cudaEventDestroy(ctx->ev[i]);
-  for (int b = 0; b < 2; b++) {
+  for (int b = 0; b < NB_MAX; b++) {
     for (int i = 0; i < 4; i++) cudaEventDestroy(ctx->bev[b][i]);
     cudaEventDestroy(ctx->ev_join[b]);
-    cudaEventDestroy(ctx->ev_pred[b]);
     cudaStreamDestroy(ctx->bstream[b]);
   }
+  for (int i = 0; i < 2; i++) cudaEventDestroy(ctx->ev_pred[i]);
   cudaEventDestroy(ctx->ev_fork);
   cudaStreamDestroy(ctx->stream);
   free(ctx);
@@ -1060,7 +1069,10 @@ static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n)
 
 /* One batch of a wave: a slice of a ray list, a slice of the trajectory pool
  * and its own counters, run as geodesic -> coefficients -> transfer on one
- * stream. */
+ * stream.  wide = 1 launches the two sequential kernels with blocks wide
+ * enough (256 and 384 threads) that their registers fill an SM: no block of
+ * another kernel fits beside them, so the rays of such a batch run at the
+ * step latency of an otherwise idle SM. */
 struct Batch {
   const int32_t *list;
   size_t run;
@@ -1072,23 +1084,25 @@ struct Batch {
   int32_t *deferred;
   cudaStream_t stream;
   cudaEvent_t *ev;
+  int wide;
 };
 
 static int launch_batch(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_pixel_out *d_out)
 {
   const int threads = 128;
+  const int tg = b.wide ? 256 : threads, tx = b.wide ? 384 : threads;
   CK(cudaEventRecord(b.ev[0], b.stream));
-  int gb = grid_blocks(ctx, (const void *)k_geodesic, threads, b.run);
-  k_geodesic<<<gb, threads, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev, b.chunk_meta, b.n_chunks,
-                                           b.cnt, ctx->d_rays, b.deferred);
+  int gb = grid_blocks(ctx, (const void *)k_geodesic, tg, b.run);
+  k_geodesic<<<gb, tg, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev, b.chunk_meta, b.n_chunks, b.cnt,
+                                      ctx->d_rays, b.deferred);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[1], b.stream));
   int cb = grid_blocks(ctx, (const void *)k_coeffs, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
   k_coeffs<<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[2], b.stream));
-  int tb = grid_blocks(ctx, (const void *)k_transfer, threads, b.run);
-  k_transfer<<<tb, threads, 0, b.stream>>>(b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);
+  int tb = grid_blocks(ctx, (const void *)k_transfer, tx, b.run);
+  k_transfer<<<tb, tx, 0, b.stream>>>(b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[3], b.stream));
   return IPG_OK;
@@ -1110,21 +1124,21 @@ static void add_batch_stats(ipg_ctx *ctx, cudaEvent_t *ev, const unsigned long l
 
 /* Length prediction and split of a wave (rays run..: the list, or the
  * identity).  Traces every ray at PRED_EPS_SCALE times the step size without
- * storing anything, sorts the rays by that step count, longest first, into
- * ctx->d_sorted, and puts the rays predicted at least PRED_LONG_FACTOR times
- * the mean into the long batch.  Returns the long batch's size in *n_long
- * and its predicted share of the steps in *share; *n_long = 0 means: do not
- * split (the wave is small, nothing is long, or the pool looks too small to
- * hold the whole wave at once). */
+ * storing anything and sorts the rays by that step count, longest first, into
+ * ctx->d_sorted.  The sorted list is cut into up to NB_MAX length classes:
+ * predicted at least PRED_VERYLONG times the mean (run wide), at least
+ * PRED_LONG times the mean, and the rest.  Returns the class sizes and
+ * predicted step shares; *nb = 0 means: do not split (the wave is small,
+ * nothing is long, or the pool looks too small to hold the wave at once). */
 #define PRED_EPS_SCALE 16.
-#define PRED_LONG_FACTOR 2.
+#define PRED_VERYLONG 4.
+#define PRED_LONG 2.
 #define SPLIT_MIN_RAYS 4096
 
 static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, size_t run, const ipg_camera *cam,
-                      size_t *n_long, double *share)
+                      int *nb, size_t sizes[NB_MAX], double shares[NB_MAX], int wide[NB_MAX])
 {
-  *n_long = 0;
-  *share = 0.;
+  *nb = 0;
   const int threads = 128;
   unsigned long long *cnt = ctx->d_cnt;
   CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
@@ -1146,26 +1160,39 @@ static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, si
   double total = 0.;
   for (int b = 0; b < LEN_BUCKETS; b++) total += (double)b * hist[b];
   if (total <= 0.) return IPG_OK;
-  double mean = total / (double)run;
-  int thr = (int)(PRED_LONG_FACTOR * mean) + 1;
-  size_t nl = 0;
-  double steps_long = 0.;
-  for (int b = LEN_BUCKETS - 1; b >= thr && b >= 0; b--) {
-    nl += (size_t)hist[b];
-    steps_long += (double)b * hist[b];
-  }
   /* the whole wave should fit: predicted steps scaled back to the real step
    * size (steps scale as 1/eps), against the pool; rays that do not fit
    * after all are deferred to the next wave like any other */
-  double need = total * PRED_EPS_SCALE;
-  if (need > (double)ctx->n_chunks * IPG_CHUNK_STEPS) return IPG_OK;
-  if (nl == 0 || nl > run / 2) return IPG_OK;
+  if (total * PRED_EPS_SCALE > (double)ctx->n_chunks * IPG_CHUNK_STEPS) return IPG_OK;
+  double mean = total / (double)run;
+  const double fac[NB_MAX - 1] = {PRED_VERYLONG, PRED_LONG};
+  int hi = LEN_BUCKETS; /* classes are bucket ranges [thr, hi) */
+  size_t used = 0;
+  int n = 0;
+  for (int c = 0; c <= NB_MAX - 1; c++) {
+    int thr = (c < NB_MAX - 1) ? (int)(fac[c] * mean) + 1 : 0;
+    if (thr > hi) thr = hi;
+    size_t cnt_c = 0;
+    double st = 0.;
+    for (int b = thr; b < hi; b++) {
+      cnt_c += (size_t)hist[b];
+      st += (double)b * hist[b];
+    }
+    hi = thr;
+    if (!cnt_c) continue;
+    sizes[n] = cnt_c;
+    shares[n] = st / total;
+    wide[n] = (c == 0);
+    used += cnt_c;
+    n++;
+  }
+  /* nothing long: no split */
+  if (n < 2 || sizes[n - 1] == run) return IPG_OK;
   k_len_scan<<<1, LEN_SCAN_THREADS, 0, ctx->stream>>>(ctx->d_len_hist);
   k_len_scatter<<<sb, 256, 0, ctx->stream>>>(list, ctx->d_pred, (int)run, 0, ctx->d_len_hist, ctx->d_sorted);
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev_pred[1], ctx->stream));
-  *n_long = nl;
-  *share = steps_long / total;
+  *nb = n;
   return IPG_OK;
 }
 
@@ -1190,14 +1217,14 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
   memset(&ctx->stats, 0, sizeof(ctx->stats));
   /* Waves: every pending ray starts; rays that find the pool full are
    * deferred to the next wave, after the finished ones have been transferred
-   * and the pool recycled.  A large wave that fits the pool is split into a
-   * batch of the rays predicted longest and a batch of the rest, run
-   * concurrently on two streams, each longest first: the long rays' walks,
-   * whose step latency bounds the kernels, start at once, and the short
-   * rays' coefficient and transfer work fills the SMs meanwhile.  A wave
-   * that finishes no ray (too many rays sharing a small pool) is retried
-   * unsplit with half as many rays; the rest of the pending list is carried
-   * over unchanged. */
+   * and the pool recycled.  A large wave that fits the pool is split into
+   * length classes by predicted step count, run concurrently on their own
+   * streams, each longest first: the long rays' walks, whose step latency
+   * bounds the sequential kernels, start at once (the longest on SMs of their
+   * own), and the short rays' coefficient and transfer work fills the other
+   * SMs meanwhile.  A wave that finishes no ray (too many rays sharing a
+   * small pool) is retried unsplit with half as many rays; the rest of the
+   * pending list is carried over unchanged. */
   const int32_t *list = NULL; /* identity on the first wave */
   size_t pending = n, wave = n;
   int cur = 0, split_ok = ctx->split;
@@ -1205,30 +1232,50 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
     size_t run = pending < wave ? pending : wave;
     size_t carry = pending - run;
     int32_t *next = ctx->d_list[cur ^ 1];
-    size_t n_long = 0, deferred = 0;
-    double share = 0.;
+    size_t deferred = 0;
+    int nb = 0;
+    size_t sizes[NB_MAX];
+    double shares[NB_MAX];
+    int wide[NB_MAX];
     if (split_ok && carry == 0 && run >= SPLIT_MIN_RAYS) {
-      rc = plan_split(ctx, d_ij, list, run, cam, &n_long, &share);
+      rc = plan_split(ctx, d_ij, list, run, cam, &nb, sizes, shares, wide);
       if (rc) return rc;
-      if (!n_long) split_ok = 0; /* later waves are this wave's leftovers */
+      if (!nb) split_ok = 0; /* later waves are this wave's leftovers */
     }
-    if (n_long) {
+    if (nb) {
       ctx->stats.launches += 4;
-      /* pool shares: the predicted share of steps, with a margin for the
-       * long batch (its rays are the hardest to predict) */
-      double f = share * 1.15 + 0.01;
-      if (f > 0.9) f = 0.9;
-      long long nc0 = (long long)(f * (double)ctx->n_chunks);
-      if (nc0 < 16) nc0 = 16;
-      if (nc0 > ctx->n_chunks - 16) nc0 = ctx->n_chunks - 16;
-      size_t off = (size_t)nc0 * IPG_CHUNK_STEPS * IPG_STEP_DOUBLES;
-      Batch bt[2] = {
-          {ctx->d_sorted, n_long, ctx->d_pool, ctx->d_chunk_prev, ctx->d_chunk_meta, nc0, ctx->d_cnt + CNT_N, next,
-           ctx->bstream[0], ctx->bev[0]},
-          {ctx->d_sorted + n_long, run - n_long, ctx->d_pool + off, ctx->d_chunk_prev + nc0, ctx->d_chunk_meta + nc0,
-           ctx->n_chunks - nc0, ctx->d_cnt + 2 * CNT_N, next + n_long, ctx->bstream[1], ctx->bev[1]}};
+      /* pool shares: the predicted share of steps with a margin for the
+       * longer classes (their rays are the hardest to predict); the last
+       * class gets the rest */
+      Batch bt[NB_MAX];
+      long long c0 = 0;
+      size_t r0 = 0;
+      for (int b = 0; b < nb; b++) {
+        long long ncb;
+        if (b < nb - 1) {
+          double f = shares[b] * 1.15 + 0.01;
+          ncb = (long long)(f * (double)ctx->n_chunks);
+          if (ncb < 16) ncb = 16;
+          if (ncb > ctx->n_chunks - c0 - 16 * (nb - 1 - b)) ncb = ctx->n_chunks - c0 - 16 * (nb - 1 - b);
+        } else {
+          ncb = ctx->n_chunks - c0;
+        }
+        bt[b].list = ctx->d_sorted + r0;
+        bt[b].run = sizes[b];
+        bt[b].pool = ctx->d_pool + (size_t)c0 * IPG_CHUNK_STEPS * IPG_STEP_DOUBLES;
+        bt[b].chunk_prev = ctx->d_chunk_prev + c0;
+        bt[b].chunk_meta = ctx->d_chunk_meta + c0;
+        bt[b].n_chunks = ncb;
+        bt[b].cnt = ctx->d_cnt + (b + 1) * CNT_N;
+        bt[b].deferred = next + r0;
+        bt[b].stream = ctx->bstream[b];
+        bt[b].ev = ctx->bev[b];
+        bt[b].wide = wide[b];
+        c0 += ncb;
+        r0 += sizes[b];
+      }
       CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
-      for (int b = 0; b < 2; b++) {
+      for (int b = 0; b < nb; b++) {
         CK(cudaStreamWaitEvent(bt[b].stream, ctx->ev_fork, 0));
         CK(cudaMemsetAsync(bt[b].cnt, 0, sizeof(unsigned long long) * CNT_N, bt[b].stream));
         rc = launch_batch(ctx, bt[b], d_ij, d_out);
@@ -1236,33 +1283,41 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
         CK(cudaEventRecord(ctx->ev_join[b], bt[b].stream));
         CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join[b], 0));
       }
-      unsigned long long cnt[2 * CNT_N];
-      CK(cudaMemcpyAsync(cnt, ctx->d_cnt + CNT_N, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+      unsigned long long cnt[NB_MAX * CNT_N];
+      CK(cudaMemcpyAsync(cnt, ctx->d_cnt + CNT_N, nb * CNT_N * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                         ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
       float pms = 0.f, wms = 0.f;
       cudaEventElapsedTime(&pms, ctx->ev_pred[0], ctx->ev_pred[1]);
       ctx->stats.predict_ms += pms;
-      cudaEventElapsedTime(&wms, ctx->ev_fork, ctx->ev_join[1]);
-      float w0 = 0.f;
-      cudaEventElapsedTime(&w0, ctx->ev_fork, ctx->ev_join[0]);
-      ctx->stats.wall_ms += (wms > w0 ? wms : w0) + pms;
-      for (int b = 0; b < 2; b++) add_batch_stats(ctx, bt[b].ev, cnt + b * CNT_N);
+      for (int b = 0; b < nb; b++) {
+        float w = 0.f;
+        cudaEventElapsedTime(&w, ctx->ev_fork, ctx->ev_join[b]);
+        if (w > wms) wms = w;
+        add_batch_stats(ctx, bt[b].ev, cnt + b * CNT_N);
+      }
+      ctx->stats.wall_ms += wms + pms;
+      ctx->stats.waves += 1;
 #ifdef IPG_DEBUG_TIMING
-      for (int b = 0; b < 2; b++) {
+      for (int b = 0; b < nb; b++) {
         float t[4];
         for (int i = 0; i < 4; i++) cudaEventElapsedTime(&t[i], ctx->ev_fork, bt[b].ev[i]);
-        fprintf(stderr, "batch %d rays %zu chunks %lld: geodesic %.1f-%.1f coeffs -%.1f transfer -%.1f ms\n", b,
-                bt[b].run, bt[b].n_chunks, t[0], t[1], t[2], t[3]);
+        fprintf(stderr, "batch %d rays %zu chunks %lld wide %d: geodesic %.1f-%.1f coeffs -%.1f transfer -%.1f ms\n", b,
+                bt[b].run, bt[b].n_chunks, bt[b].wide, t[0], t[1], t[2], t[3]);
       }
 #endif
-      ctx->stats.waves += 1;
-      size_t d0 = (size_t)cnt[CNT_DEFER], d1 = (size_t)cnt[CNT_N + CNT_DEFER];
-      if (d1 && d0 != n_long) {
-        /* close the gap between the two batches' deferred rays */
-        CK(cudaMemcpyAsync(ctx->d_pred, next + n_long, d1 * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(next + d0, ctx->d_pred, d1 * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+      /* gather the classes' deferred rays at the front of the next list */
+      size_t r = 0;
+      for (int b = 0; b < nb; b++) {
+        size_t db = (size_t)cnt[b * CNT_N + CNT_DEFER];
+        if (db && r != deferred) {
+          CK(cudaMemcpyAsync(ctx->d_pred, next + r, db * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+          CK(cudaMemcpyAsync(next + deferred, ctx->d_pred, db * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+        }
+        deferred += db;
+        r += sizes[b];
       }
-      deferred = d0 + d1;
       if (deferred == pending) split_ok = 0;
     } else {
       unsigned long long *cnt_d = ctx->d_cnt;
@@ -1282,7 +1337,7 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
         CK(cudaStreamSynchronize(ctx->stream));
       }
       Batch bt = {list, run, ctx->d_pool, ctx->d_chunk_prev, ctx->d_chunk_meta, ctx->n_chunks, cnt_d, next,
-                  ctx->stream, ctx->ev};
+                  ctx->stream, ctx->ev, 0};
       rc = launch_batch(ctx, bt, d_ij, d_out);
       if (rc) return rc;
       unsigned long long cnt[CNT_N];
