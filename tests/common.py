@@ -101,3 +101,16 @@ def image_errors(img, arrs):
         e["CP_abs"] = float(abs(cp - cpg))
         e["EVPA_deg"] = float(abs(np.degrees(ev - evg)))
     return e
+
+
+# Parity bound of the GPU tests: error <= max(base, FLOOR_FACTOR x the case's
+# reference noise floor: the largest deviation of the reference's other legal
+# builds (FMA contraction, -O2/-O3, AVX2/AVX-512) from its no-FMA build).
+BASE_TOL = dict(Ftot=1e-8, Ftot_unpol=1e-8, totQ=1e-7, totU=1e-7, totV=1e-7, pix_I_max=1e-6, pix_unpol_max=1e-6,
+                pix_QUV_over_I_max=1e-6, EVPA_deg=1e-5, LP_abs=1e-7, CP_abs=1e-7)
+FLOOR_FACTOR = 10.0
+
+
+def tolerance(meta, key):
+    floor = (meta.get("ref_noise_floor") or {}).get(key, 0.0)
+    return max(BASE_TOL[key], FLOOR_FACTOR * floor)

@@ -5,11 +5,13 @@ reference sources built with -O2 -ffp-contract=off, see oracle/Makefile) on a
 seeded synthetic iharm FMKS dump and stores its image arrays in
 tests/golden/<case>.npz together with the command-line arguments and the
 sha256 of the dump's primitives (the dump is regenerated on demand from its
-seed, so the tests check the hash before comparing).
+seed, so the tests check the hash before comparing) and the reference's own
+noise floor: how far its other legal builds (oracle/Makefile targets ref and
+noise) land from this one, per test metric.
 
     python tests/golden/make_golden.py [case ...]
 
-Needs the reference build (``make -C oracle ref``), i.e. the reference tree.
+Needs the reference builds (``make -C oracle ref noise``), i.e. the reference tree.
 """
 from __future__ import annotations
 
@@ -72,27 +74,35 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
     rec = {"unpol": img["/unpol"], "tau": img["/tau"]}
     if "/pol" in img:
         rec["pol"] = img["/pol"]
-    # the reference's own noise floor: its makefile build (FMA contraction)
-    # against this -ffp-contract=off build, in the metrics the tests use
-    floor = None
-    fma = os.path.join(os.path.dirname(binary), "ipole")
-    if os.path.exists(fma):
-        out2 = os.path.join(tmpdir, f"{case}_fma.ipgc")
-        r = subprocess.run([fma, *args[:-1], f"--outfile={out2}"], capture_output=True, text=True,
+    # the reference's own noise floor: the largest deviation from this
+    # -ffp-contract=off build among the other legal builds of the same sources
+    # (the makefile's -O3 FMA build, -O2 with FMA contraction, -O3 for
+    # AVX-512, and this build with a libm one ulp away; oracle/Makefile
+    # targets ref and noise), in the metrics the tests use
+    from tests.common import image_errors
+    floor, used = None, []
+    for other_bin in ("ipole", "ipole_o2fma", "ipole_v4", "ipole_ulp"):
+        path = os.path.join(os.path.dirname(binary), other_bin)
+        if not os.path.exists(path):
+            continue
+        out2 = os.path.join(tmpdir, f"{case}_{other_bin}.ipgc")
+        r = subprocess.run([path, *args[:-1], f"--outfile={out2}"], capture_output=True, text=True,
                            env=dict(os.environ, OMP_NUM_THREADS="8"))
-        if r.returncode == 0:
-            from tests.common import image_errors
-            other = ipgc.read(out2)
+        if r.returncode != 0:
+            continue
+        other = ipgc.read(out2)
 
-            class _Img:
-                unpol = other["/unpol"]
-                pol = other.get("/pol")
-            floor = image_errors(_Img, rec)
+        class _Img:
+            unpol = other["/unpol"]
+            pol = other.get("/pol")
+        e = image_errors(_Img, rec)
+        floor = e if floor is None else {k: max(floor[k], e[k]) for k in e}
+        used.append(other_bin)
     meta = {"case": case, "dump": dname, "dump_shape_seed": DUMPS[dname], "dump_sha256": dhash,
             "args": [*BASE, *extra], "Ftot_unpol": float(img["/Ftot_unpol"]),
             "Ftot": float(img["/Ftot"]) if "/Ftot" in img else None, "scale": float(img["/header/scale"]),
             "generator": "oracle/_ref/ipole_nofma (reference sources, -O2 -ffp-contract=off)",
-            "fma_floor": floor}
+            "ref_noise_floor": floor, "ref_noise_builds": used}
     np.savez_compressed(os.path.join(HERE, f"{case}.npz"), meta=json.dumps(meta), **rec)
     print(case, "Ftot", meta["Ftot"], "Ftot_unpol", meta["Ftot_unpol"])
 

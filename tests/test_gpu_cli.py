@@ -38,7 +38,7 @@ def test_cli_image_and_schema(dumps, tmp_path):
         assert k in img, k
     assert img["/pol"].shape == (24, 24, 5) and img["/header/evpa_0"] == "W"
     np.testing.assert_allclose(img["/pol"][..., 0], arrs["pol"][..., 0], rtol=2e-5)
-    assert abs(float(img["/Ftot"]) / meta["Ftot"] - 1) < 1e-8
+    assert abs(float(img["/Ftot"]) / meta["Ftot"] - 1) <= common.tolerance(meta, "Ftot")
 
 
 def test_cli_quench_unpol_and_exit_codes(dumps, tmp_path):

@@ -1,14 +1,15 @@
 """Parity of the sm_100a path with the reference (GPU tests).
 
 Golden images come from the reference binary (tests/golden/make_golden.py),
-which also records, per case, the reference's own noise floor: its makefile
-build (FMA contraction) against its -ffp-contract=off build.  The two differ
-by up to 4.7e-8 in total flux, 5e-7 (of total I) in total Q/U, 3e-6 per pixel
-in I, 1.8e-4 per pixel in Q/U/V and 2e-3 degree in EVPA on these images,
-because the finite-difference connection (src/geometry.c:91, DEL = 1e-7)
-amplifies last-bit differences of the metric by 1/(2 DEL), and the polarized
-step turns them into rotations through Faraday depths of ~1e3.  The GPU path
-(CUDA libm, FMA) sits on the same floor, so each metric must satisfy
+which also records, per case, the reference's own noise floor: how far its
+other legal builds (FMA contraction, -O2/-O3, AVX-512, and a libm one ulp
+away) land from its -ffp-contract=off build.  They differ by up to ~5e-8 in
+total flux, ~1e-6 (of total I) in total Q/U, 3e-6 per pixel in I, 1.8e-4 per
+pixel in Q/U/V and 2e-3 degree in EVPA on these images, because the
+finite-difference connection (src/geometry.c:91, DEL = 1e-7) amplifies
+last-bit differences of the metric by 1/(2 DEL), and the polarized step turns
+them into rotations through Faraday depths of ~1e3.  The GPU path (CUDA libm,
+FMA) sits on the same floor, so each metric must satisfy
 
     error <= max(base tolerance, 10 x the case's reference noise floor)
 
@@ -24,14 +25,7 @@ from tests import common
 
 pytestmark = pytest.mark.gpu
 
-BASE_TOL = dict(Ftot=1e-8, Ftot_unpol=1e-8, totQ=1e-7, totU=1e-7, totV=1e-7, pix_I_max=1e-6, pix_unpol_max=1e-6,
-                pix_QUV_over_I_max=1e-6, EVPA_deg=1e-5, LP_abs=1e-7, CP_abs=1e-7)
-FLOOR_FACTOR = 10.0
-
-
-def tolerance(meta, key):
-    floor = (meta.get("fma_floor") or {}).get(key, 0.0)
-    return max(BASE_TOL[key], FLOOR_FACTOR * floor)
+tolerance = common.tolerance
 
 
 @pytest.fixture(scope="module")
