@@ -14,7 +14,12 @@
  *     exact argument differences and short Taylor polynomials;
  *   - the connection is contracted with the wavevector before it is formed
  *     (Gamma^k_ij K^i K^j and Gamma^i_kl K^l), never stored as 64 numbers;
- *   - g^{mu nu} is the closed-form inverse of the FMKS Kerr-Schild metric;
+ *   - g^{mu nu} is the closed-form inverse of the FMKS Kerr-Schild metric,
+ *     with one division for its four reciprocals;
+ *   - divisions by grid constants are multiplications by reciprocals
+ *     computed once on the host, and the offset metrics of the connection take
+ *     1/rho^2 from the centre's by a two-term series (a lone ray's step is
+ *     latency-bound, and each FP64 division is a long dependent sequence);
  *   - the coherency tensor N is kept Hermitian (16 reals instead of 32), and
  *     evolve_N updates it by the 2x2 tetrad block that the step changes.
  */
@@ -95,6 +100,10 @@ struct DevGrid {
   double sigma_eq_factor;   /* ne factor when sigma == sigma_cut exactly */
   double L_unit;
   double dlfac;             /* L_unit * HPL / (ME CL^2), src/model_geodesics.c:94 */
+  /* reciprocals of the grid constants that divide in the hot loops
+   * (devgrid_derived): 1/poly_xt, 1/(poly_alpha+1),
+   * 2 poly_alpha poly_norm / ((1+poly_alpha) poly_xt), 1/dlfac */
+  double inv_xt, inv_ap1, j22c, inv_dlfac;
   long long sj, si;         /* cell strides (k fastest) */
 };
 
@@ -118,11 +127,13 @@ __constant__ DevCam c_cam;
 /* --------------------------------------------------------------------- */
 /* small helpers                                                           */
 /* --------------------------------------------------------------------- */
+/* q^n for 0 <= n < 128 by binary powering, without branches */
 __device__ __forceinline__ double ipow_int(double q, int n)
 {
   double r = 1.0, b = q;
-  while (n > 0) {
-    if (n & 1) r *= b;
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    r *= (n & 1) ? b : 1.0;
     b *= b;
     n >>= 1;
   }
@@ -163,7 +174,7 @@ __device__ __forceinline__ void x2_parts_from(double X2, double S2, double C2, X
   o->S2 = S2;
   o->C2 = C2;
   o->y = 2. * X2 - 1.;
-  double q = o->y / G.poly_xt;
+  double q = o->y * G.inv_xt;
   o->P1 = fmks_pow_am1(q);
   o->P = o->P1 * q;
 }
@@ -174,14 +185,14 @@ __device__ __forceinline__ void theta_jac(double X2, double E, const X2P &p, dou
 {
   const DevGrid &G = c_grid;
   const double omh = 1. - G.hslope;
-  double poly = 1. + p.P / (G.poly_alpha + 1.);
+  double poly = 1. + p.P * G.inv_ap1;
   double thG = IPG_PI * X2 + (omh * 0.5) * p.S2;
   double thJ = G.poly_norm * p.y * poly + 0.5 * IPG_PI;
   *th = thG + E * (thJ - thG);
   *J21 = -E * G.mks_smooth * (IPG_PI * 0.5 - IPG_PI * X2 + G.poly_norm * p.y * poly - 0.5 * omh * p.S2);
   *J22 = IPG_PI + omh * IPG_PI * p.C2 +
          E * (-IPG_PI + 2. * G.poly_norm * poly +
-              (2. * G.poly_alpha * G.poly_norm * p.y * p.P1) / ((1. + G.poly_alpha) * G.poly_xt) - omh * IPG_PI * p.C2);
+              G.j22c * p.y * p.P1 - omh * IPG_PI * p.C2);
 }
 
 /* g_{mu nu} of FMKS at (r, theta) with Jacobian J21, J22 (J11 = r) */
@@ -205,23 +216,59 @@ __device__ __forceinline__ Met met_from(double r, double sth, double cth, double
   return m;
 }
 
+/* met_from at a point a finite-difference offset away from a centre where
+ * rho^2 = rho2c and 1/rho^2 = irho2c are known: 1/rho^2 from the centre's by
+ * 1/(1+e) = 1 - e(1 - e), e ~ 1e-7 (the e^3 term is below rounding), which
+ * saves the division of each offset metric. */
+__device__ __forceinline__ Met met_from_near(double r, double sth, double cth, double J21, double J22, double rho2c,
+                                             double irho2c)
+{
+  const double a = c_grid.a;
+  double s2 = sth * sth;
+  double rho2 = r * r + a * a * cth * cth;
+  double e = (rho2 - rho2c) * irho2c;
+  double t = 2. * r * (irho2c * (1. - e * (1. - e)));
+  double G00 = -1. + t, G01 = t, G03 = -a * s2 * t, G11 = 1. + t, G13 = -a * s2 * (1. + t);
+  double G22 = rho2, G33 = s2 * (rho2 + a * a * s2 * (1. + t));
+  Met m;
+  m.g00 = G00;
+  m.g01 = G01 * r;
+  m.g03 = G03;
+  m.g11 = G11 * r * r + G22 * J21 * J21;
+  m.g12 = G22 * J21 * J22;
+  m.g13 = G13 * r;
+  m.g22 = G22 * J22 * J22;
+  m.g33 = G33;
+  return m;
+}
+
 /* Closed-form g^{mu nu} of FMKS Kerr-Schild (the reference inverts gcov by LU,
  * src/geometry.c:54-64, 252-287; both agree to rounding). */
 struct Gcon {
   double u00, u01, u02, u11, u12, u13, u22, u23, u33;  /* g^03 = 0 */
 };
 
-__device__ __forceinline__ Gcon gcon_from(double r, double sth, double cth, double J21, double J22)
+__device__ __forceinline__ Gcon gcon_from(double r, double sth, double cth, double J21, double J22,
+                                          double *rho2_out = nullptr, double *irho2_out = nullptr)
 {
   const double a = c_grid.a;
   double s2 = sth * sth;
   double rho2 = r * r + a * a * cth * cth;
-  double irho2 = 1. / rho2;
-  double ir = 1. / r;
-  double iJ22 = 1. / J22;
+  /* one division for the four reciprocals */
+  double rJ = r * J22;
+  double p2 = rho2 * rJ;
+  double inv = 1. / (p2 * s2);
+  double irho2 = inv * rJ * s2;
+  double ir = inv * rho2 * J22 * s2;
+  double iJ22 = inv * rho2 * r * s2;
+  double is2 = inv * p2;
+  if (rho2_out) {
+    *rho2_out = rho2;
+    *irho2_out = irho2;
+  }
   double Delta = r * r - 2. * r + a * a;
   double Gtt = -(1. + 2. * r * irho2), Gtr = 2. * r * irho2, Grr = Delta * irho2, Grp = a * irho2;
-  double Gthth = irho2, Gpp = irho2 / s2;
+  double Gthth = irho2, Gpp = irho2 * is2;
   double M21 = -J21 * ir * iJ22; /* dX2/dr */
   Gcon u;
   u.u00 = Gtt;
@@ -313,7 +360,8 @@ IPG_HEAVY void fd_connection(double X1, double X2, Conn *cn)
   theta_jac(X2, E, p0, &th0, &J21, &J22);
   double s0, c0;
   sincos(th0, &s0, &c0);
-  cn->gu = gcon_from(r, s0, c0, J21, J22);
+  double rho2c, irho2c;
+  cn->gu = gcon_from(r, s0, c0, J21, J22, &rho2c, &irho2c);
   cn->r = r;
 
   /* X1 +- DEL: r and E by exact offsets, theta by its exact difference */
@@ -332,8 +380,8 @@ IPG_HEAVY void fd_connection(double X1, double X2, Conn *cn)
     sincos_small(thl - th0, &sd, &cd);
     sl = s0 * cd + c0 * sd;
     cl = c0 * cd - s0 * sd;
-    Met gh = met_from(rh, sh, ch, J21h, J22h);
-    Met gl = met_from(rl, sl, cl, J21l, J22l);
+    Met gh = met_from_near(rh, sh, ch, J21h, J22h, rho2c, irho2c);
+    Met gl = met_from_near(rl, sl, cl, J21l, J22l, rho2c, irho2c);
     cn->D1 = met_diff(gh, gl, 1. / (Xh - Xl));
   }
   /* X2 +- DEL */
@@ -356,8 +404,8 @@ IPG_HEAVY void fd_connection(double X1, double X2, Conn *cn)
     sincos_small(thl - th0, &sd, &cd);
     sl = s0 * cd + c0 * sd;
     cl = c0 * cd - s0 * sd;
-    Met gh = met_from(r, sh, ch, J21h, J22h);
-    Met gl = met_from(r, sl, cl, J21l, J22l);
+    Met gh = met_from_near(r, sh, ch, J21h, J22h, rho2c, irho2c);
+    Met gl = met_from_near(r, sl, cl, J21l, J22l, rho2c, irho2c);
     cn->D2 = met_diff(gh, gl, 1. / (Xh - Xl));
   }
 }
@@ -905,12 +953,13 @@ __device__ __forceinline__ FaradayRot faraday_rot(double rQ, double rU, double r
   double rho2 = rQ * rQ + rU * rU + rV * rV;
   if (rho2 > IPG_CUT_PREVENT_NAN) {
     double rho = sqrt(rho2);
+    double irho = 1. / rho;
     double s, c;
     sincos(rho * x, &s, &c);
     double sh = sin(0.5 * rho * x);
     R.c = c;
-    R.ir = s / rho;
-    R.g = 2. * sh * sh / rho2;
+    R.ir = s * irho;
+    R.g = 2. * sh * sh * (irho * irho);
   } else {
     R.c = 1.;
     R.ir = x;
@@ -944,8 +993,9 @@ __device__ __forceinline__ void absorb_emit(const Jar &c, double x, double *SI, 
     double efacm = exp(-tauI + tauP);
     double efacp = exp(-tauI - tauP);
     double efac = exp(-tauI);
-    double i2aP = 1. / (2. * aP), i2aP2 = 1. / (2. * aP2), iaP2 = 1. / aP2;
-    double SI2 = efacm * (SI1 / 2. - ads0 * i2aP) + efacp * (SI1 / 2. + ads0 * i2aP);
+    /* four divisions in all: 1/aP2, 1/aI, 1/(aI - aP), 1/(aI + aP) */
+    double iaP2 = 1. / aP2, i2aP2 = 0.5 * iaP2, i2aP = aP * i2aP2;
+    double SI2 = efacm * (0.5 * SI1 - ads0 * i2aP) + efacp * (0.5 * SI1 + ads0 * i2aP);
     double cm = (-SI1 * aP + ads0) * i2aP2, cp = (SI1 * aP + ads0) * i2aP2;
     double SQ2 = efacm * aQ * cm + efacp * aQ * cp + efac * (SQ1 - ads0 * aQ * iaP2);
     double SU2 = efacm * aU * cm + efacp * aU * cp + efac * (SU1 - ads0 * aU * iaP2);
@@ -953,29 +1003,30 @@ __device__ __forceinline__ void absorb_emit(const Jar &c, double x, double *SI, 
     double afacm = 1. - efacm, afac = 1. - efac, afacp = 1. - efacp;
     if (tauI - tauP <= IPG_CUT_SMALL_TAU) {
       double e = tauI - tauP;
-      afacm = e * (1. - (e / 2.) * (1. - e / 3.));
+      afacm = e * (1. - (0.5 * e) * (1. - e * (1. / 3.)));
       if (tauI <= IPG_CUT_SMALL_TAU) {
         e = tauI;
-        afac = e * (1. - (e / 2.) * (1. - e / 3.));
+        afac = e * (1. - (0.5 * e) * (1. - e * (1. / 3.)));
         if (tauI + tauP <= IPG_CUT_SMALL_TAU) {
           e = tauI + tauP;
-          afacp = e * (1. - (e / 2.) * (1. - e / 3.));
+          afacp = e * (1. - (0.5 * e) * (1. - e * (1. / 3.)));
         }
       }
     }
     double iaI = 1. / aI;
-    double adjP = adj / (aI * aP2);
+    double adjP = adj * iaI * iaP2;
     SQ2 += afac * (jQ * iaI - aQ * adjP);
     SU2 += afac * (jU * iaI - aU * adjP);
     SV2 += afac * (jV * iaI - aV * adjP);
-    double m1 = (aP * jI - adj) / (2. * aP * (aI - aP));
-    double m2 = (-aP * jI + adj) / (2. * aP2 * (aI - aP));
+    double iam = 1. / (aI - aP), iap = 1. / (aI + aP);
+    double m1 = (aP * jI - adj) * i2aP * iam;
+    double m2 = (-aP * jI + adj) * i2aP2 * iam;
     SI2 += afacm * m1;
     SQ2 += afacm * aQ * m2;
     SU2 += afacm * aU * m2;
     SV2 += afacm * aV * m2;
-    double p1 = (aP * jI + adj) / (2. * aP * (aI + aP));
-    double p2 = (aP * jI + adj) / (2. * aP2 * (aI + aP));
+    double p1 = (aP * jI + adj) * i2aP * iap;
+    double p2 = (aP * jI + adj) * i2aP2 * iap;
     SI2 += afacp * p1;
     SQ2 += afacp * aQ * p2;
     SU2 += afacp * aU * p2;

@@ -678,8 +678,8 @@ __global__ void __launch_bounds__(384, IPG_XFER_MINB)
     double dl = L.rec_i[REC_DL];
     if (!unpol) {
       /* push_polar twice, src/ipolarray.c:85-89 */
-      double dlfull = dl / G.dlfac;
-      double dlhalf = (0.5 * dl) / G.dlfac;
+      double dlfull = dl * G.inv_dlfac;
+      double dlhalf = (0.5 * dl) * G.inv_dlfac;
       double A[4][4];
       HermN Nh, Nn;
       load_A(L.rec_i + REC_A1, A);
@@ -794,6 +794,15 @@ __global__ void k_fma_peak(double *out, int iters, double seed)
 /* ===================================================================== */
 /* context + C-ABI                                                        */
 /* ===================================================================== */
+/* reciprocals of grid constants used as divisors in the kernels */
+static void devgrid_derived(DevGrid *d)
+{
+  d->inv_xt = 1. / d->poly_xt;
+  d->inv_ap1 = 1. / (d->poly_alpha + 1.);
+  d->j22c = (2. * d->poly_alpha * d->poly_norm) / ((1. + d->poly_alpha) * d->poly_xt);
+  d->inv_dlfac = 1. / d->dlfac;
+}
+
 #define NB_MAX 3 /* length classes of a split wave */
 
 struct ipg_ctx {
@@ -976,6 +985,7 @@ extern "C" int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *g, const double *c
   d.si = (long long)(g->n2 + 2) * (g->n3 + 2);
   double am1 = g->poly_alpha - 1.;
   d.alpha_int = (am1 >= 0 && am1 <= 64 && am1 == (double)(int)am1) ? (int)am1 : -1;
+  devgrid_derived(&d);
   ctx->have_model = 1;
   return IPG_OK;
 }
@@ -1594,6 +1604,7 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
   d.si = (long long)(g->n2 + 2) * (g->n3 + 2);
   double am1 = g->poly_alpha - 1.;
   d.alpha_int = (am1 >= 0 && am1 <= 64 && am1 == (double)(int)am1) ? (int)am1 : -1;
+  devgrid_derived(&d);
   DevCam dc;
   make_devcam(cam, &dc);
   NA_CK(cudaMemcpyToSymbolAsync(c_grid, &d, sizeof(DevGrid), 0, cudaMemcpyHostToDevice, stream));
