@@ -102,8 +102,9 @@ struct DevGrid {
   double dlfac;             /* L_unit * HPL / (ME CL^2), src/model_geodesics.c:94 */
   /* reciprocals of the grid constants that divide in the hot loops
    * (devgrid_derived): 1/poly_xt, 1/(poly_alpha+1),
-   * 2 poly_alpha poly_norm / ((1+poly_alpha) poly_xt), 1/dlfac */
-  double inv_xt, inv_ap1, j22c, inv_dlfac;
+   * 2 poly_alpha poly_norm / ((1+poly_alpha) poly_xt), 1/dlfac,
+   * 1/(cstopx2 - cstartx2) */
+  double inv_xt, inv_ap1, j22c, inv_dlfac, inv_lx2;
   long long sj, si;         /* cell strides (k fastest) */
 };
 

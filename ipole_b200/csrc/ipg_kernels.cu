@@ -52,23 +52,24 @@ enum { CNT_POOL = 0, CNT_STEPS = 1, CNT_RAD = 2, CNT_DEFER = 3, CNT_NEXT_G = 4, 
 /* helpers                                                                */
 /* ===================================================================== */
 
-/* src/model_geodesics.c:267-293 */
+/* src/model_geodesics.c:267-293.  The reference forms three step limits
+ * dlx_i = eps c_i / (|K^i| + SS) and returns 1 / sum 1/(|dlx_i| + SS); with
+ * a_i = |K^i| + SS and b_i = eps c_i that is
+ * dl = eps b1 b2 / (eps (a1 b2 + a2 b1) + a3 b1 b2), one division instead of
+ * nine (the + SS of the inner reciprocals matters only for steps near 1e-80,
+ * i.e. a ray sitting exactly on the inner or polar boundary). */
 __device__ __forceinline__ double stepsize(const double X[4], const double K[4], double eps)
 {
   const DevGrid &G = c_grid;
   const double SS = IPG_SMALL * IPG_SMALL;
+  const double cut = 0.02;
   double deh = fmin(fabs(X[1] - G.cstartx[1]), 0.1);
-  double dlx1 = eps * (10 * deh) / (fabs(K[1]) + SS);
-  double cut = 0.02;
-  double lx2 = G.cstopx[2] - G.cstartx[2];
-  double dpole = fmin(fabs(X[2] / lx2), fabs((G.cstopx[2] - X[2]) / lx2));
-  double d2fac = (dpole < cut) ? dpole / 3 : fmin(cut / 3 + (dpole - cut) * 10., 1.);
-  double dlx2 = eps * d2fac / (fabs(K[2]) + SS);
-  double dlx3 = eps / (fabs(K[3]) + SS);
-  double idlx1 = 1. / (fabs(dlx1) + SS);
-  double idlx2 = 1. / (fabs(dlx2) + SS);
-  double idlx3 = 1. / (fabs(dlx3) + SS);
-  return 1. / (idlx1 + idlx2 + idlx3);
+  double dpole = fmin(fabs(X[2] * G.inv_lx2), fabs((G.cstopx[2] - X[2]) * G.inv_lx2));
+  double d2fac = (dpole < cut) ? dpole * (1. / 3.) : fmin(cut * (1. / 3.) + (dpole - cut) * 10., 1.);
+  double a1 = fabs(K[1]) + SS, a2 = fabs(K[2]) + SS, a3 = fabs(K[3]) + SS;
+  double b1 = eps * (10 * deh), b2 = eps * d2fac;
+  double b12 = b1 * b2;
+  return (eps * b12) / (eps * (a1 * b2 + a2 * b1) + a3 * b12);
 }
 
 /* theta of bl_coord (src/coordinates.c:75-81), for the sub-ring counter */
@@ -501,29 +502,63 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
 /* ===================================================================== */
 /* k_transfer                                                             */
 /* ===================================================================== */
+/* The coefficient block of one step record (k_coeffs' output), loaded with
+ * 16 two-double loads issued together: the transfer step then waits for one
+ * round trip to memory instead of two (flags first, the rest behind the
+ * radiating branch). */
+struct CoefBlock {
+  double flags, ju, ku, dl, jI, jQ, jV, aI, aQ, aV, nturns, rQ, rV;
+  double e1[4], e2[4], a[4], b[4]; /* tetrad rows 1, 2: covariant, contravariant */
+};
+
+__device__ __forceinline__ void load_coef(const double *__restrict__ p, CoefBlock &c)
+{
+  const double2 *q = reinterpret_cast<const double2 *>(p + REC_FLAGS);
+  double2 v[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) v[k] = q[k];
+  c.flags = v[0].x;
+  c.ju = v[0].y;
+  c.ku = v[1].x;
+  c.dl = v[1].y;
+  c.jI = v[2].x;
+  c.jQ = v[2].y;
+  c.jV = v[3].x;
+  c.aI = v[3].y;
+  c.aQ = v[4].x;
+  c.aV = v[4].y;
+  c.nturns = v[5].x;
+  c.rQ = v[5].y;
+  c.rV = v[6].x;
+  c.e1[0] = v[8].x; c.e1[1] = v[8].y; c.e1[2] = v[9].x; c.e1[3] = v[9].y;
+  c.e2[0] = v[10].x; c.e2[1] = v[10].y; c.e2[2] = v[11].x; c.e2[3] = v[11].y;
+  c.a[0] = v[12].x; c.a[1] = v[12].y; c.a[2] = v[13].x; c.a[3] = v[13].y;
+  c.b[0] = v[14].x; c.b[1] = v[14].y; c.b[2] = v[15].x; c.b[3] = v[15].y;
+}
+static_assert(REC_FLAGS == 32 && REC_JU == 33 && REC_KU == 34 && REC_DL == 35 && REC_JI == 36 &&
+                  REC_NTURNS == 42 && REC_RQ == 43 && REC_RV == 44 && REC_E1COV == 48 && REC_E2COV == 52 &&
+                  REC_E1CON == 56 && REC_E2CON == 60,
+              "load_coef follows the record layout");
+
 /* evolve_N (src/ipolarray.c:332-575) from a coefficient block: N to Stokes
  * in the plasma tetrad, Faraday half step, absorption/emission, Faraday half
  * step, back to N.  Returns the tauF / NaN oddflag bits. */
-__device__ __forceinline__ int evolve_N_rec(const double *__restrict__ p, double dlam, int zero_emission, HermN *N,
-                                            double *tauF)
+__device__ __forceinline__ int evolve_N_coef(const CoefBlock &cb, double dlam, int zero_emission, HermN *N,
+                                             double *tauF)
 {
-  double e1[4], e2[4], v[4];
-  load4(p + REC_E1COV, e1);
-  load4(p + REC_E2COV, e2);
   Jar c;
-  load4(p + REC_JI, v);
-  c.jI = v[0];
-  c.jQ = v[1];
-  c.jV = v[2];
-  c.aI = v[3];
-  c.aQ = p[REC_JI + 4];
-  c.aV = p[REC_JI + 5];
-  c.rQ = p[REC_RQ];
-  c.rV = p[REC_RV];
+  c.jI = cb.jI;
+  c.jQ = cb.jQ;
+  c.jV = cb.jV;
+  c.aI = cb.aI;
+  c.aQ = cb.aQ;
+  c.aV = cb.aV;
+  c.rQ = cb.rQ;
+  c.rV = cb.rV;
   c.jU = c.aU = c.rU = 0.;
   if (zero_emission) c.jI = c.jQ = c.jU = c.jV = 0.;
   double T11, T22, T12r, T21i;
-  hn_stokes(*N, e1, e2, &T11, &T22, &T12r, &T21i);
+  hn_stokes(*N, cb.e1, cb.e2, &T11, &T22, &T12r, &T21i);
   double SI = (T11 + T22) / 2, SQ = (T11 - T22) / 2, SU = T12r, SV = T21i;
   const FaradayRot R = faraday_rot(c.rQ, c.rU, c.rV, dlam * 0.5);
   faraday_apply(R, c.rQ, c.rU, c.rV, &SQ, &SU, &SV);
@@ -544,9 +579,7 @@ __device__ __forceinline__ int evolve_N_rec(const double *__restrict__ p, double
   }
   /* N += Econ^T (new block - old block) Econ (stokes_to_tensor +
    * complex_tetrad_to_coord_rank2, src/ipolarray.c:673-682, 730-748) */
-  double a[4], b[4];
-  load4(p + REC_E1CON, a);
-  load4(p + REC_E2CON, b);
+  const double *a = cb.a, *b = cb.b;
   double d11 = (SI + SQ) - T11, d22 = (SI - SQ) - T22, dr12 = SU - T12r, di21 = SV - T21i;
 #define DR(i, j) (a[i] * a[j] * d11 + b[i] * b[j] * d22 + (a[i] * b[j] + b[i] * a[j]) * dr12)
 #define DS(i, j) ((b[i] * a[j] - a[i] * b[j]) * di21)
@@ -563,9 +596,16 @@ __device__ __forceinline__ int evolve_N_rec(const double *__restrict__ p, double
   return flag;
 }
 
+/* block width of the transfer for the longest length class (its blocks fill
+ * an SM's registers) */
+#ifndef IPG_XFER_WIDE
+#define IPG_XFER_WIDE 256
+#endif
+
 struct XferLane {
   HermN N;
   const double *rec_i;
+  double dl_i, nturns_i; /* dl and nturns of rec_i */
   double I, tau, tauF, js, ks;
   int ray, n, chunk, flag, nrad;
   int cprev; /* chunk_prev[chunk], loaded on entry to the chunk */
@@ -620,6 +660,8 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
     /* get_jkinv at the far end of the ray, src/ipolarray.c:74 */
     L.js = L.rec_i[REC_JU];
     L.ks = L.rec_i[REC_KU];
+    L.dl_i = L.rec_i[REC_DL];
+    L.nturns_i = L.rec_i[REC_NTURNS];
     L.I = L.tau = L.tauF = 0.;
     hn_zero(&L.N);
     L.flag = 0;
@@ -628,7 +670,7 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
   }
 }
 
-__global__ void __launch_bounds__(384, IPG_XFER_MINB)
+__global__ void __launch_bounds__(IPG_XFER_WIDE, IPG_XFER_MINB)
     k_transfer(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
                const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays, ipg_pixel_out *__restrict__ out,
                unsigned long long *__restrict__ counters)
@@ -675,7 +717,9 @@ __global__ void __launch_bounds__(384, IPG_XFER_MINB)
       if ((s - 1) % IPG_CHUNK_STEPS != IPG_CHUNK_STEPS - 1) prefetch_rec(rec_f - IPG_STEP_DOUBLES);
       else if (L.cprev >= 0) prefetch_rec(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
     }
-    double dl = L.rec_i[REC_DL];
+    CoefBlock cb;
+    load_coef(rec_f, cb);
+    double dl = L.dl_i;
     if (!unpol) {
       /* push_polar twice, src/ipolarray.c:85-89 */
       double dlfull = dl * G.inv_dlfac;
@@ -688,22 +732,24 @@ __global__ void __launch_bounds__(384, IPG_XFER_MINB)
       hn_push(L.N, Nh, A, dlfull, &Nn);
       L.N = Nn;
     }
-    int flags = (int)rec_f[REC_FLAGS];
+    int flags = (int)cb.flags;
     if (flags & 1) {
       L.nrad++;
       int zero_emission = (flags & 2) ? 1 : 0;
-      if (C.target_nturns >= 0 && (int)L.rec_i[REC_NTURNS] != C.target_nturns) zero_emission = 1;
+      if (C.target_nturns >= 0 && (int)L.nturns_i != C.target_nturns) zero_emission = 1;
       double ji = L.js, ki = L.ks;
-      double jf = rec_f[REC_JU], kf = rec_f[REC_KU];
+      double jf = cb.ju, kf = cb.ku;
       L.js = jf;
       L.ks = kf;
       if (zero_emission) L.I = approximate_solve(L.I, 0, ki, 0, kf, dl, &L.tau);
       else L.I = approximate_solve(L.I, ji, ki, jf, kf, dl, &L.tau);
       if (!unpol) {
         L.flag |= flags >> 2;
-        L.flag |= evolve_N_rec(rec_f, dl, zero_emission, &L.N, &L.tauF);
+        L.flag |= evolve_N_coef(cb, dl, zero_emission, &L.N, &L.tauF);
       }
     }
+    L.dl_i = cb.dl;
+    L.nturns_i = cb.nturns;
     L.rec_i = rec_f;
     L.n--;
   }
@@ -801,6 +847,7 @@ static void devgrid_derived(DevGrid *d)
   d->inv_ap1 = 1. / (d->poly_alpha + 1.);
   d->j22c = (2. * d->poly_alpha * d->poly_norm) / ((1. + d->poly_alpha) * d->poly_xt);
   d->inv_dlfac = 1. / d->dlfac;
+  d->inv_lx2 = 1. / (d->cstopx[2] - d->cstartx[2]);
 }
 
 #define NB_MAX 3 /* length classes of a split wave */
@@ -1100,7 +1147,7 @@ struct Batch {
 static int launch_batch(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_pixel_out *d_out)
 {
   const int threads = 128;
-  const int tg = b.wide ? 256 : threads, tx = b.wide ? 384 : threads;
+  const int tg = b.wide ? 256 : threads, tx = b.wide ? IPG_XFER_WIDE : threads;
   CK(cudaEventRecord(b.ev[0], b.stream));
   int gb = grid_blocks(ctx, (const void *)k_geodesic, tg, b.run);
   k_geodesic<<<gb, tg, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev, b.chunk_meta, b.n_chunks, b.cnt,
