@@ -46,8 +46,8 @@ CPU_SAMPLE = 64  # reference / oracle sample image size (pixels per side)
 # (profiles/kernels_small_200x200_iharm128.md): FP64 flops (2 per DFMA, 1 per
 # DADD/DMUL) and DRAM bytes read + written.  k_coeffs works per step record
 # (ray-steps + one camera record per ray).
-FLOPS_PER_STEP = {"geodesic": 2275, "coeffs": 2051, "transfer": 1033}
-DRAM_BYTES_PER_STEP = {"geodesic": 377, "coeffs": 415, "transfer": 546}
+FLOPS_PER_STEP = {"geodesic": 1831, "coeffs": 1535, "transfer": 913}
+DRAM_BYTES_PER_STEP = {"geodesic": 377, "coeffs": 412, "transfer": 537}
 
 
 def data_dir():
@@ -322,8 +322,9 @@ def run_ours(args):
     dom = max(kms, key=kms.get)
     fps = FLOPS_PER_STEP[dom]
     achieved = (fps * steps / (kms[dom] / 1e3) / 1e12) if fps else None
-    # batches (launches of each kernel) per image: two when the wave was split
-    launches_dom = max(1, round(launches / args.steps / 3)) if pred_ms == 0 else 2
+    # launches of each main kernel per image: one per length class (a split
+    # wave adds 4 launches for the prediction and sort)
+    launches_dom = max(1, round((launches / args.steps - (4 if pred_ms > 0 else 0)) / 3))
     traffic = DRAM_BYTES_PER_STEP[dom] * (steps / args.steps) / launches_dom
     roofline = {"bound": "fp64", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
@@ -335,7 +336,7 @@ def run_ours(args):
                 "flops_per_ray_step": fps, "kernel_ms_per_image": kms[dom] / args.steps,
                 **{f"{k}_ms_per_image": v / args.steps for k, v in kms.items()},
                 "predict_ms_per_image": pred_ms / args.steps,
-                "note": "per-kernel times are summed over the two concurrent batches of an image"}
+                "note": "per-kernel times are summed over the concurrent length classes of an image"}
     line = {"metric": METRIC, "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -364,6 +365,32 @@ def run_ours(args):
     return 0
 
 
+def run_one_ray(args):
+    """One ray alone on the GPU: the geodesic and transfer kernels' device time
+    divided by its steps is the step latency of a lone lane, which bounds the
+    sequential kernels for the longest rays of an image."""
+    import numpy as np
+
+    import ipole_b200 as ip
+    os.environ["IPG_NO_SPLIT"] = "1"  # one wave, no length classes
+    spec = SMALL_DUMP if args.small else DUMP
+    dump = ensure_dump(spec)
+    extra = [f"--eps={args.eps}"] if args.eps else []
+    p = ip.Params.from_args(workload_args(dump, args.size, args.size, args.m_unit) + extra)
+    model = ip.Model.load(p)
+    i, j = (int(v) for v in args.ray.split(","))
+    with ip.Context(0, pool_bytes=int((args.pool_gb or 2.0) * (1 << 30))) as ctx:
+        ctx.upload(model)
+        cam = ip.camera_for(p, model.grid)
+        out = ctx.trace(cam, np.array([[i, j]], dtype=np.int32))
+        s = ctx.stats()
+    n = int(out["nstep"][0])
+    print(json.dumps({"ray": [i, j], "nstep": n, "geodesic_ms": s["geodesic_ms"], "transfer_ms": s["transfer_ms"],
+                      "geodesic_us_per_step": s["geodesic_ms"] * 1e3 / max(n, 1),
+                      "transfer_us_per_step": s["transfer_ms"] * 1e3 / max(n, 1)}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -377,11 +404,15 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (no e2e / CPU / peak legs)")
     ap.add_argument("--eps", type=float, default=0.0,
                     help="geodesic step parameter for profiling cases (0: the workload's 0.01)")
+    ap.add_argument("--ray", default="", help="I,J: trace this one pixel alone and report the step latency "
+                                              "of the sequential kernels (diagnostic)")
     ap.add_argument("--pool-gb", dest="pool_gb", type=float, default=0.0,
                     help="trajectory pool size in GiB (0: 60%% of free device memory)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.ray:
+        return run_one_ray(args)
     return run_ours(args)
 
 
