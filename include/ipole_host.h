@@ -83,8 +83,8 @@ typedef struct ipg_iharm_model {
   void *fluid_header;          /* copy of the dump's /header group (for /fluid_header) */
 } ipg_iharm_model;
 
-/* init_model: read the dump named in p->dump (IPGC container holding the
- * iharm v1 schema), build ghost zones and derived fields.  Returns
+/* init_model: read the dump named in p->dump (an iharm v1 HDF5 dump, or the
+ * same schema in an IPGC container), build ghost zones and derived fields.  Returns
  * IPG_E_IO / IPG_E_FORMAT on a bad dump (reference: exit(-1) / exit(-3)). */
 int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m);
 void ipg_iharm_free(ipg_iharm_model *m);
@@ -127,8 +127,20 @@ void ipg_print_image_stats(const ipg_image *img, const ipg_params *p, void *log)
 void ipg_image_totals(const ipg_image *img, const ipg_params *p, double tot[5]);
 
 /* dump() (src/io.c:229-273) with write_header (:140-191) and the iharm
- * output_hdf5 (model/iharm/model.c:1254-1301), as an IPGC container. */
+ * output_hdf5 (model/iharm/model.c:1254-1301): an HDF5 file with the
+ * reference's datasets and attributes, or an IPGC container when fname ends
+ * in ".ipgc". */
 int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p, const ipg_iharm_model *m);
+
+/* Copy a dump or image between the two file formats the library reads: HDF5
+ * (the reference's format, src/hdf5_utils.c over libhdf5; this library reads
+ * and writes the subset those files use without libhdf5) and the flat IPGC
+ * container.  The source format is detected from its signature; the
+ * destination is IPGC when its name ends in ".ipgc", HDF5 otherwise.  Returns
+ * IPG_E_IO on a missing or malformed file and IPG_E_FORMAT on HDF5 features
+ * outside the subset (dense groups, chunk indexes other than the version 1
+ * B-tree, filters other than deflate and shuffle). */
+int ipg_container_convert(const char *src, const char *dst);
 
 #ifdef __cplusplus
 }

@@ -25,7 +25,7 @@ import numpy as np
 from . import build as _build
 
 __all__ = ["lib", "Params", "Model", "Context", "Image", "Camera", "PixelOut", "Grid", "IpgError",
-           "PIXEL_DTYPE", "trace_pixels", "fp64_peak_tflops"]
+           "PIXEL_DTYPE", "trace_pixels", "fp64_peak_tflops", "convert_container"]
 
 IPG_OK, IPG_E_ARG, IPG_E_CUDA, IPG_E_MAXNSTEP, IPG_E_NAN, IPG_E_TIMEOUT, IPG_E_NOMEM, IPG_E_IO, IPG_E_STATE, \
     IPG_E_FORMAT = range(10)
@@ -178,6 +178,7 @@ def lib():
     L.ipg_print_image_stats.argtypes = [C.POINTER(_Image), C.POINTER(_Params), C.c_void_p]
     L.ipg_print_image_stats.restype = None
     L.ipg_write_image.argtypes = [C.c_char_p, C.POINTER(_Image), C.POINTER(_Params), C.POINTER(_Model)]
+    L.ipg_container_convert.argtypes = [C.c_char_p, C.c_char_p]
     _lib = L
     return L
 
@@ -420,6 +421,13 @@ def render_with(tracer, params: Params, model: Model) -> Image:
 
 def trace_pixels(ctx: Context, cam: Camera, ij) -> np.ndarray:
     return ctx.trace(cam, ij)
+
+
+def convert_container(src: str, dst: str) -> None:
+    """Copy a dump or image between HDF5 and the IPGC container
+    (``ipg_container_convert``): the source format is detected, the
+    destination is IPGC when its name ends in ``.ipgc``, HDF5 otherwise."""
+    _check(lib().ipg_container_convert(os.fsencode(src), os.fsencode(dst)))
 
 
 def fp64_peak_tflops(device: int = 0, ms: float = 200.0) -> float:

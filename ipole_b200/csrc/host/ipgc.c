@@ -3,6 +3,8 @@
  *   uint64 dims[rank], uint64 nbytes, data}. */
 #include "ipgc.h"
 
+#include "h5lite.h"
+
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -197,4 +199,35 @@ void ipgc_copy_subtree(const ipgc_file *src, const char *src_root, ipgc_file *ds
       ipgc_put(dst, q, e->kind, e->rank, e->dims, e->data, e->nbytes);
     }
   }
+}
+
+static char g_last[320];
+const char *ipgc_error(void) { return g_last; }
+
+int ipgc_load(const char *fname, ipgc_file *f)
+{
+  g_last[0] = 0;
+  if (h5l_is_hdf5(fname)) {
+    int rc = h5l_read(fname, f);
+    if (rc) snprintf(g_last, sizeof(g_last), "%s: %s", fname, h5l_error());
+    return rc;
+  }
+  int rc = ipgc_read(fname, f);
+  if (rc) snprintf(g_last, sizeof(g_last), "%s: cannot open, or neither HDF5 nor an IPGC container", fname);
+  return rc;
+}
+
+int ipgc_save(const char *fname, const ipgc_file *f)
+{
+  g_last[0] = 0;
+  size_t n = strlen(fname);
+  int rc;
+  if (n >= 5 && strcmp(fname + n - 5, ".ipgc") == 0) {
+    rc = ipgc_write(fname, f);
+    if (rc) snprintf(g_last, sizeof(g_last), "%s: write error", fname);
+  } else {
+    rc = h5l_write(fname, f);
+    if (rc) snprintf(g_last, sizeof(g_last), "%s: %s", fname, h5l_error());
+  }
+  return rc;
 }

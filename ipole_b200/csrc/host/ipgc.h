@@ -26,6 +26,14 @@ typedef struct {
 
 int ipgc_read(const char *fname, ipgc_file *f);            /* 0 ok, -1 error */
 int ipgc_write(const char *fname, const ipgc_file *f);     /* 0 ok, -1 error */
+/* either format: HDF5 (read by h5lite) when the file carries the HDF5
+ * signature, else IPGC.  0 ok, -1 error, -2 HDF5 feature outside the subset */
+int ipgc_load(const char *fname, ipgc_file *f);
+/* IPGC when the name ends in ".ipgc", HDF5 otherwise (the reference's image
+ * and dump files are HDF5).  0 ok, -1 error */
+int ipgc_save(const char *fname, const ipgc_file *f);
+/* message for the last failed ipgc_load/ipgc_save */
+const char *ipgc_error(void);
 void ipgc_free(ipgc_file *f);
 const ipgc_entry *ipgc_find(const ipgc_file *f, const char *path);
 ipgc_entry *ipgc_put(ipgc_file *f, const char *path, int kind, int rank, const uint64_t *dims,

@@ -116,9 +116,10 @@ int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m)
   char fname[IPG_STRLEN];
   snprintf(fname, sizeof(fname), p->dump, p->dump_min);
   fprintf(stderr, "Determining dump file type... ");
-  if (ipgc_read(fname, &file) != 0) {
-    fprintf(stderr, "! unable to open file %s. Exiting!\n", fname);
-    return IPG_E_IO;
+  int lrc = ipgc_load(fname, &file);
+  if (lrc != 0) {
+    fprintf(stderr, "! unable to open file %s. Exiting!\n  (%s)\n", fname, ipgc_error());
+    return lrc == -2 ? IPG_E_FORMAT : IPG_E_IO;
   }
   fprintf(stderr, "iharm!\n");
 

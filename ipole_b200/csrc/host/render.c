@@ -494,7 +494,23 @@ int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p
     ipgc_put_array_f64(&f, "/pol", 3, d3, buf);
   }
   free(buf);
-  int rc = ipgc_write(fname, &f) == 0 ? IPG_OK : IPG_E_IO;
+  int rc = ipgc_save(fname, &f) == 0 ? IPG_OK : IPG_E_IO;
+  if (rc) fprintf(stderr, "! %s\n", ipgc_error());
+  ipgc_free(&f);
+  return rc;
+}
+
+int ipg_container_convert(const char *src, const char *dst)
+{
+  if (!src || !dst) return IPG_E_ARG;
+  ipgc_file f;
+  int rc = ipgc_load(src, &f);
+  if (rc) {
+    fprintf(stderr, "! %s\n", ipgc_error());
+    return rc == -2 ? IPG_E_FORMAT : IPG_E_IO;
+  }
+  rc = ipgc_save(dst, &f) == 0 ? IPG_OK : IPG_E_IO;
+  if (rc) fprintf(stderr, "! %s\n", ipgc_error());
   ipgc_free(&f);
   return rc;
 }

@@ -17,16 +17,21 @@ element order) inside a flat container:
 
 Attributes are entries named "<object path>@<attribute>".  The C reader and
 writer of the host library (ipole_b200/csrc/host/ipgc.c) implement the same
-layout.
+layout.  The host library also reads and writes the same entries as HDF5
+files (ipole_b200/csrc/host/h5lite.c); ``read`` accepts either format and
+``write_hdf5`` writes HDF5 through the library.
 """
 from __future__ import annotations
 
+import os
 import struct
+import tempfile
 from typing import Dict, Union
 
 import numpy as np
 
 MAGIC = b"IPGC0001"
+HDF5_MAGIC = b"\x89HDF\r\n\x1a\n"
 GROUP, F64, I32, STR = 0, 1, 2, 3
 
 Value = Union[None, np.ndarray, str, float, int]
@@ -85,12 +90,32 @@ def write(path: str, entries: Dict[str, Value], strlen: Dict[str, int] | None = 
             f.write(data)
 
 
+def _via_library(src: str, dst: str) -> None:
+    from . import convert_container
+    convert_container(src, dst)
+
+
+def write_hdf5(path: str, entries: Dict[str, Value], strlen: Dict[str, int] | None = None) -> None:
+    """``write`` to an HDF5 file (same entries, same types) through the host
+    library's HDF5 writer."""
+    with tempfile.TemporaryDirectory() as d:
+        tmp = os.path.join(d, "x.ipgc")
+        write(tmp, entries, strlen)
+        _via_library(tmp, path)
+
+
 def read(path: str) -> Dict[str, Value]:
-    """Read a container into a dict path -> value (arrays keep their shape;
-    rank-0 numbers come back as 0-d arrays, strings as ``str``)."""
+    """Read a container or an HDF5 file into a dict path -> value (arrays
+    keep their shape; rank-0 numbers come back as 0-d arrays, strings as
+    ``str``).  HDF5 files are read by the host library."""
     out: Dict[str, Value] = {}
     with open(path, "rb") as f:
         buf = f.read()
+    if buf[:8] != MAGIC and any(buf[o:o + 8] == HDF5_MAGIC for o in (0, 512, 1024, 2048, 4096)):
+        with tempfile.TemporaryDirectory() as d:
+            tmp = os.path.join(d, "x.ipgc")
+            _via_library(path, tmp)
+            return read(tmp)
     if buf[:8] != MAGIC:
         raise ValueError(f"{path}: not an IPGC container")
     (n,) = struct.unpack_from("<I", buf, 8)

@@ -7,6 +7,7 @@ import subprocess
 import numpy as np
 import pytest
 
+import ipole_b200 as ip
 from ipole_b200 import build, ipgc
 from tests import common
 
@@ -53,3 +54,26 @@ def test_cli_quench_unpol_and_exit_codes(dumps, tmp_path):
     assert r.returncode == 255
     r = run_cli(["--histo=1"], str(tmp_path))
     assert r.returncode == 42
+
+
+def test_cli_hdf5_dump_and_image(dumps, tmp_path):
+    """The same run from an HDF5 dump to an HDF5 image (the reference's file
+    formats) gives the image of the IPGC run entry for entry, bit for bit."""
+    meta, _ = common.load_golden("c1_incl17_rot_24")
+    dump = dumps.get(meta)
+    h5 = str(tmp_path / "dump.h5")
+    ip.convert_container(dump, h5)
+    a, b = str(tmp_path / "a.ipgc"), str(tmp_path / "b.h5")
+    r = run_cli([f"--dump={dump}", *meta["args"], f"--outfile={a}"], str(tmp_path))
+    assert r.returncode == 0, r.stderr[-2000:]
+    r = run_cli([f"--dump={h5}", *meta["args"], f"--outfile={b}"], str(tmp_path))
+    assert r.returncode == 0, r.stderr[-2000:]
+    with open(b, "rb") as f:
+        assert f.read(8) == ipgc.HDF5_MAGIC
+    ia, ib = ipgc.read(a), ipgc.read(b)
+    assert sorted(ia) == sorted(ib)
+    for k in ia:
+        if isinstance(ia[k], np.ndarray):
+            assert ia[k].dtype == ib[k].dtype and np.array_equal(ia[k], ib[k]), k
+        else:
+            assert ia[k] == ib[k], k
