@@ -28,6 +28,7 @@ CLI = os.path.join(BIN, "ipole_b200")
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-v"]
 CC_FLAGS = ["-std=gnu99", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-result"]
+CU_EXTRA = ["ipg_refine.cu"]
 HOST_SRC = ["ipgc.c", "h5lite.c", "coords.c", "par.c", "model_iharm.c", "camera.c", "render.c"]
 
 
@@ -85,6 +86,14 @@ def build(force: bool = False, verbose: bool = False, defines=(), out_dir: str |
         with open(os.path.join(bdir, "ptxas.txt"), "w") as f:
             f.write(out)
         objs.append(ko)
+        for cu in CU_EXTRA:
+            o = os.path.join(bdir, cu[:-3] + ".o")
+            # no multiply-add contraction: the image driver must round as the host driver does
+            out = _run([_nvcc(), *NVCC_FLAGS, "-fmad=false", *dflags, "-I", INC, "-c", os.path.join(CSRC, cu),
+                        "-o", o], log)
+            with open(os.path.join(bdir, f"ptxas_{cu[:-3]}.txt"), "w") as f:
+                f.write(out)
+            objs.append(o)
         for s in HOST_SRC:
             o = os.path.join(bdir, s[:-2] + ".o")
             _run([_cc(), *CC_FLAGS, "-I", INC, "-c", os.path.join(HOST, s), "-o", o], log)

@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include "../ipg_constants.h"
+#include "../ipg_internal.h"
 #include "ipgc.h"
 #include "ipole_host.h"
 
@@ -104,11 +105,11 @@ static int lininterp4(ipg_image *img, int unpol, size_t i1, size_t j1, size_t i2
   return IPG_OK;
 }
 
-static void report_oddities(const ipg_params *p, const int32_t *ij, const ipg_pixel_out *o, size_t n, FILE *log)
+void ipg__report_oddities(int only_unpolarized, const int32_t *ij, const ipg_pixel_out *o, size_t n, FILE *log)
 {
   if (!log) return;
   for (size_t m = 0; m < n; m++) {
-    if (o[m].flag != 0 || (!p->only_unpolarized && o[m].I < -1.e-10)) {
+    if (o[m].flag != 0 || (!only_unpolarized && o[m].I < -1.e-10)) {
       fprintf(log, "\nOddity in pixel %d %d (flag %d):\n", ij[2 * m], ij[2 * m + 1], o[m].flag);
       fprintf(log, "nstep: %d\n", o[m].nstep);
       fprintf(log, "Final Stokes parameters: [%g %g %g %g]\n", o[m].I, o[m].Q, o[m].U, o[m].V);
@@ -142,16 +143,27 @@ static int trace_list(const tracer_t *tr, const ipg_camera *cam, const int32_t *
   return rc;
 }
 
+static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p, const ipg_iharm_model *m,
+                  ipg_image *img, FILE *log);
+
+/* With a context, the levels run on the device (ipg_refine.cu); the host
+ * loop below serves caller-supplied tracers and is the device driver's
+ * bit-for-bit reference. */
 int ipg_render_image(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, ipg_image *img, void *logp)
 {
   if (!ctx) return IPG_E_ARG;
-  return ipg_render_image_with(ctx_tracer, ctx, p, m, img, logp);
+  return render(ctx_tracer, ctx, ctx, p, m, img, (FILE *)logp);
 }
 
 int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const ipg_iharm_model *m, ipg_image *img,
                           void *logp)
 {
-  FILE *log = (FILE *)logp;
+  return render(tracer, user, NULL, p, m, img, (FILE *)logp);
+}
+
+static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p, const ipg_iharm_model *m,
+                  ipg_image *img, FILE *log)
+{
   if (!tracer || !p || !m || !img) return IPG_E_ARG;
   tracer_t tr = {tracer, user};
   memset(img, 0, sizeof(*img));
@@ -254,6 +266,27 @@ int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const
     return IPG_E_NOMEM;
   }
 
+  if (dev) {
+    ipg_refine_args ra;
+    ra.nx = nx;
+    ra.ny = ny;
+    ra.nxmin = nxmin;
+    ra.nymin = nymin;
+    ra.refine_level = refine_level;
+    ra.params_nx = p->nx;
+    ra.params_ny = p->ny;
+    ra.f3 = pow(p->freqcgs, 3);
+    ra.only_unpolarized = p->only_unpolarized;
+    ra.qu_conv = p->qu_conv;
+    ra.nearest_neighbor = p->nearest_neighbor;
+    ra.refine_abs = p->refine_abs;
+    ra.refine_rel = p->refine_rel;
+    ra.refine_cut = p->refine_cut;
+    free(ij);
+    free(out);
+    return ipg__render_levels_device(dev, cam, &ra, img, log);
+  }
+
   /* base image, main.c:535-615 */
   size_t sx = (nx - 1) / (nxmin - 1);
   size_t sy = (ny - 1) / (nymin - 1);
@@ -267,7 +300,7 @@ int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const
     }
   rc = trace_list(&tr, cam, ij, n, out, log);
   if (rc) goto done;
-  report_oddities(p, ij, out, n, log);
+  ipg__report_oddities(p->only_unpolarized, ij, out, n, log);
   for (size_t q = 0; q < n; q++) {
     size_t i = (size_t)ij[2 * q], j = (size_t)ij[2 * q + 1];
     rc = save_pixel(img, p, i, j, &out[q]);
@@ -276,6 +309,7 @@ int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const
     if (refine_level > 1) {
       double Intensity = out[q].I_unpol;
       size_t loc = i / sy * nymin + j / sx;
+      if (loc >= nxmin * nymin) continue; /* only when sx != sy */
       if (i % (nx - 1) != 0 && j % (ny - 1) != 0) prelim[loc] = Intensity * sx * sx;
       else if ((i == 0 && j % (ny - 1) != 0) || (i % (nx - 1) != 0 && j == 0))
         prelim[loc] = Intensity * (sx / 2 + 1) * sx;
@@ -299,14 +333,24 @@ int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const
     size_t nsx = sx / pow(2, lvl);
     size_t nsy = sy / pow(2, lvl);
     size_t psx = nsx * 2, psy = nsy * 2;
+    if (nsx < 1 || nsy < 1) { /* the reference loops forever here */
+      if (log) fprintf(log, "refinement spacing below one pixel at level %d: nx_min/ny_min too small\n", lvl + 1);
+      rc = IPG_E_ARG;
+      goto done;
+    }
     if (log) fprintf(log, "Refining level %d of %d, spacing %zu,%zu\n", lvl + 1, refine_level, nsx, nsy);
     n = 0;
     for (size_t i = 0; i < nx; i += nsx)
       for (size_t j = 0; j < ny; j += nsy) {
         if (i % psx == 0 && j % psy == 0) continue;
-        double I1, I2, I3, err_abs, err_rel;
+        double I1 = 0, I2, I3, err_abs = 0, err_rel = 0;
         int trace;
-        if (i % psx == 0) {
+        /* the +ns neighbours exist unless the spacing does not divide the
+         * image (a base-to-final ratio that is not a power of two), where the
+         * reference reads past the image: such a pixel is traced */
+        int inside = (i % psx == 0 || i + nsx <= nx - 1) && (j % psy == 0 || j + nsy <= ny - 1);
+        if (!inside) {
+        } else if (i % psx == 0) {
           I1 = img->image[i * ny + j - nsy];
           I2 = img->image[i * ny + j + nsy];
           err_abs = (I2 - I1) / 2 / Iavg;
@@ -323,7 +367,7 @@ int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const
           err_abs = ((I2 + I3) / 2 - I1) / Iavg;
           err_rel = (I2 + I3) / (2 * I1) - 1.;
         }
-        trace = (fabs(err_abs) > p->refine_abs && fabs(err_rel) > p->refine_rel) && fabs(I1) > p->refine_cut;
+        trace = !inside || ((fabs(err_abs) > p->refine_abs && fabs(err_rel) > p->refine_rel) && fabs(I1) > p->refine_cut);
         if (trace) {
           ij[2 * n] = (int32_t)i;
           ij[2 * n + 1] = (int32_t)j;
@@ -353,7 +397,7 @@ int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const
     if (n) {
       rc = trace_list(&tr, cam, ij, n, out, log);
       if (rc) goto done;
-      report_oddities(p, ij, out, n, log);
+      ipg__report_oddities(p->only_unpolarized, ij, out, n, log);
       for (size_t q = 0; q < n; q++) {
         rc = save_pixel(img, p, (size_t)ij[2 * q], (size_t)ij[2 * q + 1], &out[q]);
         if (rc) goto done;

@@ -1,0 +1,60 @@
+/* Internal interface between the library's translation units (not installed,
+ * not part of the C-ABI).
+ *
+ * ipg_kernels.cu owns the context and the ray kernels; ipg_refine.cu holds
+ * the on-device image driver (base image and refinement levels of
+ * src/main.c:520-792); host/render.c calls that driver and shares its
+ * oddity report with it.  Everything here is plain C so that render.c can
+ * include it. */
+#ifndef IPG_INTERNAL_H
+#define IPG_INTERNAL_H
+
+#include <stdio.h>
+
+#include "ipole_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- provided by ipg_kernels.cu ---- */
+/* trace n pixels from the device list d_ij into d_out on the context's
+ * stream (no host copies, no MaxNStep check: the caller inspects d_out) */
+int ipg__trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n, ipg_pixel_out *d_out);
+/* the context's cudaStream_t */
+void *ipg__stream(const ipg_ctx *ctx);
+/* records `msg` as the context's last error (ipg_last_error) */
+void ipg__set_error(ipg_ctx *ctx, const char *msg);
+/* per-context storage owned by ipg_refine.cu; ipg_destroy releases it with
+ * ipg__refine_release */
+void **ipg__refine_slot(ipg_ctx *ctx);
+
+/* ---- provided by ipg_refine.cu ---- */
+void ipg__refine_release(void *bufs);
+
+/* what the image driver needs beyond the camera: the sizes and keys of
+ * src/main.c:102-123 and the save_pixel/refinement parameters */
+typedef struct ipg_refine_args {
+  size_t nx, ny;       /* internal image size */
+  size_t nxmin, nymin; /* internal size of the base image */
+  int refine_level;    /* 1: no refinement */
+  int params_nx, params_ny;
+  double f3;           /* freqcgs^3 (save_pixel) */
+  int only_unpolarized, qu_conv, nearest_neighbor;
+  double refine_abs, refine_rel, refine_cut;
+} ipg_refine_args;
+
+/* Base image and refinement levels on the device, with the host driver's
+ * results, log lines and error codes; fills img->image, taus, imageS (when
+ * polarized), interp_flag, oddflag, nstep and traced (arrays allocated by
+ * the caller, nx*ny). */
+int ipg__render_levels_device(ipg_ctx *ctx, const ipg_camera *cam, const ipg_refine_args *a, void *img, FILE *log);
+
+/* ---- provided by host/render.c ---- */
+/* the oddity lines of get_pixel (src/main.c:852-869) for a traced list */
+void ipg__report_oddities(int only_unpolarized, const int32_t *ij, const ipg_pixel_out *o, size_t n, FILE *log);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "ipg_device.cuh"
+#include "ipg_internal.h"
 #include "ipole_b200.h"
 
 struct RayRec {
@@ -880,6 +881,7 @@ struct ipg_ctx {
   size_t cap;
   int n_sm;
   ipg_stats stats;
+  void *refine; /* buffers of the on-device image driver (ipg_refine.cu) */
   char err[512];
 };
 
@@ -957,6 +959,7 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
 {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  ipg__refine_release(ctx->refine);
   cudaFree(ctx->d_fields);
   cudaFree(ctx->d_pool);
   cudaFree(ctx->d_chunk_prev);
@@ -1421,6 +1424,16 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
   }
   return IPG_OK;
 }
+
+extern "C" int ipg__trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n,
+                               ipg_pixel_out *d_out)
+{
+  if (!ctx || !cam || n == 0 || n > 0x7fffffff) return IPG_E_ARG;
+  return trace_core(ctx, cam, d_ij, n, d_out);
+}
+extern "C" void *ipg__stream(const ipg_ctx *ctx) { return (void *)ctx->stream; }
+extern "C" void ipg__set_error(ipg_ctx *ctx, const char *msg) { snprintf(ctx->err, sizeof(ctx->err), "%s", msg); }
+extern "C" void **ipg__refine_slot(ipg_ctx *ctx) { return &ctx->refine; }
 
 extern "C" int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n,
                                        ipg_pixel_out *d_out, void *stream)
