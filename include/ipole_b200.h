@@ -38,7 +38,12 @@ extern "C" {
 #define IPG_E_FORMAT 9    /* unsupported dump content (metric, schema) */
 
 /* ---- grid / coordinate description (coordinates.h:25-33, grid.h:6) ----
- * FMKS ("funky" modified Kerr-Schild) only, metric == METRIC_FMKS. */
+ * Native coordinates: FMKS ("funky" modified Kerr-Schild) for iharm dumps;
+ * the known-answer models use MKS (hslope = 1) and eMinkowski. */
+#define IPG_METRIC_FMKS 0        /* METRIC_FMKS (coordinates.h) */
+#define IPG_METRIC_MKS 1         /* METRIC_MKS */
+#define IPG_METRIC_MINKOWSKI 2   /* METRIC_MINKOWSKI: r = X1 */
+#define IPG_METRIC_EMINKOWSKI 3  /* METRIC_EMINKOWSKI: r = exp(X1) */
 typedef struct ipg_grid {
   int n1, n2, n3;                 /* physical zones (ghost zones excluded) */
   double startx[4], stopx[4], dx[4];
@@ -51,6 +56,7 @@ typedef struct ipg_grid {
   double sigma_cut;               /* emission cut: ne = 0 where sigma > sigma_cut */
   double sigma_cut_high;          /* model key sigma_cut_high (<= 0: off), only decides sigma == sigma_cut */
   double L_unit;                  /* GM/c^2 in cm */
+  int metric;                     /* IPG_METRIC_*; 0 (FMKS) for iharm dumps */
 } ipg_grid;
 
 /* Field order of ipg_upload_iharm: primitives U1..3, B1..3 (native FMKS
@@ -108,6 +114,28 @@ const char *ipg_last_error(const ipg_ctx *ctx);
  * of get_model_fourv / get_model_ne / get_model_thetae / get_model_b /
  * get_model_sigma point queries. */
 int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *grid, const double *const fields[IPG_NFIELD]);
+
+/* ---- known-answer models (model/analytic/model.c, model/sphere/model.c) ----
+ * The reference builds one binary per model (makefile:2, MODEL=...); here the
+ * context is switched to a model by uploading it, and the ray kernels run
+ * their instantiation for it.  The grid carries the model's geometry
+ * (startx/stopx/cstartx/cstopx, a, Rh, rmin_geo, rmax_geo, L_unit) and its
+ * metric: IPG_METRIC_MKS for the analytic models, IPG_METRIC_EMINKOWSKI for
+ * the sphere. */
+#define IPG_PLUGIN_IHARM 0
+#define IPG_PLUGIN_ANALYTIC 1  /* Gold et al. 2020 GRRT problems, emission_type 10 */
+#define IPG_PLUGIN_SPHERE 2    /* isothermal sphere, thermal emission_type 4 or 1 */
+typedef struct ipg_plugin {
+  int kind;                       /* IPG_PLUGIN_* */
+  int model;                      /* analytic problem number 1..5 */
+  /* analytic: init_model's problem constants and units (model/analytic/model.c:79-140) */
+  double A, alpha, height, l0, freqcgs, rho_unit;
+  /* sphere: derived density, temperature and field (model/sphere/model.c:53-85) */
+  double R0, Ne0, Thetae0, B0;
+} ipg_plugin;
+/* Upload a known-answer model; replaces any model of the context.  Returns
+ * IPG_E_ARG for an unknown kind or a grid whose metric does not match it. */
+int ipg_upload_plugin(ipg_ctx *ctx, const ipg_grid *grid, const ipg_plugin *plugin);
 
 /* Trace n pixels (ij[2*m] = i, ij[2*m+1] = j) and return get_pixel's
  * outputs for each.  Host buffers; the call copies in, runs, copies out.

@@ -57,6 +57,15 @@ typedef struct ipg_params {
   int variable_kappa;
   double variable_kappa_min, variable_kappa_interp_start, variable_kappa_max;
   int bremss, bremss_type;
+  /* Model selection (the reference selects at build time, makefile:2
+   * MODEL=...): key "plugin" = iharm (default), analytic or sphere. */
+  char plugin[IPG_STRLEN];
+  int MBH_set;              /* 1 once the "MBH" key was given (each model has its own default) */
+  /* analytic keys (model/analytic/model.c:56-72) */
+  int analytic_model;       /* "model": problem 1..5 of Gold et al. 2020 */
+  double rho_unit;          /* "rho_unit" (<= 0: 3e-18) */
+  /* sphere keys (model/sphere/model.c:37-46); tp_over_te is shared with iharm */
+  double sphere_Thetae0, sphere_R0, sphere_tau0, sphere_beta0, sphere_gam;
 } ipg_params;
 
 /* Defaults of load_par_from_argv (src/par.c:48-100) and the model/radiation
@@ -81,13 +90,21 @@ typedef struct ipg_iharm_model {
   int electrons;
   double gam, game, gamp;
   void *fluid_header;          /* copy of the dump's /header group (for /fluid_header) */
+  ipg_plugin plugin;           /* kind IPG_PLUGIN_IHARM, or a known-answer model (no fields) */
 } ipg_iharm_model;
 
 /* init_model: read the dump named in p->dump (an iharm v1 HDF5 dump, or the
  * same schema in an IPGC container), build ghost zones and derived fields.  Returns
- * IPG_E_IO / IPG_E_FORMAT on a bad dump (reference: exit(-1) / exit(-3)). */
+ * IPG_E_IO / IPG_E_FORMAT on a bad dump (reference: exit(-1) / exit(-3)).
+ * With p->plugin "analytic" or "sphere", the known-answer model's init_model
+ * instead (model/analytic/model.c:79-160, model/sphere/model.c:53-110):
+ * geometry, units and model constants, no dump.  Returns IPG_E_ARG for an
+ * unknown plugin name. */
 int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m);
 void ipg_iharm_free(ipg_iharm_model *m);
+/* Upload the loaded model to a context: ipg_upload_iharm for a dump,
+ * ipg_upload_plugin for a known-answer model. */
+int ipg_upload_model(ipg_ctx *ctx, const ipg_iharm_model *m);
 
 /* A rendered image, internal size nx x ny (params.nx + 1 when refining an
  * even size, main.c:107-123), arrays as in main.c:184-197. */

@@ -48,7 +48,8 @@ class Grid(C.Structure):
                 ("poly_norm", C.c_double),
                 ("Rin", C.c_double), ("Rout", C.c_double), ("Rh", C.c_double),
                 ("rmin_geo", C.c_double), ("rmax_geo", C.c_double), ("th_beg", C.c_double),
-                ("sigma_cut", C.c_double), ("sigma_cut_high", C.c_double), ("L_unit", C.c_double)]
+                ("sigma_cut", C.c_double), ("sigma_cut_high", C.c_double), ("L_unit", C.c_double),
+                ("metric", C.c_int)]
 
 
 class Camera(C.Structure):
@@ -104,7 +105,18 @@ class _Params(C.Structure):
                 ("powerlaw_gamma_max", C.c_double), ("powerlaw_p", C.c_double), ("powerlaw_eta", C.c_double),
                 ("variable_kappa", C.c_int), ("variable_kappa_min", C.c_double),
                 ("variable_kappa_interp_start", C.c_double), ("variable_kappa_max", C.c_double),
-                ("bremss", C.c_int), ("bremss_type", C.c_int)]
+                ("bremss", C.c_int), ("bremss_type", C.c_int),
+                ("plugin", C.c_char * STRLEN), ("MBH_set", C.c_int), ("analytic_model", C.c_int),
+                ("rho_unit", C.c_double), ("sphere_Thetae0", C.c_double), ("sphere_R0", C.c_double),
+                ("sphere_tau0", C.c_double), ("sphere_beta0", C.c_double), ("sphere_gam", C.c_double)]
+
+
+class Plugin(C.Structure):
+    """ipg_plugin: a known-answer model (kind 0 = the iharm dump model)."""
+    _fields_ = [("kind", C.c_int), ("model", C.c_int),
+                ("A", C.c_double), ("alpha", C.c_double), ("height", C.c_double), ("l0", C.c_double),
+                ("freqcgs", C.c_double), ("rho_unit", C.c_double),
+                ("R0", C.c_double), ("Ne0", C.c_double), ("Thetae0", C.c_double), ("B0", C.c_double)]
 
 
 class _Model(C.Structure):
@@ -113,7 +125,8 @@ class _Model(C.Structure):
                 ("U_unit", C.c_double), ("B_unit", C.c_double), ("Te_unit", C.c_double), ("MBH", C.c_double),
                 ("Mdot_dump", C.c_double), ("MdotEdd_dump", C.c_double), ("Ladv_dump", C.c_double),
                 ("t", C.c_double), ("DTd", C.c_double), ("electrons", C.c_int),
-                ("gam", C.c_double), ("game", C.c_double), ("gamp", C.c_double), ("fluid_header", C.c_void_p)]
+                ("gam", C.c_double), ("game", C.c_double), ("gamp", C.c_double), ("fluid_header", C.c_void_p),
+                ("plugin", Plugin)]
 
 
 class _Image(C.Structure):
@@ -149,6 +162,8 @@ def lib():
     L.ipg_last_error.restype = C.c_char_p
     L.ipg_last_error.argtypes = [C.c_void_p]
     L.ipg_upload_iharm.argtypes = [C.c_void_p, C.POINTER(Grid), C.POINTER(C.POINTER(C.c_double))]
+    L.ipg_upload_plugin.argtypes = [C.c_void_p, C.POINTER(Grid), C.POINTER(Plugin)]
+    L.ipg_upload_model.argtypes = [C.c_void_p, C.POINTER(_Model)]
     L.ipg_trace_pixels.argtypes = [C.c_void_p, C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p]
     L.ipg_trace_pixels_device.argtypes = [C.c_void_p, C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p,
                                           C.c_void_p]
@@ -339,8 +354,9 @@ class Context:
             pass
 
     def upload(self, model: Model):
-        fields = (C.POINTER(C.c_double) * NFIELD)(*[model._m.fields[i] for i in range(NFIELD)])
-        _check(lib().ipg_upload_iharm(self._h, C.byref(model._m.grid), fields), self._h)
+        """The loaded model: an iharm dump's fields, or a known-answer model
+        (ipg_upload_model)."""
+        _check(lib().ipg_upload_model(self._h, C.byref(model._m)), self._h)
 
     def upload_arrays(self, grid: Grid, fields):
         arrs = [np.ascontiguousarray(f, dtype=np.float64).ravel() for f in fields]

@@ -1,4 +1,5 @@
-/* Host-side FMKS geometry for set-up code.  Each function follows the
+/* Host-side geometry (FMKS, and the MKS / flat metrics of the known-answer
+ * models) for set-up code.  Each function follows the
  * operation order of the reference function it names (cited), so that the
  * camera tetrad and derived fluid fields match the reference bit for bit when
  * both are compiled without FMA contraction. */
@@ -9,10 +10,23 @@
 
 #define SMALL 1.e-40
 
-/* src/coordinates.c:46-97 (METRIC_FMKS branch) */
+/* src/coordinates.c:46-97 (METRIC_MINKOWSKI, EMINKOWSKI, MKS, FMKS branches) */
 void hc_bl_coord(const ipg_grid *g, const double X[NDIM], double *r, double *th)
 {
+  if (g->metric == IPG_METRIC_MINKOWSKI) {
+    *r = X[1];
+    *th = X[2];
+    return;
+  } else if (g->metric == IPG_METRIC_EMINKOWSKI) {
+    *r = exp(X[1]);
+    *th = X[2];
+    return;
+  }
   *r = exp(X[1]);
+  if (g->metric == IPG_METRIC_MKS) {
+    *th = M_PI * X[2] + ((1. - g->hslope) / 2.) * sin(2. * M_PI * X[2]);
+    return;
+  }
   double thG = M_PI * X[2] + ((1. - g->hslope) / 2.) * sin(2. * M_PI * X[2]);
   double y = 2 * X[2] - 1.;
   double thJ = g->poly_norm * y * (1. + pow(y / g->poly_xt, g->poly_alpha) / (g->poly_alpha + 1.)) + 0.5 * M_PI;
@@ -40,7 +54,7 @@ void hc_gcov_ks(const ipg_grid *g, double r, double th, double gcov[NDIM][NDIM])
   gcov[3][3] = s2 * (rho2 + a * a * s2 * (1. + 2. * r / rho2));
 }
 
-/* src/coordinates.c:263-305 (METRIC_FMKS branch) */
+/* src/coordinates.c:263-348 (METRIC_FMKS, MKS, MINKOWSKI, EMINKOWSKI branches) */
 void hc_set_dxdX(const ipg_grid *g, const double X[NDIM], double dxdX[NDIM][NDIM])
 {
   const double hslope = g->hslope, poly_xt = g->poly_xt, poly_alpha = g->poly_alpha;
@@ -48,6 +62,15 @@ void hc_set_dxdX(const ipg_grid *g, const double X[NDIM], double dxdX[NDIM][NDIM
   for (int mu = 0; mu < NDIM; mu++)
     for (int nu = 0; nu < NDIM; nu++) dxdX[mu][nu] = (mu == nu);
   dxdX[1][1] = exp(X[1]);
+  if (g->metric == IPG_METRIC_MKS) {
+    dxdX[2][2] = M_PI + (1 - hslope) * M_PI * cos(2. * M_PI * X[2]);
+    return;
+  } else if (g->metric == IPG_METRIC_MINKOWSKI) {
+    dxdX[1][1] = 1.;
+    return;
+  } else if (g->metric == IPG_METRIC_EMINKOWSKI) {
+    return;
+  }
   dxdX[2][1] = -exp(mks_smooth * (g->startx[1] - X[1])) * mks_smooth *
                (M_PI / 2. - M_PI * X[2] +
                 poly_norm * (2. * X[2] - 1.) * (1 + (pow((-1. + 2 * X[2]) / poly_xt, poly_alpha)) / (1 + poly_alpha)) -
@@ -65,6 +88,14 @@ void hc_gcov_func(const ipg_grid *g, const double X[NDIM], double gcov[NDIM][NDI
 {
   double r, th;
   hc_bl_coord(g, X, &r, &th);
+  if (g->metric == IPG_METRIC_MINKOWSKI || g->metric == IPG_METRIC_EMINKOWSKI) {
+    memset(gcov, 0, sizeof(double) * 16);
+    gcov[0][0] = -1;
+    gcov[1][1] = (g->metric == IPG_METRIC_MINKOWSKI) ? 1 : r * r;
+    gcov[2][2] = r * r;
+    gcov[3][3] = r * r * sin(th) * sin(th);
+    return;
+  }
   double Gcov_ks[NDIM][NDIM];
   hc_gcov_ks(g, r, th, Gcov_ks);
   double dxdX[NDIM][NDIM];
@@ -352,6 +383,13 @@ static double root_find(const ipg_grid *g, const double X[NDIM])
 /* src/coordinates.c:375-387 */
 void hc_native_coord(const ipg_grid *g, double r, double th_deg, double phi_deg, double X[NDIM])
 {
+  if (g->metric == IPG_METRIC_MINKOWSKI || g->metric == IPG_METRIC_EMINKOWSKI) {
+    X[0] = 1;
+    X[1] = (g->metric == IPG_METRIC_MINKOWSKI) ? r : log(r);
+    X[2] = th_deg / 180 * M_PI;
+    X[3] = phi_deg / 180 * M_PI;
+    return;
+  }
   double x[NDIM] = {0., r, th_deg / 180. * M_PI, phi_deg / 180. * M_PI};
   X[0] = 0.0;
   X[1] = log(r);

@@ -52,7 +52,7 @@ int main(int argc, char *argv[])
     ipg_iharm_free(&m);
     return exit_code(rc);
   }
-  rc = ipg_upload_iharm(ctx, &m.grid, (const double *const *)m.fields);
+  rc = ipg_upload_model(ctx, &m);
   if (rc) {
     fprintf(stderr, "model upload failed: %s (%s)\n", ipg_strerror(rc), ipg_last_error(ctx));
     ipg_destroy(ctx);

@@ -12,6 +12,7 @@
 #include "../ipg_constants.h"
 #include "coords.h"
 #include "ipgc.h"
+#include "../ipg_internal.h"
 #include "ipole_host.h"
 
 #define KRHO 0
@@ -110,6 +111,8 @@ void ipg_iharm_free(ipg_iharm_model *m)
 
 int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m)
 {
+  int prc;
+  if (ipg__plugin_load(p, m, &prc)) return prc;
   memset(m, 0, sizeof(*m));
   ipg_grid *g = &m->grid;
   ipgc_file file;

@@ -35,6 +35,12 @@ void ipg_params_default(ipg_params *p)
   p->perform_check = 0;
   p->old_centering = 0;
   p->emission_type = 4;
+  strcpy(p->plugin, "iharm");
+  p->sphere_R0 = 100.;
+  p->sphere_tau0 = 1.e-5;
+  p->sphere_Thetae0 = 10.;
+  p->sphere_beta0 = 20.;
+  p->sphere_gam = 13. / 9;
   p->stokes_floors = 0;
   p->isolate_counterjet = 0;
   p->rcam = 1000.;
@@ -103,6 +109,16 @@ void ipg_params_default(ipg_params *p)
 static void set_model_parameter(ipg_params *p, const char *word, const char *value)
 {
   set_by_word_val(word, value, "MBH", &p->MBH_solar, TYPE_DBL);
+  if (strcmp(word, "MBH") == 0) p->MBH_set = 1;
+  /* model selection and the known-answer models' keys */
+  set_by_word_val(word, value, "plugin", p->plugin, TYPE_STR);
+  set_by_word_val(word, value, "model", &p->analytic_model, TYPE_INT);
+  set_by_word_val(word, value, "rho_unit", &p->rho_unit, TYPE_DBL);
+  set_by_word_val(word, value, "Thetae0", &p->sphere_Thetae0, TYPE_DBL);
+  set_by_word_val(word, value, "R0", &p->sphere_R0, TYPE_DBL);
+  set_by_word_val(word, value, "tau0", &p->sphere_tau0, TYPE_DBL);
+  set_by_word_val(word, value, "beta0", &p->sphere_beta0, TYPE_DBL);
+  set_by_word_val(word, value, "gam", &p->sphere_gam, TYPE_DBL);
   set_by_word_val(word, value, "M_unit", &p->M_unit, TYPE_DBL);
   set_by_word_val(word, value, "mdot", &p->target_mdot, TYPE_DBL);
   set_by_word_val(word, value, "dump", p->dump, TYPE_STR);

@@ -500,7 +500,9 @@ int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p
   ipgc_put_f64(&f, "/header/camera/yoff", p->yoff);
   uint64_t d4 = 4;
   ipgc_put_array_f64(&f, "/header/camera/x", 1, &d4, img->Xcam);
-  if (m) {
+  if (m && m->plugin.kind != IPG_PLUGIN_IHARM) {
+    ipg__plugin_write_header(&f, m);
+  } else if (m) {
     if (m->fluid_header) ipgc_copy_subtree((const ipgc_file *)m->fluid_header, "", &f, "/fluid_header");
     ipgc_put_f64(&f, "/Mdot", m->Mdot_dump);
     ipgc_put_f64(&f, "/MdotEdd", m->MdotEdd_dump);

@@ -91,6 +91,14 @@
 #define IPG_RAY_MAXNSTEP 1
 #define IPG_RAY_POOL_FULL 2
 
+/* Metrics of the native coordinates (src/coordinates.h:8-19): the iharm
+ * FMKS, MKS (the analytic models, hslope = 1), flat space in spherical
+ * coordinates with r = X1 (Minkowski) or r = exp(X1) (eMinkowski). */
+#define IPG_MET_FMKS 0
+#define IPG_MET_MKS 1
+#define IPG_MET_MINK 2
+#define IPG_MET_EMINK 3
+
 struct DevGrid {
   int n1, n2, n3;
   int alpha_int;            /* poly_alpha - 1 as an integer exponent, or -1 */
@@ -306,11 +314,44 @@ struct PointGeo {
   Met g;
 };
 
+/* r of bl_coord (src/coordinates.c:46-58) */
+template <int MET>
+__device__ __forceinline__ double geo_r(double X1)
+{
+  return (MET == IPG_MET_MINK) ? X1 : exp(X1);
+}
+
+/* flat space in spherical coordinates (src/coordinates.c:180-193) */
+template <int MET>
+__device__ __forceinline__ Met met_flat(double r, double sth)
+{
+  Met m;
+  m.g00 = -1.;
+  m.g01 = m.g03 = m.g12 = m.g13 = 0.;
+  m.g11 = (MET == IPG_MET_MINK) ? 1. : r * r;
+  m.g22 = r * r;
+  m.g33 = r * r * sth * sth;
+  return m;
+}
+
+/* point evaluation for metric MET: FMKS as written above; MKS is FMKS with
+ * the jet term switched off (theta = thetaG, src/coordinates.c:68-70,
+ * 278-280), which keeps its arithmetic; the flat metrics have theta = X2 */
+template <int MET = IPG_MET_FMKS>
 __device__ __forceinline__ void point_geo(double X1, double X2, PointGeo *pg)
 {
   const DevGrid &G = c_grid;
+  if constexpr (MET == IPG_MET_MINK || MET == IPG_MET_EMINK) {
+    pg->r = geo_r<MET>(X1);
+    pg->th = X2;
+    sincos(X2, &pg->sth, &pg->cth);
+    pg->J21 = 0.;
+    pg->J22 = 1.;
+    pg->g = met_flat<MET>(pg->r, pg->sth);
+    return;
+  }
   double r = exp(X1);
-  double E = exp(G.mks_smooth * (G.startx[1] - X1));
+  double E = (MET == IPG_MET_FMKS) ? exp(G.mks_smooth * (G.startx[1] - X1)) : 0.;
   double S2, C2;
   sincospi(2. * X2, &S2, &C2);
   X2P p;
@@ -346,13 +387,48 @@ __device__ __forceinline__ Met met_diff(const Met &h, const Met &l, double inv)
   return d;
 }
 
+/* g^{mu nu} of the flat metrics (the reference inverts by LU; diagonal) */
+template <int MET>
+__device__ __forceinline__ Gcon gcon_flat(double r, double sth)
+{
+  Gcon u;
+  u.u00 = -1.;
+  u.u01 = u.u02 = u.u12 = u.u13 = u.u23 = 0.;
+  u.u11 = (MET == IPG_MET_MINK) ? 1. : 1. / (r * r);
+  u.u22 = 1. / (r * r);
+  u.u33 = 1. / (r * r * sth * sth);
+  return u;
+}
+
+template <int MET>
+__device__ void fd_connection_flat(double X1, double X2, Conn *cn)
+{
+  double r = geo_r<MET>(X1), s0, c0;
+  sincos(X2, &s0, &c0);
+  cn->gu = gcon_flat<MET>(r, s0);
+  cn->r = r;
+  {
+    double Xh = X1 + IPG_DEL, Xl = X1 - IPG_DEL;
+    cn->D1 = met_diff(met_flat<MET>(geo_r<MET>(Xh), s0), met_flat<MET>(geo_r<MET>(Xl), s0), 1. / (Xh - Xl));
+  }
+  {
+    double Xh = X2 + IPG_DEL, Xl = X2 - IPG_DEL;
+    cn->D2 = met_diff(met_flat<MET>(r, sin(Xh)), met_flat<MET>(r, sin(Xl)), 1. / (Xh - Xl));
+  }
+}
+
+template <int MET = IPG_MET_FMKS>
 IPG_HEAVY void fd_connection(double X1, double X2, Conn *cn)
 {
+  if constexpr (MET == IPG_MET_MINK || MET == IPG_MET_EMINK) {
+    fd_connection_flat<MET>(X1, X2, cn);
+    return;
+  }
   const DevGrid &G = c_grid;
   const double sm = G.mks_smooth;
   /* center */
   double r = exp(X1);
-  double E = exp(sm * (G.startx[1] - X1));
+  double E = (MET == IPG_MET_FMKS) ? exp(sm * (G.startx[1] - X1)) : 0.;
   double S2, C2;
   sincospi(2. * X2, &S2, &C2);
   X2P p0;
@@ -1104,6 +1180,19 @@ __device__ __forceinline__ double det4(const double E[4][4])
 
 /* Econ[a][mu] rows; returns oddflag bits 1 / 16.  Only Ecov rows 1 and 2
  * and Econ rows 1 and 2 are consumed downstream. */
+/* sqrt|det g| at a point (check_handedness): Kerr-Schild based metrics
+ * rho^2 sin(th) r J22; flat r^2 sin(th) (Minkowski), r^3 sin(th) (eMinkowski) */
+template <int MET = IPG_MET_FMKS>
+__device__ __forceinline__ double pg_gdet(const PointGeo &pg)
+{
+  if constexpr (MET == IPG_MET_MINK) return fabs(pg.r * pg.r * pg.sth);
+  if constexpr (MET == IPG_MET_EMINK) return fabs(pg.r * pg.r * pg.r * pg.sth);
+  const double a = c_grid.a;
+  double rho2 = pg.r * pg.r + a * a * pg.cth * pg.cth;
+  return fabs(rho2 * pg.sth * pg.r * pg.J22);
+}
+
+template <int MET = IPG_MET_FMKS>
 IPG_HEAVY int plasma_tetrad(const double Ucon[4], const double Kcon[4], const double Bcon[4], const Met &g,
                              const PointGeo &pg, double Econ[4][4], double Ecov1[4], double Ecov2[4])
 {
@@ -1129,11 +1218,8 @@ IPG_HEAVY int plasma_tetrad(const double Ucon[4], const double Kcon[4], const do
   t_project_out(Econ[1], Econ[2], g2, s2);
   t_project_out(Econ[1], Econ[3], g3, s3);
   t_normalize(g, Econ[1], g1, &s1);
-  /* check_handedness: sqrt|det g| * det(Econ); det g = -(rho^2 sin(th) r J22)^2 */
-  const double a = c_grid.a;
-  double rho2 = pg.r * pg.r + a * a * pg.cth * pg.cth;
-  double gdet = fabs(rho2 * pg.sth * pg.r * pg.J22);
-  double dot = gdet * det4(Econ);
+  /* check_handedness: sqrt|det g| * det(Econ) */
+  double dot = pg_gdet<MET>(pg) * det4(Econ);
   int flag = 0;
   if (fabs(fabs(dot) - 1.) > 1.e-10) flag |= 1;
   double sgn = (dot < 0.) ? -1. : 1.;

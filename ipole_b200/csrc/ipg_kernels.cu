@@ -38,6 +38,7 @@
 
 #include "ipg_device.cuh"
 #include "ipg_internal.h"
+#include "ipg_plugins.cuh"
 #include "ipole_b200.h"
 
 struct RayRec {
@@ -71,20 +72,6 @@ __device__ __forceinline__ double stepsize(const double X[4], const double K[4],
   double b1 = eps * (10 * deh), b2 = eps * d2fac;
   double b12 = b1 * b2;
   return (eps * b12) / (eps * (a1 * b2 + a2 * b1) + a3 * b12);
-}
-
-/* theta of bl_coord (src/coordinates.c:75-81), for the sub-ring counter */
-__device__ __forceinline__ double bl_theta(double X1, double X2)
-{
-  const DevGrid &G = c_grid;
-  double E = exp(G.mks_smooth * (G.startx[1] - X1));
-  double S2, C2;
-  sincospi(2. * X2, &S2, &C2);
-  X2P p;
-  x2_parts_from(X2, S2, C2, &p);
-  double th, j1, j2;
-  theta_jac(X2, E, p, &th, &j1, &j2);
-  return th;
 }
 
 __device__ __forceinline__ double *step_ptr(double *pool, int chunk, int slot)
@@ -165,13 +152,6 @@ __device__ __forceinline__ void init_ray(int i, int j, double X[4], double K[4])
   }
 }
 
-/* radiating_region, model/iharm/model.c:2093-2098 */
-__device__ __forceinline__ int radiating(const PointGeo &pg)
-{
-  const DevGrid &G = c_grid;
-  return (pg.r > G.rmin_geo && pg.r < G.rmax_geo && pg.th > G.th_beg && pg.th < (IPG_PI - G.th_beg));
-}
-
 /* ===================================================================== */
 /* k_geodesic                                                             */
 /* ===================================================================== */
@@ -229,6 +209,7 @@ __device__ __forceinline__ bool geo_fetch(GeoLane &L, const int32_t *__restrict_
 }
 
 /* Sub-ring counter, src/model_geodesics.c:129-165, after step nstep */
+template <int MET>
 __device__ __forceinline__ void count_turns(GeoLane &L)
 {
   const DevCam &C = c_cam;
@@ -243,9 +224,9 @@ __device__ __forceinline__ void count_turns(GeoLane &L)
       double dX2a = L.X2m1 - L.X2m2, dX2b = L.X[2] - L.X2m1;
       if (dX2a * dX2b < 0) L.nturns++;
     } else {
-      double ra = exp(L.X1m2), rb = exp(L.X1m1), rc = exp(L.X[1]);
-      double za = ra * cos(bl_theta(L.X1m2, L.X2m2)), zb = rb * cos(bl_theta(L.X1m1, L.X2m1));
-      double zc = rc * cos(bl_theta(L.X[1], L.X[2]));
+      double ra = geo_r<MET>(L.X1m2), rb = geo_r<MET>(L.X1m1), rc = geo_r<MET>(L.X[1]);
+      double za = ra * cos(bl_theta<MET>(L.X1m2, L.X2m2)), zb = rb * cos(bl_theta<MET>(L.X1m1, L.X2m1));
+      double zc = rc * cos(bl_theta<MET>(L.X[1], L.X[2]));
       if ((zb - za) * (zc - zb) < 0) L.nturns++;
     }
   }
@@ -261,6 +242,7 @@ __device__ __forceinline__ void count_turns(GeoLane &L)
  * holds one copy of it, which keeps the loop body small: a lone ray's step
  * time is set by instruction-fetch and dependency latency, not by the FP64
  * throughput of the SM. */
+template <int P>
 __global__ void __launch_bounds__(256, IPG_GEO_MINB)
     k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list,
                double *__restrict__ pool, int *__restrict__ chunk_prev, int2 *__restrict__ chunk_meta,
@@ -280,7 +262,7 @@ __global__ void __launch_bounds__(256, IPG_GEO_MINB)
     if (ph == 0) {
       /* stop_backward_integration, src/model_geodesics.c:218-254, and the
        * step limit of trace_geodesic's loop (:71) */
-      double r = exp(L.X[1]);
+      double r = geo_r<PlugT<P>::MET>(L.X[1]);
       if ((r > G.rmax_geo && L.K[1] < 0.) || r < (G.Rh + 0.0001) || !(L.nstep < C.maxnstep - 1)) {
         int status = (L.nstep >= C.maxnstep - 1) ? IPG_RAY_MAXNSTEP : IPG_RAY_OK;
         if (status != IPG_RAY_OK || !pol || L.nstep == 0) {
@@ -298,7 +280,7 @@ __global__ void __launch_bounds__(256, IPG_GEO_MINB)
     for (int k = 0; k < 4; k++) Ke[k] = ph ? L.Kh[k] : L.K[k];
     Conn cn;
     double acc[4], A[4][4];
-    fd_connection(ph ? L.Xh[1] : L.X[1], ph ? L.Xh[2] : L.X[2], &cn);
+    fd_connection<PlugT<P>::MET>(ph ? L.Xh[1] : L.X[1], ph ? L.Xh[2] : L.X[2], &cn);
     if (pol) {
       /* the transfer needs Gamma K at X_n and at Xhalf_n for each step */
       transport_matrix(cn, Ke, A);
@@ -333,7 +315,7 @@ __global__ void __launch_bounds__(256, IPG_GEO_MINB)
     L.phase = 0;
     double dl = -L.h;
     double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
-    if (track) count_turns(L);
+    if (track) count_turns<PlugT<P>::MET>(L);
     int slot = L.nstep % IPG_CHUNK_STEPS;
     if (slot == 0) {
       long long nc = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
@@ -360,6 +342,7 @@ __global__ void __launch_bounds__(256, IPG_GEO_MINB)
  * trace can start the longest rays first.  pred[t] is the count of list
  * entry t; a ray whose position turns non-finite, or that passes step_cap,
  * stops there. */
+template <int P>
 __global__ void __launch_bounds__(128, IPG_GEO_MINB)
     k_geodesic_count(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list, double eps_scale,
                      int step_cap, int32_t *__restrict__ pred, unsigned long long *__restrict__ counter)
@@ -386,7 +369,7 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
     if (!__any_sync(0xffffffffu, has)) break;
     if (!has) continue;
     if (phase == 0) {
-      double r = exp(X[1]);
+      double r = geo_r<PlugT<P>::MET>(X[1]);
       if ((r > G.rmax_geo && K[1] < 0.) || r < (G.Rh + 0.0001) || !(nstep < step_cap) || !isfinite(X[1])) {
         pred[t] = nstep;
         has = false;
@@ -398,7 +381,7 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
     for (int k = 0; k < 4; k++) Ke[k] = phase ? Kh[k] : K[k];
     Conn cn;
     double acc[4];
-    fd_connection(phase ? Xh[1] : X[1], phase ? Xh[2] : X[2], &cn);
+    fd_connection<PlugT<P>::MET>(phase ? Xh[1] : X[1], phase ? Xh[2] : X[2], &cn);
     geo_accel(cn, Ke, acc);
     if (phase == 0) {
       nstep++;
@@ -427,6 +410,7 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
  * step ending at s needs that does not depend on the radiation field.  The
  * record's geodesic block is overwritten by the coefficient block; dl and
  * nturns keep their slots. */
+template <int P>
 __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     k_coeffs(double *__restrict__ pool, const int2 *__restrict__ chunk_meta,
              const unsigned long long *__restrict__ counters, long long n_chunks,
@@ -450,8 +434,8 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     double K[4];
     load4(p + REC_K, K);
     PointGeo pg;
-    point_geo(X1, X2, &pg);
-    int flags = radiating(pg) ? 1 : 0;
+    point_geo<PlugT<P>::MET>(X1, X2, &pg);
+    int flags = radiating_t<P>(pg) ? 1 : 0;
     /* isolate_counterjet, src/ipolarray.c:128-136 */
     if (C.counterjet == 1) {
       if (X2 < (G.cstopx[2] - G.cstartx[2]) / 2) flags |= 2;
@@ -468,9 +452,9 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
      * (src/ipolarray.c:357-384) at radiating points */
     if ((flags & 1) || s == rec.nstep) {
       ModelPt mp;
-      model_point(fields, X1, X2, X3, pg, &mp);
+      model_point_t<P>(fields, X1, X2, X3, pg, &mp);
       int want_pol = pol && (flags & 1);
-      jar_both(mp, K, want_pol, C.emission_type, &ju, &ku, &jar);
+      coeffs_t<P>(mp, K, want_pol, C.emission_type, &ju, &ku, &jar);
       if (want_pol) {
         double Bcon[4] = {mp.Bcon[0], mp.Bcon[1], mp.Bcon[2], mp.Bcon[3]};
         double bsq = Bcon[0] * mp.Bcov[0] + Bcon[1] * mp.Bcov[1] + Bcon[2] * mp.Bcov[2] + Bcon[3] * mp.Bcov[3];
@@ -480,7 +464,7 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
           Bcon[2] = 1.;
           Bcon[3] = 1.;
         }
-        int tf = plasma_tetrad(mp.Ucon, K, Bcon, mp.geo.g, mp.geo, Econ, e1, e2);
+        int tf = plasma_tetrad<PlugT<P>::MET>(mp.Ucon, K, Bcon, mp.geo.g, mp.geo, Econ, e1, e2);
         if (isnan(mp.Ucov[0])) tf |= 8;
         flags |= tf << 2;
       }
@@ -863,7 +847,9 @@ struct ipg_ctx {
   double *d_fields;
   size_t ncell;
   int have_model;
+  int plug;     /* IPG_PLUG_*: the model the kernels are instantiated for */
   DevGrid dg;
+  DevPlug dp;   /* constants of a known-answer model */
   double *d_pool;
   int *d_chunk_prev;
   int2 *d_chunk_meta;
@@ -985,6 +971,8 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   free(ctx);
 }
 
+static void devgrid_from(const ipg_grid *g, DevGrid *d);
+
 extern "C" int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *g, const double *const fields[IPG_NFIELD])
 {
   if (!ctx || !g || !fields || g->n1 <= 0 || g->n2 <= 0 || g->n3 <= 0) return IPG_E_ARG;
@@ -1005,7 +993,63 @@ extern "C" int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *g, const double *c
   if (!ctx->d_fields) CK(cudaMalloc(&ctx->d_fields, ncell * IPG_NFIELD * sizeof(double)));
   CK(cudaMemcpy(ctx->d_fields, aos.data(), ncell * IPG_NFIELD * sizeof(double), cudaMemcpyHostToDevice));
   ctx->ncell = ncell;
-  DevGrid &d = ctx->dg;
+  devgrid_from(g, &ctx->dg);
+  memset(&ctx->dp, 0, sizeof(ctx->dp));
+  ctx->plug = IPG_PLUG_IHARM;
+  ctx->have_model = 1;
+  return IPG_OK;
+}
+
+/* The known-answer models (model/analytic, model/sphere): no field arrays,
+ * the model's constants go to the kernels' constant bank. */
+extern "C" int ipg_upload_plugin(ipg_ctx *ctx, const ipg_grid *g, const ipg_plugin *pl)
+{
+  if (!ctx || !g || !pl) return IPG_E_ARG;
+  int plug, met;
+  if (pl->kind == IPG_PLUGIN_ANALYTIC) {
+    plug = IPG_PLUG_ANALYTIC;
+    met = IPG_METRIC_MKS;
+  } else if (pl->kind == IPG_PLUGIN_SPHERE) {
+    plug = IPG_PLUG_SPHERE;
+    met = IPG_METRIC_EMINKOWSKI;
+  } else {
+    snprintf(ctx->err, sizeof(ctx->err), "unknown model plugin %d", pl->kind);
+    return IPG_E_ARG;
+  }
+  if (g->metric != met) {
+    snprintf(ctx->err, sizeof(ctx->err), "model plugin %d needs metric %d, grid has %d", pl->kind, met, g->metric);
+    return IPG_E_ARG;
+  }
+  CK(cudaSetDevice(ctx->device));
+  ipg_grid gg = *g;
+  if (met != IPG_METRIC_FMKS) {
+    /* the FMKS jet-coordinate constants are unused; keep them finite */
+    gg.poly_xt = 1.;
+    gg.poly_alpha = 1.;
+    gg.poly_norm = 0.;
+    gg.mks_smooth = 0.;
+  }
+  devgrid_from(&gg, &ctx->dg);
+  DevPlug &d = ctx->dp;
+  memset(&d, 0, sizeof(d));
+  d.A = pl->A;
+  d.alpha = pl->alpha;
+  d.height = pl->height;
+  d.l0 = pl->l0;
+  d.freqcgs = pl->freqcgs;
+  d.rho_unit = pl->rho_unit;
+  d.R0 = pl->R0;
+  d.Ne0 = pl->Ne0;
+  d.Thetae0 = pl->Thetae0;
+  d.B0 = pl->B0;
+  ctx->plug = plug;
+  ctx->have_model = 1;
+  return IPG_OK;
+}
+
+static void devgrid_from(const ipg_grid *g, DevGrid *dp)
+{
+  DevGrid &d = *dp;
   memset(&d, 0, sizeof(d));
   d.n1 = g->n1;
   d.n2 = g->n2;
@@ -1036,8 +1080,6 @@ extern "C" int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *g, const double *c
   double am1 = g->poly_alpha - 1.;
   d.alpha_int = (am1 >= 0 && am1 <= 64 && am1 == (double)(int)am1) ? (int)am1 : -1;
   devgrid_derived(&d);
-  ctx->have_model = 1;
-  return IPG_OK;
 }
 
 /* The trajectory pool: 70% of the free device memory unless the caller asked
@@ -1147,18 +1189,19 @@ struct Batch {
   int wide;
 };
 
-static int launch_batch(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_pixel_out *d_out)
+template <int P>
+static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_pixel_out *d_out)
 {
   const int threads = 128;
   const int tg = b.wide ? 256 : threads, tx = b.wide ? IPG_XFER_WIDE : threads;
   CK(cudaEventRecord(b.ev[0], b.stream));
-  int gb = grid_blocks(ctx, (const void *)k_geodesic, tg, b.run);
-  k_geodesic<<<gb, tg, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev, b.chunk_meta, b.n_chunks, b.cnt,
-                                      ctx->d_rays, b.deferred);
+  int gb = grid_blocks(ctx, (const void *)k_geodesic<P>, tg, b.run);
+  k_geodesic<P><<<gb, tg, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev, b.chunk_meta, b.n_chunks,
+                                         b.cnt, ctx->d_rays, b.deferred);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[1], b.stream));
-  int cb = grid_blocks(ctx, (const void *)k_coeffs, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
-  k_coeffs<<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields);
+  int cb = grid_blocks(ctx, (const void *)k_coeffs<P>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
+  k_coeffs<P><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[2], b.stream));
   int tb = grid_blocks(ctx, (const void *)k_transfer, tx, b.run);
@@ -1166,6 +1209,16 @@ static int launch_batch(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_p
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[3], b.stream));
   return IPG_OK;
+}
+
+/* the model is fixed per context (ipg_upload_iharm / ipg_upload_plugin) */
+static int launch_batch(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_pixel_out *d_out)
+{
+  switch (ctx->plug) {
+    case IPG_PLUG_ANALYTIC: return launch_batch_t<IPG_PLUG_ANALYTIC>(ctx, b, d_ij, d_out);
+    case IPG_PLUG_SPHERE: return launch_batch_t<IPG_PLUG_SPHERE>(ctx, b, d_ij, d_out);
+    default: return launch_batch_t<IPG_PLUG_IHARM>(ctx, b, d_ij, d_out);
+  }
 }
 
 static void add_batch_stats(ipg_ctx *ctx, cudaEvent_t *ev, const unsigned long long *cnt)
@@ -1191,6 +1244,15 @@ static void add_batch_stats(ipg_ctx *ctx, cudaEvent_t *ev, const unsigned long l
  * predicted step shares; *nb = 0 means: do not split (the wave is small,
  * nothing is long, or the pool looks too small to hold the wave at once). */
 #define PRED_EPS_SCALE 16.
+
+template <int P>
+static void launch_count_t(ipg_ctx *ctx, int threads, const int32_t *d_ij, const int32_t *list, size_t run, int cap,
+                           unsigned long long *counter)
+{
+  int gb = grid_blocks(ctx, (const void *)k_geodesic_count<P>, threads, run);
+  k_geodesic_count<P><<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, PRED_EPS_SCALE, cap, ctx->d_pred,
+                                                       counter);
+}
 #define PRED_VERYLONG 4.
 #define PRED_LONG 2.
 #define SPLIT_MIN_RAYS 4096
@@ -1205,9 +1267,11 @@ static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, si
   int cap = (int)(cam->maxnstep / PRED_EPS_SCALE) + 1;
   if (cap > LEN_BUCKETS - 1) cap = LEN_BUCKETS - 1;
   CK(cudaEventRecord(ctx->ev_pred[0], ctx->stream));
-  int gb = grid_blocks(ctx, (const void *)k_geodesic_count, threads, run);
-  k_geodesic_count<<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, PRED_EPS_SCALE, cap, ctx->d_pred,
-                                                     cnt + CNT_NEXT_G);
+  switch (ctx->plug) {
+    case IPG_PLUG_ANALYTIC: launch_count_t<IPG_PLUG_ANALYTIC>(ctx, threads, d_ij, list, run, cap, cnt + CNT_NEXT_G); break;
+    case IPG_PLUG_SPHERE: launch_count_t<IPG_PLUG_SPHERE>(ctx, threads, d_ij, list, run, cap, cnt + CNT_NEXT_G); break;
+    default: launch_count_t<IPG_PLUG_IHARM>(ctx, threads, d_ij, list, run, cap, cnt + CNT_NEXT_G);
+  }
   CK(cudaGetLastError());
   CK(cudaMemsetAsync(ctx->d_len_hist, 0, LEN_BUCKETS * sizeof(int), ctx->stream));
   int sb = (int)((run + 255) / 256);
@@ -1260,9 +1324,10 @@ static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, si
 static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n, ipg_pixel_out *d_out)
 {
   if (!ctx->have_model) return IPG_E_STATE;
-  if (cam->emission_type != 4 && cam->emission_type != 1) {
-    snprintf(ctx->err, sizeof(ctx->err), "emission_type %d not supported (thermal types 1 and 4 only)",
-             cam->emission_type);
+  if (ctx->plug == IPG_PLUG_ANALYTIC ? cam->emission_type != 10
+                                     : (cam->emission_type != 4 && cam->emission_type != 1)) {
+    snprintf(ctx->err, sizeof(ctx->err), "emission_type %d not supported by this model (%s)", cam->emission_type,
+             ctx->plug == IPG_PLUG_ANALYTIC ? "its own coefficients, type 10, only" : "thermal types 1 and 4 only");
     return IPG_E_ARG;
   }
   if (cam->maxnstep < 2 || cam->nx <= 0 || cam->ny <= 0) return IPG_E_ARG;
@@ -1273,6 +1338,7 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
   DevCam dc;
   make_devcam(cam, &dc);
   CK(cudaMemcpyToSymbolAsync(c_grid, &ctx->dg, sizeof(DevGrid), 0, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyToSymbolAsync(c_plug, &ctx->dp, sizeof(DevPlug), 0, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyToSymbolAsync(c_cam, &dc, sizeof(DevCam), 0, cudaMemcpyHostToDevice, ctx->stream));
   memset(&ctx->stats, 0, sizeof(ctx->stats));
   /* Waves: every pending ray starts; rays that find the pool full are
@@ -1692,12 +1758,12 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
       NA_CK(cudaMemcpyAsync(cnt_d + CNT_DEFER, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
       NA_CK(cudaStreamSynchronize(stream));
     }
-    int gb = na_blocks(n_sm, (const void *)k_geodesic, threads, run);
-    k_geodesic<<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta, n_chunks, cnt_d, rays,
-                                           lists[cur ^ 1]);
+    int gb = na_blocks(n_sm, (const void *)k_geodesic<IPG_PLUG_IHARM>, threads, run);
+    k_geodesic<IPG_PLUG_IHARM><<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta,
+                                                           n_chunks, cnt_d, rays, lists[cur ^ 1]);
     NA_CK(cudaGetLastError());
-    int cb = na_blocks(n_sm, (const void *)k_coeffs, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
-    k_coeffs<<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
+    int cb = na_blocks(n_sm, (const void *)k_coeffs<IPG_PLUG_IHARM>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
+    k_coeffs<IPG_PLUG_IHARM><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
     NA_CK(cudaGetLastError());
     int tb = na_blocks(n_sm, (const void *)k_transfer, threads, run);
     k_transfer<<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev, rays, d_out, cnt_d);

@@ -14,8 +14,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
 
 
-def golden_names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+PLUGIN_PREFIXES = ("analytic_", "sphere_")
+
+
+def golden_names(plugins=True):
+    """Golden case names; plugins=False leaves out the known-answer models'
+    cases (which the C restatement of the iharm path does not cover)."""
+    names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    return names if plugins else [n for n in names if not n.startswith(PLUGIN_PREFIXES)]
 
 
 def load_golden(name):
@@ -31,7 +37,10 @@ class DumpCache:
         self.paths = {}
 
     def get(self, meta):
+        """The case's dump path, or None for a known-answer model (no dump)."""
         key = meta["dump"]
+        if meta.get("dump_shape_seed") is None:
+            return None
         if key not in self.paths:
             n1, n2, n3, seed = meta["dump_shape_seed"]
             path = os.path.join(self.root, f"dump_{key}.ipgc")
@@ -42,7 +51,8 @@ class DumpCache:
 
 
 def params_for(meta, dump_path, extra=()):
-    return ip.Params.from_args([f"--dump={dump_path}", *meta["args"], *extra])
+    head = [f"--dump={dump_path}"] if dump_path else []
+    return ip.Params.from_args([*head, *meta["args"], *extra])
 
 
 def oracle_tracer(orc, threads=8):

@@ -1,5 +1,10 @@
 """Generate the golden images used by the parity tests.
 
+Cases on a dump run the reference's iharm build; cases whose "dump" is the
+name of a known-answer model (analytic, sphere) run the reference built with
+that model (oracle/_ref/ipole_<model>, no dump; ``make -C oracle plugins``)
+and take their noise floor from its FMA build (ipole_<model>_fma).
+
 Each case runs the reference ipole itself (oracle/_ref/ipole_nofma: the
 reference sources built with -O2 -ffp-contract=off, see oracle/Makefile) on a
 seeded synthetic iharm FMKS dump and stores its image arrays in
@@ -55,6 +60,23 @@ CASES = {
 }
 
 
+# known-answer models: the reference test's parameters (tests/analytic/analytic.par,
+# tests/isothermal_sphere/info) at sizes the reference finishes in seconds
+ANALYTIC = ["--plugin=analytic", "--emission_type=10", "--rcam=1000", "--thetacam=60", "--phicam=0", "--dx=30",
+            "--dy=30", "--dsource=7778", "--freqcgs=230.e9", "--MBH=4.063e6"]
+SPHERE = ["--plugin=sphere", "--dsource=8000", "--fov=1200"]
+PLUGIN_CASES = {
+    **{f"analytic_m{m}_32": ("analytic", [*ANALYTIC, f"--model={m}", "--nx=32", "--ny=32"]) for m in range(1, 6)},
+    "sphere_f223_i90_32": ("sphere", [*SPHERE, "--freqcgs=223005000000.0", "--thetacam=90", "--nx=32", "--ny=32"]),
+    "sphere_f49_i90_32": ("sphere", [*SPHERE, "--freqcgs=49731200000.0", "--thetacam=90", "--nx=32", "--ny=32"]),
+    "sphere_f223_i30_32": ("sphere", [*SPHERE, "--freqcgs=223005000000.0", "--thetacam=30", "--nx=32", "--ny=32"]),
+    "sphere_pandya_24": ("sphere", [*SPHERE, "--freqcgs=106682000000.0", "--thetacam=60", "--emission_type=1",
+                                    "--nx=24", "--ny=24"]),
+}
+PLUGINS = ("analytic", "sphere")
+CASES.update(PLUGIN_CASES)
+
+
 def dump_path(name: str, tmpdir: str) -> tuple[str, str]:
     n1, n2, n3, seed = DUMPS[name]
     path = os.path.join(tmpdir, f"dump_{name}.ipgc")
@@ -64,9 +86,15 @@ def dump_path(name: str, tmpdir: str) -> tuple[str, str]:
 
 def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
     dname, extra = CASES[case]
-    dpath, dhash = dumps[dname]
     out = os.path.join(tmpdir, f"{case}.ipgc")
-    args = [f"--dump={dpath}", *BASE, *extra, f"--outfile={out}"]
+    if dname in PLUGINS:
+        binary = os.path.join(os.path.dirname(binary), f"ipole_{dname}")
+        base, dhash, others = [], None, (f"ipole_{dname}_fma",)
+        args = [*extra, f"--outfile={out}"]
+    else:
+        dpath, dhash = dumps[dname]
+        base, others = BASE, ("ipole", "ipole_o2fma", "ipole_v4", "ipole_ulp")
+        args = [f"--dump={dpath}", *BASE, *extra, f"--outfile={out}"]
     r = subprocess.run([binary, *args], capture_output=True, text=True, env=dict(os.environ, OMP_NUM_THREADS="8"))
     if r.returncode != 0:
         raise RuntimeError(f"{case}: reference exited {r.returncode}\n{r.stderr[-2000:]}")
@@ -81,7 +109,7 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
     # targets ref and noise), in the metrics the tests use
     from tests.common import image_errors
     floor, used = None, []
-    for other_bin in ("ipole", "ipole_o2fma", "ipole_v4", "ipole_ulp"):
+    for other_bin in others:
         path = os.path.join(os.path.dirname(binary), other_bin)
         if not os.path.exists(path):
             continue
@@ -98,10 +126,10 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
         e = image_errors(_Img, rec)
         floor = e if floor is None else {k: max(floor[k], e[k]) for k in e}
         used.append(other_bin)
-    meta = {"case": case, "dump": dname, "dump_shape_seed": DUMPS[dname], "dump_sha256": dhash,
-            "args": [*BASE, *extra], "Ftot_unpol": float(img["/Ftot_unpol"]),
+    meta = {"case": case, "dump": dname, "dump_shape_seed": DUMPS.get(dname), "dump_sha256": dhash,
+            "args": [*base, *extra], "Ftot_unpol": float(img["/Ftot_unpol"]),
             "Ftot": float(img["/Ftot"]) if "/Ftot" in img else None, "scale": float(img["/header/scale"]),
-            "generator": "oracle/_ref/ipole_nofma (reference sources, -O2 -ffp-contract=off)",
+            "generator": f"oracle/_ref/{os.path.basename(binary)} (reference sources, -O2 -ffp-contract=off)",
             "ref_noise_floor": floor, "ref_noise_builds": used}
     np.savez_compressed(os.path.join(HERE, f"{case}.npz"), meta=json.dumps(meta), **rec)
     print(case, "Ftot", meta["Ftot"], "Ftot_unpol", meta["Ftot_unpol"])
@@ -115,7 +143,7 @@ def main(cases):
         dumps = {}
         for c in cases:
             d = CASES[c][0]
-            if d not in dumps:
+            if d not in dumps and d not in PLUGINS:
                 dumps[d] = dump_path(d, td)
             make_case(c, binary, td, dumps)
 

@@ -1,0 +1,72 @@
+"""Known-answer models on the GPU (ipole_b200/csrc/ipg_plugins.cuh): the
+reference's own known answers, through the same ray kernels as the iharm
+path.
+
+  analytic  the five GRRT test problems of Gold et al. 2020 at the
+            parameters and size of the reference's tests/analytic/analytic.par,
+            against the published total fluxes with the reference test's own
+            2% tolerance (tests/analytic/analytic_test.py).
+  sphere    the isothermal sphere at the rows of
+            tests/isothermal_sphere/thermal.txt, run as its info file says
+            (80x80, fov 1200 muas, dsource 8 kpc).  The table was made by an
+            older ipole in plain Kerr-Schild coordinates; the reference
+            built here (eMinkowski) lands within 0.38% of it on every row
+            (Ftot_unpol about +0.25% throughout), and this build must land
+            within SPHERE_TOL = 1%.
+
+Image-level parity with the reference's builds of these models is in
+test_gpu_parity.py (golden cases analytic_* and sphere_*)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import ipole_b200 as ip
+from tests import common
+
+pytestmark = pytest.mark.gpu
+
+KA = json.load(open(os.path.join(common.GOLDEN, "known_answers.json")))
+SPHERE_TOL = 0.01
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = ip.Context()
+    yield c
+    c.close()
+
+
+def render(ctx, args):
+    p = ip.Params.from_args(args)
+    m = ip.Model.load(p)
+    ctx.upload(m)
+    return ctx.render(p, m)
+
+
+@pytest.mark.parametrize("idx", range(5))
+def test_analytic_published_flux(ctx, idx):
+    a = KA["analytic"]
+    model, pub = a["models"][idx], a["published_Ftot_unpol"][idx]
+    par = {k: v for k, v in a["par"].items() if k not in ("model", "quench_output")}
+    img = render(ctx, ["--plugin=analytic", *[f"--{k}={v}" for k, v in par.items()], f"--model={model}"])
+    f = img.totals()["Ftot_unpol"]
+    err = abs(f / pub - 1)
+    print(f"analytic model {model}: Ftot_unpol {f:.6g} Jy, published {pub}, relative error {err:.3%}")
+    assert err <= a["tolerance"]
+    assert np.all(img.oddflag == 0)
+
+
+ROWS = KA["sphere_thermal"]["rows"]
+
+
+@pytest.mark.parametrize("row", range(0, len(ROWS), 3))
+def test_sphere_thermal_table(ctx, row):
+    f, inc, ftot, funpol = ROWS[row]
+    img = render(ctx, ["--plugin=sphere", f"--freqcgs={f!r}", "--dsource=8000", f"--thetacam={inc!r}",
+                       "--maxnstep=1000000", "--nx=80", "--ny=80", "--fov=1200"])
+    t = img.totals()
+    e1, e2 = abs(t["Ftot"] / ftot - 1), abs(t["Ftot_unpol"] / funpol - 1)
+    print(f"sphere {f:.4g} Hz, i={inc}: Ftot {t['Ftot']:.6g} ({e1:.2%}), Ftot_unpol {t['Ftot_unpol']:.6g} ({e2:.2%})")
+    assert e1 <= SPHERE_TOL and e2 <= SPHERE_TOL
