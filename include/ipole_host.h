@@ -149,6 +149,14 @@ void ipg_image_totals(const ipg_image *img, const ipg_params *p, double tot[5]);
  * in ".ipgc". */
 int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p, const ipg_iharm_model *m);
 
+/* Check mode (-check, src/main.c:538-575): ipg_render_image traces every
+ * IPG_CHECK_SKIP-th pixel (i, j) and its mirror (nx - i - offset, j) and
+ * saves them at reduced indices; ipg_write_check then appends them to an
+ * existing image file as unpol/tau/pol _check and _recheck (dump_check,
+ * src/io.c:193-227).  Check mode needs nx_min = nx. */
+#define IPG_CHECK_SKIP 10
+int ipg_write_check(const char *fname, const ipg_image *img, const ipg_params *p);
+
 /* Copy a dump or image between the two file formats the library reads: HDF5
  * (the reference's format, src/hdf5_utils.c over libhdf5; this library reads
  * and writes the subset those files use without libhdf5) and the flat IPGC

@@ -65,7 +65,9 @@ int main(int argc, char *argv[])
   rc = ipg_render_image(ctx, &p, &m, &img, stderr);
   if (rc == IPG_OK) {
     ipg_print_image_stats(&img, &p, stderr);
-    if (!p.quench_output) {
+    if (!p.quench_output && p.perform_check) {
+      rc = ipg_write_check(p.outf, &img, &p);
+    } else if (!p.quench_output) {
       if (ipg_write_image(p.outf, &img, &p, &m) != IPG_OK) {
         fprintf(stderr, "could not write image file '%s'\n", p.outf);
         rc = IPG_E_IO;

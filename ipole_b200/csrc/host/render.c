@@ -147,12 +147,12 @@ static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p,
                   ipg_image *img, FILE *log);
 
 /* With a context, the levels run on the device (ipg_refine.cu); the host
- * loop below serves caller-supplied tracers and is the device driver's
- * bit-for-bit reference. */
+ * loop below serves caller-supplied tracers and check mode, and is the
+ * device driver's bit-for-bit reference. */
 int ipg_render_image(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, ipg_image *img, void *logp)
 {
   if (!ctx) return IPG_E_ARG;
-  return render(ctx_tracer, ctx, ctx, p, m, img, (FILE *)logp);
+  return render(ctx_tracer, ctx, p->perform_check ? NULL : ctx, p, m, img, (FILE *)logp);
 }
 
 int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const ipg_iharm_model *m, ipg_image *img,
@@ -167,10 +167,7 @@ static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p,
   if (!tracer || !p || !m || !img) return IPG_E_ARG;
   tracer_t tr = {tracer, user};
   memset(img, 0, sizeof(*img));
-  if (p->perform_check) {
-    if (log) fprintf(log, "-check (check/recheck output) is not supported by this build\n");
-    return IPG_E_ARG;
-  }
+  if (p->perform_check && log) fprintf(log, "Running in check mode...\n");
   if (p->nx_min < 0) {
     p->nx_min = p->nx;
     p->ny_min = p->ny;
@@ -264,6 +261,42 @@ static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p,
     free(ij);
     free(out);
     return IPG_E_NOMEM;
+  }
+
+  if (p->perform_check) {
+    /* check mode, main.c:538-575: every CHECK_SKIP-th pixel and its mirror
+     * in i, saved side by side at reduced indices (check, then recheck) */
+    if (refine_level > 1) {
+      if (log) fprintf(log, "check mode needs an unrefined image (nx_min = nx)\n");
+      free(ij);
+      free(out);
+      return IPG_E_ARG;
+    }
+    const size_t skip = IPG_CHECK_SKIP;
+    size_t offset = nx % skip;
+    if (offset == 0) offset = skip;
+    size_t n = 0;
+    for (size_t i = 0; i < nx; i++)
+      for (size_t j = 0; j < ny; j++) {
+        if (i % skip != 0 || j % skip != 0) continue;
+        ij[2 * n] = (int32_t)i;
+        ij[2 * n + 1] = (int32_t)j;
+        n++;
+        ij[2 * n] = (int32_t)(nx - i - offset);
+        ij[2 * n + 1] = (int32_t)j;
+        n++;
+      }
+    rc = trace_list(&tr, cam, ij, n, out, log);
+    if (rc == IPG_OK) ipg__report_oddities(p->only_unpolarized, ij, out, n, log);
+    for (size_t q = 0; rc == IPG_OK && q < n; q += 2) {
+      size_t i = (size_t)ij[2 * q], j = (size_t)ij[2 * q + 1], i2 = (size_t)ij[2 * q + 2];
+      rc = save_pixel(img, p, i / skip, j / skip, &out[q]);
+      if (rc == IPG_OK) rc = save_pixel(img, p, (nx / skip) + i2 / skip, j / skip, &out[q + 1]);
+    }
+    img->traced = n;
+    free(ij);
+    free(out);
+    return rc;
   }
 
   if (dev) {
@@ -538,6 +571,48 @@ int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p
     for (size_t i = 0; i < nx; i++)
       memcpy(buf + i * ny * NIMG, img->imageS + i * img->ny * NIMG, ny * NIMG * sizeof(double));
     ipgc_put_array_f64(&f, "/pol", 3, d3, buf);
+  }
+  free(buf);
+  int rc = ipgc_save(fname, &f) == 0 ? IPG_OK : IPG_E_IO;
+  if (rc) fprintf(stderr, "! %s\n", ipgc_error());
+  ipgc_free(&f);
+  return rc;
+}
+
+/* dump_check, src/io.c:193-227: appends the check and recheck blocks of a
+ * check-mode image (rows [0, nx/skip) and [nx/skip, 2 nx/skip), columns
+ * [0, ny/skip)) to an existing image file; without one it only says so. */
+int ipg_write_check(const char *fname, const ipg_image *img, const ipg_params *p)
+{
+  ipgc_file f;
+  if (ipgc_load(fname, &f) != 0) {
+    fprintf(stderr, "oh no :(\nno file to check.\n\n");
+    return IPG_OK;
+  }
+  const size_t skip = IPG_CHECK_SKIP, nx = (size_t)p->nx, ny = (size_t)p->ny, ld = img->ny;
+  const size_t fx = nx / skip, fy = ny / skip;
+  const int unpol = p->only_unpolarized;
+  double *buf = (double *)malloc((fx * fy * NIMG + 1) * sizeof(double));
+  uint64_t d2[2] = {fx, fy}, d3[3] = {fx, fy, NIMG};
+  for (int pass = 0; pass < 2; pass++) {
+    const size_t r0 = pass ? fx : 0;
+    const char *sfx = pass ? "recheck" : "check";
+    char name[32];
+    for (size_t i = 0; i < fx; i++)
+      for (size_t j = 0; j < fy; j++) buf[i * fy + j] = img->image[(r0 + i) * ld + j];
+    snprintf(name, sizeof(name), "/unpol_%s", sfx);
+    ipgc_put_array_f64(&f, name, 2, d2, buf);
+    for (size_t i = 0; i < fx; i++)
+      for (size_t j = 0; j < fy; j++) buf[i * fy + j] = img->taus[(r0 + i) * ld + j];
+    snprintf(name, sizeof(name), "/tau_%s", sfx);
+    ipgc_put_array_f64(&f, name, 2, d2, buf);
+    if (!unpol) {
+      for (size_t i = 0; i < fx; i++)
+        for (size_t j = 0; j < fy; j++)
+          for (int c = 0; c < NIMG; c++) buf[(i * fy + j) * NIMG + c] = img->imageS[((r0 + i) * ld + j) * NIMG + c];
+      snprintf(name, sizeof(name), "/pol_%s", sfx);
+      ipgc_put_array_f64(&f, name, 3, d3, buf);
+    }
   }
   free(buf);
   int rc = ipgc_save(fname, &f) == 0 ? IPG_OK : IPG_E_IO;

@@ -76,6 +76,23 @@ PLUGIN_CASES = {
 PLUGINS = ("analytic", "sphere")
 CASES.update(PLUGIN_CASES)
 
+# check mode (-check, src/main.c:538-575, src/io.c:193-227): the reference
+# writes the image, then a -check run appends the check/recheck blocks to it
+CHECK_CASES = {
+    "check_c1_48": ("c1", ["--M_unit=3e27", "--nx=48", "--ny=44"]),
+    "check_c1_unpol_40": ("c1", ["--M_unit=3e27", "-unpol", "--nx=40", "--ny=40"]),
+}
+CASES.update(CHECK_CASES)
+CHECK_KEYS = ("unpol", "tau", "pol")
+
+
+def run_checked(binary, args, out, env):
+    """the reference's check run: normal image first, then -check appends"""
+    r = subprocess.run([binary, *args], capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        return r
+    return subprocess.run([binary, *args, "-check"], capture_output=True, text=True, env=env)
+
 
 def dump_path(name: str, tmpdir: str) -> tuple[str, str]:
     n1, n2, n3, seed = DUMPS[name]
@@ -95,13 +112,24 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
         dpath, dhash = dumps[dname]
         base, others = BASE, ("ipole", "ipole_o2fma", "ipole_v4", "ipole_ulp")
         args = [f"--dump={dpath}", *BASE, *extra, f"--outfile={out}"]
-    r = subprocess.run([binary, *args], capture_output=True, text=True, env=dict(os.environ, OMP_NUM_THREADS="8"))
+    env = dict(os.environ, OMP_NUM_THREADS="8")
+    check = case in CHECK_CASES
+    r = run_checked(binary, args, out, env) if check else subprocess.run([binary, *args], capture_output=True,
+                                                                          text=True, env=env)
     if r.returncode != 0:
         raise RuntimeError(f"{case}: reference exited {r.returncode}\n{r.stderr[-2000:]}")
     img = ipgc.read(out)
+    if check:
+        # the check block is compared like an image; the recheck block rides along
+        img = {**img, "/unpol": img["/unpol_check"], "/tau": img["/tau_check"],
+               **({"/pol": img["/pol_check"]} if "/pol_check" in img else {})}
     rec = {"unpol": img["/unpol"], "tau": img["/tau"]}
     if "/pol" in img:
         rec["pol"] = img["/pol"]
+    if check:
+        for k in CHECK_KEYS:
+            if f"/{k}_recheck" in img:
+                rec[f"{k}_recheck"] = img[f"/{k}_recheck"]
     # the reference's own noise floor: the largest deviation from this
     # -ffp-contract=off build among the other legal builds of the same sources
     # (the makefile's -O3 FMA build, -O2 with FMA contraction, -O3 for
@@ -114,11 +142,14 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
         if not os.path.exists(path):
             continue
         out2 = os.path.join(tmpdir, f"{case}_{other_bin}.ipgc")
-        r = subprocess.run([path, *args[:-1], f"--outfile={out2}"], capture_output=True, text=True,
-                           env=dict(os.environ, OMP_NUM_THREADS="8"))
+        oargs = [*args[:-1], f"--outfile={out2}"]
+        r = run_checked(path, oargs, out2, env) if check else subprocess.run([path, *oargs], capture_output=True,
+                                                                             text=True, env=env)
         if r.returncode != 0:
             continue
         other = ipgc.read(out2)
+        if check:
+            other = {"/unpol": other["/unpol_check"], "/pol": other.get("/pol_check")}
 
         class _Img:
             unpol = other["/unpol"]
@@ -129,6 +160,7 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
     meta = {"case": case, "dump": dname, "dump_shape_seed": DUMPS.get(dname), "dump_sha256": dhash,
             "args": [*base, *extra], "Ftot_unpol": float(img["/Ftot_unpol"]),
             "Ftot": float(img["/Ftot"]) if "/Ftot" in img else None, "scale": float(img["/header/scale"]),
+            "check": check,
             "generator": f"oracle/_ref/{os.path.basename(binary)} (reference sources, -O2 -ffp-contract=off)",
             "ref_noise_floor": floor, "ref_noise_builds": used}
     np.savez_compressed(os.path.join(HERE, f"{case}.npz"), meta=json.dumps(meta), **rec)

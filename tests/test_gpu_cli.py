@@ -77,3 +77,33 @@ def test_cli_hdf5_dump_and_image(dumps, tmp_path):
             assert ia[k].dtype == ib[k].dtype and np.array_equal(ia[k], ib[k]), k
         else:
             assert ia[k] == ib[k], k
+
+
+@pytest.mark.parametrize("case", common.golden_names(check=True))
+def test_cli_check_mode(case, dumps, tmp_path):
+    """-check (src/main.c:538-575): every 10th pixel and its mirror in i,
+    appended to the existing image file as the _check / _recheck blocks
+    (src/io.c:193-227), against the reference's own check run."""
+    meta, arrs = common.load_golden(case)
+    out = str(tmp_path / "img.h5")
+    base = [f"--dump={dumps.get(meta)}", *meta["args"], f"--outfile={out}"]
+    r = run_cli([*base[:-1], f"--outfile={tmp_path}/none.h5", "-check"], str(tmp_path))
+    assert r.returncode == 0 and "no file to check" in r.stderr and not os.path.exists(tmp_path / "none.h5")
+    r = run_cli(base, str(tmp_path))
+    assert r.returncode == 0, r.stderr[-2000:]
+    r = run_cli([*base, "-check"], str(tmp_path))
+    assert r.returncode == 0 and "Running in check mode" in r.stderr, r.stderr[-2000:]
+    img = ipgc.read(out)
+    assert "/unpol" in img  # the original image stays
+    for blk, sfx in (("", "check"), ("_recheck", "recheck")):
+        class _Img:
+            unpol = img[f"/unpol_{sfx}"]
+            pol = img.get(f"/pol_{sfx}")
+        gold = {"unpol": arrs["unpol" + blk]}
+        if "pol" + blk in arrs:
+            gold["pol"] = arrs["pol" + blk]
+        e = common.image_errors(_Img, gold)
+        bad = {k: (e[k], common.tolerance(meta, k)) for k in e if k in common.BASE_TOL
+               and not e[k] <= common.tolerance(meta, k)}
+        assert not bad, (sfx, bad)
+        assert img[f"/tau_{sfx}"].shape == arrs["tau" + blk].shape
