@@ -132,6 +132,9 @@ typedef struct ipg_plugin {
   double A, alpha, height, l0, freqcgs, rho_unit;
   /* sphere: derived density, temperature and field (model/sphere/model.c:53-85) */
   double R0, Ne0, Thetae0, B0;
+  /* read by the trace output only: analytic B_unit; sphere get_model_sigma
+   * and get_model_beta inside the sphere (model/sphere/model.c:161-185) */
+  double B_unit, sigma0, beta0;
 } ipg_plugin;
 /* Upload a known-answer model; replaces any model of the context.  Returns
  * IPG_E_ARG for an unknown kind or a grid whose metric does not match it. */
@@ -187,6 +190,53 @@ int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *
 #define IPG_NOALLOC_SCRATCH_BYTES 27806720
 int ipg_trace_pixels_noalloc(const ipg_grid *grid, const double *d_fields, const ipg_camera *cam,
                              const int32_t *d_ij, size_t n, ipg_pixel_out *d_out, void *stream);
+
+/* ---- per-step trace of one ray (dump_var_along, src/io.c:279-543) ----
+ * Traces pixel (i, j) with the same kernels as the image and returns, for
+ * steps s = 0..nstep, one row of IPG_TRACE_DOUBLES doubles: the quantities
+ * the reference records along the ray, with its index conventions (rows 1
+ * .. nstep-1 filled, e2Transported one row down, I_unpol the intensity of
+ * the one step from s+1 to s).  steps holds max_steps rows (zero-filled by
+ * the call); returns IPG_E_ARG when the ray has more than max_steps - 1
+ * steps, IPG_E_MAXNSTEP when it hits maxnstep.  For an iharm model the
+ * primitives rho, u and beta come from ipg_upload_trace_fields (zero until
+ * it is called).  Columns: */
+#define IPG_TRACE_B 0           /* get_model_b */
+#define IPG_TRACE_NE 1          /* get_model_ne */
+#define IPG_TRACE_THETAE 2      /* get_model_thetae */
+#define IPG_TRACE_NU 3          /* get_fluid_nu */
+#define IPG_TRACE_BK_ANGLE 4    /* get_bk_angle */
+#define IPG_TRACE_SIGMA 5       /* get_model_sigma */
+#define IPG_TRACE_BETA 6        /* get_model_beta */
+#define IPG_TRACE_DL 7          /* traj[s].dl */
+#define IPG_TRACE_R 8           /* bl_coord r, th; X[3] */
+#define IPG_TRACE_TH 9
+#define IPG_TRACE_PHI 10
+#define IPG_TRACE_J_UNPOL 11    /* get_jkinv */
+#define IPG_TRACE_K_UNPOL 12
+#define IPG_TRACE_I_UNPOL 13
+#define IPG_TRACE_X 14          /* [4] X, Kcon */
+#define IPG_TRACE_KCON 18
+#define IPG_TRACE_J_INV 22      /* [4] jar_calc jI..jV, aI..aV, (0, rQ, rU, rV) */
+#define IPG_TRACE_ALPHA_INV 26
+#define IPG_TRACE_RHO_INV 30
+#define IPG_TRACE_STOKES 34     /* [4] I, Q, U, V of N in the plasma tetrad */
+#define IPG_TRACE_E2C 38        /* [4] e2Constructed, e2ConstructedCov, e2Transported, e2TransportedCov */
+#define IPG_TRACE_E2C_COV 42
+#define IPG_TRACE_E2T 46
+#define IPG_TRACE_E2T_COV 50
+#define IPG_TRACE_PRIMS 54      /* [8] get_model_primitives */
+#define IPG_TRACE_NTETRAD 62    /* [16] real parts of N_tetrad, N_coord; Econ, Ecov */
+#define IPG_TRACE_NCOORD 78
+#define IPG_TRACE_ECON 94
+#define IPG_TRACE_ECOV 110
+#define IPG_TRACE_FLAG 126      /* integrate_emission's flag of the step */
+#define IPG_TRACE_DOUBLES 127
+int ipg_trace_ray(ipg_ctx *ctx, const ipg_camera *cam, int i, int j, size_t max_steps, double *steps,
+                  int32_t *nstep);
+/* rho, u and beta per ghost-padded cell ([i][j][k], k fastest, as the
+ * fields of ipg_upload_iharm) for the trace's primitives and beta */
+int ipg_upload_trace_fields(ipg_ctx *ctx, const double *const extra[3]);
 
 /* Kernel statistics of the last trace call: total ray-steps of the geodesic
  * pass, steps inside the radiating region, number of kernel launches and

@@ -91,6 +91,7 @@ typedef struct ipg_iharm_model {
   double gam, game, gamp;
   void *fluid_header;          /* copy of the dump's /header group (for /fluid_header) */
   ipg_plugin plugin;           /* kind IPG_PLUGIN_IHARM, or a known-answer model (no fields) */
+  double *trace_fields[3];     /* rho, u, beta per ghost-padded cell (trace output; NULL for plugins) */
 } ipg_iharm_model;
 
 /* init_model: read the dump named in p->dump (an iharm v1 HDF5 dump, or the
@@ -156,6 +157,19 @@ int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p
  * src/io.c:193-227).  Check mode needs nx_min = nx. */
 #define IPG_CHECK_SKIP 10
 int ipg_write_check(const char *fname, const ipg_image *img, const ipg_params *p);
+
+/* Trace output (dump_var_along, src/io.c:279-543, for the pixels that
+ * src/main.c:865-879 selects): with p->trace set, every traced pixel (i, j)
+ * of the image with i and j multiples of trace_stride, or only (trace_i,
+ * trace_j) when both are >= 0, is traced again step by step
+ * (ipg_trace_ray) and written to p->trace_outf: the image header, "nstep"
+ * [nx'][ny'] and the per-step datasets [nx'][ny'][L](4)(4) of the
+ * reference (nx' = nx / trace_stride, or 1).  The step axis L is the longest
+ * traced ray's nstep + 1, where the reference's chunked datasets run to
+ * maxnstep (their entries past a ray's end are zero, as here).  An existing
+ * file keeps the pixels it holds.  "Flagged integration when tracing" lines
+ * go to stdout as in the reference. */
+int ipg_write_traces(ipg_ctx *ctx, const ipg_image *img, const ipg_params *p, const ipg_iharm_model *m);
 
 /* Copy a dump or image between the two file formats the library reads: HDF5
  * (the reference's format, src/hdf5_utils.c over libhdf5; this library reads

@@ -31,6 +31,15 @@ IPG_OK, IPG_E_ARG, IPG_E_CUDA, IPG_E_MAXNSTEP, IPG_E_NAN, IPG_E_TIMEOUT, IPG_E_N
     IPG_E_FORMAT = range(10)
 NFIELD = 10
 STRLEN = 2048
+# per-step trace columns (include/ipole_b200.h, IPG_TRACE_*)
+TRACE_DOUBLES = 127
+TRACE_COLS = {"b": (0, 1), "ne": (1, 1), "thetae": (2, 1), "nu": (3, 1), "b_k_angle": (4, 1), "sigma": (5, 1),
+              "beta": (6, 1), "dl": (7, 1), "r": (8, 1), "th": (9, 1), "phi": (10, 1), "j_unpol": (11, 1),
+              "k_unpol": (12, 1), "I_unpol": (13, 1), "X": (14, 4), "Kcon": (18, 4), "j_inv": (22, 4),
+              "alpha_inv": (26, 4), "rho_inv": (30, 4), "stokes": (34, 4), "e2Constructed": (38, 4),
+              "e2ConstructedCov": (42, 4), "e2Transported": (46, 4), "e2TransportedCov": (50, 4),
+              "prims": (54, 8), "ntetrad": (62, 16), "ncoord": (78, 16), "Econ": (94, 16), "Ecov": (110, 16),
+              "flag": (126, 1)}
 
 
 class IpgError(RuntimeError):
@@ -116,7 +125,8 @@ class Plugin(C.Structure):
     _fields_ = [("kind", C.c_int), ("model", C.c_int),
                 ("A", C.c_double), ("alpha", C.c_double), ("height", C.c_double), ("l0", C.c_double),
                 ("freqcgs", C.c_double), ("rho_unit", C.c_double),
-                ("R0", C.c_double), ("Ne0", C.c_double), ("Thetae0", C.c_double), ("B0", C.c_double)]
+                ("R0", C.c_double), ("Ne0", C.c_double), ("Thetae0", C.c_double), ("B0", C.c_double),
+                ("B_unit", C.c_double), ("sigma0", C.c_double), ("beta0", C.c_double)]
 
 
 class _Model(C.Structure):
@@ -126,7 +136,7 @@ class _Model(C.Structure):
                 ("Mdot_dump", C.c_double), ("MdotEdd_dump", C.c_double), ("Ladv_dump", C.c_double),
                 ("t", C.c_double), ("DTd", C.c_double), ("electrons", C.c_int),
                 ("gam", C.c_double), ("game", C.c_double), ("gamp", C.c_double), ("fluid_header", C.c_void_p),
-                ("plugin", Plugin)]
+                ("plugin", Plugin), ("trace_fields", C.POINTER(C.c_double) * 3)]
 
 
 class _Image(C.Structure):
@@ -164,6 +174,10 @@ def lib():
     L.ipg_upload_iharm.argtypes = [C.c_void_p, C.POINTER(Grid), C.POINTER(C.POINTER(C.c_double))]
     L.ipg_upload_plugin.argtypes = [C.c_void_p, C.POINTER(Grid), C.POINTER(Plugin)]
     L.ipg_upload_model.argtypes = [C.c_void_p, C.POINTER(_Model)]
+    L.ipg_upload_trace_fields.argtypes = [C.c_void_p, C.POINTER(C.POINTER(C.c_double))]
+    L.ipg_trace_ray.argtypes = [C.c_void_p, C.POINTER(Camera), C.c_int, C.c_int, C.c_size_t, C.c_void_p,
+                                C.POINTER(C.c_int32)]
+    L.ipg_write_traces.argtypes = [C.c_void_p, C.POINTER(_Image), C.POINTER(_Params), C.POINTER(_Model)]
     L.ipg_trace_pixels.argtypes = [C.c_void_p, C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p]
     L.ipg_trace_pixels_device.argtypes = [C.c_void_p, C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p,
                                           C.c_void_p]
@@ -371,6 +385,21 @@ class Context:
         if not (allow_maxnstep and rc == IPG_E_MAXNSTEP):
             _check(rc, self._h)
         return out
+
+    def trace_ray(self, cam: Camera, i: int, j: int, model: "Model" = None, max_steps: int = 50001):
+        """Per-step trace of pixel (i, j) (ipg_trace_ray): (nstep, rows), rows
+        an (nstep + 1, TRACE_DOUBLES) array in the IPG_TRACE_* column
+        layout.  With an iharm model, its rho, u and beta are uploaded first
+        so the primitives and beta columns are filled."""
+        L = lib()
+        if model is not None and model._m.plugin.kind == 0 and model._m.trace_fields[0]:
+            ptrs = (C.POINTER(C.c_double) * 3)(*[model._m.trace_fields[k] for k in range(3)])
+            _check(L.ipg_upload_trace_fields(self._h, ptrs), self._h)
+        buf = np.zeros((max_steps, TRACE_DOUBLES))
+        n = C.c_int32(0)
+        _check(L.ipg_trace_ray(self._h, C.byref(cam), int(i), int(j), max_steps, buf.ctypes.data, C.byref(n)),
+               self._h)
+        return int(n.value), buf[:n.value + 1].copy()
 
     def trace_device(self, cam: Camera, d_ij_ptr: int, n: int, d_out_ptr: int, stream: int = 0):
         """ipg_trace_pixels_device on device pointers (e.g. torch tensors' data_ptr())."""

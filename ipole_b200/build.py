@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-v"]
 CC_FLAGS = ["-std=gnu99", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-result"]
 CU_EXTRA = ["ipg_refine.cu"]
-HOST_SRC = ["ipgc.c", "h5lite.c", "plugins.c", "coords.c", "par.c", "model_iharm.c", "camera.c", "render.c"]
+HOST_SRC = ["ipgc.c", "h5lite.c", "plugins.c", "trace.c", "coords.c", "par.c", "model_iharm.c", "camera.c", "render.c"]
 
 
 def _nvcc() -> str:

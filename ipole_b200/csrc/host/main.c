@@ -63,6 +63,10 @@ int main(int argc, char *argv[])
 
   ipg_image img;
   rc = ipg_render_image(ctx, &p, &m, &img, stderr);
+  if (rc == IPG_OK && p.trace && !p.perform_check) {
+    rc = ipg_write_traces(ctx, &img, &p, &m);
+    if (rc) fprintf(stderr, "trace output failed: %s (%s)\n", ipg_strerror(rc), ipg_last_error(ctx));
+  }
   if (rc == IPG_OK) {
     ipg_print_image_stats(&img, &p, stderr);
     if (!p.quench_output && p.perform_check) {

@@ -102,6 +102,10 @@ void ipg_iharm_free(ipg_iharm_model *m)
     free(m->fields[f]);
     m->fields[f] = NULL;
   }
+  for (int f = 0; f < 3; f++) {
+    free(m->trace_fields[f]);
+    m->trace_fields[f] = NULL;
+  }
   if (m->fluid_header) {
     ipgc_free((ipgc_file *)m->fluid_header);
     free(m->fluid_header);
@@ -363,6 +367,16 @@ int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m)
     m->fields[IPG_F_B][c] = bb;
     m->fields[IPG_F_THETAE][c] = thetae;
     m->fields[IPG_F_SIGMA][c] = fmax(sigma_m, IPG_SMALL);
+  }
+  /* rho, u and beta for the trace output (fmax(beta, SMALL), model/iharm/model.c:700) */
+  m->trace_fields[0] = f.p[KRHO];
+  m->trace_fields[1] = f.p[UU];
+  f.p[KRHO] = f.p[UU] = NULL;
+  m->trace_fields[2] = (double *)malloc(ncell * sizeof(double));
+  for (size_t c = 0; c < ncell; c++) {
+    double bsq = f.b[c] * rf / m->B_unit;
+    bsq = bsq * bsq;
+    m->trace_fields[2][c] = fmax(m->trace_fields[1][c] * (gam - 1.) / 0.5 / bsq, IPG_SMALL);
   }
   for (int l = 0; l < NPRIM_STORE; l++) free(f.p[l]);
   free(f.b);

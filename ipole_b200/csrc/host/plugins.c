@@ -41,6 +41,7 @@ static void analytic_init(const ipg_params *p, ipg_iharm_model *m)
   m->B_unit = IPG_CL * sqrt(4. * M_PI * m->RHO_unit);
   m->M_unit = 0.;
   pl->rho_unit = m->RHO_unit;
+  pl->B_unit = m->B_unit;
   memset(g, 0, sizeof(*g));
   g->metric = IPG_METRIC_MKS;
   g->hslope = 1.0;
@@ -84,6 +85,8 @@ static void sphere_init(const ipg_params *p, ipg_iharm_model *m)
   double THETAE_UNIT = IPG_MP / IPG_ME * (gam - 1.) / (1. + p->tp_over_te);
   pl->B0 = IPG_CL * sqrt(8 * M_PI * (gam - 1.) * (IPG_MP + IPG_ME) / p->sphere_beta0) * sqrt(pl->Ne0 * pl->Thetae0) /
            sqrt(THETAE_UNIT);
+  pl->sigma0 = pl->Thetae0 * p->tp_over_te / p->sphere_beta0;
+  pl->beta0 = p->sphere_beta0;
   fprintf(stderr, "Running with isothermal sphere model.\n");
   fprintf(stderr, "MBH, L_unit: %g [Msun], %g\n", MBH / IPG_MSUN, m->L_unit);
   fprintf(stderr, "Ne, Thetae, B: %g %g %g\n", pl->Ne0, pl->Thetae0, pl->B0);

@@ -505,9 +505,11 @@ void ipg_print_image_stats(const ipg_image *img, const ipg_params *p, void *logp
 
 /* dump (src/io.c:229-273) + write_header (:140-191) + output_hdf5
  * (model/iharm/model.c:1254-1301) */
-int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p, const ipg_iharm_model *m)
+/* write_header, src/io.c:140-191 (the image file and the trace file) */
+void ipg__write_header(void *fp, const ipg_image *img, const ipg_params *p)
 {
-  ipgc_file f = {0};
+  ipgc_file *fh = (ipgc_file *)fp;
+#define f (*fh)
   ipgc_put_str(&f, "/@githash", "b200", 20);
   ipgc_put_group(&f, "/header");
   ipgc_put_str(&f, "/header/version", IPG_VERSION_STRING, 20);
@@ -533,6 +535,13 @@ int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p
   ipgc_put_f64(&f, "/header/camera/yoff", p->yoff);
   uint64_t d4 = 4;
   ipgc_put_array_f64(&f, "/header/camera/x", 1, &d4, img->Xcam);
+#undef f
+}
+
+int ipg_write_image(const char *fname, const ipg_image *img, const ipg_params *p, const ipg_iharm_model *m)
+{
+  ipgc_file f = {0};
+  ipg__write_header(&f, img, p);
   if (m && m->plugin.kind != IPG_PLUGIN_IHARM) {
     ipg__plugin_write_header(&f, m);
   } else if (m) {

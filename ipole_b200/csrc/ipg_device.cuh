@@ -52,6 +52,7 @@
 #define REC_XH1 40
 #define REC_XH2 41
 #define REC_NTURNS 42
+#define REC_X0 43    /* X^0 (trace output only; k_coeffs overwrites it) */
 #define REC_KH 44
 #define REC_FLAGS 32 /* bit 0 radiating, bit 1 counterjet cut, bits 2.. oddflag of the point */
 #define REC_JU 33    /* unpolarized j_I / nu^2 and alpha_I (get_jkinv) */

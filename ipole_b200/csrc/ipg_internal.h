@@ -53,6 +53,7 @@ int ipg__render_levels_device(ipg_ctx *ctx, const ipg_camera *cam, const ipg_ref
 /* ---- provided by host/plugins.c ---- */
 struct ipg_params;
 struct ipg_iharm_model;
+struct ipg_image;
 /* the known-answer models' init_model; returns 1 (and *rc) when p->plugin
  * names one of them (or an unknown plugin), 0 for iharm */
 int ipg__plugin_load(const struct ipg_params *p, struct ipg_iharm_model *m, int *rc);
@@ -60,6 +61,8 @@ int ipg__plugin_load(const struct ipg_params *p, struct ipg_iharm_model *m, int 
 void ipg__plugin_write_header(void *ipgc_file_ptr, const struct ipg_iharm_model *m);
 
 /* ---- provided by host/render.c ---- */
+/* write_header (src/io.c:140-191) into an ipgc_file */
+void ipg__write_header(void *ipgc_file_ptr, const struct ipg_image *img, const struct ipg_params *p);
 /* the oddity lines of get_pixel (src/main.c:852-869) for a traced list */
 void ipg__report_oddities(int only_unpolarized, const int32_t *ij, const ipg_pixel_out *o, size_t n, FILE *log);
 

@@ -115,14 +115,15 @@ __device__ __forceinline__ void accel_from_A(const double A[4][4], const double 
   for (int k = 0; k < 4; k++) acc[k] = A[k][0] * K[0] + A[k][1] * K[1] + A[k][2] * K[2] + A[k][3] * K[3];
 }
 
-/* Geodesic state of a record.  X0 and Xh3 never enter the fast-light
- * computation and are not kept. */
+/* Geodesic state of a record.  Xh3 never enters the fast-light computation
+ * and is not kept; X0 rides in the slot after nturns (read only by the
+ * trace output, before k_coeffs reuses the slot). */
 __device__ __forceinline__ void store_geo(double *p, const double X[4], const double K[4], const double Xh[4],
                                           const double Kh[4], double dl, double nturns)
 {
   store4(p + REC_X1, X[1], X[2], X[3], dl);
   store4(p + REC_K, K[0], K[1], K[2], K[3]);
-  store4(p + REC_XH1, Xh[1], Xh[2], nturns, 0.);
+  store4(p + REC_XH1, Xh[1], Xh[2], nturns, X[0]); /* X0: for the trace output only */
   store4(p + REC_KH, Kh[0], Kh[1], Kh[2], Kh[3]);
 }
 
@@ -868,6 +869,7 @@ struct ipg_ctx {
   int n_sm;
   ipg_stats stats;
   void *refine; /* buffers of the on-device image driver (ipg_refine.cu) */
+  double *d_trace_extra; /* rho, u, beta per cell for the trace output (ipg_upload_trace_fields) */
   char err[512];
 };
 
@@ -946,6 +948,7 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   ipg__refine_release(ctx->refine);
+  cudaFree(ctx->d_trace_extra);
   cudaFree(ctx->d_fields);
   cudaFree(ctx->d_pool);
   cudaFree(ctx->d_chunk_prev);
@@ -990,6 +993,8 @@ extern "C" int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *g, const double *c
     cudaFree(ctx->d_fields);
     ctx->d_fields = NULL;
   }
+  cudaFree(ctx->d_trace_extra); /* belongs to the previous dump */
+  ctx->d_trace_extra = NULL;
   if (!ctx->d_fields) CK(cudaMalloc(&ctx->d_fields, ncell * IPG_NFIELD * sizeof(double)));
   CK(cudaMemcpy(ctx->d_fields, aos.data(), ncell * IPG_NFIELD * sizeof(double), cudaMemcpyHostToDevice));
   ctx->ncell = ncell;
@@ -1042,6 +1047,9 @@ extern "C" int ipg_upload_plugin(ipg_ctx *ctx, const ipg_grid *g, const ipg_plug
   d.Ne0 = pl->Ne0;
   d.Thetae0 = pl->Thetae0;
   d.B0 = pl->B0;
+  d.b_unit = pl->B_unit;
+  d.sigma0 = pl->sigma0;
+  d.beta0 = pl->beta0;
   ctx->plug = plug;
   ctx->have_model = 1;
   return IPG_OK;
@@ -1790,3 +1798,6 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
   NA_CK(cudaStreamSynchronize(stream));
   return n_maxn ? IPG_E_MAXNSTEP : IPG_OK;
 }
+
+/* per-step trace of single rays (dump_var_along) */
+#include "ipg_trace.cuh"

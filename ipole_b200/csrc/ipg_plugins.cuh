@@ -29,6 +29,8 @@ struct DevPlug {
   double A, alpha, height, l0, freqcgs, rho_unit;
   /* sphere (model/sphere/model.c:19-35, 53-85) */
   double R0, Ne0, Thetae0, B0;
+  /* trace output only: analytic B_unit; sphere sigma and beta (model/sphere/model.c:161-185) */
+  double b_unit, sigma0, beta0;
 };
 __constant__ DevPlug c_plug;
 
@@ -133,7 +135,10 @@ __device__ __forceinline__ void model_point_t(const double *__restrict__ fields,
     analytic_fourv(pg, mp->Ucon, mp->Ucov, mp->Bcon, mp->Bcov);
     mp->ne = analytic_ne(pg);
     mp->thetae = 0.;
-    mp->bmag = 0.;
+    /* get_model_b, model/analytic/model.c:300-308 (not used by its coefficients) */
+    mp->bmag = sqrt(mp->Bcon[0] * mp->Bcov[0] + mp->Bcon[1] * mp->Bcov[1] + mp->Bcon[2] * mp->Bcov[2] +
+                    mp->Bcon[3] * mp->Bcov[3]) *
+               c_plug.b_unit;
   } else {
     /* model/sphere/model.c:124-197: fluid at rest, poloidal field */
     mp->geo = pg;

@@ -16,17 +16,20 @@ GOLDEN = os.path.join(HERE, "golden")
 
 PLUGIN_PREFIXES = ("analytic_", "sphere_")
 CHECK_PREFIX = "check_"
+TRACE_PREFIX = "trace_"
 
 
-def golden_names(plugins=True, check=False):
+def golden_names(plugins=True, check=False, trace=False):
     """Golden image cases; plugins=False leaves out the known-answer models'
     cases (which the C restatement of the iharm path does not cover),
     check=True gives the check-mode cases instead (their arrays are the
-    check/recheck blocks, not an image)."""
+    check/recheck blocks, not an image), trace=True the per-step traces."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
     if check:
         return [n for n in names if n.startswith(CHECK_PREFIX)]
-    names = [n for n in names if not n.startswith(CHECK_PREFIX)]
+    if trace:
+        return [n for n in names if n.startswith(TRACE_PREFIX)]
+    names = [n for n in names if not n.startswith((CHECK_PREFIX, TRACE_PREFIX))]
     return names if plugins else [n for n in names if not n.startswith(PLUGIN_PREFIXES)]
 
 

@@ -85,6 +85,57 @@ CHECK_CASES = {
 CASES.update(CHECK_CASES)
 CHECK_KEYS = ("unpol", "tau", "pol")
 
+# trace output (dump_var_along, src/io.c:279-543) of one pixel; the arrays
+# kept are the ray's rows 0..nstep of each per-step dataset
+TRACE_CASES = {
+    "trace_c1_32_p14_17": ("c1", ["--M_unit=3e27", "--nx=32", "--ny=32", "--trace=1", "--trace_i=14",
+                                  "--trace_j=17"]),
+    "trace_c1_unpol_24_p11_12": ("c1", ["--M_unit=3e27", "-unpol", "--nx=24", "--ny=24", "--trace=1",
+                                        "--trace_i=11", "--trace_j=12"]),
+}
+CASES.update(TRACE_CASES)
+
+
+def make_trace_case(case, binary, tmpdir, dumps):
+    dname, extra = CASES[case]
+    dpath, dhash = dumps[dname]
+    env = dict(os.environ, OMP_NUM_THREADS="8")
+
+    def run(bin_name):
+        tr = os.path.join(tmpdir, f"{case}_{bin_name}_trace.ipgc")
+        out = os.path.join(tmpdir, f"{case}_{bin_name}.ipgc")
+        if os.path.exists(tr):
+            os.remove(tr)
+        r = subprocess.run([os.path.join(os.path.dirname(binary), bin_name), f"--dump={dpath}", *BASE, *extra,
+                            f"--trace_outf={tr}", f"--outfile={out}"], capture_output=True, text=True, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"{case}: {bin_name} exited {r.returncode}\n{r.stderr[-2000:]}")
+        t = ipgc.read(tr)
+        n = int(t["/nstep"][0, 0])
+        return n, {k[1:]: v[0, 0, :n + 1] for k, v in t.items() if isinstance(v, np.ndarray) and v.ndim >= 3}
+
+    n, rec = run("ipole_nofma")
+    # per dataset: the largest deviation of the other builds, relative to the
+    # dataset's largest magnitude along the ray
+    floor, used = {}, []
+    for other in ("ipole", "ipole_o2fma", "ipole_v4", "ipole_ulp"):
+        if not os.path.exists(os.path.join(os.path.dirname(binary), other)):
+            continue
+        n2, rec2 = run(other)
+        if n2 != n:
+            floor["nstep_differs"] = 1.0
+            continue
+        for k, v in rec.items():
+            sc = float(np.max(np.abs(v))) or 1.0
+            floor[k] = max(floor.get(k, 0.0), float(np.max(np.abs(rec2[k] - v))) / sc)
+        used.append(other)
+    meta = {"case": case, "dump": dname, "dump_shape_seed": DUMPS[dname], "dump_sha256": dhash,
+            "args": [*BASE, *extra], "nstep": n, "trace": True,
+            "generator": "oracle/_ref/ipole_nofma (reference sources, -O2 -ffp-contract=off)",
+            "ref_noise_floor": floor, "ref_noise_builds": used}
+    np.savez_compressed(os.path.join(HERE, f"{case}.npz"), meta=json.dumps(meta), **rec)
+    print(case, "nstep", n, "floor", {k: f"{v:.1e}" for k, v in floor.items()})
+
 
 def run_checked(binary, args, out, env):
     """the reference's check run: normal image first, then -check appends"""
@@ -177,7 +228,10 @@ def main(cases):
             d = CASES[c][0]
             if d not in dumps and d not in PLUGINS:
                 dumps[d] = dump_path(d, td)
-            make_case(c, binary, td, dumps)
+            if c in TRACE_CASES:
+                make_trace_case(c, binary, td, dumps)
+            else:
+                make_case(c, binary, td, dumps)
 
 
 if __name__ == "__main__":
