@@ -243,8 +243,8 @@ __device__ __forceinline__ void count_turns(GeoLane &L)
  * holds one copy of it, which keeps the loop body small: a lone ray's step
  * time is set by instruction-fetch and dependency latency, not by the FP64
  * throughput of the SM. */
-template <int P>
-__global__ void __launch_bounds__(256, IPG_GEO_MINB)
+template <int P, int TPB = 256, int MINB = IPG_GEO_MINB>
+__global__ void __launch_bounds__(TPB, MINB)
     k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list,
                double *__restrict__ pool, int *__restrict__ chunk_prev, int2 *__restrict__ chunk_meta,
                long long n_chunks, unsigned long long *__restrict__ counters, RayRec *__restrict__ rays,
@@ -656,7 +656,8 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
   }
 }
 
-__global__ void __launch_bounds__(IPG_XFER_WIDE, IPG_XFER_MINB)
+template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB>
+__global__ void __launch_bounds__(TPB, MINB)
     k_transfer(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
                const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays, ipg_pixel_out *__restrict__ out,
                unsigned long long *__restrict__ counters)
@@ -1201,19 +1202,33 @@ template <int P>
 static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_pixel_out *d_out)
 {
   const int threads = 128;
-  const int tg = b.wide ? 256 : threads, tx = b.wide ? IPG_XFER_WIDE : threads;
   CK(cudaEventRecord(b.ev[0], b.stream));
-  int gb = grid_blocks(ctx, (const void *)k_geodesic<P>, tg, b.run);
-  k_geodesic<P><<<gb, tg, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev, b.chunk_meta, b.n_chunks,
-                                         b.cnt, ctx->d_rays, b.deferred);
+  if (b.wide) {
+    int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 256, IPG_GEO_MINB>, 256, b.run);
+    k_geodesic<P, 256, IPG_GEO_MINB><<<gb, 256, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev,
+                                                                b.chunk_meta, b.n_chunks, b.cnt, ctx->d_rays,
+                                                                b.deferred);
+  } else {
+    int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 128, IPG_GEO_MINB_BULK>, threads, b.run);
+    k_geodesic<P, 128, IPG_GEO_MINB_BULK><<<gb, threads, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool,
+                                                                        b.chunk_prev, b.chunk_meta, b.n_chunks,
+                                                                        b.cnt, ctx->d_rays, b.deferred);
+  }
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[1], b.stream));
   int cb = grid_blocks(ctx, (const void *)k_coeffs<P>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
   k_coeffs<P><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[2], b.stream));
-  int tb = grid_blocks(ctx, (const void *)k_transfer, tx, b.run);
-  k_transfer<<<tb, tx, 0, b.stream>>>(b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);
+  if (b.wide) {
+    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB>, IPG_XFER_WIDE, b.run);
+    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB><<<tb, IPG_XFER_WIDE, 0, b.stream>>>(
+        b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);
+  } else {
+    int tb = grid_blocks(ctx, (const void *)k_transfer<128, IPG_XFER_MINB_BULK>, threads, b.run);
+    k_transfer<128, IPG_XFER_MINB_BULK><<<tb, threads, 0, b.stream>>>(b.list, (int)b.run, b.pool, b.chunk_prev,
+                                                                     ctx->d_rays, d_out, b.cnt);
+  }
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[3], b.stream));
   return IPG_OK;
@@ -1261,8 +1276,12 @@ static void launch_count_t(ipg_ctx *ctx, int threads, const int32_t *d_ij, const
   k_geodesic_count<P><<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, PRED_EPS_SCALE, cap, ctx->d_pred,
                                                        counter);
 }
+#ifndef PRED_VERYLONG
 #define PRED_VERYLONG 4.
+#endif
+#ifndef PRED_LONG
 #define PRED_LONG 2.
+#endif
 #define SPLIT_MIN_RAYS 4096
 
 static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, size_t run, const ipg_camera *cam,
@@ -1766,15 +1785,15 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
       NA_CK(cudaMemcpyAsync(cnt_d + CNT_DEFER, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
       NA_CK(cudaStreamSynchronize(stream));
     }
-    int gb = na_blocks(n_sm, (const void *)k_geodesic<IPG_PLUG_IHARM>, threads, run);
-    k_geodesic<IPG_PLUG_IHARM><<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta,
+    int gb = na_blocks(n_sm, (const void *)k_geodesic<IPG_PLUG_IHARM, 128, IPG_GEO_MINB_BULK>, threads, run);
+    k_geodesic<IPG_PLUG_IHARM, 128, IPG_GEO_MINB_BULK><<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta,
                                                            n_chunks, cnt_d, rays, lists[cur ^ 1]);
     NA_CK(cudaGetLastError());
     int cb = na_blocks(n_sm, (const void *)k_coeffs<IPG_PLUG_IHARM>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
     k_coeffs<IPG_PLUG_IHARM><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
     NA_CK(cudaGetLastError());
-    int tb = na_blocks(n_sm, (const void *)k_transfer, threads, run);
-    k_transfer<<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev, rays, d_out, cnt_d);
+    int tb = na_blocks(n_sm, (const void *)k_transfer<128, IPG_XFER_MINB_BULK>, threads, run);
+    k_transfer<128, IPG_XFER_MINB_BULK><<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev, rays, d_out, cnt_d);
     NA_CK(cudaGetLastError());
     unsigned long long cnt[CNT_N];
     NA_CK(cudaMemcpyAsync(cnt, cnt_d, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
