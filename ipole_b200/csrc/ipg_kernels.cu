@@ -256,6 +256,82 @@ __global__ void __launch_bounds__(TPB, MINB)
   const int track = C.target_nturns >= 0;
   GeoLane L;
   bool has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+#ifdef IPG_GEO_FULLSTEP
+  /* One iteration is one whole midpoint step.  The second connection is
+   * taken at Xhalf = X + h K / 2, which needs only the step size, not the
+   * first connection: the two connections are independent chains, evaluated
+   * side by side; only their contractions with K and Khalf are sequential. */
+  while (__any_sync(0xffffffffu, has)) {
+    if (!has) continue;
+    /* stop_backward_integration, src/model_geodesics.c:218-254, and the step
+     * limit of trace_geodesic's loop (:71) */
+    double r = geo_r<PlugT<P>::MET>(L.X[1]);
+    if ((r > G.rmax_geo && L.K[1] < 0.) || r < (G.Rh + 0.0001) || !(L.nstep < C.maxnstep - 1)) {
+      int status = (L.nstep >= C.maxnstep - 1) ? IPG_RAY_MAXNSTEP : IPG_RAY_OK;
+      if (status == IPG_RAY_OK && pol && L.nstep != 0) {
+        /* the walk back starts at the last point: its Gamma(X) K too */
+        Conn cn;
+        double A[4][4];
+        fd_connection<PlugT<P>::MET>(L.X[1], L.X[2], &cn);
+        transport_matrix(cn, L.K, A);
+        store_A(L.prev + REC_A1, A);
+      }
+      RayRec rec = {L.chunk, L.nstep, status, 0};
+      rays[L.ray] = rec;
+      atomicAdd(&counters[CNT_STEPS], (unsigned long long)L.nstep);
+      has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+      continue;
+    }
+    L.nstep++;
+    L.h = -stepsize(L.X, L.K, C.eps);
+#pragma unroll
+    for (int k = 0; k < 4; k++) L.Xh[k] = L.X[k] + 0.5 * L.h * L.K[k];
+    Conn c0, c1;
+    fd_connection<PlugT<P>::MET>(L.X[1], L.X[2], &c0);
+    fd_connection<PlugT<P>::MET>(L.Xh[1], L.Xh[2], &c1);
+    double acc[4], A[4][4];
+    if (pol) {
+      transport_matrix(c0, L.K, A);
+      accel_from_A(A, L.K, acc);
+      store_A(L.prev + REC_A1, A);
+    } else {
+      geo_accel(c0, L.K, acc);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) L.Kh[k] = L.K[k] - 0.5 * L.h * acc[k];
+    if (pol) {
+      transport_matrix(c1, L.Kh, A);
+      accel_from_A(A, L.Kh, acc);
+    } else {
+      geo_accel(c1, L.Kh, acc);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      L.K[k] = L.K[k] - L.h * acc[k];
+      L.X[k] = L.X[k] + L.h * L.Kh[k];
+    }
+    double dl = -L.h;
+    double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
+    if (track) count_turns<PlugT<P>::MET>(L);
+    int slot = L.nstep % IPG_CHUNK_STEPS;
+    if (slot == 0) {
+      long long nc = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
+      if (nc >= n_chunks) {
+        RayRec rec = {L.chunk, L.nstep, IPG_RAY_POOL_FULL, 0};
+        rays[L.ray] = rec;
+        deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = L.ray;
+        has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+        continue;
+      }
+      chunk_prev[(int)nc] = L.chunk;
+      chunk_meta[(int)nc] = make_int2(L.ray, L.nstep);
+      L.chunk = (int)nc;
+    }
+    L.prev = step_ptr(pool, L.chunk, slot);
+    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
+    if (pol) store_A(L.prev + REC_A2, A); /* Gamma(Xh_n) Kh_n */
+  }
+#else
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
     const int ph = L.phase;
@@ -335,6 +411,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
     if (pol) store_A(L.prev + REC_A2, A); /* Gamma(Xh_n) Kh_n */
   }
+#endif
 }
 
 
