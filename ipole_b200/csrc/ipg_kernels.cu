@@ -914,7 +914,14 @@ static void devgrid_derived(DevGrid *d)
   d->inv_lx2 = 1. / (d->cstopx[2] - d->cstartx[2]);
 }
 
-#define NB_MAX 3 /* length classes of a split wave */
+/* Length classes of a split wave: rays predicted at least PRED_CLASS_FACS[c]
+ * times the mean length go to class c (the first class runs wide), the rest
+ * to the last class. */
+#ifndef PRED_CLASS_FACS
+#define PRED_CLASS_FACS 4., 2.
+#endif
+static const double k_class_facs[] = {PRED_CLASS_FACS};
+#define NB_MAX ((int)(sizeof(k_class_facs) / sizeof(k_class_facs[0])) + 1)
 
 struct ipg_ctx {
   int device;
@@ -1338,12 +1345,13 @@ static void add_batch_stats(ipg_ctx *ctx, cudaEvent_t *ev, const unsigned long l
 /* Length prediction and split of a wave (rays run..: the list, or the
  * identity).  Traces every ray at PRED_EPS_SCALE times the step size without
  * storing anything and sorts the rays by that step count, longest first, into
- * ctx->d_sorted.  The sorted list is cut into up to NB_MAX length classes:
- * predicted at least PRED_VERYLONG times the mean (run wide), at least
- * PRED_LONG times the mean, and the rest.  Returns the class sizes and
+ * ctx->d_sorted.  The sorted list is cut into up to NB_MAX length classes
+ * at the thresholds k_class_facs (times the mean).  Returns the class sizes and
  * predicted step shares; *nb = 0 means: do not split (the wave is small,
  * nothing is long, or the pool looks too small to hold the wave at once). */
-#define PRED_EPS_SCALE 16.
+#ifndef PRED_EPS_SCALE
+#define PRED_EPS_SCALE 12.
+#endif
 
 template <int P>
 static void launch_count_t(ipg_ctx *ctx, int threads, const int32_t *d_ij, const int32_t *list, size_t run, int cap,
@@ -1353,12 +1361,6 @@ static void launch_count_t(ipg_ctx *ctx, int threads, const int32_t *d_ij, const
   k_geodesic_count<P><<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, PRED_EPS_SCALE, cap, ctx->d_pred,
                                                        counter);
 }
-#ifndef PRED_VERYLONG
-#define PRED_VERYLONG 4.
-#endif
-#ifndef PRED_LONG
-#define PRED_LONG 2.
-#endif
 #define SPLIT_MIN_RAYS 4096
 
 static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, size_t run, const ipg_camera *cam,
@@ -1393,12 +1395,11 @@ static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, si
    * after all are deferred to the next wave like any other */
   if (total * PRED_EPS_SCALE > (double)ctx->n_chunks * IPG_CHUNK_STEPS) return IPG_OK;
   double mean = total / (double)run;
-  const double fac[NB_MAX - 1] = {PRED_VERYLONG, PRED_LONG};
   int hi = LEN_BUCKETS; /* classes are bucket ranges [thr, hi) */
   size_t used = 0;
   int n = 0;
   for (int c = 0; c <= NB_MAX - 1; c++) {
-    int thr = (c < NB_MAX - 1) ? (int)(fac[c] * mean) + 1 : 0;
+    int thr = (c < NB_MAX - 1) ? (int)(k_class_facs[c] * mean) + 1 : 0;
     if (thr > hi) thr = hi;
     size_t cnt_c = 0;
     double st = 0.;
