@@ -243,7 +243,13 @@ __device__ __forceinline__ void count_turns(GeoLane &L)
  * holds one copy of it, which keeps the loop body small: a lone ray's step
  * time is set by instruction-fetch and dependency latency, not by the FP64
  * throughput of the SM. */
-template <int P, int TPB = 256, int MINB = IPG_GEO_MINB>
+#ifndef IPG_GEO_FULLSTEP
+#define IPG_GEO_FULLSTEP 0 /* whole midpoint steps in every class */
+#endif
+#ifndef IPG_WIDE_FULLSTEP
+#define IPG_WIDE_FULLSTEP 1 /* whole midpoint steps in the longest class */
+#endif
+template <int P, int TPB = 256, int MINB = IPG_GEO_MINB, bool FULL = (IPG_GEO_FULLSTEP != 0)>
 __global__ void __launch_bounds__(TPB, MINB)
     k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list,
                double *__restrict__ pool, int *__restrict__ chunk_prev, int2 *__restrict__ chunk_meta,
@@ -256,11 +262,13 @@ __global__ void __launch_bounds__(TPB, MINB)
   const int track = C.target_nturns >= 0;
   GeoLane L;
   bool has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
-#ifdef IPG_GEO_FULLSTEP
+  if constexpr (FULL) {
   /* One iteration is one whole midpoint step.  The second connection is
    * taken at Xhalf = X + h K / 2, which needs only the step size, not the
    * first connection: the two connections are independent chains, evaluated
-   * side by side; only their contractions with K and Khalf are sequential. */
+   * side by side; only their contractions with K and Khalf are sequential.
+   * This shortens a lone ray's step at the cost of registers (250 instead of
+   * 226), so it pays where a class has SMs of its own. */
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
     /* stop_backward_integration, src/model_geodesics.c:218-254, and the step
@@ -331,7 +339,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
     if (pol) store_A(L.prev + REC_A2, A); /* Gamma(Xh_n) Kh_n */
   }
-#else
+  } else {
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
     const int ph = L.phase;
@@ -411,7 +419,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
     if (pol) store_A(L.prev + REC_A2, A); /* Gamma(Xh_n) Kh_n */
   }
-#endif
+  }
 }
 
 
@@ -1288,8 +1296,8 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
   const int threads = 128;
   CK(cudaEventRecord(b.ev[0], b.stream));
   if (b.wide) {
-    int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 256, IPG_GEO_MINB>, 256, b.run);
-    k_geodesic<P, 256, IPG_GEO_MINB><<<gb, 256, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev,
+    int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 256, IPG_GEO_MINB, IPG_WIDE_FULLSTEP != 0>, 256, b.run);
+    k_geodesic<P, 256, IPG_GEO_MINB, IPG_WIDE_FULLSTEP != 0><<<gb, 256, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev,
                                                                 b.chunk_meta, b.n_chunks, b.cnt, ctx->d_rays,
                                                                 b.deferred);
   } else {
