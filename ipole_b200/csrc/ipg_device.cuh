@@ -78,14 +78,6 @@
 #ifndef IPG_XFER_MINB
 #define IPG_XFER_MINB 1
 #endif
-/* the same kernels for the bulk length classes (blocks of 128, many rays
- * per SM): a register cap that buys more resident warps */
-#ifndef IPG_GEO_MINB_BULK
-#define IPG_GEO_MINB_BULK 1
-#endif
-#ifndef IPG_XFER_MINB_BULK
-#define IPG_XFER_MINB_BULK 1
-#endif
 #ifndef IPG_COEF_MINB
 #define IPG_COEF_MINB 4
 #endif

@@ -244,10 +244,7 @@ __device__ __forceinline__ void count_turns(GeoLane &L)
  * time is set by instruction-fetch and dependency latency, not by the FP64
  * throughput of the SM. */
 #ifndef IPG_GEO_FULLSTEP
-#define IPG_GEO_FULLSTEP 0 /* whole midpoint steps in every class */
-#endif
-#ifndef IPG_WIDE_FULLSTEP
-#define IPG_WIDE_FULLSTEP 1 /* whole midpoint steps in the longest class */
+#define IPG_GEO_FULLSTEP 0 /* whole midpoint steps (build option) */
 #endif
 template <int P, int TPB = 256, int MINB = IPG_GEO_MINB, bool FULL = (IPG_GEO_FULLSTEP != 0)>
 __global__ void __launch_bounds__(TPB, MINB)
@@ -267,8 +264,7 @@ __global__ void __launch_bounds__(TPB, MINB)
    * taken at Xhalf = X + h K / 2, which needs only the step size, not the
    * first connection: the two connections are independent chains, evaluated
    * side by side; only their contractions with K and Khalf are sequential.
-   * This shortens a lone ray's step at the cost of registers (250 instead of
-   * 226), so it pays where a class has SMs of its own. */
+   * It takes 250 registers instead of 226 and gives the same records. */
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
     /* stop_backward_integration, src/model_geodesics.c:218-254, and the step
@@ -934,9 +930,9 @@ static const double k_class_facs[] = {PRED_CLASS_FACS};
 struct ipg_ctx {
   int device;
   cudaStream_t stream;
-  cudaEvent_t ev[4];
+  cudaEvent_t ev[5];
   cudaStream_t bstream[NB_MAX]; /* the length classes of a split wave */
-  cudaEvent_t bev[NB_MAX][4];   /* per class: geodesic, coeffs, transfer boundaries */
+  cudaEvent_t bev[NB_MAX][5];   /* per class: geodesic, coeffs, transfer boundaries (and coeffs start) */
   cudaEvent_t ev_fork, ev_join[NB_MAX], ev_pred[2];
   double *d_fields;
   size_t ncell;
@@ -1008,7 +1004,7 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
   ctx->pool_bytes_req = pool_bytes;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-  for (int i = 0; e == cudaSuccess && i < 4; i++) e = cudaEventCreate(&ctx->ev[i]);
+  for (int i = 0; e == cudaSuccess && i < 5; i++) e = cudaEventCreate(&ctx->ev[i]);
   /* the longest class gets the highest stream priority: the block scheduler
    * then places its (SM-filling) blocks before any block of the other
    * classes takes a slot */
@@ -1018,7 +1014,7 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
     int prio = prio_hi + b;
     if (prio > prio_lo) prio = prio_lo;
     e = cudaStreamCreateWithPriority(&ctx->bstream[b], cudaStreamNonBlocking, prio);
-    for (int i = 0; e == cudaSuccess && i < 4; i++) e = cudaEventCreate(&ctx->bev[b][i]);
+    for (int i = 0; e == cudaSuccess && i < 5; i++) e = cudaEventCreate(&ctx->bev[b][i]);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_join[b]);
   }
   for (int i = 0; e == cudaSuccess && i < 2; i++) e = cudaEventCreate(&ctx->ev_pred[i]);
@@ -1055,9 +1051,9 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   cudaFree(ctx->d_len_hist);
   cudaFree(ctx->d_ij);
   cudaFree(ctx->d_out);
-  for (int i = 0; i < 4; i++) cudaEventDestroy(ctx->ev[i]);
+  for (int i = 0; i < 5; i++) cudaEventDestroy(ctx->ev[i]);
   for (int b = 0; b < NB_MAX; b++) {
-    for (int i = 0; i < 4; i++) cudaEventDestroy(ctx->bev[b][i]);
+    for (int i = 0; i < 5; i++) cudaEventDestroy(ctx->bev[b][i]);
     cudaEventDestroy(ctx->ev_join[b]);
     cudaStreamDestroy(ctx->bstream[b]);
   }
@@ -1288,39 +1284,34 @@ struct Batch {
   cudaStream_t stream;
   cudaEvent_t *ev;
   int wide;
+  cudaEvent_t coef_after; /* k_coeffs waits for this event (or none) */
 };
 
 template <int P>
 static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg_pixel_out *d_out)
 {
+  /* Every class launches the same compiled geodesic and transfer kernels
+   * (SM-filling blocks for the longest class, 128-thread blocks, two per SM,
+   * for the others): classes that run side by side then share their
+   * instructions instead of competing for instruction-cache space. */
   const int threads = 128;
+  const int gthreads = b.wide ? 256 : threads, xthreads = b.wide ? IPG_XFER_WIDE : threads;
   CK(cudaEventRecord(b.ev[0], b.stream));
-  if (b.wide) {
-    int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 256, IPG_GEO_MINB, IPG_WIDE_FULLSTEP != 0>, 256, b.run);
-    k_geodesic<P, 256, IPG_GEO_MINB, IPG_WIDE_FULLSTEP != 0><<<gb, 256, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev,
-                                                                b.chunk_meta, b.n_chunks, b.cnt, ctx->d_rays,
-                                                                b.deferred);
-  } else {
-    int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 128, IPG_GEO_MINB_BULK>, threads, b.run);
-    k_geodesic<P, 128, IPG_GEO_MINB_BULK><<<gb, threads, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool,
-                                                                        b.chunk_prev, b.chunk_meta, b.n_chunks,
-                                                                        b.cnt, ctx->d_rays, b.deferred);
-  }
+  int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 256, IPG_GEO_MINB>, gthreads, b.run);
+  k_geodesic<P, 256, IPG_GEO_MINB><<<gb, gthreads, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev,
+                                                                  b.chunk_meta, b.n_chunks, b.cnt, ctx->d_rays,
+                                                                  b.deferred);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[1], b.stream));
+  if (b.coef_after) CK(cudaStreamWaitEvent(b.stream, b.coef_after, 0));
+  CK(cudaEventRecord(b.ev[4], b.stream)); /* coefficients start (after any wait) */
   int cb = grid_blocks(ctx, (const void *)k_coeffs<P>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
   k_coeffs<P><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[2], b.stream));
-  if (b.wide) {
-    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB>, IPG_XFER_WIDE, b.run);
-    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB><<<tb, IPG_XFER_WIDE, 0, b.stream>>>(
-        b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);
-  } else {
-    int tb = grid_blocks(ctx, (const void *)k_transfer<128, IPG_XFER_MINB_BULK>, threads, b.run);
-    k_transfer<128, IPG_XFER_MINB_BULK><<<tb, threads, 0, b.stream>>>(b.list, (int)b.run, b.pool, b.chunk_prev,
-                                                                     ctx->d_rays, d_out, b.cnt);
-  }
+  int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB>, xthreads, b.run);
+  k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB><<<tb, xthreads, 0, b.stream>>>(b.list, (int)b.run, b.pool, b.chunk_prev,
+                                                                         ctx->d_rays, d_out, b.cnt);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[3], b.stream));
   return IPG_OK;
@@ -1340,7 +1331,7 @@ static void add_batch_stats(ipg_ctx *ctx, cudaEvent_t *ev, const unsigned long l
 {
   float a = 0, b = 0, c = 0;
   cudaEventElapsedTime(&a, ev[0], ev[1]);
-  cudaEventElapsedTime(&b, ev[1], ev[2]);
+  cudaEventElapsedTime(&b, ev[4], ev[2]); /* from the coefficients' start */
   cudaEventElapsedTime(&c, ev[2], ev[3]);
   ctx->stats.geodesic_ms += a;
   ctx->stats.coeffs_ms += b;
@@ -1510,6 +1501,11 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
         bt[b].stream = ctx->bstream[b];
         bt[b].ev = ctx->bev[b];
         bt[b].wide = wide[b];
+        bt[b].coef_after = nullptr;
+        /* the shorter classes' coefficient passes wait for the longest
+         * class's geodesics: run beside them, they slow the longest rays'
+         * steps four- to eightfold (those rays' SMs hold no other block) */
+        if (b > 0 && wide[0]) bt[b].coef_after = ctx->bev[0][1];
         c0 += ncb;
         r0 += sizes[b];
       }
@@ -1871,15 +1867,15 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
       NA_CK(cudaMemcpyAsync(cnt_d + CNT_DEFER, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
       NA_CK(cudaStreamSynchronize(stream));
     }
-    int gb = na_blocks(n_sm, (const void *)k_geodesic<IPG_PLUG_IHARM, 128, IPG_GEO_MINB_BULK>, threads, run);
-    k_geodesic<IPG_PLUG_IHARM, 128, IPG_GEO_MINB_BULK><<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta,
+    int gb = na_blocks(n_sm, (const void *)k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB>, threads, run);
+    k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB><<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta,
                                                            n_chunks, cnt_d, rays, lists[cur ^ 1]);
     NA_CK(cudaGetLastError());
     int cb = na_blocks(n_sm, (const void *)k_coeffs<IPG_PLUG_IHARM>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
     k_coeffs<IPG_PLUG_IHARM><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
     NA_CK(cudaGetLastError());
-    int tb = na_blocks(n_sm, (const void *)k_transfer<128, IPG_XFER_MINB_BULK>, threads, run);
-    k_transfer<128, IPG_XFER_MINB_BULK><<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev, rays, d_out, cnt_d);
+    int tb = na_blocks(n_sm, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB>, threads, run);
+    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB><<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev, rays, d_out, cnt_d);
     NA_CK(cudaGetLastError());
     unsigned long long cnt[CNT_N];
     NA_CK(cudaMemcpyAsync(cnt, cnt_d, sizeof(cnt), cudaMemcpyDeviceToHost, stream));

@@ -370,17 +370,17 @@ extern "C" int ipg_trace_ray(ipg_ctx *ctx, const ipg_camera *cam, int i, int j, 
   CK(cudaMemsetAsync(ctx->d_cnt, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
   switch (ctx->plug) {
     case IPG_PLUG_ANALYTIC:
-      k_geodesic<IPG_PLUG_ANALYTIC, 128, IPG_GEO_MINB_BULK><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
+      k_geodesic<IPG_PLUG_ANALYTIC, 256, IPG_GEO_MINB><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
                                                               ctx->d_chunk_meta, ctx->n_chunks, ctx->d_cnt,
                                                               ctx->d_rays, ctx->d_list[1]);
       break;
     case IPG_PLUG_SPHERE:
-      k_geodesic<IPG_PLUG_SPHERE, 128, IPG_GEO_MINB_BULK><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
+      k_geodesic<IPG_PLUG_SPHERE, 256, IPG_GEO_MINB><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
                                                             ctx->d_chunk_meta, ctx->n_chunks, ctx->d_cnt,
                                                             ctx->d_rays, ctx->d_list[1]);
       break;
     default:
-      k_geodesic<IPG_PLUG_IHARM, 128, IPG_GEO_MINB_BULK><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
+      k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
                                                            ctx->d_chunk_meta, ctx->n_chunks, ctx->d_cnt, ctx->d_rays,
                                                            ctx->d_list[1]);
   }
