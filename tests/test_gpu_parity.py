@@ -165,3 +165,28 @@ def test_device_pointer_entry(dumps):
         c.trace_device(cam, d_ij.data_ptr(), len(ij), d_out.data_ptr())
         dev = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=ip.PIXEL_DTYPE)
     assert dev.tobytes() == host.tobytes()
+
+
+def test_length_classes_match_single_wave(dumps, monkeypatch):
+    """A wave of at least 4096 rays is split into length classes: a coarse
+    length prediction, a longest-first order, and concurrent classes on their
+    own streams, with the shorter classes' coefficient passes waiting for the
+    longest class's geodesics.  Its results must be bit-identical to the same
+    rays traced as one unsplit wave."""
+    meta, _ = common.load_golden("c1_bright_32")
+    p = common.params_for(meta, dumps.get(meta), ["--nx=96", "--ny=96"])
+    m = ip.Model.load(p)
+    cam = ip.camera_for(p, m.grid)
+    ij = np.array([(i, j) for i in range(96) for j in range(96)], dtype=np.int32)
+    with ip.Context() as a:
+        a.upload(m)
+        r1 = a.trace(cam, ij)
+        s1 = a.stats()
+    monkeypatch.setenv("IPG_NO_SPLIT", "1")
+    with ip.Context() as b:
+        b.upload(m)
+        r2 = b.trace(cam, ij)
+        s2 = b.stats()
+    print("launches split / unsplit:", s1["launches"], s2["launches"])
+    assert s2["launches"] == 3 and s1["launches"] > 3
+    assert r1.tobytes() == r2.tobytes()
