@@ -1005,15 +1005,15 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   for (int i = 0; e == cudaSuccess && i < 5; i++) e = cudaEventCreate(&ctx->ev[i]);
-  /* the longest class gets the highest stream priority: the block scheduler
-   * then places its (SM-filling) blocks before any block of the other
-   * classes takes a slot */
+  /* the length classes' streams share the highest priority.  Ranking them
+   * (longest class first) measured 199-205 ms per 400x400 image against
+   * 190-198 ms for equal ranks: once the shorter classes' coefficient passes
+   * wait for the longest class's geodesics, the end of the image is the
+   * shortest class's chain, which a lower rank delays. */
   int prio_lo = 0, prio_hi = 0;
   if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
   for (int b = 0; e == cudaSuccess && b < NB_MAX; b++) {
-    int prio = prio_hi + b;
-    if (prio > prio_lo) prio = prio_lo;
-    e = cudaStreamCreateWithPriority(&ctx->bstream[b], cudaStreamNonBlocking, prio);
+    e = cudaStreamCreateWithPriority(&ctx->bstream[b], cudaStreamNonBlocking, prio_hi);
     for (int i = 0; e == cudaSuccess && i < 5; i++) e = cudaEventCreate(&ctx->bev[b][i]);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_join[b]);
   }
