@@ -664,7 +664,7 @@ __device__ __forceinline__ int evolve_N_coef(const CoefBlock &cb, double dlam, i
 }
 
 /* block width of the transfer for the longest length class (its blocks fill
- * an SM's registers) */
+ * an SM's registers); the compiled kernel's thread bound for every class */
 #ifndef IPG_XFER_WIDE
 #define IPG_XFER_WIDE 256
 #endif
@@ -1268,10 +1268,10 @@ static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n)
 
 /* One batch of a wave: a slice of a ray list, a slice of the trajectory pool
  * and its own counters, run as geodesic -> coefficients -> transfer on one
- * stream.  wide = 1 launches the two sequential kernels with blocks wide
- * enough (256 and 384 threads) that their registers fill an SM: no block of
- * another kernel fits beside them, so the rays of such a batch run at the
- * step latency of an otherwise idle SM. */
+ * stream.  wide = 1 launches the two sequential kernels in 256-thread blocks,
+ * whose registers fill an SM: no block of another kernel fits beside them.
+ * coef_after, when set, holds the batch's coefficient pass until another
+ * batch's geodesics are done. */
 struct Batch {
   const int32_t *list;
   size_t run;
