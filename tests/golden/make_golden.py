@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 from ipole_b200 import ipgc, synthdump  # noqa: E402
 
 # dump name -> (n1, n2, n3, seed)
-DUMPS = {"c1": (128, 64, 64, 1)}
+DUMPS = {"c1": (128, 64, 64, 1), "c2": (288, 128, 128, 1)}
 
 BASE = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
         "--fov=160", "--trat_large=20", "--trat_small=1"]
@@ -57,6 +57,10 @@ CASES = {
     "c1_counterjet_16": ("c1", ["--M_unit=3e27", "--counterjet=1", "--nx=16", "--ny=16"]),
     "c1_xoff_floors_16": ("c1", ["--M_unit=3e27", "--xoff=0.3", "--yoff=-0.2", "--stokes_floors=1",
                                  "--eps=0.02", "--nx=16", "--ny=20"]),
+    # the production dump shape (288x128x128, seed 1) at both inclinations and
+    # both R_high of the 400x400 workload, on small images
+    "c2_rhigh1_incl17_24": ("c2", ["--M_unit=7.5e27", "--trat_large=1", "--thetacam=17", "--nx=24", "--ny=24"]),
+    "c2_rhigh160_incl163_24": ("c2", ["--M_unit=7.5e27", "--trat_large=160", "--nx=24", "--ny=24"]),
 }
 
 
