@@ -190,3 +190,31 @@ def test_length_classes_match_single_wave(dumps, monkeypatch):
     print("launches split / unsplit:", s1["launches"], s2["launches"])
     assert s2["launches"] == 3 and s1["launches"] > 3
     assert r1.tobytes() == r2.tobytes()
+
+
+def test_length_classes_with_tight_pools(dumps):
+    """Pools around a 96x96 image's actual need.  When a class's slice of
+    the pool overflows, its rays are deferred, and the classes' deferred rays
+    are gathered at the front of the next wave.  A pool below the predicted
+    need is traced unsplit, in several waves.  Every pool size gives
+    bit-identical results."""
+    meta, _ = common.load_golden("c1_bright_32")
+    p = common.params_for(meta, dumps.get(meta), ["--nx=96", "--ny=96"])
+    m = ip.Model.load(p)
+    cam = ip.camera_for(p, m.grid)
+    ij = np.array([(i, j) for i in range(96) for j in range(96)], dtype=np.int32)
+    with ip.Context() as a:
+        a.upload(m)
+        ref = a.trace(cam, ij)
+        steps = a.stats()["ray_steps"]
+    chunk_bytes = 32 * 64 * 8  # steps per chunk x doubles per step record
+    need = steps // 32 + len(ij)  # every ray's last chunk may be partly empty
+    waves = {}
+    for frac in (1.08, 0.95, 0.6):
+        with ip.Context(pool_bytes=int(need * frac) * chunk_bytes) as b:
+            b.upload(m)
+            r = b.trace(cam, ij)
+            waves[frac] = b.stats()["waves"]
+        assert r.tobytes() == ref.tobytes(), frac
+    print("waves per pool fraction:", waves)
+    assert waves[0.6] > 1
