@@ -252,6 +252,8 @@ def run_ours(args):
     p = ip.Params.from_args(workload_args(dump, nx, ny, args.m_unit) + extra)
     model = ip.Model.load(p)
     ctx = ip.Context(local, pool_bytes=int(args.pool_gb * (1 << 30)))
+    if args.records == "mixed":
+        ctx.set_record_precision(ip.IPG_RECORDS_MIXED)
     ctx.upload(model)
     cam = ip.camera_for(p, model.grid)
     ij = np.array([(i, j) for i in range(nx) for j in range(ny)], dtype=np.int32)
@@ -324,6 +326,34 @@ def run_ours(args):
            "d2h_bytes_per_step": int(img_bytes),
            "api": "ipg_render_image: host parameters in, host image out (pixel lists built on the device)"}
 
+    # the compact-record form (ipg_set_record_precision): the same image with
+    # the transport matrices and tetrad rows stored in FP32 between the
+    # kernels, timed like the headline, and its error against that image
+    ctx.set_record_precision(ip.IPG_RECORDS_MIXED)
+    ctx.trace_device(cam, d_ij.data_ptr(), n, d_out.data_ptr())
+    torch.cuda.synchronize()
+    barrier(world)
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    for _ in range(args.steps):
+        ctx.trace_device(cam, d_ij.data_ptr(), n, d_out.data_ptr())
+    m1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    mixed_ms = max_over_ranks(m0.elapsed_time(m1), world)
+    mo = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=ip.PIXEL_DTYPE)
+    ctx.set_record_precision(ip.IPG_RECORDS_FP64)
+    I0, Q0, U0, V0 = (float(out[k].sum()) for k in "IQUV")
+    I1, Q1, U1, V1 = (float(mo[k].sum()) for k in "IQUV")
+    bright = out["I"] > 1e-6 * out["I"].max()
+    mixed = {"value": images_per_s(world, args.steps, mixed_ms), "unit": "images/s",
+             "ms_per_step": mixed_ms / args.steps,
+             "records": "transport matrices and tetrad rows in FP32; coefficients and all arithmetic in FP64",
+             "vs_fp64": {"Ftot_rel": abs(I1 / I0 - 1), "Q_rel_to_I": abs(Q1 - Q0) / abs(I0),
+                         "U_rel_to_I": abs(U1 - U0) / abs(I0), "V_rel_to_I": abs(V1 - V0) / abs(I0),
+                         "EVPA_deg": abs(float(np.degrees(0.5 * (np.arctan2(U1, Q1) - np.arctan2(U0, Q0))))),
+                         "pix_I_max_rel": float(np.max(np.abs(mo["I"][bright] / out["I"][bright] - 1)))}}
+
     peak = ip.fp64_peak_tflops(local, 300.0)
     dom = max(kms, key=kms.get)
     fps = FLOPS_PER_STEP[dom]
@@ -353,7 +383,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2: 392 MB field array + trajectory pool writes per step"},
             "ray_steps_per_s": total_steps / (ms_max / 1e3), "ray_steps_per_image": steps / args.steps,
             "radiating_fraction": rad / max(steps, 1), "Ftot_Jy": ftot, "e2e": e2e, "roofline": roofline,
-            "clocks": clk, "gpu_launches": launches}
+            "clocks": clk, "gpu_launches": launches, "mixed_records": mixed}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             cb = cpu_reference_sample(dump, args.m_unit)
@@ -414,6 +444,8 @@ def main():
                                               "of the sequential kernels (diagnostic)")
     ap.add_argument("--pool-gb", dest="pool_gb", type=float, default=0.0,
                     help="trajectory pool size in GiB (0: 60%% of free device memory)")
+    ap.add_argument("--records", default="fp64", choices=["fp64", "mixed"],
+                    help="step-record storage between the kernels (ipg_set_record_precision); with --quick only")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -257,6 +257,20 @@ typedef struct ipg_stats {
 } ipg_stats;
 int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 
+/* Storage precision of the step records between the three kernels (no
+ * counterpart in the reference, whose integrate_emission holds one step in
+ * registers).  IPG_RECORDS_FP64 (the default) keeps every value in FP64: the
+ * plain tier.  IPG_RECORDS_MIXED stores the transport matrices and the plasma
+ * tetrad rows (order-one values) in FP32 and the emission, absorption and
+ * rotation coefficients in FP64; all arithmetic stays FP64, and the walk back
+ * reads 296 bytes per step instead of 512.  Its images differ from the FP64
+ * records' by the FP32 rounding of those values (the test of this mode states
+ * the errors); ipg_trace_ray and ipg_trace_pixels_noalloc always use FP64.
+ * Returns IPG_E_ARG for another value. */
+#define IPG_RECORDS_FP64 0
+#define IPG_RECORDS_MIXED 1
+int ipg_set_record_precision(ipg_ctx *ctx, int precision);
+
 /* The context's CUDA stream (a cudaStream_t), on which every kernel of the
  * context is launched; lets a caller bracket calls with its own events. */
 int ipg_get_stream(const ipg_ctx *ctx, void **stream);

@@ -31,6 +31,8 @@ IPG_OK, IPG_E_ARG, IPG_E_CUDA, IPG_E_MAXNSTEP, IPG_E_NAN, IPG_E_TIMEOUT, IPG_E_N
     IPG_E_FORMAT = range(10)
 NFIELD = 10
 STRLEN = 2048
+# step-record storage precision (ipg_set_record_precision)
+IPG_RECORDS_FP64, IPG_RECORDS_MIXED = 0, 1
 # per-step trace columns (include/ipole_b200.h, IPG_TRACE_*)
 TRACE_DOUBLES = 127
 TRACE_COLS = {"b": (0, 1), "ne": (1, 1), "thetae": (2, 1), "nu": (3, 1), "b_k_angle": (4, 1), "sigma": (5, 1),
@@ -183,6 +185,7 @@ def lib():
                                           C.c_void_p]
     L.ipg_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
     L.ipg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.ipg_set_record_precision.argtypes = [C.c_void_p, C.c_int]
     L.ipg_camera_setup.argtypes = [C.POINTER(Grid)] + [C.c_double] * 9 + [C.c_int, C.c_int, C.c_double, C.c_int,
                                                                           C.POINTER(Camera), C.POINTER(C.c_double),
                                                                           C.POINTER(C.c_double),
@@ -405,6 +408,12 @@ class Context:
         """ipg_trace_pixels_device on device pointers (e.g. torch tensors' data_ptr())."""
         _check(lib().ipg_trace_pixels_device(self._h, C.byref(cam), C.c_void_p(d_ij_ptr), n, C.c_void_p(d_out_ptr),
                                              C.c_void_p(stream)), self._h)
+
+    def set_record_precision(self, precision: int):
+        """ipg_set_record_precision: IPG_RECORDS_FP64 (default) or
+        IPG_RECORDS_MIXED (transport matrices and tetrad rows stored in
+        FP32 between the kernels)."""
+        _check(lib().ipg_set_record_precision(self._h, int(precision)), self._h)
 
     def stream(self) -> int:
         """The context's cudaStream_t as an integer handle."""

@@ -128,6 +128,7 @@ struct DevCam {
   double eps;
   int nx, ny, maxnstep;
   int unpol, emission_type, stokes_floors, target_nturns, subring_dtheta, counterjet;
+  int mixed; /* IPG_RECORDS_MIXED: compact step records (ipg_set_record_precision) */
 };
 
 /* Defined here: the header is included by exactly one translation unit. */

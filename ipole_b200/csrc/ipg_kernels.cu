@@ -108,6 +108,55 @@ __device__ __forceinline__ void load_A(const double *p, double A[4][4])
   for (int i = 0; i < 4; i++) load4(p + 4 * i, A[i]);
 }
 
+/* Compact step records (IPG_RECORDS_MIXED), same 512-byte stride:
+ *   floats  0..15  A1, floats 16..31  A2                      (bytes   0-127)
+ *   doubles 16..28 flags ju ku dl jI jQ jV aI aQ aV nturns rQ rV (128-231)
+ *   floats 60..75  tetrad rows e1, e2 (covariant), a, b (contravariant)
+ *                                                             (bytes 240-303)
+ * The geodesic state (doubles 32..47, bytes 256-383) stays where the FP64
+ * layout has it; k_coeffs reads it before writing the coefficients, whose
+ * tetrad floats overlap its first doubles. */
+#define RECM_A1F 0
+#define RECM_A2F 16
+#define RECM_COEF 16
+#define RECM_TETF 60
+static_assert(RECM_COEF * 2 >= RECM_A2F + 16 && RECM_TETF >= (RECM_COEF + 13) * 2 && RECM_TETF + 16 <= 128,
+              "compact record layout");
+
+__device__ __forceinline__ void store_A_f(float *p, const double A[4][4])
+{
+  float4 *q = reinterpret_cast<float4 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    q[i] = make_float4((float)A[i][0], (float)A[i][1], (float)A[i][2], (float)A[i][3]);
+}
+
+__device__ __forceinline__ void load_A_f(const float *p, double A[4][4])
+{
+  const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    float4 v = q[i];
+    A[i][0] = v.x;
+    A[i][1] = v.y;
+    A[i][2] = v.z;
+    A[i][3] = v.w;
+  }
+}
+
+/* A1 (which = 0) or A2 (which = 1) of a record, in the record's layout */
+__device__ __forceinline__ void store_A_rec(double *rec, int which, const double A[4][4])
+{
+  if (c_cam.mixed) store_A_f(reinterpret_cast<float *>(rec) + (which ? RECM_A2F : RECM_A1F), A);
+  else store_A(rec + (which ? REC_A2 : REC_A1), A);
+}
+
+__device__ __forceinline__ void load_A_rec(const double *rec, int which, double A[4][4])
+{
+  if (c_cam.mixed) load_A_f(reinterpret_cast<const float *>(rec) + (which ? RECM_A2F : RECM_A1F), A);
+  else load_A(rec + (which ? REC_A2 : REC_A1), A);
+}
+
 /* Gamma^k_ij K^i K^j = A^k_i K^i */
 __device__ __forceinline__ void accel_from_A(const double A[4][4], const double K[4], double acc[4])
 {
@@ -278,7 +327,7 @@ __global__ void __launch_bounds__(TPB, MINB)
         double A[4][4];
         fd_connection<PlugT<P>::MET>(L.X[1], L.X[2], &cn);
         transport_matrix(cn, L.K, A);
-        store_A(L.prev + REC_A1, A);
+        store_A_rec(L.prev, 0, A);
       }
       RayRec rec = {L.chunk, L.nstep, status, 0};
       rays[L.ray] = rec;
@@ -297,7 +346,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     if (pol) {
       transport_matrix(c0, L.K, A);
       accel_from_A(A, L.K, acc);
-      store_A(L.prev + REC_A1, A);
+      store_A_rec(L.prev, 0, A);
     } else {
       geo_accel(c0, L.K, acc);
     }
@@ -333,7 +382,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     }
     L.prev = step_ptr(pool, L.chunk, slot);
     store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
-    if (pol) store_A(L.prev + REC_A2, A); /* Gamma(Xh_n) Kh_n */
+    if (pol) store_A_rec(L.prev, 1, A); /* Gamma(Xh_n) Kh_n */
   }
   } else {
   while (__any_sync(0xffffffffu, has)) {
@@ -370,7 +419,7 @@ __global__ void __launch_bounds__(TPB, MINB)
       geo_accel(cn, Ke, acc);
     }
     if (ph == 0) {
-      if (pol) store_A(L.prev + REC_A1, A);
+      if (pol) store_A_rec(L.prev, 0, A);
       if (stop) {
         RayRec rec = {L.chunk, L.nstep, IPG_RAY_OK, 0};
         rays[L.ray] = rec;
@@ -413,7 +462,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     }
     L.prev = step_ptr(pool, L.chunk, slot);
     store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
-    if (pol) store_A(L.prev + REC_A2, A); /* Gamma(Xh_n) Kh_n */
+    if (pol) store_A_rec(L.prev, 1, A); /* Gamma(Xh_n) Kh_n */
   }
   }
 }
@@ -551,6 +600,23 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
         flags |= tf << 2;
       }
     }
+    if (C.mixed) {
+      /* the compact layout: coefficients in FP64, tetrad rows in FP32; dl and
+       * nturns move from the geodesic state, which this pass has not yet
+       * overwritten */
+      const double dl_rec = p[REC_DL], nturns_rec = p[REC_NTURNS];
+      double *q = p + RECM_COEF;
+      store4(q, (double)flags, ju, ku, dl_rec);
+      store4(q + 4, jar.jI, jar.jQ, jar.jV, jar.aI);
+      store4(q + 8, jar.aQ, jar.aV, nturns_rec, jar.rQ);
+      q[12] = jar.rV;
+      float4 *t = reinterpret_cast<float4 *>(reinterpret_cast<float *>(p) + RECM_TETF);
+      t[0] = make_float4((float)e1[0], (float)e1[1], (float)e1[2], (float)e1[3]);
+      t[1] = make_float4((float)e2[0], (float)e2[1], (float)e2[2], (float)e2[3]);
+      t[2] = make_float4((float)Econ[1][0], (float)Econ[1][1], (float)Econ[1][2], (float)Econ[1][3]);
+      t[3] = make_float4((float)Econ[2][0], (float)Econ[2][1], (float)Econ[2][2], (float)Econ[2][3]);
+      continue;
+    }
     p[REC_FLAGS] = (double)flags;
     p[REC_JU] = ju;
     p[REC_KU] = ku;
@@ -606,6 +672,36 @@ static_assert(REC_FLAGS == 32 && REC_JU == 33 && REC_KU == 34 && REC_DL == 35 &&
                   REC_NTURNS == 42 && REC_RQ == 43 && REC_RV == 44 && REC_E1COV == 48 && REC_E2COV == 52 &&
                   REC_E1CON == 56 && REC_E2CON == 60,
               "load_coef follows the record layout");
+
+/* the same from a compact record (IPG_RECORDS_MIXED) */
+__device__ __forceinline__ void load_coef_m(const double *__restrict__ p, CoefBlock &c)
+{
+  const double2 *q = reinterpret_cast<const double2 *>(p + RECM_COEF);
+  double2 v[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) v[k] = q[k];
+  const float4 *t = reinterpret_cast<const float4 *>(reinterpret_cast<const float *>(p) + RECM_TETF);
+  float4 w[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) w[k] = t[k];
+  c.flags = v[0].x;
+  c.ju = v[0].y;
+  c.ku = v[1].x;
+  c.dl = v[1].y;
+  c.jI = v[2].x;
+  c.jQ = v[2].y;
+  c.jV = v[3].x;
+  c.aI = v[3].y;
+  c.aQ = v[4].x;
+  c.aV = v[4].y;
+  c.nturns = v[5].x;
+  c.rQ = v[5].y;
+  c.rV = v[6].x;
+  c.e1[0] = w[0].x; c.e1[1] = w[0].y; c.e1[2] = w[0].z; c.e1[3] = w[0].w;
+  c.e2[0] = w[1].x; c.e2[1] = w[1].y; c.e2[2] = w[1].z; c.e2[3] = w[1].w;
+  c.a[0] = w[2].x; c.a[1] = w[2].y; c.a[2] = w[2].z; c.a[3] = w[2].w;
+  c.b[0] = w[3].x; c.b[1] = w[3].y; c.b[2] = w[3].z; c.b[3] = w[3].w;
+}
 
 /* evolve_N (src/ipolarray.c:332-575) from a coefficient block: N to Stokes
  * in the plasma tetrad, Faraday half step, absorption/emission, Faraday half
@@ -687,12 +783,16 @@ struct XferLane {
 #endif
 __device__ __forceinline__ void prefetch_rec(const double *p)
 {
+  /* the compact layout's walk reads only the first three 128-byte lines */
+  const int nl = c_cam.mixed ? 3 : 4;
 #if IPG_XFER_PREFETCH == 1
 #pragma unroll
-  for (int l = 0; l < 4; l++) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + 16 * l));
+  for (int l = 0; l < 4; l++)
+    if (l < nl) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + 16 * l));
 #elif IPG_XFER_PREFETCH == 2
 #pragma unroll
-  for (int l = 0; l < 4; l++) asm volatile("prefetch.global.L1 [%0];" ::"l"(p + 16 * l));
+  for (int l = 0; l < 4; l++)
+    if (l < nl) asm volatile("prefetch.global.L1 [%0];" ::"l"(p + 16 * l));
 #endif
 }
 
@@ -725,10 +825,17 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
     prefetch_rec(L.rec_i);
     if (L.n % IPG_CHUNK_STEPS) prefetch_rec(L.rec_i - IPG_STEP_DOUBLES);
     /* get_jkinv at the far end of the ray, src/ipolarray.c:74 */
-    L.js = L.rec_i[REC_JU];
-    L.ks = L.rec_i[REC_KU];
-    L.dl_i = L.rec_i[REC_DL];
-    L.nturns_i = L.rec_i[REC_NTURNS];
+    if (c_cam.mixed) {
+      L.js = L.rec_i[RECM_COEF + 1];
+      L.ks = L.rec_i[RECM_COEF + 2];
+      L.dl_i = L.rec_i[RECM_COEF + 3];
+      L.nturns_i = L.rec_i[RECM_COEF + 10];
+    } else {
+      L.js = L.rec_i[REC_JU];
+      L.ks = L.rec_i[REC_KU];
+      L.dl_i = L.rec_i[REC_DL];
+      L.nturns_i = L.rec_i[REC_NTURNS];
+    }
     L.I = L.tau = L.tauF = 0.;
     hn_zero(&L.N);
     L.flag = 0;
@@ -786,7 +893,8 @@ __global__ void __launch_bounds__(TPB, MINB)
       else if (L.cprev >= 0) prefetch_rec(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
     }
     CoefBlock cb;
-    load_coef(rec_f, cb);
+    if (C.mixed) load_coef_m(rec_f, cb);
+    else load_coef(rec_f, cb);
     double dl = L.dl_i;
     if (!unpol) {
       /* push_polar twice, src/ipolarray.c:85-89 */
@@ -794,9 +902,9 @@ __global__ void __launch_bounds__(TPB, MINB)
       double dlhalf = (0.5 * dl) * G.inv_dlfac;
       double A[4][4];
       HermN Nh, Nn;
-      load_A(L.rec_i + REC_A1, A);
+      load_A_rec(L.rec_i, 0, A);
       hn_push(L.N, L.N, A, dlhalf, &Nh);
-      load_A(L.rec_i + REC_A2, A);
+      load_A_rec(L.rec_i, 1, A);
       hn_push(L.N, Nh, A, dlfull, &Nn);
       L.N = Nn;
     }
@@ -952,6 +1060,7 @@ struct ipg_ctx {
   int32_t *d_pred;   /* predicted step counts (list positions), also staging */
   int *d_len_hist;   /* LEN_BUCKETS counters of the sort */
   int split;         /* 1: split waves into long and short batches */
+  int rec_mixed;     /* IPG_RECORDS_MIXED: compact step records */
   int32_t *d_ij;
   ipg_pixel_out *d_out;
   size_t cap;
@@ -1441,6 +1550,7 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
   if (rc) return rc;
   DevCam dc;
   make_devcam(cam, &dc);
+  dc.mixed = ctx->rec_mixed;
   CK(cudaMemcpyToSymbolAsync(c_grid, &ctx->dg, sizeof(DevGrid), 0, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyToSymbolAsync(c_plug, &ctx->dp, sizeof(DevPlug), 0, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyToSymbolAsync(c_cam, &dc, sizeof(DevCam), 0, cudaMemcpyHostToDevice, ctx->stream));
@@ -1656,6 +1766,13 @@ extern "C" int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats)
 {
   if (!ctx || !stats) return IPG_E_ARG;
   *stats = ctx->stats;
+  return IPG_OK;
+}
+
+extern "C" int ipg_set_record_precision(ipg_ctx *ctx, int precision)
+{
+  if (!ctx || (precision != IPG_RECORDS_FP64 && precision != IPG_RECORDS_MIXED)) return IPG_E_ARG;
+  ctx->rec_mixed = precision == IPG_RECORDS_MIXED;
   return IPG_OK;
 }
 

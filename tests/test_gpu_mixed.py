@@ -1,0 +1,51 @@
+"""Compact step records (ipg_set_record_precision(IPG_RECORDS_MIXED)) against
+the FP64 records on the same images.
+
+The compact layout stores the transport matrices A1/A2 (Gamma K at X and at
+Xhalf, which push_polar applies to N, src/ipolarray.c:253-289) and the plasma
+tetrad rows (src/model_tetrads.c:35-127) in FP32 between the kernels; the
+coefficients and all arithmetic stay FP64.  The errors against the FP64
+records are printed per case; the bounds are the ones stated for the mixed
+tier (total flux 1e-3 relative, flux-weighted EVPA 0.5 degree), with the
+per-pixel and polarization-fraction bounds below.
+"""
+import numpy as np
+import pytest
+
+import ipole_b200 as ip
+from tests import common
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["c1_bright_32", "c1_faraday_24", "c1_thick_24", "c1_incl17_rot_24", "c2_rhigh160_incl163_24",
+         "c2_rhigh1_incl17_24"]
+BOUNDS = {"Ftot": 1e-3, "Ftot_unpol": 1e-3, "EVPA_deg": 0.5, "LP_abs": 1e-3, "CP_abs": 1e-3,
+          "pix_I_max": 1e-2, "pix_unpol_max": 1e-2}
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_mixed_records_against_fp64(case, dumps):
+    meta, _ = common.load_golden(case)
+    p = common.params_for(meta, dumps.get(meta))
+    m = ip.Model.load(p)
+    with ip.Context() as c:
+        c.upload(m)
+        full = c.render(p, m)
+        c.set_record_precision(ip.IPG_RECORDS_MIXED)
+        mixed = c.render(p, m)
+        c.set_record_precision(ip.IPG_RECORDS_FP64)
+        again = c.render(p, m)
+    assert again.pol.tobytes() == full.pol.tobytes()  # the setting is undone
+    ref = {"unpol": full.unpol, "pol": full.pol}
+    e = common.image_errors(mixed, ref)
+    print(case, {k: f"{v:.2e}" for k, v in e.items()})
+    assert np.array_equal(mixed.nstep, full.nstep)  # the geodesics are the same
+    bad = {k: v for k, v in e.items() if k in BOUNDS and not v <= BOUNDS[k]}
+    assert not bad, bad
+
+
+def test_record_precision_argument():
+    with ip.Context() as c:
+        with pytest.raises(ip.IpgError) as err:
+            c.set_record_precision(7)
+        assert err.value.code == ip.IPG_E_ARG
