@@ -66,6 +66,10 @@ typedef struct ipg_params {
   double rho_unit;          /* "rho_unit" (<= 0: 3e-18) */
   /* sphere keys (model/sphere/model.c:37-46); tp_over_te is shared with iharm */
   double sphere_Thetae0, sphere_R0, sphere_tau0, sphere_beta0, sphere_gam;
+  /* "mixed_records" (no reference counterpart): 1 stores the step records
+   * compactly between the kernels (ipg_set_record_precision,
+   * IPG_RECORDS_MIXED); 0, the default, keeps them in FP64 */
+  int mixed_records;
 } ipg_params;
 
 /* Defaults of load_par_from_argv (src/par.c:48-100) and the model/radiation

@@ -119,7 +119,8 @@ class _Params(C.Structure):
                 ("bremss", C.c_int), ("bremss_type", C.c_int),
                 ("plugin", C.c_char * STRLEN), ("MBH_set", C.c_int), ("analytic_model", C.c_int),
                 ("rho_unit", C.c_double), ("sphere_Thetae0", C.c_double), ("sphere_R0", C.c_double),
-                ("sphere_tau0", C.c_double), ("sphere_beta0", C.c_double), ("sphere_gam", C.c_double)]
+                ("sphere_tau0", C.c_double), ("sphere_beta0", C.c_double), ("sphere_gam", C.c_double),
+                ("mixed_records", C.c_int)]
 
 
 class Plugin(C.Structure):

@@ -52,7 +52,8 @@ int main(int argc, char *argv[])
     ipg_iharm_free(&m);
     return exit_code(rc);
   }
-  rc = ipg_upload_model(ctx, &m);
+  if (p.mixed_records) rc = ipg_set_record_precision(ctx, IPG_RECORDS_MIXED);
+  if (!rc) rc = ipg_upload_model(ctx, &m);
   if (rc) {
     fprintf(stderr, "model upload failed: %s (%s)\n", ipg_strerror(rc), ipg_last_error(ctx));
     ipg_destroy(ctx);

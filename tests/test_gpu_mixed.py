@@ -49,3 +49,25 @@ def test_record_precision_argument():
         with pytest.raises(ip.IpgError) as err:
             c.set_record_precision(7)
         assert err.value.code == ip.IPG_E_ARG
+
+
+def test_cli_mixed_records_key(dumps, tmp_path):
+    """--mixed_records=1 on the command line gives the compact records'
+    image, and its difference from the default run stays within the bounds."""
+    import subprocess
+
+    from ipole_b200 import build, ipgc
+    meta, _ = common.load_golden("c1_faraday_24")
+    build.build()
+    imgs = {}
+    for tag, extra in (("fp64", []), ("mixed", ["--mixed_records=1"])):
+        out = str(tmp_path / f"{tag}.h5")
+        r = subprocess.run([build.CLI, f"--dump={dumps.get(meta)}", *meta["args"], *extra, f"--outfile={out}"],
+                           capture_output=True, text=True, cwd=str(tmp_path), timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        imgs[tag] = ipgc.read(out)
+    a, b = imgs["fp64"]["/pol"], imgs["mixed"]["/pol"]
+    assert not np.array_equal(a, b)  # the key took effect
+    e = abs(b[..., 0].sum() / a[..., 0].sum() - 1)
+    print("CLI mixed_records: total flux relative difference", e)
+    assert e <= BOUNDS["Ftot"]
