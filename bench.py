@@ -12,8 +12,12 @@ One *step* is one complete 400^2 image (every pixel traced, no refinement).
 `value` = images/s with the pixel list and outputs resident in device memory
 (ipg_trace_pixels_device), `e2e` = images/s through the host image driver
 (ipg_render_image: host pixel lists, host output arrays, copies in the timed
-region).  Under torchrun each rank renders its own image (weak scaling, no
-collective on the data path); time is the max over ranks.  The reference arm
+region).  `mixed_records` times the same image with compact step records
+(ipg_set_record_precision: transport matrices and tetrad rows in FP32
+between the kernels) and gives its error against the FP64 image;
+`--records mixed` does the same for a --quick run.  Under torchrun each rank
+renders its own image (weak scaling, no collective on the data path); time
+is the max over ranks.  The reference arm
 runs the reference ipole built from its sources (oracle/_ref/ipole, the
 makefile's -O3 flags, OpenMP on every host core) on a bounded 64^2 sample of
 the same workload and scales it to a 400^2 image.
