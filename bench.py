@@ -12,10 +12,10 @@ One *step* is one complete 400^2 image (every pixel traced, no refinement).
 `value` = images/s with the pixel list and outputs resident in device memory
 (ipg_trace_pixels_device), `e2e` = images/s through the host image driver
 (ipg_render_image: host pixel lists, host output arrays, copies in the timed
-region).  `mixed_records` times the same image with compact step records
-(ipg_set_record_precision: transport matrices and tetrad rows in FP32
-between the kernels) and gives its error against the FP64 image;
-`--records mixed` does the same for a --quick run.  Under torchrun each rank
+region).  `mixed_records` times the same image in the mixed form: compact
+step records (ipg_set_record_precision) and the polarized step in FP32
+(ipg_set_step_precision), with its error against the FP64 image;
+`--records mixed --step fp32` select them for a --quick run.  Under torchrun each rank
 renders its own image (weak scaling, no collective on the data path); time
 is the max over ranks.  The reference arm
 runs the reference ipole built from its sources (oracle/_ref/ipole, the
@@ -258,6 +258,8 @@ def run_ours(args):
     ctx = ip.Context(local, pool_bytes=int(args.pool_gb * (1 << 30)))
     if args.records == "mixed":
         ctx.set_record_precision(ip.IPG_RECORDS_MIXED)
+    if args.step == "fp32":
+        ctx.set_step_precision(ip.IPG_STEP_FP32)
     ctx.upload(model)
     cam = ip.camera_for(p, model.grid)
     ij = np.array([(i, j) for i in range(nx) for j in range(ny)], dtype=np.int32)
@@ -334,6 +336,7 @@ def run_ours(args):
     # the transport matrices and tetrad rows stored in FP32 between the
     # kernels, timed like the headline, and its error against that image
     ctx.set_record_precision(ip.IPG_RECORDS_MIXED)
+    ctx.set_step_precision(ip.IPG_STEP_FP32)
     ctx.trace_device(cam, d_ij.data_ptr(), n, d_out.data_ptr())
     torch.cuda.synchronize()
     barrier(world)
@@ -347,12 +350,15 @@ def run_ours(args):
     mixed_ms = max_over_ranks(m0.elapsed_time(m1), world)
     mo = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=ip.PIXEL_DTYPE)
     ctx.set_record_precision(ip.IPG_RECORDS_FP64)
+    ctx.set_step_precision(ip.IPG_STEP_FP64)
     I0, Q0, U0, V0 = (float(out[k].sum()) for k in "IQUV")
     I1, Q1, U1, V1 = (float(mo[k].sum()) for k in "IQUV")
     bright = out["I"] > 1e-6 * out["I"].max()
     mixed = {"value": images_per_s(world, args.steps, mixed_ms), "unit": "images/s",
              "ms_per_step": mixed_ms / args.steps,
-             "records": "transport matrices and tetrad rows in FP32; coefficients and all arithmetic in FP64",
+             "form": "compact step records (transport matrices and tetrad rows in FP32) and the polarized "
+                     "step (Faraday rotation, absorption/emission) in FP32; geodesics, metric, tetrads, jar "
+                     "fits and the accumulation of N in FP64",
              "vs_fp64": {"Ftot_rel": abs(I1 / I0 - 1), "Q_rel_to_I": abs(Q1 - Q0) / abs(I0),
                          "U_rel_to_I": abs(U1 - U0) / abs(I0), "V_rel_to_I": abs(V1 - V0) / abs(I0),
                          "EVPA_deg": abs(float(np.degrees(0.5 * (np.arctan2(U1, Q1) - np.arctan2(U0, Q0))))),
@@ -450,6 +456,8 @@ def main():
                     help="trajectory pool size in GiB (0: 60%% of free device memory)")
     ap.add_argument("--records", default="fp64", choices=["fp64", "mixed"],
                     help="step-record storage between the kernels (ipg_set_record_precision); with --quick only")
+    ap.add_argument("--step", default="fp64", choices=["fp64", "fp32"],
+                    help="arithmetic of the polarized step (ipg_set_step_precision); with --quick only")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

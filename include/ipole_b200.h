@@ -271,6 +271,17 @@ int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 #define IPG_RECORDS_MIXED 1
 int ipg_set_record_precision(ipg_ctx *ctx, int precision);
 
+/* Arithmetic of the polarized transfer step (no counterpart in the
+ * reference).  IPG_STEP_FP64 (the default) is evolve_N of
+ * src/ipolarray.c:332-575 in FP64.  IPG_STEP_FP32 evaluates its Faraday
+ * rotation and absorption/emission in FP32, written in optical depths with
+ * the Stokes vector and emission scaled by a power of two per step; the
+ * projection of N and its update stay FP64.  The test of this mode states
+ * its errors against the FP64 step.  Returns IPG_E_ARG for another value. */
+#define IPG_STEP_FP64 0
+#define IPG_STEP_FP32 1
+int ipg_set_step_precision(ipg_ctx *ctx, int precision);
+
 /* The context's CUDA stream (a cudaStream_t), on which every kernel of the
  * context is launched; lets a caller bracket calls with its own events. */
 int ipg_get_stream(const ipg_ctx *ctx, void **stream);

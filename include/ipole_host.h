@@ -70,6 +70,9 @@ typedef struct ipg_params {
    * compactly between the kernels (ipg_set_record_precision,
    * IPG_RECORDS_MIXED); 0, the default, keeps them in FP64 */
   int mixed_records;
+  /* "fp32_step" (no reference counterpart): 1 evaluates the polarized step
+   * in FP32 (ipg_set_step_precision, IPG_STEP_FP32); 0, the default, FP64 */
+  int fp32_step;
 } ipg_params;
 
 /* Defaults of load_par_from_argv (src/par.c:48-100) and the model/radiation

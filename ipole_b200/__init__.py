@@ -33,6 +33,8 @@ NFIELD = 10
 STRLEN = 2048
 # step-record storage precision (ipg_set_record_precision)
 IPG_RECORDS_FP64, IPG_RECORDS_MIXED = 0, 1
+# arithmetic of the polarized step (ipg_set_step_precision)
+IPG_STEP_FP64, IPG_STEP_FP32 = 0, 1
 # per-step trace columns (include/ipole_b200.h, IPG_TRACE_*)
 TRACE_DOUBLES = 127
 TRACE_COLS = {"b": (0, 1), "ne": (1, 1), "thetae": (2, 1), "nu": (3, 1), "b_k_angle": (4, 1), "sigma": (5, 1),
@@ -120,7 +122,7 @@ class _Params(C.Structure):
                 ("plugin", C.c_char * STRLEN), ("MBH_set", C.c_int), ("analytic_model", C.c_int),
                 ("rho_unit", C.c_double), ("sphere_Thetae0", C.c_double), ("sphere_R0", C.c_double),
                 ("sphere_tau0", C.c_double), ("sphere_beta0", C.c_double), ("sphere_gam", C.c_double),
-                ("mixed_records", C.c_int)]
+                ("mixed_records", C.c_int), ("fp32_step", C.c_int)]
 
 
 class Plugin(C.Structure):
@@ -187,6 +189,7 @@ def lib():
     L.ipg_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
     L.ipg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.ipg_set_record_precision.argtypes = [C.c_void_p, C.c_int]
+    L.ipg_set_step_precision.argtypes = [C.c_void_p, C.c_int]
     L.ipg_camera_setup.argtypes = [C.POINTER(Grid)] + [C.c_double] * 9 + [C.c_int, C.c_int, C.c_double, C.c_int,
                                                                           C.POINTER(Camera), C.POINTER(C.c_double),
                                                                           C.POINTER(C.c_double),
@@ -415,6 +418,12 @@ class Context:
         IPG_RECORDS_MIXED (transport matrices and tetrad rows stored in
         FP32 between the kernels)."""
         _check(lib().ipg_set_record_precision(self._h, int(precision)), self._h)
+
+    def set_step_precision(self, precision: int):
+        """ipg_set_step_precision: IPG_STEP_FP64 (default) or IPG_STEP_FP32
+        (the polarized step's Faraday rotation and absorption/emission in
+        FP32)."""
+        _check(lib().ipg_set_step_precision(self._h, int(precision)), self._h)
 
     def stream(self) -> int:
         """The context's cudaStream_t as an integer handle."""

@@ -762,6 +762,139 @@ __device__ __forceinline__ int evolve_N_coef(const CoefBlock &cb, double dlam, i
   return flag;
 }
 
+
+/* (1 - e^-t) / t, bounded for every t (its limit 1 at t = 0) */
+__device__ __forceinline__ float one_minus_exp_over(float t)
+{
+  return (fabsf(t) < 1e-6f) ? 1.f - 0.5f * t : -expm1f(-t) / t;
+}
+
+/* The same Faraday and absorption/emission step as evolve_N_coef, in FP32
+ * (ipg_set_step_precision, IPG_STEP_FP32).  It is written in optical depths
+ * tau = alpha dl and emission j dl: the divisions by alpha of absorb_emit
+ * (src/ipolarray.c:410-500) become (1 - e^-tau) / tau factors, bounded for
+ * optically thin points where 1/alpha would overflow FP32.  S and j dl are
+ * scaled by one power of two taken from the step's magnitudes, so that the
+ * FP32 values stay in range (the step is linear in S and j, so the scaling is
+ * exact).  The Faraday angle is reduced modulo 2 pi in FP64 before its FP32
+ * sine and cosine.  The N to Stokes projection and the update of N stay
+ * FP64, so the accumulation along the ray is FP64. */
+__device__ __forceinline__ int evolve_N_coef_f32(const CoefBlock &cb, double dlam, int zero_emission, HermN *N,
+                                              double *tauF)
+{
+  double T11, T22, T12r, T21i;
+  hn_stokes(*N, cb.e1, cb.e2, &T11, &T22, &T12r, &T21i);
+  const double SId = (T11 + T22) / 2, SQd = (T11 - T22) / 2, SUd = T12r, SVd = T21i;
+  const double jxId = zero_emission ? 0. : cb.jI * dlam, jxQd = zero_emission ? 0. : cb.jQ * dlam,
+               jxVd = zero_emission ? 0. : cb.jV * dlam;
+  const int ex = ilogb(fmax(fmax(fabs(SId), fabs(jxId)), 1e-300));
+  const double sc = ldexp(1.0, -ex);
+  float SI = (float)(SId * sc), SQ = (float)(SQd * sc), SU = (float)(SUd * sc), SV = (float)(SVd * sc);
+  const float jI = (float)(jxId * sc), jQ = (float)(jxQd * sc), jV = (float)(jxVd * sc);
+  /* Faraday half step (rU = 0): S turns about r by rho dl / 2 */
+  const double rho2 = cb.rQ * cb.rQ + cb.rV * cb.rV;
+  float fc, fs, fg, nQ, nV;
+  if (rho2 > IPG_CUT_PREVENT_NAN) {
+    const double rho = sqrt(rho2), phi = rho * dlam * 0.5;
+    const float ph = (float)remainder(phi, 2. * IPG_PI);
+    float sh = sinf(0.5f * ph);
+    sincosf(ph, &fs, &fc);
+    fg = 2.f * sh * sh;
+    nQ = (float)(cb.rQ / rho);
+    nV = (float)(cb.rV / rho);
+  } else {
+    /* the linear form: c = 1, no axial term, sin(rho x) / rho = x */
+    fc = 1.f;
+    fg = 0.f;
+    fs = 1.f;
+    nQ = (float)(cb.rQ * dlam * 0.5);
+    nV = (float)(cb.rV * dlam * 0.5);
+  }
+  auto faraday = [&](float &Q, float &U, float &V) {
+    const float Q0 = Q, U0 = U, V0 = V;
+    const float f = (nQ * Q0 + nV * V0) * fg;
+    Q = Q0 * fc + nQ * f - nV * U0 * fs;
+    U = U0 * fc + (nV * Q0 - nQ * V0) * fs;
+    V = V0 * fc + nV * f + nQ * U0 * fs;
+  };
+  faraday(SQ, SU, SV);
+  /* absorption and emission over dl (aU = jU = 0).  The polarized form
+   * divides by tau_P^2; below tau_P^2 = 1e-30 (where its FP32 square would
+   * leave the normal range) the polarization coupling is negligible against
+   * FP32's precision and the step takes the unpolarized-absorption form, as
+   * the FP64 step does below alpha_P^2 = 1e-80 */
+  const double tP2d = (cb.aQ * cb.aQ + cb.aV * cb.aV) * dlam * dlam;
+  const float tI = (float)(cb.aI * dlam), tQ = (float)(cb.aQ * dlam), tV = (float)(cb.aV * dlam);
+  if (tP2d > 1e-30) {
+    const float tP2 = tQ * tQ + tV * tV, tP = sqrtf(tP2), itP2 = 1.f / tP2, ih = 0.5f / tP;
+    const float ads0 = tQ * SQ + tV * SV, adj = tQ * jQ + tV * jV;
+    const float em = expf(-(tI - tP)), ep = expf(-(tI + tP)), e0 = expf(-tI);
+    float SI2 = em * (0.5f * SI - ads0 * ih) + ep * (0.5f * SI + ads0 * ih);
+    const float cm = (-SI * tP + ads0) * (0.5f * itP2), cp = (SI * tP + ads0) * (0.5f * itP2);
+    float SQ2 = em * tQ * cm + ep * tQ * cp + e0 * (SQ - ads0 * tQ * itP2);
+    float SU2 = e0 * SU;
+    float SV2 = em * tV * cm + ep * tV * cp + e0 * (SV - ads0 * tV * itP2);
+    const float q0 = one_minus_exp_over(tI), qm = one_minus_exp_over(tI - tP), qp = one_minus_exp_over(tI + tP);
+    const float adjP = adj * itP2;
+    SQ2 += q0 * (jQ - tQ * adjP);
+    SV2 += q0 * (jV - tV * adjP);
+    SI2 += qm * (0.5f * jI - adj * ih) + qp * (0.5f * jI + adj * ih);
+    const float m2 = qm * (-tP * jI + adj) * (0.5f * itP2), p2 = qp * (tP * jI + adj) * (0.5f * itP2);
+    SQ2 += tQ * (m2 + p2);
+    SV2 += tV * (m2 + p2);
+    SI = SI2;
+    SQ = SQ2;
+    SU = SU2;
+    SV = SV2;
+  } else {
+    /* approximate_solve per component with constant j and alpha_I */
+    if (tI < 1e-3f) {
+      const float w = 1.f - (0.5f * tI) * (1.f - tI * (1.f / 3.f));
+      SI += (jI - SI * tI) * w;
+      SQ += (jQ - SQ * tI) * w;
+      SU += (0.f - SU * tI) * w;
+      SV += (jV - SV * tI) * w;
+    } else {
+      const float e0 = expf(-tI), q0 = one_minus_exp_over(tI);
+      SI = SI * e0 + jI * q0;
+      SQ = SQ * e0 + jQ * q0;
+      SU = SU * e0;
+      SV = SV * e0 + jV * q0;
+    }
+  }
+  faraday(SQ, SU, SV);
+  *tauF += dlam * fabs(cb.rV);
+  const double is = ldexp(1.0, ex);
+  double SIo = SI * is, SQo = SQ * is, SUo = SU * is, SVo = SV * is;
+  if (c_cam.stokes_floors) {
+    if (SIo < 0) {
+      SIo = SQo = SUo = SVo = 0;
+    } else {
+      double pf = sqrt(SQo * SQo + SUo * SUo + SVo * SVo) / SIo;
+      if (pf > 1.) {
+        SQo /= pf;
+        SUo /= pf;
+        SVo /= pf;
+      }
+    }
+  }
+  const double *a = cb.a, *b = cb.b;
+  double d11 = (SIo + SQo) - T11, d22 = (SIo - SQo) - T22, dr12 = SUo - T12r, di21 = SVo - T21i;
+#define DR(i, j) (a[i] * a[j] * d11 + b[i] * b[j] * d22 + (a[i] * b[j] + b[i] * a[j]) * dr12)
+#define DS(i, j) ((b[i] * a[j] - a[i] * b[j]) * di21)
+  N->r00 += DR(0, 0); N->r01 += DR(0, 1); N->r02 += DR(0, 2); N->r03 += DR(0, 3);
+  N->r11 += DR(1, 1); N->r12 += DR(1, 2); N->r13 += DR(1, 3);
+  N->r22 += DR(2, 2); N->r23 += DR(2, 3); N->r33 += DR(3, 3);
+  N->s01 += DS(0, 1); N->s02 += DS(0, 2); N->s03 += DS(0, 3);
+  N->s12 += DS(1, 2); N->s13 += DS(1, 3); N->s23 += DS(2, 3);
+#undef DR
+#undef DS
+  int flag = 0;
+  if (*tauF > 1.e100 || *tauF < -1.e100 || isnan(*tauF)) flag |= 2;
+  if (isnan(N->r00) || isnan(SIo)) flag |= 4;
+  return flag;
+}
+
 /* block width of the transfer for the longest length class (its blocks fill
  * an SM's registers); the compiled kernel's thread bound for every class */
 #ifndef IPG_XFER_WIDE
@@ -847,7 +980,7 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
   }
 }
 
-template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB>
+template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false>
 __global__ void __launch_bounds__(TPB, MINB)
     k_transfer(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
                const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays, ipg_pixel_out *__restrict__ out,
@@ -924,7 +1057,8 @@ __global__ void __launch_bounds__(TPB, MINB)
       else L.I = approximate_solve(L.I, ji, ki, jf, kf, dl, &L.tau);
       if (!unpol) {
         L.flag |= flags >> 2;
-        L.flag |= evolve_N_coef(cb, dl, zero_emission, &L.N, &L.tauF);
+        if constexpr (S32) L.flag |= evolve_N_coef_f32(cb, dl, zero_emission, &L.N, &L.tauF);
+        else L.flag |= evolve_N_coef(cb, dl, zero_emission, &L.N, &L.tauF);
       }
     }
     L.dl_i = cb.dl;
@@ -1065,6 +1199,7 @@ struct ipg_ctx {
   int split;         /* 1: split waves into long and short batches */
   int emission_type; /* of the camera being traced */
   int rec_mixed;     /* IPG_RECORDS_MIXED: compact step records */
+  int step32;        /* IPG_STEP_FP32: the polarized step in FP32 */
   int32_t *d_ij;
   ipg_pixel_out *d_out;
   size_t cap;
@@ -1438,9 +1573,16 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[2], b.stream));
-  int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB>, xthreads, b.run);
-  k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB><<<tb, xthreads, 0, b.stream>>>(b.list, (int)b.run, b.pool, b.chunk_prev,
-                                                                         ctx->d_rays, d_out, b.cnt);
+  if (ctx->step32) {
+    /* IPG_STEP_FP32: its own compiled kernel, so the FP64 one is unchanged */
+    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, true>, xthreads, b.run);
+    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, true><<<tb, xthreads, 0, b.stream>>>(
+        b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);
+  } else {
+    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB>, xthreads, b.run);
+    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB><<<tb, xthreads, 0, b.stream>>>(b.list, (int)b.run, b.pool,
+                                                                           b.chunk_prev, ctx->d_rays, d_out, b.cnt);
+  }
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[3], b.stream));
   return IPG_OK;
@@ -1794,6 +1936,13 @@ extern "C" int ipg_set_record_precision(ipg_ctx *ctx, int precision)
 {
   if (!ctx || (precision != IPG_RECORDS_FP64 && precision != IPG_RECORDS_MIXED)) return IPG_E_ARG;
   ctx->rec_mixed = precision == IPG_RECORDS_MIXED;
+  return IPG_OK;
+}
+
+extern "C" int ipg_set_step_precision(ipg_ctx *ctx, int precision)
+{
+  if (!ctx || (precision != IPG_STEP_FP64 && precision != IPG_STEP_FP32)) return IPG_E_ARG;
+  ctx->step32 = precision == IPG_STEP_FP32;
   return IPG_OK;
 }
 

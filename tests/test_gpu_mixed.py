@@ -54,22 +54,51 @@ def test_record_precision_argument():
 
 
 def test_cli_mixed_records_key(dumps, tmp_path):
-    """--mixed_records=1 on the command line gives the compact records'
-    image, and its difference from the default run stays within the bounds."""
+    """--mixed_records=1 (and --fp32_step=1) on the command line give the
+    mixed forms' images, whose differences from the default run stay within
+    the bounds."""
     import subprocess
 
     from ipole_b200 import build, ipgc
     meta, _ = common.load_golden("c1_faraday_24")
     build.build()
     imgs = {}
-    for tag, extra in (("fp64", []), ("mixed", ["--mixed_records=1"])):
+    for tag, extra in (("fp64", []), ("mixed", ["--mixed_records=1"]),
+                       ("mixed_fp32", ["--mixed_records=1", "--fp32_step=1"])):
         out = str(tmp_path / f"{tag}.h5")
         r = subprocess.run([build.CLI, f"--dump={dumps.get(meta)}", *meta["args"], *extra, f"--outfile={out}"],
                            capture_output=True, text=True, cwd=str(tmp_path), timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         imgs[tag] = ipgc.read(out)
-    a, b = imgs["fp64"]["/pol"], imgs["mixed"]["/pol"]
-    assert not np.array_equal(a, b)  # the key took effect
-    e = abs(b[..., 0].sum() / a[..., 0].sum() - 1)
-    print("CLI mixed_records: total flux relative difference", e)
-    assert e <= BOUNDS["Ftot"]
+    a = imgs["fp64"]["/pol"]
+    for tag in ("mixed", "mixed_fp32"):
+        b = imgs[tag]["/pol"]
+        assert not np.array_equal(a, b)  # the keys took effect
+        e = abs(b[..., 0].sum() / a[..., 0].sum() - 1)
+        print(f"CLI {tag}: total flux relative difference", e)
+        assert e <= BOUNDS["Ftot"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fp32_step_against_fp64(case, dumps):
+    """ipg_set_step_precision(IPG_STEP_FP32): the polarized step's Faraday
+    rotation and absorption/emission in FP32 (optical-depth form, Stokes
+    vector and emission scaled by a power of two per step), alone and with
+    the compact records, against the FP64 step on the same image."""
+    meta, _ = common.load_golden(case)
+    p = common.params_for(meta, dumps.get(meta))
+    m = ip.Model.load(p)
+    with ip.Context() as c:
+        c.upload(m)
+        full = c.render(p, m)
+        c.set_step_precision(ip.IPG_STEP_FP32)
+        step = c.render(p, m)
+        c.set_record_precision(ip.IPG_RECORDS_MIXED)
+        both = c.render(p, m)
+    ref = {"unpol": full.unpol, **({"pol": full.pol} if full.pol is not None else {})}
+    for tag, img in (("fp32 step", step), ("fp32 step + compact records", both)):
+        e = common.image_errors(img, ref)
+        print(case, tag, {k: f"{v:.2e}" for k, v in e.items()})
+        assert np.array_equal(img.nstep, full.nstep)
+        bad = {k: v for k, v in e.items() if k in BOUNDS and not v <= BOUNDS[k]}
+        assert not bad, (tag, bad)
