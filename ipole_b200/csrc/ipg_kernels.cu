@@ -763,6 +763,57 @@ __device__ __forceinline__ int evolve_N_coef(const CoefBlock &cb, double dlam, i
 }
 
 
+
+/* push_polar (src/ipolarray.c:253-289) with its increment in FP32, for the
+ * FP32-step kernel: Mh is scaled by a power of two taken from its largest
+ * diagonal entry (for N = sum f f^dagger every |N^ij| is at most the largest
+ * N^ii), the products A Mh run in FP32, and the unscaled increment is
+ * subtracted from base in FP64. */
+__device__ __forceinline__ void hn_push_f32(const HermN &base, const HermN &Mh, const double A[4][4], double dl,
+                                            HermN *out)
+{
+  const double big = fmax(fmax(fabs(Mh.r00), fabs(Mh.r11)), fmax(fmax(fabs(Mh.r22), fabs(Mh.r33)), 1e-300));
+  const int ex = ilogb(big);
+  const double sc = ldexp(1.0, -ex), us = ldexp(dl, ex);
+  const float r00 = (float)(Mh.r00 * sc), r01 = (float)(Mh.r01 * sc), r02 = (float)(Mh.r02 * sc),
+              r03 = (float)(Mh.r03 * sc), r11 = (float)(Mh.r11 * sc), r12 = (float)(Mh.r12 * sc),
+              r13 = (float)(Mh.r13 * sc), r22 = (float)(Mh.r22 * sc), r23 = (float)(Mh.r23 * sc),
+              r33 = (float)(Mh.r33 * sc);
+  const float s01 = (float)(Mh.s01 * sc), s02 = (float)(Mh.s02 * sc), s03 = (float)(Mh.s03 * sc),
+              s12 = (float)(Mh.s12 * sc), s13 = (float)(Mh.s13 * sc), s23 = (float)(Mh.s23 * sc);
+  const float R[4][4] = {{r00, r01, r02, r03}, {r01, r11, r12, r13}, {r02, r12, r22, r23}, {r03, r13, r23, r33}};
+  const float S[4][4] = {{0.f, s01, s02, s03}, {-s01, 0.f, s12, s13}, {-s02, -s12, 0.f, s23}, {-s03, -s13, -s23, 0.f}};
+  float Af[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) Af[i][j] = (float)A[i][j];
+  float AR[4][4], AS[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      AR[i][j] = Af[i][0] * R[0][j] + Af[i][1] * R[1][j] + Af[i][2] * R[2][j] + Af[i][3] * R[3][j];
+      AS[i][j] = Af[i][0] * S[0][j] + Af[i][1] * S[1][j] + Af[i][2] * S[2][j] + Af[i][3] * S[3][j];
+    }
+  out->r00 = base.r00 - us * (double)(AR[0][0] + AR[0][0]);
+  out->r01 = base.r01 - us * (double)(AR[0][1] + AR[1][0]);
+  out->r02 = base.r02 - us * (double)(AR[0][2] + AR[2][0]);
+  out->r03 = base.r03 - us * (double)(AR[0][3] + AR[3][0]);
+  out->r11 = base.r11 - us * (double)(AR[1][1] + AR[1][1]);
+  out->r12 = base.r12 - us * (double)(AR[1][2] + AR[2][1]);
+  out->r13 = base.r13 - us * (double)(AR[1][3] + AR[3][1]);
+  out->r22 = base.r22 - us * (double)(AR[2][2] + AR[2][2]);
+  out->r23 = base.r23 - us * (double)(AR[2][3] + AR[3][2]);
+  out->r33 = base.r33 - us * (double)(AR[3][3] + AR[3][3]);
+  out->s01 = base.s01 - us * (double)(AS[0][1] - AS[1][0]);
+  out->s02 = base.s02 - us * (double)(AS[0][2] - AS[2][0]);
+  out->s03 = base.s03 - us * (double)(AS[0][3] - AS[3][0]);
+  out->s12 = base.s12 - us * (double)(AS[1][2] - AS[2][1]);
+  out->s13 = base.s13 - us * (double)(AS[1][3] - AS[3][1]);
+  out->s23 = base.s23 - us * (double)(AS[2][3] - AS[3][2]);
+}
+
 /* (1 - e^-t) / t, bounded for every t (its limit 1 at t = 0) */
 __device__ __forceinline__ float one_minus_exp_over(float t)
 {
@@ -899,6 +950,10 @@ __device__ __forceinline__ int evolve_N_coef_f32(const CoefBlock &cb, double dla
  * an SM's registers); the compiled kernel's thread bound for every class */
 #ifndef IPG_XFER_WIDE
 #define IPG_XFER_WIDE 256
+#endif
+/* the FP32-step kernel also pushes N with FP32 increments */
+#ifndef IPG_S32_PUSH
+#define IPG_S32_PUSH 1
 #endif
 
 struct XferLane {
@@ -1039,9 +1094,15 @@ __global__ void __launch_bounds__(TPB, MINB)
       double A[4][4];
       HermN Nh, Nn;
       load_A_rec(L.rec_i, 0, A);
-      hn_push(L.N, L.N, A, dlhalf, &Nh);
-      load_A_rec(L.rec_i, 1, A);
-      hn_push(L.N, Nh, A, dlfull, &Nn);
+      if constexpr (S32 && IPG_S32_PUSH) {
+        hn_push_f32(L.N, L.N, A, dlhalf, &Nh);
+        load_A_rec(L.rec_i, 1, A);
+        hn_push_f32(L.N, Nh, A, dlfull, &Nn);
+      } else {
+        hn_push(L.N, L.N, A, dlhalf, &Nh);
+        load_A_rec(L.rec_i, 1, A);
+        hn_push(L.N, Nh, A, dlfull, &Nn);
+      }
       L.N = Nn;
     }
     int flags = (int)cb.flags;
