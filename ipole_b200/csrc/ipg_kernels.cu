@@ -173,7 +173,9 @@ __device__ __forceinline__ void store_geo(double *p, const double X[4], const do
   store4(p + REC_X1, X[1], X[2], X[3], dl);
   store4(p + REC_K, K[0], K[1], K[2], K[3]);
   store4(p + REC_XH1, Xh[1], Xh[2], nturns, X[0]); /* X0: for the trace output only */
-  store4(p + REC_KH, Kh[0], Kh[1], Kh[2], Kh[3]);
+  /* K at the half step: read only by the per-step trace, which always uses
+   * the FP64 layout; the compact layout skips it */
+  if (!c_cam.mixed) store4(p + REC_KH, Kh[0], Kh[1], Kh[2], Kh[3]);
 }
 
 /* init_XK, src/model_geodesics.c:178-212, and Kcon *= freq (src/main.c:837).
