@@ -263,7 +263,7 @@ int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
  * plain tier.  IPG_RECORDS_MIXED stores the transport matrices and the plasma
  * tetrad rows (order-one values) in FP32 and the emission, absorption and
  * rotation coefficients in FP64; all arithmetic stays FP64, and the walk back
- * reads 296 bytes per step instead of 512.  Its images differ from the FP64
+ * reads 320 bytes per step instead of 512.  Its images differ from the FP64
  * records' by the FP32 rounding of those values (the test of this mode states
  * the errors); ipg_trace_ray and ipg_trace_pixels_noalloc always use FP64.
  * Returns IPG_E_ARG for another value. */

@@ -110,17 +110,19 @@ __device__ __forceinline__ void load_A(const double *p, double A[4][4])
 
 /* Compact step records (IPG_RECORDS_MIXED), same 512-byte stride:
  *   floats  0..15  A1, floats 16..31  A2                      (bytes   0-127)
- *   doubles 16..28 flags ju ku dl jI jQ jV aI aQ aV nturns rQ rV (128-231)
- *   floats 60..75  tetrad rows e1, e2 (covariant), a, b (contravariant)
- *                                                             (bytes 240-303)
- * The geodesic state (doubles 32..47, bytes 256-383) stays where the FP64
- * layout has it; k_coeffs reads it before writing the coefficients, whose
- * tetrad floats overlap its first doubles. */
+ *   doubles 16..28 flags ju ku dl jI jQ jV aI aQ aV nturns rQ rV, then
+ *                  3 doubles of padding                       (bytes 128-255)
+ *   floats 64..79  tetrad rows e1, e2 (covariant), a, b (contravariant)
+ *                                                             (bytes 256-319)
+ * Every write covers whole 32-byte sectors, so none needs the sector read
+ * first.  The geodesic state (doubles 32..47, bytes 256-383) stays where the
+ * FP64 layout has it; k_coeffs reads it before writing the coefficients,
+ * whose tetrad floats overwrite its first 64 bytes. */
 #define RECM_A1F 0
 #define RECM_A2F 16
 #define RECM_COEF 16
-#define RECM_TETF 60
-static_assert(RECM_COEF * 2 >= RECM_A2F + 16 && RECM_TETF >= (RECM_COEF + 13) * 2 && RECM_TETF + 16 <= 128,
+#define RECM_TETF 64
+static_assert(RECM_COEF * 2 >= RECM_A2F + 16 && RECM_TETF >= (RECM_COEF + 16) * 2 && RECM_TETF + 16 <= 128,
               "compact record layout");
 
 __device__ __forceinline__ void store_A_f(float *p, const double A[4][4])
@@ -614,7 +616,7 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
       store4(q, (double)flags, ju, ku, dl_rec);
       store4(q + 4, jar.jI, jar.jQ, jar.jV, jar.aI);
       store4(q + 8, jar.aQ, jar.aV, nturns_rec, jar.rQ);
-      q[12] = jar.rV;
+      store4(q + 12, jar.rV, 0., 0., 0.); /* padding: whole sectors */
       float4 *t = reinterpret_cast<float4 *>(reinterpret_cast<float *>(p) + RECM_TETF);
       t[0] = make_float4((float)e1[0], (float)e1[1], (float)e1[2], (float)e1[3]);
       t[1] = make_float4((float)e2[0], (float)e2[1], (float)e2[2], (float)e2[3]);
