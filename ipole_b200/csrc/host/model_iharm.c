@@ -144,7 +144,7 @@ int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m)
   char metric_name[32] = {0};
   if (ipgc_get_str(&file, "/header/metric", metric_name, sizeof(metric_name)) != 0 ||
       (strncmp(metric_name, "MMKS", 19) != 0 && strncmp(metric_name, "FMKS", 19) != 0)) {
-    fprintf(stderr, "File is in metric '%s'; this build supports FMKS/MMKS only.\n", metric_name);
+    fprintf(stderr, "File is in metric '%s'; this program supports FMKS/MMKS only.\n", metric_name);
     ipgc_free(&file);
     return IPG_E_FORMAT;
   }

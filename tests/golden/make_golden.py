@@ -188,7 +188,7 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
     # the reference's own noise floor: the largest deviation from this
     # -ffp-contract=off build among the other legal builds of the same sources
     # (the makefile's -O3 FMA build, -O2 with FMA contraction, -O3 for
-    # AVX-512, and this build with a libm one ulp away; oracle/Makefile
+    # AVX-512, and the no-FMA build with a libm one ulp away; oracle/Makefile
     # targets ref and noise), in the metrics the tests use
     from tests.common import image_errors
     floor, used = None, []

@@ -11,7 +11,7 @@ path.
             (80x80, fov 1200 muas, dsource 8 kpc).  The table was made by an
             older ipole in plain Kerr-Schild coordinates; the reference
             built here (eMinkowski) lands within 0.38% of it on every row
-            (Ftot_unpol about +0.25% throughout), and this build must land
+            (Ftot_unpol about +0.25% throughout), and the GPU path must land
             within SPHERE_TOL = 1%.
 
 Image-level parity with the reference's builds of these models is in
