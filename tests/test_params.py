@@ -55,3 +55,15 @@ def test_missing_par_file():
     with pytest.raises(ip.IpgError) as e:
         ip.Params.from_args(["-par", "/nonexistent/file.par"])
     assert e.value.code == ip.IPG_E_IO
+
+
+def test_mixed_precision_keys(tmp_path):
+    """mixed_records and fp32_step (keys of this implementation, no reference
+    counterpart) are off by default and read from the command line and from
+    -par files like any other integer key."""
+    p = ip.Params()
+    assert p.mixed_records == 0 and p.fp32_step == 0
+    par = tmp_path / "m.par"
+    par.write_text("fp32_step 1\n")
+    q = ip.Params.from_args(["--mixed_records=1", "-par", str(par)])
+    assert q.mixed_records == 1 and q.fp32_step == 1
