@@ -153,9 +153,10 @@ __device__ __forceinline__ void store_A_rec(double *rec, int which, const double
   else store_A(rec + (which ? REC_A2 : REC_A1), A);
 }
 
+template <int RM = -1>
 __device__ __forceinline__ void load_A_rec(const double *rec, int which, double A[4][4])
 {
-  if (c_cam.mixed) load_A_f(reinterpret_cast<const float *>(rec) + (which ? RECM_A2F : RECM_A1F), A);
+  if (RM < 0 ? c_cam.mixed : RM) load_A_f(reinterpret_cast<const float *>(rec) + (which ? RECM_A2F : RECM_A1F), A);
   else load_A(rec + (which ? REC_A2 : REC_A1), A);
 }
 
@@ -976,10 +977,11 @@ struct XferLane {
 #ifndef IPG_XFER_PREFETCH
 #define IPG_XFER_PREFETCH 1
 #endif
+template <int RM = -1>
 __device__ __forceinline__ void prefetch_rec(const double *p)
 {
   /* the compact layout's walk reads only the first three 128-byte lines */
-  const int nl = c_cam.mixed ? 3 : 4;
+  const int nl = (RM < 0 ? c_cam.mixed : RM) ? 3 : 4;
 #if IPG_XFER_PREFETCH == 1
 #pragma unroll
   for (int l = 0; l < 4; l++)
@@ -993,6 +995,7 @@ __device__ __forceinline__ void prefetch_rec(const double *p)
 
 /* Take the next ray whose trajectory is complete; rays that hit maxnstep get
  * an all-zero result, deferred rays are left for their next wave. */
+template <int RM = -1>
 __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restrict__ list, int n_list,
                                            const double *__restrict__ pool, const int *__restrict__ chunk_prev,
                                            const RayRec *__restrict__ rays,
@@ -1017,10 +1020,10 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
     L.chunk = rec.last_chunk;
     L.rec_i = step_ptr(const_cast<double *>(pool), L.chunk, L.n % IPG_CHUNK_STEPS);
     L.cprev = chunk_prev[L.chunk];
-    prefetch_rec(L.rec_i);
-    if (L.n % IPG_CHUNK_STEPS) prefetch_rec(L.rec_i - IPG_STEP_DOUBLES);
+    prefetch_rec<RM>(L.rec_i);
+    if (L.n % IPG_CHUNK_STEPS) prefetch_rec<RM>(L.rec_i - IPG_STEP_DOUBLES);
     /* get_jkinv at the far end of the ray, src/ipolarray.c:74 */
-    if (c_cam.mixed) {
+    if (RM < 0 ? c_cam.mixed : RM) {
       L.js = L.rec_i[RECM_COEF + 1];
       L.ks = L.rec_i[RECM_COEF + 2];
       L.dl_i = L.rec_i[RECM_COEF + 3];
@@ -1039,7 +1042,9 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
   }
 }
 
-template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false>
+/* RM: the step-record layout, 0 FP64, 1 compact, -1 from the camera (the
+ * no-alloc path) */
+template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false, int RM = -1>
 __global__ void __launch_bounds__(TPB, MINB)
     k_transfer(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
                const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays, ipg_pixel_out *__restrict__ out,
@@ -1049,7 +1054,7 @@ __global__ void __launch_bounds__(TPB, MINB)
   const DevCam &C = c_cam;
   const int unpol = C.unpol;
   XferLane L;
-  bool has = xfer_fetch(L, list, n_list, pool, chunk_prev, rays, out, counters);
+  bool has = xfer_fetch<RM>(L, list, n_list, pool, chunk_prev, rays, out, counters);
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
     if (L.n == 0) {
@@ -1072,7 +1077,7 @@ __global__ void __launch_bounds__(TPB, MINB)
       o.flag = L.flag;
       out[L.ray] = o;
       atomicAdd(&counters[CNT_RAD], (unsigned long long)L.nrad);
-      has = xfer_fetch(L, list, n_list, pool, chunk_prev, rays, out, counters);
+      has = xfer_fetch<RM>(L, list, n_list, pool, chunk_prev, rays, out, counters);
       continue;
     }
     /* step n -> n-1 of integrate_emission's loop, src/ipolarray.c:78-244 */
@@ -1084,11 +1089,11 @@ __global__ void __launch_bounds__(TPB, MINB)
     const double *rec_f = step_ptr(const_cast<double *>(pool), L.chunk, s % IPG_CHUNK_STEPS);
     /* the record the next iteration reads (step s-1), and the one after */
     if (s >= 1) {
-      if ((s - 1) % IPG_CHUNK_STEPS != IPG_CHUNK_STEPS - 1) prefetch_rec(rec_f - IPG_STEP_DOUBLES);
-      else if (L.cprev >= 0) prefetch_rec(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
+      if ((s - 1) % IPG_CHUNK_STEPS != IPG_CHUNK_STEPS - 1) prefetch_rec<RM>(rec_f - IPG_STEP_DOUBLES);
+      else if (L.cprev >= 0) prefetch_rec<RM>(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
     }
     CoefBlock cb;
-    if (C.mixed) load_coef_m(rec_f, cb);
+    if (RM < 0 ? C.mixed : RM) load_coef_m(rec_f, cb);
     else load_coef(rec_f, cb);
     double dl = L.dl_i;
     if (!unpol) {
@@ -1097,14 +1102,14 @@ __global__ void __launch_bounds__(TPB, MINB)
       double dlhalf = (0.5 * dl) * G.inv_dlfac;
       double A[4][4];
       HermN Nh, Nn;
-      load_A_rec(L.rec_i, 0, A);
+      load_A_rec<RM>(L.rec_i, 0, A);
       if constexpr (S32 && IPG_S32_PUSH) {
         hn_push_f32(L.N, L.N, A, dlhalf, &Nh);
-        load_A_rec(L.rec_i, 1, A);
+        load_A_rec<RM>(L.rec_i, 1, A);
         hn_push_f32(L.N, Nh, A, dlfull, &Nn);
       } else {
         hn_push(L.N, L.N, A, dlhalf, &Nh);
-        load_A_rec(L.rec_i, 1, A);
+        load_A_rec<RM>(L.rec_i, 1, A);
         hn_push(L.N, Nh, A, dlfull, &Nn);
       }
       L.N = Nn;
@@ -1638,16 +1643,23 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[2], b.stream));
+  /* one compiled transfer per step arithmetic and record layout, each
+   * holding only its own paths */
+#define IPG_LAUNCH_XFER(S32, RM)                                                                              \
+  do {                                                                                                       \
+    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM>, xthreads,    \
+                         b.run);                                                                             \
+    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM><<<tb, xthreads, 0, b.stream>>>(                       \
+        b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);                                \
+  } while (0)
   if (ctx->step32) {
-    /* IPG_STEP_FP32: its own compiled kernel, so the FP64 one is unchanged */
-    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, true>, xthreads, b.run);
-    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, true><<<tb, xthreads, 0, b.stream>>>(
-        b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);
+    if (ctx->rec_mixed) IPG_LAUNCH_XFER(true, 1);
+    else IPG_LAUNCH_XFER(true, 0);
   } else {
-    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB>, xthreads, b.run);
-    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB><<<tb, xthreads, 0, b.stream>>>(b.list, (int)b.run, b.pool,
-                                                                           b.chunk_prev, ctx->d_rays, d_out, b.cnt);
+    if (ctx->rec_mixed) IPG_LAUNCH_XFER(false, 1);
+    else IPG_LAUNCH_XFER(false, 0);
   }
+#undef IPG_LAUNCH_XFER
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[3], b.stream));
   return IPG_OK;
