@@ -46,9 +46,9 @@ M_UNIT = 7.5e27
 BASE_ARGS = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
              "--fov=160", "--trat_large=160", "--trat_small=1"]
 CPU_SAMPLE = 64  # reference / oracle sample image size (pixels per side)
-# Work per ray-step of each kernel, from the ncu capture of the small case
-# (profiles/kernels_small_200x200_iharm128.md): FP64 flops (2 per DFMA, 1 per
-# DADD/DMUL) and DRAM bytes read + written.  k_coeffs works per step record
+# Work per ray-step of each kernel, from the ncu capture of a 200x200 image of
+# the 128x64x64 dump: FP64 flops (2 per DFMA, 1 per DADD/DMUL) and DRAM bytes
+# read + written.  k_coeffs works per step record
 # (ray-steps + one camera record per ray).
 FLOPS_PER_STEP = {"geodesic": 1831, "coeffs": 1535, "transfer": 913}
 DRAM_BYTES_PER_STEP = {"geodesic": 377, "coeffs": 412, "transfer": 537}

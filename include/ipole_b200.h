@@ -112,7 +112,8 @@ const char *ipg_last_error(const ipg_ctx *ctx);
  * exactly the arrays model/iharm/model.c keeps in data[0] (p[U1..B3], ne,
  * thetae, b, sigma).  Replaces the model's static field storage as the source
  * of get_model_fourv / get_model_ne / get_model_thetae / get_model_b /
- * get_model_sigma point queries. */
+ * get_model_sigma point queries.  Returns IPG_E_ARG unless grid->metric is
+ * IPG_METRIC_FMKS. */
 int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *grid, const double *const fields[IPG_NFIELD]);
 
 /* ---- known-answer models (model/analytic/model.c, model/sphere/model.c) ----
@@ -173,6 +174,7 @@ int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *
  * which is synchronised before the call returns.
  *
  * Limits: n <= IPG_NOALLOC_MAX_RAYS and cam->maxnstep <= IPG_NOALLOC_MAX_STEPS,
+ * otherwise IPG_E_ARG; grid->metric must be IPG_METRIC_FMKS (an iharm dump),
  * otherwise IPG_E_ARG.  The scratch holds IPG_NOALLOC_MAX_STEPS trajectory
  * steps at a time, so a batch runs in as many waves as it needs and is much
  * slower than ipg_trace_pixels_device.  Returns IPG_E_MAXNSTEP like
@@ -180,11 +182,15 @@ int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *
  *
  * The first call on a device sets the call up: it looks up the device address
  * of the scratch array, which may load the library's device code, so make
- * that first call before any stream capture begins.  All calls share the
+ * that first call before any stream capture begins.  The address is kept for
+ * the life of the process, so resetting the device (cudaDeviceReset) between
+ * calls is not supported.  Every call synchronises `stream` and copies a few
+ * status words back to the host before it returns.  All calls share the
  * scratch array and the kernels' constant parameters, which keep what the last
  * call wrote: calls whose work overlaps on the GPU (from other streams or host
  * threads, or a context's ipg_trace_pixels* calls) race and give wrong
- * results, so serialise them. */
+ * results, so serialise them.  Per ray, the results are the bits that
+ * ipg_trace_pixels_device gives with FP64 step records. */
 #define IPG_NOALLOC_MAX_RAYS 65536
 #define IPG_NOALLOC_MAX_STEPS 51200
 #define IPG_NOALLOC_SCRATCH_BYTES 27806720

@@ -1388,6 +1388,11 @@ extern "C" int ipg_upload_iharm(ipg_ctx *ctx, const ipg_grid *g, const double *c
   if (!ctx || !g || !fields || g->n1 <= 0 || g->n2 <= 0 || g->n3 <= 0) return IPG_E_ARG;
   for (int f = 0; f < IPG_NFIELD; f++)
     if (!fields[f]) return IPG_E_ARG;
+  if (g->metric != IPG_METRIC_FMKS) {
+    snprintf(ctx->err, sizeof(ctx->err), "an iharm dump needs the FMKS metric (%d), grid has %d", IPG_METRIC_FMKS,
+             g->metric);
+    return IPG_E_ARG;
+  }
   CK(cudaSetDevice(ctx->device));
   size_t ncell = (size_t)(g->n1 + 2) * (g->n2 + 2) * (g->n3 + 2);
   /* cell-major (AoS) layout: the 10 fields of a zone are 80 contiguous bytes
@@ -2153,7 +2158,7 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
 {
   if (!g || !d_fields || !cam || (n && (!d_ij || !d_out))) return IPG_E_ARG;
   if (n > IPG_NOALLOC_MAX_RAYS || cam->maxnstep > IPG_NOALLOC_MAX_STEPS) return IPG_E_ARG;
-  if (g->n1 <= 0 || g->n2 <= 0 || g->n3 <= 0) return IPG_E_ARG;
+  if (g->n1 <= 0 || g->n2 <= 0 || g->n3 <= 0 || g->metric != IPG_METRIC_FMKS) return IPG_E_ARG;
   if (cam->emission_type != 4 && cam->emission_type != 1) return IPG_E_ARG;
   if (cam->maxnstep < 2 || cam->nx <= 0 || cam->ny <= 0) return IPG_E_ARG;
   if (n == 0) return IPG_OK;
@@ -2174,36 +2179,7 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
 
   /* grid constants as ipg_upload_iharm derives them */
   DevGrid d;
-  memset(&d, 0, sizeof(d));
-  d.n1 = g->n1;
-  d.n2 = g->n2;
-  d.n3 = g->n3;
-  for (int i = 0; i < 4; i++) {
-    d.startx[i] = g->startx[i];
-    d.stopx[i] = g->stopx[i];
-    d.dx[i] = g->dx[i];
-    d.cstartx[i] = g->cstartx[i];
-    d.cstopx[i] = g->cstopx[i];
-  }
-  d.a = g->a;
-  d.hslope = g->hslope;
-  d.poly_xt = g->poly_xt;
-  d.poly_alpha = g->poly_alpha;
-  d.mks_smooth = g->mks_smooth;
-  d.poly_norm = g->poly_norm;
-  d.Rh = g->Rh;
-  d.rmin_geo = g->rmin_geo;
-  d.rmax_geo = g->rmax_geo;
-  d.th_beg = g->th_beg;
-  d.sigma_cut = g->sigma_cut;
-  d.sigma_eq_factor = (g->sigma_cut_high > 0 && g->sigma_cut_high > g->sigma_cut) ? 1. : 0.;
-  d.L_unit = g->L_unit;
-  d.dlfac = g->L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
-  d.sj = g->n3 + 2;
-  d.si = (long long)(g->n2 + 2) * (g->n3 + 2);
-  double am1 = g->poly_alpha - 1.;
-  d.alpha_int = (am1 >= 0 && am1 <= 64 && am1 == (double)(int)am1) ? (int)am1 : -1;
-  devgrid_derived(&d);
+  devgrid_from(g, &d);
   DevCam dc;
   make_devcam(cam, &dc);
   NA_CK(cudaMemcpyToSymbolAsync(c_grid, &d, sizeof(DevGrid), 0, cudaMemcpyHostToDevice, stream));
@@ -2235,11 +2211,19 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
     k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB><<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta,
                                                            n_chunks, cnt_d, rays, lists[cur ^ 1]);
     NA_CK(cudaGetLastError());
-    int cb = na_blocks(n_sm, (const void *)k_coeffs<IPG_PLUG_IHARM>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
-    k_coeffs<IPG_PLUG_IHARM><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
+    /* the compiled kernels of a context's FP64 path, so that both give the
+     * same bits for every ray */
+    if (cam->emission_type == 1) {
+      int cb = na_blocks(n_sm, (const void *)k_coeffs<IPG_PLUG_IHARM, 1>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
+      k_coeffs<IPG_PLUG_IHARM, 1><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
+    } else {
+      int cb = na_blocks(n_sm, (const void *)k_coeffs<IPG_PLUG_IHARM, 4>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
+      k_coeffs<IPG_PLUG_IHARM, 4><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
+    }
     NA_CK(cudaGetLastError());
-    int tb = na_blocks(n_sm, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB>, threads, run);
-    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB><<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev, rays, d_out, cnt_d);
+    int tb = na_blocks(n_sm, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0>, threads, run);
+    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0><<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev,
+                                                                                   rays, d_out, cnt_d);
     NA_CK(cudaGetLastError());
     unsigned long long cnt[CNT_N];
     NA_CK(cudaMemcpyAsync(cnt, cnt_d, sizeof(cnt), cudaMemcpyDeviceToHost, stream));

@@ -40,11 +40,13 @@ class OrcCamera(C.Structure):
                 ("target_nturns", C.c_int), ("subring_dtheta", C.c_int), ("counterjet", C.c_int)]
 
 
-def build(ref: bool = False) -> str:
-    """make the restatement (and, when the reference tree is present and
-    ref=True, the reference binaries)."""
-    targets = ["oracle"] + (["ref"] if ref and os.path.isdir(os.environ.get("IPG_REFERENCE", "/root/reference"))
-                            else [])
+def build(ref_dir: str | None = None) -> str:
+    """make the restatement and, when a reference checkout is given (ref_dir,
+    else the IPG_REFERENCE environment variable) and present, the reference
+    binaries compiled from its sources."""
+    ref_dir = ref_dir or os.environ.get("IPG_REFERENCE")
+    have_ref = bool(ref_dir) and os.path.isdir(ref_dir)
+    targets = ["oracle"] + (["ref", f"REF={ref_dir}"] if have_ref else [])
     r = subprocess.run(["make", "-C", HERE, *targets], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)

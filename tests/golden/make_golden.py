@@ -2,7 +2,7 @@
 
 Cases on a dump run the reference's iharm build; cases whose "dump" is the
 name of a known-answer model (analytic, sphere) run the reference built with
-that model (oracle/_ref/ipole_<model>, no dump; ``make -C oracle plugins``)
+that model (oracle/_ref/ipole_<model>, no dump; ``make -C oracle plugins REF=<checkout>``)
 and take their noise floor from its FMA build (ipole_<model>_fma).
 
 Each case runs the reference ipole itself (oracle/_ref/ipole_nofma: the
@@ -16,7 +16,7 @@ noise) land from this one, per test metric.
 
     python tests/golden/make_golden.py [case ...]
 
-Needs the reference builds (``make -C oracle ref noise``), i.e. the reference tree.
+Needs the reference builds (``make -C oracle ref noise REF=<checkout>``), i.e. the reference tree.
 """
 from __future__ import annotations
 
@@ -225,7 +225,7 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
 def main(cases):
     binary = os.path.join(ROOT, "oracle", "_ref", "ipole_nofma")
     if not os.path.exists(binary):
-        raise SystemExit("build the reference first: make -C oracle ref")
+        raise SystemExit("build the reference first: make -C oracle ref REF=<reference checkout>")
     with tempfile.TemporaryDirectory() as td:
         dumps = {}
         for c in cases:
