@@ -134,6 +134,10 @@ struct DevCam {
 /* Defined here: the header is included by exactly one translation unit. */
 __constant__ DevGrid c_grid;
 __constant__ DevCam c_cam;
+/* Cameras of a batch of image instances, one per camera group (instances
+ * whose geodesics coincide share one entry). */
+#define IPG_BATCH_MAX_GROUPS 64
+__constant__ DevCam c_cams[IPG_BATCH_MAX_GROUPS];
 
 /* --------------------------------------------------------------------- */
 /* small helpers                                                           */
@@ -721,27 +725,18 @@ struct ModelPt {
   int in_domain;
 };
 
-__device__ __forceinline__ void model_point(const double *__restrict__ fields, double X1, double X2, double X3,
-                                            const PointGeo &pg, ModelPt *mp)
+/* Xtoijk_ghost (src/grid.c:216-283) and the trilinear weights of
+ * interp_scalar (src/grid.c:15-44): the four (i, j) columns of the k, k+1
+ * cell pairs the gather reads, as cell indices, and the eight weights in the
+ * order [2 cc + kk] (column cc, cell k + kk). */
+struct GridLoc {
+  long long cs[4];
+  double w[8];
+};
+
+__device__ __forceinline__ void grid_locate(double X1, double X2, double X3, GridLoc *gl)
 {
   const DevGrid &G = c_grid;
-  mp->geo = pg;
-  mp->gu = gcon_from(mp->geo.r, mp->geo.sth, mp->geo.cth, mp->geo.J21, mp->geo.J22);
-  const Met &g = mp->geo.g;
-  mp->in_domain = !(X1 < G.startx[1] || X1 >= G.stopx[1] || X2 < G.startx[2] || X2 >= G.stopx[2]);
-  if (!mp->in_domain) {
-    double u0 = -1. / sqrt(-mp->gu.u00);
-    mp->Ucov[0] = u0;
-    mp->Ucov[1] = mp->Ucov[2] = mp->Ucov[3] = 0.;
-    mp->Ucon[0] = u0 * mp->gu.u00;
-    mp->Ucon[1] = u0 * mp->gu.u01;
-    mp->Ucon[2] = u0 * mp->gu.u02;
-    mp->Ucon[3] = 0.;
-    for (int m = 0; m < 4; m++) mp->Bcon[m] = mp->Bcov[m] = 0.;
-    mp->ne = mp->thetae = mp->bmag = 0.;
-    return;
-  }
-  /* Xtoijk_ghost, src/grid.c:216-283 */
   double phi = fmod(X3, G.cstopx[3]);
   if (phi < 0.0) phi = G.cstopx[3] + phi;
   int i = (int)((X1 - G.startx[1]) / G.dx[1] - 0.5 + 1000) - 1000;
@@ -759,32 +754,52 @@ __device__ __forceinline__ void model_point(const double *__restrict__ fields, d
   i += 1;
   j += 1;
   k += 1;
-  /* interp_scalar, src/grid.c:15-44, for all 10 fields at once */
   double b1 = 1. - d1, b2 = 1. - d2, b3 = 1. - d3;
-  double w[8] = {b1 * b2 * b3, b1 * b2 * d3, b1 * d2 * b3, b1 * d2 * d3,
-                 d1 * b2 * b3, d1 * b2 * d3, d1 * d2 * b3, d1 * d2 * d3};
+  gl->w[0] = b1 * b2 * b3;
+  gl->w[1] = b1 * b2 * d3;
+  gl->w[2] = b1 * d2 * b3;
+  gl->w[3] = b1 * d2 * d3;
+  gl->w[4] = d1 * b2 * b3;
+  gl->w[5] = d1 * b2 * d3;
+  gl->w[6] = d1 * d2 * b3;
+  gl->w[7] = d1 * d2 * d3;
   long long c0 = ((long long)i * G.si + (long long)j * G.sj + k);
-  long long cs[4] = {c0, c0 + G.sj, c0 + G.si, c0 + G.si + G.sj};
-  double acc[10];
+  gl->cs[0] = c0;
+  gl->cs[1] = c0 + G.sj;
+  gl->cs[2] = c0 + G.si;
+  gl->cs[3] = c0 + G.si + G.sj;
+}
+
+/* interp_scalar for NF fields at once from a cell-major array (the NF
+ * fields of a cell contiguous): each column's k and k+1 cells are 2 NF
+ * contiguous doubles.  Every field sums its eight corners in the same order
+ * whatever NF is, so the same values give the same bits from any layout. */
+template <int NF>
+__device__ __forceinline__ void gather_cells(const double *__restrict__ fields, const GridLoc &gl, double acc[NF])
+{
+  static_assert(NF % 2 == 0, "pairs of fields are loaded together");
 #pragma unroll
-  for (int f = 0; f < 10; f++) acc[f] = 0.;
+  for (int f = 0; f < NF; f++) acc[f] = 0.;
 #pragma unroll
   for (int cc = 0; cc < 4; cc++) {
-    const double2 *p = reinterpret_cast<const double2 *>(fields + cs[cc] * 10);
-    /* two adjacent cells in k: 20 contiguous doubles */
+    const double2 *p = reinterpret_cast<const double2 *>(fields + gl.cs[cc] * NF);
 #pragma unroll
-    for (int h = 0; h < 10; h++) {
+    for (int h = 0; h < NF; h++) {
       double2 v = __ldg(p + h);
-      int f0 = (2 * h) % 10, kk = (2 * h) / 10;
-      double wt = w[2 * cc + kk];
+      int f0 = (2 * h) % NF, kk = (2 * h) / NF;
+      double wt = gl.w[2 * cc + kk];
       acc[f0] += wt * v.x;
       acc[f0 + 1] += wt * v.y;
     }
   }
-  double V1 = acc[0], V2 = acc[1], V3 = acc[2];
-  double Bp1 = acc[3], Bp2 = acc[4], Bp3 = acc[5];
-  double ne = acc[6], th_e = acc[7], bm = acc[8], sig = acc[9];
-  /* get_model_fourv, model/iharm/model.c:455-492 */
+}
+
+/* get_model_fourv, model/iharm/model.c:455-492, from the interpolated
+ * velocity and field primitives (code units) */
+__device__ __forceinline__ void fourv_from(double V1, double V2, double V3, double Bp1, double Bp2, double Bp3,
+                                           ModelPt *mp)
+{
+  const Met &g = mp->geo.g;
   double VdotV = g.g11 * V1 * V1 + g.g12 * V1 * V2 + g.g13 * V1 * V3 + g.g12 * V2 * V1 + g.g22 * V2 * V2 +
                  g.g13 * V3 * V1 + g.g33 * V3 * V3;
   double Vfac = sqrt(-1. / mp->gu.u00 * (1. + fabs(VdotV)));
@@ -799,12 +814,56 @@ __device__ __forceinline__ void model_point(const double *__restrict__ fields, d
   mp->Bcon[2] = (Bp2 + mp->Ucon[2] * mp->Bcon[0]) * iu0;
   mp->Bcon[3] = (Bp3 + mp->Ucon[3] * mp->Bcon[0]) * iu0;
   lower(g, mp->Bcon, mp->Bcov);
-  /* get_model_ne with the geodesic sigma cut, model/iharm/model.c:567-593 */
-  if (sig > G.sigma_cut) ne = 0.;
-  else if (!(sig < G.sigma_cut)) ne = ne * G.sigma_eq_factor;
-  mp->ne = ne;
-  mp->thetae = th_e;
-  mp->bmag = bm;
+}
+
+/* the point outside the grid: normal observer, no field
+ * (model/iharm/model.c:427-446) */
+__device__ __forceinline__ void outside_point(ModelPt *mp)
+{
+  double u0 = -1. / sqrt(-mp->gu.u00);
+  mp->Ucov[0] = u0;
+  mp->Ucov[1] = mp->Ucov[2] = mp->Ucov[3] = 0.;
+  mp->Ucon[0] = u0 * mp->gu.u00;
+  mp->Ucon[1] = u0 * mp->gu.u01;
+  mp->Ucon[2] = u0 * mp->gu.u02;
+  mp->Ucon[3] = 0.;
+  for (int m = 0; m < 4; m++) mp->Bcon[m] = mp->Bcov[m] = 0.;
+  mp->ne = mp->thetae = mp->bmag = 0.;
+}
+
+/* get_model_ne's sigma cut, model/iharm/model.c:567-593 */
+__device__ __forceinline__ double sigma_cut_ne(double ne, double sig)
+{
+  const DevGrid &G = c_grid;
+  if (sig > G.sigma_cut) return 0.;
+  if (!(sig < G.sigma_cut)) return ne * G.sigma_eq_factor;
+  return ne;
+}
+
+__device__ __forceinline__ bool in_grid(double X1, double X2)
+{
+  const DevGrid &G = c_grid;
+  return !(X1 < G.startx[1] || X1 >= G.stopx[1] || X2 < G.startx[2] || X2 >= G.stopx[2]);
+}
+
+__device__ __forceinline__ void model_point(const double *__restrict__ fields, double X1, double X2, double X3,
+                                            const PointGeo &pg, ModelPt *mp)
+{
+  mp->geo = pg;
+  mp->gu = gcon_from(mp->geo.r, mp->geo.sth, mp->geo.cth, mp->geo.J21, mp->geo.J22);
+  mp->in_domain = in_grid(X1, X2);
+  if (!mp->in_domain) {
+    outside_point(mp);
+    return;
+  }
+  GridLoc gl;
+  grid_locate(X1, X2, X3, &gl);
+  double acc[10];
+  gather_cells<10>(fields, gl, acc);
+  fourv_from(acc[0], acc[1], acc[2], acc[3], acc[4], acc[5], mp);
+  mp->ne = sigma_cut_ne(acc[6], acc[9]);
+  mp->thetae = acc[7];
+  mp->bmag = acc[8];
 }
 
 /* --------------------------------------------------------------------- */

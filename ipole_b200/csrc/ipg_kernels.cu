@@ -49,6 +49,10 @@ struct RayRec {
 };
 
 enum { CNT_POOL = 0, CNT_STEPS = 1, CNT_RAD = 2, CNT_DEFER = 3, CNT_NEXT_G = 4, CNT_NEXT_T = 5, CNT_N = 6 };
+/* the counters of a batch wave (ipg_batch.cuh) continue the list: transfer
+ * items deferred, the wave's step budget (0: none), the budget-spent flag,
+ * transfer steps done */
+enum { CNT_XDEFER = CNT_N, CNT_BUDGET, CNT_TIMEOUT, CNT_XSTEPS, CNT_NB };
 
 /* ===================================================================== */
 /* helpers                                                                */
@@ -147,9 +151,9 @@ __device__ __forceinline__ void load_A_f(const float *p, double A[4][4])
 }
 
 /* A1 (which = 0) or A2 (which = 1) of a record, in the record's layout */
-__device__ __forceinline__ void store_A_rec(double *rec, int which, const double A[4][4])
+__device__ __forceinline__ void store_A_rec(double *rec, int which, const double A[4][4], int mixed)
 {
-  if (c_cam.mixed) store_A_f(reinterpret_cast<float *>(rec) + (which ? RECM_A2F : RECM_A1F), A);
+  if (mixed) store_A_f(reinterpret_cast<float *>(rec) + (which ? RECM_A2F : RECM_A1F), A);
   else store_A(rec + (which ? REC_A2 : REC_A1), A);
 }
 
@@ -171,22 +175,21 @@ __device__ __forceinline__ void accel_from_A(const double A[4][4], const double 
  * and is not kept; X0 rides in the slot after nturns (read only by the
  * trace output, before k_coeffs reuses the slot). */
 __device__ __forceinline__ void store_geo(double *p, const double X[4], const double K[4], const double Xh[4],
-                                          const double Kh[4], double dl, double nturns)
+                                          const double Kh[4], double dl, double nturns, int mixed)
 {
   store4(p + REC_X1, X[1], X[2], X[3], dl);
   store4(p + REC_K, K[0], K[1], K[2], K[3]);
   store4(p + REC_XH1, Xh[1], Xh[2], nturns, X[0]); /* X0: for the trace output only */
   /* K at the half step: read only by the per-step trace, which always uses
    * the FP64 layout; the compact layout skips it */
-  if (!c_cam.mixed) store4(p + REC_KH, Kh[0], Kh[1], Kh[2], Kh[3]);
+  if (!mixed) store4(p + REC_KH, Kh[0], Kh[1], Kh[2], Kh[3]);
 }
 
 /* init_XK, src/model_geodesics.c:178-212, and Kcon *= freq (src/main.c:837).
  * Explicit round-to-nearest operations keep this block free of FMA
  * contraction so the initial wavevector matches the reference's bits. */
-__device__ __forceinline__ void init_ray(int i, int j, double X[4], double K[4])
+__device__ __forceinline__ void init_ray(const DevCam &C, int i, int j, double X[4], double K[4])
 {
-  const DevCam &C = c_cam;
   double dxoff = __dadd_rn(__ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn((double)i, 0.5), C.xoff), -0.01), (double)C.nx), -0.5);
   double dyoff = __dadd_rn(__ddiv_rn(__dadd_rn(__dadd_rn((double)j, 0.5), C.yoff), (double)C.ny), -0.5);
   double kt1 = __dmul_rn(__dsub_rn(__dmul_rn(dxoff, C.crot), __dmul_rn(dyoff, C.srot)), C.fovx);
@@ -210,6 +213,19 @@ __device__ __forceinline__ void init_ray(int i, int j, double X[4], double K[4])
 /* ===================================================================== */
 /* k_geodesic                                                             */
 /* ===================================================================== */
+/* Camera of a ray: the context's one camera (CamOne), or a batch's camera
+ * table indexed by the ray's camera group (CamTable).  Batched geodesic
+ * kernels read the group of each ray from a list; CamOne compiles to the
+ * constant-bank reads of the single-image path. */
+struct CamOne {
+  static constexpr bool batch = false;
+  __device__ __forceinline__ static const DevCam &get(int) { return c_cam; }
+};
+struct CamTable {
+  static constexpr bool batch = true;
+  __device__ __forceinline__ static const DevCam &get(int g) { return c_cams[g]; }
+};
+
 struct GeoLane {
   double X[4], K[4], Xh[4], Kh[4];
   double X1m1, X2m1, X1m2, X2m2; /* sub-ring bookkeeping: X1, X2 of steps n-1, n-2 */
@@ -217,22 +233,33 @@ struct GeoLane {
   double *prev;                  /* record of the last stored step */
   int ray, nstep, chunk, passed, nturns;
   int phase;                     /* 0: next is Gamma at X, 1: Gamma at Xhalf */
+  int grp;                       /* camera group of the ray (batches; 0 otherwise) */
 };
 
 /* Take the next ray from the wave's queue and store its camera point as
  * step 0; rays that find the pool full are deferred.  False when the queue
  * is empty. */
+template <class CS>
 __device__ __forceinline__ bool geo_fetch(GeoLane &L, const int32_t *__restrict__ ij, const int32_t *__restrict__ list,
                                           int n_list, double *__restrict__ pool, int *__restrict__ chunk_prev,
                                           int2 *__restrict__ chunk_meta, long long n_chunks,
                                           unsigned long long *__restrict__ counters, RayRec *__restrict__ rays,
-                                          int32_t *__restrict__ deferred)
+                                          int32_t *__restrict__ deferred, const int32_t *__restrict__ ray_grp)
 {
-  const DevCam &C = c_cam;
   while (true) {
     unsigned long long t = atomicAdd(&counters[CNT_NEXT_G], 1ULL);
     if (t >= (unsigned long long)n_list) return false;
     int ray = list ? list[t] : (int)t;
+    if constexpr (CS::batch) {
+      /* a batch's step budget: once it is spent no further ray starts */
+      const unsigned long long budget = counters[CNT_BUDGET];
+      if (budget && *(volatile unsigned long long *)&counters[CNT_STEPS] >= budget) {
+        counters[CNT_TIMEOUT] = 1;
+        return false;
+      }
+    }
+    const int grp = CS::batch ? ray_grp[ray] : 0;
+    const DevCam &C = CS::get(grp);
     long long c = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
     if (c >= n_chunks) {
       RayRec rec = {-1, 0, IPG_RAY_POOL_FULL, 0};
@@ -241,7 +268,8 @@ __device__ __forceinline__ bool geo_fetch(GeoLane &L, const int32_t *__restrict_
       continue;
     }
     L.ray = ray;
-    init_ray(ij[2 * ray], ij[2 * ray + 1], L.X, L.K);
+    L.grp = grp;
+    init_ray(C, ij[2 * ray], ij[2 * ray + 1], L.X, L.K);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       L.Xh[k] = L.X[k];
@@ -251,7 +279,7 @@ __device__ __forceinline__ bool geo_fetch(GeoLane &L, const int32_t *__restrict_
     chunk_prev[L.chunk] = -1;
     chunk_meta[L.chunk] = make_int2(ray, 0);
     L.prev = step_ptr(pool, L.chunk, 0);
-    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, 0., 0.);
+    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, 0., 0., C.mixed);
     L.nstep = 0;
     L.phase = 0;
     L.h = 0.;
@@ -265,9 +293,8 @@ __device__ __forceinline__ bool geo_fetch(GeoLane &L, const int32_t *__restrict_
 
 /* Sub-ring counter, src/model_geodesics.c:129-165, after step nstep */
 template <int MET>
-__device__ __forceinline__ void count_turns(GeoLane &L)
+__device__ __forceinline__ void count_turns(const DevCam &C, GeoLane &L)
 {
-  const DevCam &C = c_cam;
   if (L.passed != 0) {
     if (L.passed > 0) {
       if (L.X[2] > 0.5) L.passed = 0;
@@ -303,19 +330,16 @@ __device__ __forceinline__ void count_turns(GeoLane &L)
 #ifndef IPG_GEO_FULLSTEP
 #define IPG_GEO_FULLSTEP 0 /* whole midpoint steps (build option) */
 #endif
-template <int P, int TPB = 256, int MINB = IPG_GEO_MINB, bool FULL = (IPG_GEO_FULLSTEP != 0)>
+template <int P, int TPB = 256, int MINB = IPG_GEO_MINB, bool FULL = (IPG_GEO_FULLSTEP != 0), class CS = CamOne>
 __global__ void __launch_bounds__(TPB, MINB)
     k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list,
                double *__restrict__ pool, int *__restrict__ chunk_prev, int2 *__restrict__ chunk_meta,
                long long n_chunks, unsigned long long *__restrict__ counters, RayRec *__restrict__ rays,
-               int32_t *__restrict__ deferred)
+               int32_t *__restrict__ deferred, const int32_t *__restrict__ ray_grp)
 {
   const DevGrid &G = c_grid;
-  const DevCam &C = c_cam;
-  const int pol = !C.unpol;
-  const int track = C.target_nturns >= 0;
   GeoLane L;
-  bool has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+  bool has = geo_fetch<CS>(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred, ray_grp);
   if constexpr (FULL) {
   /* One iteration is one whole midpoint step.  The second connection is
    * taken at Xhalf = X + h K / 2, which needs only the step size, not the
@@ -324,6 +348,9 @@ __global__ void __launch_bounds__(TPB, MINB)
    * It takes 250 registers instead of 226 and gives the same records. */
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
+    const DevCam &C = CS::get(L.grp);
+    const int pol = !C.unpol;
+    const int track = C.target_nturns >= 0;
     /* stop_backward_integration, src/model_geodesics.c:218-254, and the step
      * limit of trace_geodesic's loop (:71) */
     double r = geo_r<PlugT<P>::MET>(L.X[1]);
@@ -335,12 +362,12 @@ __global__ void __launch_bounds__(TPB, MINB)
         double A[4][4];
         fd_connection<PlugT<P>::MET>(L.X[1], L.X[2], &cn);
         transport_matrix(cn, L.K, A);
-        store_A_rec(L.prev, 0, A);
+        store_A_rec(L.prev, 0, A, C.mixed);
       }
       RayRec rec = {L.chunk, L.nstep, status, 0};
       rays[L.ray] = rec;
       atomicAdd(&counters[CNT_STEPS], (unsigned long long)L.nstep);
-      has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+      has = geo_fetch<CS>(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred, ray_grp);
       continue;
     }
     L.nstep++;
@@ -354,7 +381,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     if (pol) {
       transport_matrix(c0, L.K, A);
       accel_from_A(A, L.K, acc);
-      store_A_rec(L.prev, 0, A);
+      store_A_rec(L.prev, 0, A, C.mixed);
     } else {
       geo_accel(c0, L.K, acc);
     }
@@ -373,7 +400,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     }
     double dl = -L.h;
     double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
-    if (track) count_turns<PlugT<P>::MET>(L);
+    if (track) count_turns<PlugT<P>::MET>(C, L);
     int slot = L.nstep % IPG_CHUNK_STEPS;
     if (slot == 0) {
       long long nc = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
@@ -381,7 +408,7 @@ __global__ void __launch_bounds__(TPB, MINB)
         RayRec rec = {L.chunk, L.nstep, IPG_RAY_POOL_FULL, 0};
         rays[L.ray] = rec;
         deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = L.ray;
-        has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+        has = geo_fetch<CS>(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred, ray_grp);
         continue;
       }
       chunk_prev[(int)nc] = L.chunk;
@@ -389,12 +416,15 @@ __global__ void __launch_bounds__(TPB, MINB)
       L.chunk = (int)nc;
     }
     L.prev = step_ptr(pool, L.chunk, slot);
-    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
-    if (pol) store_A_rec(L.prev, 1, A); /* Gamma(Xh_n) Kh_n */
+    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns, C.mixed);
+    if (pol) store_A_rec(L.prev, 1, A, C.mixed); /* Gamma(Xh_n) Kh_n */
   }
   } else {
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
+    const DevCam &C = CS::get(L.grp);
+    const int pol = !C.unpol;
+    const int track = C.target_nturns >= 0;
     const int ph = L.phase;
     int stop = 0;
     if (ph == 0) {
@@ -407,7 +437,7 @@ __global__ void __launch_bounds__(TPB, MINB)
           RayRec rec = {L.chunk, L.nstep, status, 0};
           rays[L.ray] = rec;
           atomicAdd(&counters[CNT_STEPS], (unsigned long long)L.nstep);
-          has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+          has = geo_fetch<CS>(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred, ray_grp);
           continue;
         }
         stop = 1; /* the walk back starts at the last point: its Gamma(X) K too */
@@ -427,12 +457,12 @@ __global__ void __launch_bounds__(TPB, MINB)
       geo_accel(cn, Ke, acc);
     }
     if (ph == 0) {
-      if (pol) store_A_rec(L.prev, 0, A);
+      if (pol) store_A_rec(L.prev, 0, A, C.mixed);
       if (stop) {
         RayRec rec = {L.chunk, L.nstep, IPG_RAY_OK, 0};
         rays[L.ray] = rec;
         atomicAdd(&counters[CNT_STEPS], (unsigned long long)L.nstep);
-        has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+        has = geo_fetch<CS>(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred, ray_grp);
         continue;
       }
       L.nstep++;
@@ -453,7 +483,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     L.phase = 0;
     double dl = -L.h;
     double dl_cgs = dl * G.L_unit * IPG_HPL / (IPG_ME * IPG_CL * IPG_CL);
-    if (track) count_turns<PlugT<P>::MET>(L);
+    if (track) count_turns<PlugT<P>::MET>(C, L);
     int slot = L.nstep % IPG_CHUNK_STEPS;
     if (slot == 0) {
       long long nc = (long long)atomicAdd(&counters[CNT_POOL], 1ULL);
@@ -461,7 +491,7 @@ __global__ void __launch_bounds__(TPB, MINB)
         RayRec rec = {L.chunk, L.nstep, IPG_RAY_POOL_FULL, 0};
         rays[L.ray] = rec;
         deferred[atomicAdd(&counters[CNT_DEFER], 1ULL)] = L.ray;
-        has = geo_fetch(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred);
+        has = geo_fetch<CS>(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred, ray_grp);
         continue;
       }
       chunk_prev[(int)nc] = L.chunk;
@@ -469,8 +499,8 @@ __global__ void __launch_bounds__(TPB, MINB)
       L.chunk = (int)nc;
     }
     L.prev = step_ptr(pool, L.chunk, slot);
-    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns);
-    if (pol) store_A_rec(L.prev, 1, A); /* Gamma(Xh_n) Kh_n */
+    store_geo(L.prev, L.X, L.K, L.Xh, L.Kh, dl_cgs, (double)L.nturns, C.mixed);
+    if (pol) store_A_rec(L.prev, 1, A, C.mixed); /* Gamma(Xh_n) Kh_n */
   }
   }
 }
@@ -500,7 +530,7 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
       if (has) {
         t = (int)q;
         int ray = list ? list[t] : t;
-        init_ray(ij[2 * ray], ij[2 * ray + 1], X, K);
+        init_ray(C, ij[2 * ray], ij[2 * ray + 1], X, K);
         nstep = 0;
         phase = 0;
       }
@@ -715,7 +745,7 @@ __device__ __forceinline__ void load_coef_m(const double *__restrict__ p, CoefBl
  * in the plasma tetrad, Faraday half step, absorption/emission, Faraday half
  * step, back to N.  Returns the tauF / NaN oddflag bits. */
 __device__ __forceinline__ int evolve_N_coef(const CoefBlock &cb, double dlam, int zero_emission, HermN *N,
-                                             double *tauF)
+                                             double *tauF, int stokes_floors)
 {
   Jar c;
   c.jI = cb.jI;
@@ -736,7 +766,7 @@ __device__ __forceinline__ int evolve_N_coef(const CoefBlock &cb, double dlam, i
   absorb_emit(c, dlam, &SI, &SQ, &SU, &SV);
   faraday_apply(R, c.rQ, c.rU, c.rV, &SQ, &SU, &SV);
   *tauF += dlam * fabs(c.rV);
-  if (c_cam.stokes_floors) {
+  if (stokes_floors) {
     if (SI < 0) {
       SI = SQ = SU = SV = 0;
     } else {
@@ -836,7 +866,7 @@ __device__ __forceinline__ float one_minus_exp_over(float t)
  * sine and cosine.  The N to Stokes projection and the update of N stay
  * FP64, so the accumulation along the ray is FP64. */
 __device__ __forceinline__ int evolve_N_coef_f32(const CoefBlock &cb, double dlam, int zero_emission, HermN *N,
-                                              double *tauF)
+                                              double *tauF, int stokes_floors)
 {
   double T11, T22, T12r, T21i;
   hn_stokes(*N, cb.e1, cb.e2, &T11, &T22, &T12r, &T21i);
@@ -922,7 +952,7 @@ __device__ __forceinline__ int evolve_N_coef_f32(const CoefBlock &cb, double dla
   *tauF += dlam * fabs(cb.rV);
   const double is = ldexp(1.0, ex);
   double SIo = SI * is, SQo = SQ * is, SUo = SU * is, SVo = SV * is;
-  if (c_cam.stokes_floors) {
+  if (stokes_floors) {
     if (SIo < 0) {
       SIo = SQo = SUo = SVo = 0;
     } else {
@@ -1042,6 +1072,75 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
   }
 }
 
+/* One step n -> n-1 of integrate_emission's loop (src/ipolarray.c:78-244)
+ * for a lane whose record of step n is L.rec_i and whose coefficients of
+ * step n-1 are cb: push_polar twice, then the unpolarized and polarized
+ * transfer steps at radiating points. */
+template <bool S32, int RM, class Lane>
+__device__ __forceinline__ void xfer_step(const DevCam &C, Lane &L, const CoefBlock &cb, int unpol)
+{
+  const DevGrid &G = c_grid;
+  double dl = L.dl_i;
+  if (!unpol) {
+    /* push_polar twice, src/ipolarray.c:85-89 */
+    double dlfull = dl * G.inv_dlfac;
+    double dlhalf = (0.5 * dl) * G.inv_dlfac;
+    double A[4][4];
+    HermN Nh, Nn;
+    load_A_rec<RM>(L.rec_i, 0, A);
+    if constexpr (S32 && IPG_S32_PUSH) {
+      hn_push_f32(L.N, L.N, A, dlhalf, &Nh);
+      load_A_rec<RM>(L.rec_i, 1, A);
+      hn_push_f32(L.N, Nh, A, dlfull, &Nn);
+    } else {
+      hn_push(L.N, L.N, A, dlhalf, &Nh);
+      load_A_rec<RM>(L.rec_i, 1, A);
+      hn_push(L.N, Nh, A, dlfull, &Nn);
+    }
+    L.N = Nn;
+  }
+  int flags = (int)cb.flags;
+  if (flags & 1) {
+    L.nrad++;
+    int zero_emission = (flags & 2) ? 1 : 0;
+    if (C.target_nturns >= 0 && (int)L.nturns_i != C.target_nturns) zero_emission = 1;
+    double ji = L.js, ki = L.ks;
+    double jf = cb.ju, kf = cb.ku;
+    L.js = jf;
+    L.ks = kf;
+    if (zero_emission) L.I = approximate_solve(L.I, 0, ki, 0, kf, dl, &L.tau);
+    else L.I = approximate_solve(L.I, ji, ki, jf, kf, dl, &L.tau);
+    if (!unpol) {
+      L.flag |= flags >> 2;
+      if constexpr (S32) L.flag |= evolve_N_coef_f32(cb, dl, zero_emission, &L.N, &L.tauF, C.stokes_floors);
+      else L.flag |= evolve_N_coef(cb, dl, zero_emission, &L.N, &L.tauF, C.stokes_floors);
+    }
+  }
+}
+
+/* get_pixel's outputs at the end of a lane's walk: project_N
+ * (src/ipolarray.c:578-598) in the camera's tetrad */
+template <class Lane>
+__device__ __forceinline__ void xfer_result(const DevCam &C, const Lane &L, int unpol, int nstep, ipg_pixel_out *o)
+{
+  o->I_unpol = L.I;
+  o->tau = L.tau;
+  o->tauF = L.tauF;
+  o->I = o->Q = o->U = o->V = 0.;
+  if (!unpol) {
+    /* project_N, src/ipolarray.c:578-598 */
+    double T11, T22, T12r, T21i;
+    hn_stokes(L.N, C.Ecov[1], C.Ecov[2], &T11, &T22, &T12r, &T21i);
+    double Q = (T11 - T22) / 2, U = T12r;
+    o->I = (T11 + T22) / 2;
+    o->Q = Q * C.cproj - U * C.sproj;
+    o->U = Q * C.sproj + U * C.cproj;
+    o->V = T21i;
+  }
+  o->nstep = nstep;
+  o->flag = L.flag;
+}
+
 /* RM: the step-record layout, 0 FP64, 1 compact, -1 from the camera (the
  * no-alloc path) */
 template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false, int RM = -1>
@@ -1059,22 +1158,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     if (!has) continue;
     if (L.n == 0) {
       ipg_pixel_out o;
-      o.I_unpol = L.I;
-      o.tau = L.tau;
-      o.tauF = L.tauF;
-      o.I = o.Q = o.U = o.V = 0.;
-      if (!unpol) {
-        /* project_N, src/ipolarray.c:578-598 */
-        double T11, T22, T12r, T21i;
-        hn_stokes(L.N, C.Ecov[1], C.Ecov[2], &T11, &T22, &T12r, &T21i);
-        double Q = (T11 - T22) / 2, U = T12r;
-        o.I = (T11 + T22) / 2;
-        o.Q = Q * C.cproj - U * C.sproj;
-        o.U = Q * C.sproj + U * C.cproj;
-        o.V = T21i;
-      }
-      o.nstep = rays[L.ray].nstep;
-      o.flag = L.flag;
+      xfer_result(C, L, unpol, rays[L.ray].nstep, &o);
       out[L.ray] = o;
       atomicAdd(&counters[CNT_RAD], (unsigned long long)L.nrad);
       has = xfer_fetch<RM>(L, list, n_list, pool, chunk_prev, rays, out, counters);
@@ -1095,42 +1179,7 @@ __global__ void __launch_bounds__(TPB, MINB)
     CoefBlock cb;
     if (RM < 0 ? C.mixed : RM) load_coef_m(rec_f, cb);
     else load_coef(rec_f, cb);
-    double dl = L.dl_i;
-    if (!unpol) {
-      /* push_polar twice, src/ipolarray.c:85-89 */
-      double dlfull = dl * G.inv_dlfac;
-      double dlhalf = (0.5 * dl) * G.inv_dlfac;
-      double A[4][4];
-      HermN Nh, Nn;
-      load_A_rec<RM>(L.rec_i, 0, A);
-      if constexpr (S32 && IPG_S32_PUSH) {
-        hn_push_f32(L.N, L.N, A, dlhalf, &Nh);
-        load_A_rec<RM>(L.rec_i, 1, A);
-        hn_push_f32(L.N, Nh, A, dlfull, &Nn);
-      } else {
-        hn_push(L.N, L.N, A, dlhalf, &Nh);
-        load_A_rec<RM>(L.rec_i, 1, A);
-        hn_push(L.N, Nh, A, dlfull, &Nn);
-      }
-      L.N = Nn;
-    }
-    int flags = (int)cb.flags;
-    if (flags & 1) {
-      L.nrad++;
-      int zero_emission = (flags & 2) ? 1 : 0;
-      if (C.target_nturns >= 0 && (int)L.nturns_i != C.target_nturns) zero_emission = 1;
-      double ji = L.js, ki = L.ks;
-      double jf = cb.ju, kf = cb.ku;
-      L.js = jf;
-      L.ks = kf;
-      if (zero_emission) L.I = approximate_solve(L.I, 0, ki, 0, kf, dl, &L.tau);
-      else L.I = approximate_solve(L.I, ji, ki, jf, kf, dl, &L.tau);
-      if (!unpol) {
-        L.flag |= flags >> 2;
-        if constexpr (S32) L.flag |= evolve_N_coef_f32(cb, dl, zero_emission, &L.N, &L.tauF);
-        else L.flag |= evolve_N_coef(cb, dl, zero_emission, &L.N, &L.tauF);
-      }
-    }
+    xfer_step<S32, RM>(C, L, cb, unpol);
     L.dl_i = cb.dl;
     L.nturns_i = cb.nturns;
     L.rec_i = rec_f;
@@ -1623,7 +1672,7 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
   int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 256, IPG_GEO_MINB>, gthreads, b.run);
   k_geodesic<P, 256, IPG_GEO_MINB><<<gb, gthreads, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev,
                                                                   b.chunk_meta, b.n_chunks, b.cnt, ctx->d_rays,
-                                                                  b.deferred);
+                                                                  b.deferred, nullptr);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[1], b.stream));
   if (b.coef_after) CK(cudaStreamWaitEvent(b.stream, b.coef_after, 0));
@@ -2209,7 +2258,7 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
     }
     int gb = na_blocks(n_sm, (const void *)k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB>, threads, run);
     k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB><<<gb, threads, 0, stream>>>(d_ij, list, (int)run, pool, chunk_prev, chunk_meta,
-                                                           n_chunks, cnt_d, rays, lists[cur ^ 1]);
+                                                           n_chunks, cnt_d, rays, lists[cur ^ 1], nullptr);
     NA_CK(cudaGetLastError());
     /* the compiled kernels of a context's FP64 path, so that both give the
      * same bits for every ray */

@@ -312,7 +312,7 @@ __global__ void k_trace_walk(int nstep, double *__restrict__ out, const CoefBloc
       else I = approximate_solve(0., ti.ju, ti.ku, tf.ju, tf.ku, dl, &tau);
       if (!C.unpol) {
         flag |= flags >> 2;
-        flag |= evolve_N_coef(tf, dl, zero_emission, &N, &tauF);
+        flag |= evolve_N_coef(tf, dl, zero_emission, &N, &tauF, c_cam.stokes_floors);
       }
     }
     o[IPG_TRACE_I_UNPOL] = I;
@@ -372,17 +372,17 @@ extern "C" int ipg_trace_ray(ipg_ctx *ctx, const ipg_camera *cam, int i, int j, 
     case IPG_PLUG_ANALYTIC:
       k_geodesic<IPG_PLUG_ANALYTIC, 256, IPG_GEO_MINB><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
                                                               ctx->d_chunk_meta, ctx->n_chunks, ctx->d_cnt,
-                                                              ctx->d_rays, ctx->d_list[1]);
+                                                              ctx->d_rays, ctx->d_list[1], nullptr);
       break;
     case IPG_PLUG_SPHERE:
       k_geodesic<IPG_PLUG_SPHERE, 256, IPG_GEO_MINB><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
                                                             ctx->d_chunk_meta, ctx->n_chunks, ctx->d_cnt,
-                                                            ctx->d_rays, ctx->d_list[1]);
+                                                            ctx->d_rays, ctx->d_list[1], nullptr);
       break;
     default:
       k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB><<<1, 32, 0, ctx->stream>>>(ctx->d_ij, NULL, 1, ctx->d_pool, ctx->d_chunk_prev,
                                                            ctx->d_chunk_meta, ctx->n_chunks, ctx->d_cnt, ctx->d_rays,
-                                                           ctx->d_list[1]);
+                                                           ctx->d_list[1], nullptr);
   }
   CK(cudaGetLastError());
   RayRec rec;

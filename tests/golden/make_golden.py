@@ -61,7 +61,21 @@ CASES = {
     # both R_high of the 400x400 workload, on small images
     "c2_rhigh1_incl17_24": ("c2", ["--M_unit=7.5e27", "--trat_large=1", "--thetacam=17", "--nx=24", "--ny=24"]),
     "c2_rhigh160_incl163_24": ("c2", ["--M_unit=7.5e27", "--trat_large=160", "--nx=24", "--ny=24"]),
+    # the full-size workloads: the 128x64x64 dump's own 128x128 image, and the
+    # production dump at its four (inclination, R_high) pairs with M_unit set
+    # for a total flux of 0.6 Jy (tests/golden/tune_munit.py) -- the 400x400
+    # bench image itself and the other three at 128x128
+    "c1_full_128": ("c1", ["--M_unit=1e25", "--nx=128", "--ny=128"]),
+    "c2_rhigh160_incl163_400": ("c2", ["--M_unit=7.96e27", "--trat_large=160", "--nx=400", "--ny=400"]),
+    "c2_rhigh1_incl163_128": ("c2", ["--M_unit=3.05e26", "--trat_large=1", "--nx=128", "--ny=128"]),
+    "c2_rhigh160_incl17_128": ("c2", ["--M_unit=7.97e27", "--trat_large=160", "--thetacam=17", "--nx=128",
+                                      "--ny=128"]),
+    "c2_rhigh1_incl17_128": ("c2", ["--M_unit=3.05e26", "--trat_large=1", "--thetacam=17", "--nx=128",
+                                    "--ny=128"]),
 }
+# cases stored without tau and the tauF channel (the parity metrics use
+# neither), to keep the 400x400 fixture at 6.4 MB
+SLIM = {"c2_rhigh160_incl163_400"}
 
 
 # known-answer models: the reference test's parameters (tests/analytic/analytic.par,
@@ -103,7 +117,7 @@ CASES.update(TRACE_CASES)
 def make_trace_case(case, binary, tmpdir, dumps):
     dname, extra = CASES[case]
     dpath, dhash = dumps[dname]
-    env = dict(os.environ, OMP_NUM_THREADS="8")
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "8"))
 
     def run(bin_name):
         tr = os.path.join(tmpdir, f"{case}_{bin_name}_trace.ipgc")
@@ -167,7 +181,7 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
         dpath, dhash = dumps[dname]
         base, others = BASE, ("ipole", "ipole_o2fma", "ipole_v4", "ipole_ulp")
         args = [f"--dump={dpath}", *BASE, *extra, f"--outfile={out}"]
-    env = dict(os.environ, OMP_NUM_THREADS="8")
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "8"))
     check = case in CHECK_CASES
     r = run_checked(binary, args, out, env) if check else subprocess.run([binary, *args], capture_output=True,
                                                                           text=True, env=env)
@@ -181,6 +195,9 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
     rec = {"unpol": img["/unpol"], "tau": img["/tau"]}
     if "/pol" in img:
         rec["pol"] = img["/pol"]
+    if case in SLIM:
+        del rec["tau"]
+        rec["pol"] = np.ascontiguousarray(rec["pol"][..., :4])
     if check:
         for k in CHECK_KEYS:
             if f"/{k}_recheck" in img:
