@@ -30,6 +30,7 @@
 #include <stdint.h>
 
 #include "ipg_constants.h"
+#include "ipg_dual.cuh"
 
 #define IPG_DEL 1.e-7            /* finite-difference step, src/geometry.c:91 */
 #define IPG_CUT_SMALL_TAU 1e-5   /* src/ipolarray.c:34 */
@@ -869,18 +870,50 @@ __device__ __forceinline__ void model_point(const double *__restrict__ fields, d
 /* --------------------------------------------------------------------- */
 /* Radiation coefficients (src/model_radiation.c:145-332, src/radiation.c) */
 /* --------------------------------------------------------------------- */
-/* src/radiation.c:14-23 */
-__device__ __forceinline__ double Bnu_inv(double nu, double Thetae)
+/* The fits below are written once for any number type R: double for the
+ * image, and the dual numbers of ipg_dual.cuh for the adjoint, which carry
+ * the derivatives with respect to ne, Theta_e and |B| through the same
+ * operations.  NumT<R>::c(v) is a constant of type R. */
+template <class R>
+struct NumT {
+  __device__ __forceinline__ static R c(double v) { return v; }
+};
+template <int D>
+struct NumT<Dual<D>> {
+  __device__ __forceinline__ static Dual<D> c(double v) { return dconst<D>(v); }
+};
+
+/* K0, K1, K2 of a dual argument: the values of bessel_k012 and the
+ * derivatives K0' = -K1, K1' = -K0 - K1/x, K2' = -K1 - 2 K2/x */
+__device__ __forceinline__ void bessel_k012_t(double x, double *k0, double *k1, double *k2)
 {
-  double x = IPG_HPL * nu / (IPG_ME * IPG_CL * IPG_CL * Thetae);
+  bessel_k012(x, k0, k1, k2);
+}
+template <int D>
+__device__ __forceinline__ void bessel_k012_t(const Dual<D> &x, Dual<D> *k0, Dual<D> *k1, Dual<D> *k2)
+{
+  double a, b, c;
+  bessel_k012(x.v, &a, &b, &c);
+  *k0 = dchain(x, a, -b);
+  *k1 = dchain(x, b, -a - b / x.v);
+  *k2 = dchain(x, c, -b - 2. * c / x.v);
+}
+
+/* src/radiation.c:14-23 */
+template <class R>
+__device__ __forceinline__ R Bnu_inv(double nu, R Thetae)
+{
+  R x = IPG_HPL * nu / (IPG_ME * IPG_CL * IPG_CL * Thetae);
   if (x < 2.e-3)
     return ((2. * IPG_HPL / (IPG_CL * IPG_CL)) / (x / 24. * (24. + x * (12. + x * (4. + x)))));
   return ((2. * IPG_HPL / (IPG_CL * IPG_CL)) / (exp(x) - 1.));
 }
 
-struct Jar {
-  double jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV;
+template <class R>
+struct JarT {
+  R jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV;
 };
+typedef JarT<double> Jar;
 
 /* Faraday rotativities rho_Q (Dexter 2016), rho_V (Shcherbakov 2008, or
  * Dexter's g(X) when dexter_v and K2 > 0), both times nu
@@ -888,112 +921,115 @@ struct Jar {
  * angle between k and B.  Regrouped for the GPU: the three powers of x share
  * one log(x), and divisions by constants are multiplications by their
  * reciprocals (last-bit changes only). */
-__device__ __forceinline__ void rho_QV(double Ne, double nu, double Thetae, double B, double sth, double cth,
-                                       double k0, double k1, double k2, int want_q, int dexter_v, double *rQ,
-                                       double *rV)
+template <class R>
+__device__ __forceinline__ void rho_QV(R Ne, double nu, R Thetae, R B, double sth, double cth, R k0, R k1, R k2,
+                                       int want_q, int dexter_v, R *rQ, R *rV)
 {
   const double pi = 3.1415926535897932384;
-  double omega0 = (IPG_EE / (IPG_ME * IPG_CL)) * B;
-  double wp2 = (4. * pi * IPG_EE * IPG_EE / IPG_ME) * Ne;
+  R omega0 = (IPG_EE / (IPG_ME * IPG_CL)) * B;
+  R wp2 = (4. * pi * IPG_EE * IPG_EE / IPG_ME) * Ne;
   double tpn = 2. * pi * nu;
   double itpn = 1. / tpn;
-  double x = Thetae * sqrt(1.4142135623730951 * sth * (1.e3 * omega0 * itpn));
-  double ik2 = (k2 > 0) ? 1. / k2 : 0.;
+  R x = Thetae * sqrt(1.4142135623730951 * sth * (1.e3 * omega0 * itpn));
+  R ik2 = (k2 > 0.) ? 1. / k2 : NumT<R>::c(0.);
   if (want_q) {
-    double lx = log(x);
-    double l16 = (x + 1.e-16 == x) ? lx : log(x + 1.e-16);
-    double e472 = exp(x * (-1. / 47.2));
-    double extraterm = (.011 * e472 - 0.011767707320949831 * pi * 1.e4 * exp((-8. / 3.) * l16)) *
-                       (0.5 + 0.5 * tanh((lx - 4.78749174278204599425) * 10.));
-    double jffunc = 2.011 * exp(exp(1.035 * lx) * (-1. / 4.7)) - cos(0.5 * x) * exp(exp(1.2 * lx) * (-1. / 2.73)) -
-                    .011 * e472 + extraterm;
-    double k_ratio = (k2 > 0) ? k1 * ik2 : 1;
+    R lx = log(x);
+    R l16 = (val(x) + 1.e-16 == val(x)) ? lx : log(x + 1.e-16);
+    R e472 = exp(x * (-1. / 47.2));
+    R extraterm = (.011 * e472 - 0.011767707320949831 * pi * 1.e4 * exp((-8. / 3.) * l16)) *
+                  (0.5 + 0.5 * tanh((lx - 4.78749174278204599425) * 10.));
+    R jffunc = 2.011 * exp(exp(1.035 * lx) * (-1. / 4.7)) - cos(0.5 * x) * exp(exp(1.2 * lx) * (-1. / 2.73)) -
+               .011 * e472 + extraterm;
+    R k_ratio = (k2 > 0.) ? k1 * ik2 : NumT<R>::c(1.);
     double itpn2 = itpn * itpn;
-    double eps11m22 = jffunc * wp2 * (omega0 * omega0) * (itpn2 * itpn2) * (k_ratio + 6. * Thetae) * (sth * sth);
+    R eps11m22 = jffunc * wp2 * (omega0 * omega0) * (itpn2 * itpn2) * (k_ratio + 6. * Thetae) * (sth * sth);
     *rQ = tpn * (0.5 / IPG_CL) * eps11m22 * nu;
   }
-  double fit_factor;
-  if (dexter_v && k2 > 0) {
-    double shgmfunc = 0.43793091 * log(1. + 0.00185777 * pow(x, 1.50316886));
+  R fit_factor;
+  if (dexter_v && k2 > 0.) {
+    R shgmfunc = 0.43793091 * log(1. + 0.00185777 * pow(x, 1.50316886));
     fit_factor = (k0 - shgmfunc) * ik2;
   } else {
-    double k_ratio = (k2 > 0) ? k0 * ik2 : 1;
-    double shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
+    R k_ratio = (k2 > 0.) ? k0 * ik2 : NumT<R>::c(1.);
+    R shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
     fit_factor = k_ratio * shgmfunc;
   }
-  double eps12 = wp2 * omega0 * (itpn * itpn * itpn) * fit_factor * cth;
+  R eps12 = wp2 * omega0 * (itpn * itpn * itpn) * fit_factor * cth;
   *rV = tpn * (1. / IPG_CL) * eps12 * nu;
 }
 
-/* Coefficients at one point for both calls the reference makes there:
- * pol = 0 (get_jkinv: Leung j_I / nu^2, Kirchhoff a_I) into (*ju, *ku) and
- * pol = 1 (jar_calc) into *jr.  src/model_radiation.c:145-332 with
- * emission_type 4 (Dexter) or 1 (Pandya); U components are zero.
- * sin and cos of the k-B angle come from its cosine directly
- * (sin = sqrt((1-mu)(1+mu)), cos = mu) instead of through acos; the angle
- * itself is formed only where a fit needs it. */
-IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int emission_type, double *ju,
-                         double *ku, Jar *jr)
+/* The geometry of the coefficients at a point: the fluid-frame frequency
+ * (get_fluid_nu, src/radiation.c:26-44) and the k-B angle (get_bk_angle,
+ * src/radiation.c:47-72).  sin and cos of the angle come from its cosine
+ * directly (sin = sqrt((1-mu)(1+mu)), cos = mu) instead of through acos; the
+ * angle itself is formed only where a fit needs it (theta, Pandya's fits). */
+struct JarGeo {
+  double nu, inusq, sth, cth, theta;
+  int along; /* theta = 0 or pi: no emission or absorption, only rho_V */
+};
+
+__device__ __forceinline__ void jar_geo(const ModelPt &mp, const double K[4], int emission_type, JarGeo *jg)
 {
   const double pi = IPG_PI;
-  Jar z = {0., 0., 0., 0., 0., 0., 0., 0., 0., 0., 0.};
-  *jr = z;
-  *ju = 0.;
-  *ku = 0.;
-  double Ne = mp.ne;
-  if (Ne <= 0.) return;
-  /* get_fluid_nu, src/radiation.c:26-44 */
   double kdu = K[0] * mp.Ucov[0] + K[1] * mp.Ucov[1] + K[2] * mp.Ucov[2] + K[3] * mp.Ucov[3];
-  double nu = -kdu * IPG_ME * IPG_CL * IPG_CL / IPG_HPL;
-  double inusq = 1. / (nu * nu);
-  /* get_bk_angle, src/radiation.c:47-72 */
-  double theta = pi / 2., sth, cth;
-  int along = 0; /* theta = 0 or pi: no emission or absorption, only rho_V */
-  {
-    double Bm = sqrt(fabs(mp.Bcon[0] * mp.Bcov[0] + mp.Bcon[1] * mp.Bcov[1] + mp.Bcon[2] * mp.Bcov[2] +
-                          mp.Bcon[3] * mp.Bcov[3]));
-    if (Bm == 0.) {
-      sth = 1.;                    /* sin(pi/2) */
-      cth = 6.123233995736766e-17; /* cos(pi/2) in double */
+  jg->nu = -kdu * IPG_ME * IPG_CL * IPG_CL / IPG_HPL;
+  jg->inusq = 1. / (jg->nu * jg->nu);
+  jg->theta = pi / 2.;
+  jg->along = 0;
+  double Bm = sqrt(fabs(mp.Bcon[0] * mp.Bcov[0] + mp.Bcon[1] * mp.Bcov[1] + mp.Bcon[2] * mp.Bcov[2] +
+                        mp.Bcon[3] * mp.Bcov[3]));
+  if (Bm == 0.) {
+    jg->sth = 1.;                    /* sin(pi/2) */
+    jg->cth = 6.123233995736766e-17; /* cos(pi/2) in double */
+  } else {
+    double kk = fabs(kdu);
+    double mu = (K[0] * mp.Bcov[0] + K[1] * mp.Bcov[1] + K[2] * mp.Bcov[2] + K[3] * mp.Bcov[3]) / (kk * Bm);
+    if (fabs(mu) > 1.) mu /= fabs(mu);
+    if (mu >= 1. || mu <= -1.) {
+      jg->along = 1;
+      jg->theta = (mu >= 1.) ? 0. : pi;
+      sincos(jg->theta, &jg->sth, &jg->cth);
     } else {
-      double kk = fabs(kdu);
-      double mu = (K[0] * mp.Bcov[0] + K[1] * mp.Bcov[1] + K[2] * mp.Bcov[2] + K[3] * mp.Bcov[3]) / (kk * Bm);
-      if (fabs(mu) > 1.) mu /= fabs(mu);
-      if (mu >= 1. || mu <= -1.) {
-        along = 1;
-        theta = (mu >= 1.) ? 0. : pi;
-        sincos(theta, &sth, &cth);
-      } else {
-        cth = mu;
-        sth = sqrt((1. - mu) * (1. + mu));
-        if (emission_type == 1) theta = acos(mu);
-      }
+      jg->cth = mu;
+      jg->sth = sqrt((1. - mu) * (1. + mu));
+      if (emission_type == 1) jg->theta = acos(mu);
     }
   }
-  double Thetae = mp.thetae, B = mp.bmag;
-  double k0, k1, k2;
-  bessel_k012(1. / Thetae, &k0, &k1, &k2);
-  if (along) {
+}
+
+/* The fits of both calls the reference makes at a point: pol = 0
+ * (get_jkinv: Leung j_I / nu^2, Kirchhoff a_I) into (*ju, *ku) and pol = 1
+ * (jar_calc) into *jr, src/model_radiation.c:145-332 with emission_type 4
+ * (Dexter) or 1 (Pandya); U components are zero.  Ne > 0. */
+template <class R>
+__device__ __forceinline__ void jar_fits(R Ne, R Thetae, R B, const JarGeo &jg, int want_pol, int emission_type,
+                                         R *ju, R *ku, JarT<R> *jr)
+{
+  const double pi = IPG_PI;
+  const double nu = jg.nu, inusq = jg.inusq, sth = jg.sth, cth = jg.cth, theta = jg.theta;
+  R k0, k1, k2;
+  bessel_k012_t(1. / Thetae, &k0, &k1, &k2);
+  if (jg.along) {
     /* only rho_V; the reference still has dexter_fit = 1 set for the Dexter
      * emission type here (src/model_radiation.c:202-207, 212-221) */
     if (want_pol) {
-      double rq;
+      R rq;
       rho_QV(Ne, nu, Thetae, B, sth, cth, k0, k1, k2, 0, emission_type == 4, &rq, &jr->rV);
     }
     return;
   }
-  double Bnuinv = Bnu_inv(nu, Thetae);
-  double bnu = (Bnuinv > 0) ? 1. / Bnuinv : 0.; /* Kirchhoff: a = j / B_nu-inverse */
-  const double Th2 = Thetae * Thetae;
+  R Bnuinv = Bnu_inv(nu, Thetae);
+  R bnu = (Bnuinv > 0.) ? 1. / Bnuinv : NumT<R>::c(0.); /* Kirchhoff: a = j / B_nu-inverse */
+  const R Th2 = Thetae * Thetae;
   /* pol = 0: Leung fit, src/symphony/maxwell_juettner_fits.c:368-395 */
   {
-    double K2 = fmax(k2, IPG_SMALL);
-    double nus = ((2. / 9.) * IPG_EE / (2. * pi * IPG_ME * IPG_CL)) * B * Th2 * sth;
-    double j = 0.;
-    if (!(nu > 1.e12 * nus)) {
-      double x = nu / nus;
-      double cx = cbrt(x);
-      double f = sqrt(x) + 1.8877486253633868 * sqrt(cx); /* 2^(11/12) x^(1/6) */
+    R K2 = fmax(k2, IPG_SMALL);
+    R nus = ((2. / 9.) * IPG_EE / (2. * pi * IPG_ME * IPG_CL)) * B * Th2 * sth;
+    R j = NumT<R>::c(0.);
+    if (!(nu > val(1.e12 * nus))) {
+      R x = nu / nus;
+      R cx = cbrt(x);
+      R f = sqrt(x) + 1.8877486253633868 * sqrt(cx); /* 2^(11/12) x^(1/6) */
       f = f * f;
       j = ((1.4142135623730951 * pi * IPG_EE * IPG_EE / (3. * IPG_CL)) * Ne * nus / K2) * f * exp(-cx);
     }
@@ -1002,38 +1038,38 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
   }
   if (!want_pol) return;
   /* pol = 1 */
-  double jI, jQ, jV;
+  R jI, jQ, jV;
   if (emission_type == 1) {
     /* Pandya+ 2016, src/symphony/maxwell_juettner_fits.c:27-129 */
-    double nu_c = IPG_EE * B / (2. * pi * IPG_ME * IPG_CL);
-    double nu_s = (2. / 9.) * nu_c * sth * Th2;
-    double X = nu / nu_s;
-    double prefactor = (Ne * (IPG_EE * IPG_EE) * nu_c) / IPG_CL;
-    double cX = cbrt(X);
-    double eX = exp(-cX);
-    double sX = sqrt(X), X16 = sqrt(cX);
+    R nu_c = IPG_EE * B / (2. * pi * IPG_ME * IPG_CL);
+    R nu_s = (2. / 9.) * nu_c * sth * Th2;
+    R X = nu / nu_s;
+    R prefactor = (Ne * (IPG_EE * IPG_EE) * nu_c) / IPG_CL;
+    R cX = cbrt(X);
+    R eX = exp(-cX);
+    R sX = sqrt(X), X16 = sqrt(cX);
     double t1 = 1.4142135623730951 * pi / 27. * sth;
-    double tI = sX + 1.8877486253633868 * X16;
+    R tI = sX + 1.8877486253633868 * X16;
     jI = prefactor * t1 * (tI * tI) * eX;
-    double te = pow(Thetae, 24. / 25.);
-    double tq = (7. * te + 35.) / (10. * te + 75.);
-    double tQ = sX + tq * 1.8877486253633868 * X16;
+    R te = pow(Thetae, 24. / 25.);
+    R tq = (7. * te + 35.) / (10. * te + 75.);
+    R tQ = sX + tq * 1.8877486253633868 * X16;
     jQ = prefactor * t1 * (tQ * tQ) * eX;
-    double v1 = (37. - 87. * sin(theta - 28. / 25.)) / (100. * (Thetae + 1.));
-    double v2 = pow(1. + (pow(Thetae, 3. / 5.) / 25. + 7. / 10.) * pow(X, 9. / 25.), 5. / 3.);
+    R v1 = (37. - 87. * sin(theta - 28. / 25.)) / (100. * (Thetae + 1.));
+    R v2 = pow(1. + (pow(Thetae, 3. / 5.) / 25. + 7. / 10.) * pow(X, 9. / 25.), 5. / 3.);
     jV = prefactor * v1 * v2 * eX;
   } else {
     /* Dexter 2016, src/symphony/maxwell_juettner_fits.c:287-356 */
-    double nus = (3.0 * IPG_EE / (4.0 * pi * IPG_ME * IPG_CL)) * B * sth * Th2 + 1.0;
-    double x = nu / nus;
-    double cx = cbrt(x), icx = 1. / cx;
-    double icx2 = icx * icx;
-    double ex = exp(-1.8899 * cx);
-    double iTh2 = 1. / Th2;
-    double pre = (IPG_EE * IPG_EE / (2. * 1.7320508075688772 * IPG_CL)) * Ne * nu * iTh2;
-    double II = 2.5651 * (1 + 1.92 * icx + 0.9977 * icx2) * ex;
-    double IQ = 2.5651 * (1 + 0.93193 * icx + 0.499873 * icx2) * ex;
-    double IV = (1.81384 * (icx2 * icx) + 3.42319 * icx2 + 0.0292545 * rsqrt(x) + 2.03773 * icx) * ex;
+    R nus = (3.0 * IPG_EE / (4.0 * pi * IPG_ME * IPG_CL)) * B * sth * Th2 + 1.0;
+    R x = nu / nus;
+    R cx = cbrt(x), icx = 1. / cx;
+    R icx2 = icx * icx;
+    R ex = exp(-1.8899 * cx);
+    R iTh2 = 1. / Th2;
+    R pre = (IPG_EE * IPG_EE / (2. * 1.7320508075688772 * IPG_CL)) * Ne * nu * iTh2;
+    R II = 2.5651 * (1 + 1.92 * icx + 0.9977 * icx2) * ex;
+    R IQ = 2.5651 * (1 + 0.93193 * icx + 0.499873 * icx2) * ex;
+    R IV = (1.81384 * (icx2 * icx) + 3.42319 * icx2 + 0.0292545 * rsqrt(x) + 2.03773 * icx) * ex;
     jI = pre * II;
     jQ = pre * IQ;
     jV = (2. * IPG_EE * IPG_EE / (3. * 1.7320508075688772 * IPG_CL)) * Ne * nu * (cth / sth) * (iTh2 / Thetae) * IV;
@@ -1041,10 +1077,10 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
   jI *= inusq;
   jQ *= inusq;
   jV *= inusq;
-  double jU = -0. * inusq;
-  double jP = sqrt(jQ * jQ + jU * jU + jV * jV);
+  R jU = NumT<R>::c(-0. * inusq);
+  R jP = sqrt(jQ * jQ + jU * jU + jV * jV);
   if (jI < jP / 0.99) {
-    double pf = jI / jP * 0.99;
+    R pf = jI / jP * 0.99;
     jQ *= pf;
     jU *= pf;
     jV *= pf;
@@ -1058,22 +1094,49 @@ IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int 
   jr->aU = jU * bnu;
   jr->aV = jV * bnu;
   rho_QV(Ne, nu, Thetae, B, sth, cth, k0, k1, k2, 1, 0, &jr->rQ, &jr->rV);
-  jr->rU = 0.;
+  jr->rU = NumT<R>::c(0.);
+}
+
+/* Coefficients at one point for both calls the reference makes there:
+ * pol = 0 (get_jkinv) into (*ju, *ku) and pol = 1 (jar_calc) into *jr. */
+IPG_HEAVY void jar_both(const ModelPt &mp, const double K[4], int want_pol, int emission_type, double *ju,
+                         double *ku, Jar *jr)
+{
+  Jar z = {0., 0., 0., 0., 0., 0., 0., 0., 0., 0., 0.};
+  *jr = z;
+  *ju = 0.;
+  *ku = 0.;
+  double Ne = mp.ne;
+  if (Ne <= 0.) return;
+  JarGeo jg;
+  jar_geo(mp, K, emission_type, &jg);
+  jar_fits(Ne, mp.thetae, mp.bmag, jg, want_pol, emission_type, ju, ku, jr);
 }
 
 /* --------------------------------------------------------------------- */
 /* Transfer steps (src/ipolarray.c:332-628)                               */
 /* --------------------------------------------------------------------- */
+/* The transfer step below is written once for any number type R, like the
+ * fits: double for the image, dual numbers for the adjoint (derivatives
+ * with respect to the Stokes vector and the coefficients).  Same<R>::T keeps
+ * R deduced from the first argument only. */
+template <class R>
+struct Same {
+  typedef R T;
+};
+
 /* src/ipolarray.c:607-628 */
-__device__ __forceinline__ double approximate_solve(double Ii, double ji, double ki, double jf, double kf, double dl,
-                                                    double *tau)
+template <class R>
+__device__ __forceinline__ R approximate_solve(R Ii, typename Same<R>::T ji, typename Same<R>::T ki,
+                                               typename Same<R>::T jf, typename Same<R>::T kf, double dl,
+                                               typename Same<R>::T *tau)
 {
-  double javg = (ji + jf) / 2.;
-  double kavg = (ki + kf) / 2.;
-  double dtau = dl * kavg;
+  R javg = (ji + jf) / 2.;
+  R kavg = (ki + kf) / 2.;
+  R dtau = dl * kavg;
   *tau += dtau;
   if (dtau < 1.e-3) return Ii + (javg - Ii * kavg) * dl * (1. - (dtau / 2.) * (1. - dtau / 3.));
-  double efac = exp(-dtau);
+  R efac = exp(-dtau);
   return Ii * efac + (javg / kavg) * (1. - efac);
 }
 
@@ -1081,66 +1144,71 @@ __device__ __forceinline__ double approximate_solve(double Ii, double ji, double
  * turns S by the same angle in both of its half steps, so the sines and
  * cosines are computed once (faraday_rot) and applied twice (faraday_apply);
  * the small-rho branch is the linear form: c = 1, f = 0, s/rho = x. */
-struct FaradayRot {
-  double c, ir, g; /* cos(rho x), sin(rho x) / rho, 2 sin^2(rho x / 2) / rho^2 */
+template <class R>
+struct FaradayRotT {
+  R c, ir, g; /* cos(rho x), sin(rho x) / rho, 2 sin^2(rho x / 2) / rho^2 */
 };
+typedef FaradayRotT<double> FaradayRot;
 
-__device__ __forceinline__ FaradayRot faraday_rot(double rQ, double rU, double rV, double x)
+template <class R>
+__device__ __forceinline__ FaradayRotT<R> faraday_rot(R rQ, R rU, R rV, double x)
 {
-  FaradayRot R;
-  double rho2 = rQ * rQ + rU * rU + rV * rV;
+  FaradayRotT<R> F;
+  R rho2 = rQ * rQ + rU * rU + rV * rV;
   if (rho2 > IPG_CUT_PREVENT_NAN) {
-    double rho = sqrt(rho2);
-    double irho = 1. / rho;
-    double s, c;
+    R rho = sqrt(rho2);
+    R irho = 1. / rho;
+    R s, c;
     sincos(rho * x, &s, &c);
-    double sh = sin(0.5 * rho * x);
-    R.c = c;
-    R.ir = s * irho;
-    R.g = 2. * sh * sh * (irho * irho);
+    R sh = sin(0.5 * rho * x);
+    F.c = c;
+    F.ir = s * irho;
+    F.g = 2. * sh * sh * (irho * irho);
   } else {
-    R.c = 1.;
-    R.ir = x;
-    R.g = 0.;
+    F.c = NumT<R>::c(1.);
+    F.ir = NumT<R>::c(x);
+    F.g = NumT<R>::c(0.);
   }
-  return R;
+  return F;
 }
 
-__device__ __forceinline__ void faraday_apply(const FaradayRot &R, double rQ, double rU, double rV, double *SQ,
-                                              double *SU, double *SV)
+template <class R>
+__device__ __forceinline__ void faraday_apply(const FaradayRotT<R> &F, typename Same<R>::T rQ,
+                                              typename Same<R>::T rU, typename Same<R>::T rV, R *SQ, R *SU, R *SV)
 {
-  double SQ0 = *SQ, SU0 = *SU, SV0 = *SV;
-  double f = (rQ * SQ0 + rU * SU0 + rV * SV0) * R.g;
-  *SQ = SQ0 * R.c + rQ * f + (rU * SV0 - rV * SU0) * R.ir;
-  *SU = SU0 * R.c + rU * f + (rV * SQ0 - rQ * SV0) * R.ir;
-  *SV = SV0 * R.c + rV * f + (rQ * SU0 - rU * SQ0) * R.ir;
+  R SQ0 = *SQ, SU0 = *SU, SV0 = *SV;
+  R f = (rQ * SQ0 + rU * SU0 + rV * SV0) * F.g;
+  *SQ = SQ0 * F.c + rQ * f + (rU * SV0 - rV * SU0) * F.ir;
+  *SU = SU0 * F.c + rU * f + (rV * SQ0 - rQ * SV0) * F.ir;
+  *SV = SV0 * F.c + rV * f + (rQ * SU0 - rU * SQ0) * F.ir;
 }
 
 /* Absorption/emission full step (src/ipolarray.c:410-500) */
-__device__ __forceinline__ void absorb_emit(const Jar &c, double x, double *SI, double *SQ, double *SU, double *SV)
+template <class R>
+__device__ __forceinline__ void absorb_emit(const JarT<R> &c, double x, R *SI, R *SQ, R *SU, R *SV)
 {
-  double SI1 = *SI, SQ1 = *SQ, SU1 = *SU, SV1 = *SV;
-  double aI = c.aI, aQ = c.aQ, aU = c.aU, aV = c.aV, jI = c.jI, jQ = c.jQ, jU = c.jU, jV = c.jV;
-  double aP2 = aQ * aQ + aU * aU + aV * aV;
+  R SI1 = *SI, SQ1 = *SQ, SU1 = *SU, SV1 = *SV;
+  R aI = c.aI, aQ = c.aQ, aU = c.aU, aV = c.aV, jI = c.jI, jQ = c.jQ, jU = c.jU, jV = c.jV;
+  R aP2 = aQ * aQ + aU * aU + aV * aV;
   if (aP2 > IPG_CUT_PREVENT_NAN) {
-    double aP = sqrt(aP2);
-    double tauP = aP * x;
-    double tauI = aI * x;
-    double ads0 = aQ * SQ1 + aU * SU1 + aV * SV1;
-    double adj = aQ * jQ + aU * jU + aV * jV;
-    double efacm = exp(-tauI + tauP);
-    double efacp = exp(-tauI - tauP);
-    double efac = exp(-tauI);
+    R aP = sqrt(aP2);
+    R tauP = aP * x;
+    R tauI = aI * x;
+    R ads0 = aQ * SQ1 + aU * SU1 + aV * SV1;
+    R adj = aQ * jQ + aU * jU + aV * jV;
+    R efacm = exp(-tauI + tauP);
+    R efacp = exp(-tauI - tauP);
+    R efac = exp(-tauI);
     /* four divisions in all: 1/aP2, 1/aI, 1/(aI - aP), 1/(aI + aP) */
-    double iaP2 = 1. / aP2, i2aP2 = 0.5 * iaP2, i2aP = aP * i2aP2;
-    double SI2 = efacm * (0.5 * SI1 - ads0 * i2aP) + efacp * (0.5 * SI1 + ads0 * i2aP);
-    double cm = (-SI1 * aP + ads0) * i2aP2, cp = (SI1 * aP + ads0) * i2aP2;
-    double SQ2 = efacm * aQ * cm + efacp * aQ * cp + efac * (SQ1 - ads0 * aQ * iaP2);
-    double SU2 = efacm * aU * cm + efacp * aU * cp + efac * (SU1 - ads0 * aU * iaP2);
-    double SV2 = efacm * aV * cm + efacp * aV * cp + efac * (SV1 - ads0 * aV * iaP2);
-    double afacm = 1. - efacm, afac = 1. - efac, afacp = 1. - efacp;
+    R iaP2 = 1. / aP2, i2aP2 = 0.5 * iaP2, i2aP = aP * i2aP2;
+    R SI2 = efacm * (0.5 * SI1 - ads0 * i2aP) + efacp * (0.5 * SI1 + ads0 * i2aP);
+    R cm = (-SI1 * aP + ads0) * i2aP2, cp = (SI1 * aP + ads0) * i2aP2;
+    R SQ2 = efacm * aQ * cm + efacp * aQ * cp + efac * (SQ1 - ads0 * aQ * iaP2);
+    R SU2 = efacm * aU * cm + efacp * aU * cp + efac * (SU1 - ads0 * aU * iaP2);
+    R SV2 = efacm * aV * cm + efacp * aV * cp + efac * (SV1 - ads0 * aV * iaP2);
+    R afacm = 1. - efacm, afac = 1. - efac, afacp = 1. - efacp;
     if (tauI - tauP <= IPG_CUT_SMALL_TAU) {
-      double e = tauI - tauP;
+      R e = tauI - tauP;
       afacm = e * (1. - (0.5 * e) * (1. - e * (1. / 3.)));
       if (tauI <= IPG_CUT_SMALL_TAU) {
         e = tauI;
@@ -1151,20 +1219,20 @@ __device__ __forceinline__ void absorb_emit(const Jar &c, double x, double *SI, 
         }
       }
     }
-    double iaI = 1. / aI;
-    double adjP = adj * iaI * iaP2;
+    R iaI = 1. / aI;
+    R adjP = adj * iaI * iaP2;
     SQ2 += afac * (jQ * iaI - aQ * adjP);
     SU2 += afac * (jU * iaI - aU * adjP);
     SV2 += afac * (jV * iaI - aV * adjP);
-    double iam = 1. / (aI - aP), iap = 1. / (aI + aP);
-    double m1 = (aP * jI - adj) * i2aP * iam;
-    double m2 = (-aP * jI + adj) * i2aP2 * iam;
+    R iam = 1. / (aI - aP), iap = 1. / (aI + aP);
+    R m1 = (aP * jI - adj) * i2aP * iam;
+    R m2 = (-aP * jI + adj) * i2aP2 * iam;
     SI2 += afacm * m1;
     SQ2 += afacm * aQ * m2;
     SU2 += afacm * aU * m2;
     SV2 += afacm * aV * m2;
-    double p1 = (aP * jI + adj) * i2aP * iap;
-    double p2 = (aP * jI + adj) * i2aP2 * iap;
+    R p1 = (aP * jI + adj) * i2aP * iap;
+    R p2 = (aP * jI + adj) * i2aP2 * iap;
     SI2 += afacp * p1;
     SQ2 += afacp * aQ * p2;
     SU2 += afacp * aU * p2;
@@ -1174,7 +1242,7 @@ __device__ __forceinline__ void absorb_emit(const Jar &c, double x, double *SI, 
     *SU = SU2;
     *SV = SV2;
   } else {
-    double tf = 0;
+    R tf = NumT<R>::c(0.);
     *SI = approximate_solve(SI1, jI, aI, jI, aI, x, &tf);
     *SQ = approximate_solve(SQ1, jQ, aI, jQ, aI, x, &tf);
     *SU = approximate_solve(SU1, jU, aI, jU, aI, x, &tf);
