@@ -31,7 +31,7 @@ extern "C" {
 #define IPG_E_CUDA 2      /* CUDA runtime error or no device */
 #define IPG_E_MAXNSTEP 3  /* a geodesic hit maxnstep (reference: exit(-10), src/main.c:841-845) */
 #define IPG_E_NAN 4       /* NaN in the image (reference: exit(-1), src/main.c:905-908) */
-#define IPG_E_TIMEOUT 5   /* a device-side step budget ran out */
+#define IPG_E_TIMEOUT 5   /* a batch's step budget ran out (ipg_render_batch) */
 #define IPG_E_NOMEM 6     /* device or trajectory-pool memory exhausted */
 #define IPG_E_IO 7        /* file read/write error */
 #define IPG_E_STATE 8     /* call order error (e.g. tracing before a model upload) */
@@ -196,6 +196,69 @@ int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *
 #define IPG_NOALLOC_SCRATCH_BYTES 27806720
 int ipg_trace_pixels_noalloc(const ipg_grid *grid, const double *d_fields, const ipg_camera *cam,
                              const int32_t *d_ij, size_t n, ipg_pixel_out *d_out, void *stream);
+
+/* ---- batches of image instances ----
+ * No counterpart in the reference, which renders one image per run
+ * (src/main.c:506-811).  A batch renders many images of one iharm dump in
+ * one call: instances may differ in camera (inclination, frequency,
+ * resolution, refinement keys) and electron model (M_unit, R_high, R_low,
+ * beta_crit).  Instances whose cameras coincide share their geodesics, the
+ * four-vectors and the plasma tetrads of every step; each instance's image
+ * is the image ipg_render_image gives for the same parameters, bit for bit.
+ *
+ * The dump is uploaded once, as primitives: rho, u, U1..3, B1..3 with their
+ * ghost zones filled (populate_boundary_conditions, model/iharm/model.c:
+ * 1314-1370), and sqrt(b^2) in code units at the interior cells; gam, game,
+ * gamp are the model's adiabatic indices.  The derived fields of each
+ * electron model are computed on the device as init_physical_quantities
+ * computes them (model/iharm/model.c:610-717, ELECTRONS == 2). */
+enum {
+  IPG_BP_RHO = 0, IPG_BP_UU, IPG_BP_U1, IPG_BP_U2, IPG_BP_U3, IPG_BP_B1, IPG_BP_B2, IPG_BP_B3, IPG_BP_BMAG,
+  IPG_NBPRIM
+};
+int ipg_upload_iharm_batch(ipg_ctx *ctx, const ipg_grid *grid, const double *const prims[IPG_NBPRIM], double gam,
+                           double game, double gamp);
+
+/* electron model of an instance: set_units (model/iharm/model.c:595-608)
+ * for its M_unit, and the R_high/R_low temperature ratio */
+typedef struct ipg_electrons {
+  double RHO_unit, B_unit;                /* M_unit / L_unit^3, CL sqrt(4 pi RHO_unit) */
+  double trat_large, trat_small, beta_crit;
+} ipg_electrons;
+
+/* one image of a batch: its camera (as for ipg_trace_pixels), electron
+ * model and the image driver's sizes and keys (src/main.c:102-123,
+ * 520-792): internal size nx, ny (params.nx + 1 when refining an even size),
+ * internal base size nx_min, ny_min, refinement levels (1: none), and
+ * save_pixel's freqcgs^3 and qu_conv */
+typedef struct ipg_instance {
+  ipg_camera cam;
+  ipg_electrons el;
+  int nx, ny, nx_min, ny_min, refine_level;
+  double f3;
+  int qu_conv, nearest_neighbor;
+  double refine_abs, refine_rel, refine_cut;
+} ipg_instance;
+
+/* caller-owned host arrays of one instance's image, internal size nx * ny,
+ * as ipg_image holds them (imageS may be NULL for -unpol) */
+typedef struct ipg_instance_image {
+  double *image, *imageS, *taus;
+  int32_t *interp_flag, *oddflag, *nstep;
+  size_t traced; /* set by the call: pixels traced */
+} ipg_instance_image;
+
+/* Render n instances (needs ipg_upload_iharm_batch).  All instances share
+ * emission_type (4 or 1) and -unpol; at most IPG_BATCH_MAX_CAMERAS distinct
+ * cameras and IPG_BATCH_MAX_PER_CAMERA instances per camera.  The images
+ * come back in out[0..n).  step_budget > 0 caps the geodesic plus transfer
+ * steps of the whole call: once they are spent no further ray starts and
+ * the call returns IPG_E_TIMEOUT.  Returns IPG_E_MAXNSTEP / IPG_E_NAN as
+ * ipg_render_image does for any instance (ipg_last_error names it). */
+#define IPG_BATCH_MAX_CAMERAS 64
+#define IPG_BATCH_MAX_PER_CAMERA 32
+int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n, ipg_instance_image *out,
+                     uint64_t step_budget);
 
 /* ---- per-step trace of one ray (dump_var_along, src/io.c:279-543) ----
  * Traces pixel (i, j) with the same kernels as the image and returns, for

@@ -99,6 +99,7 @@ typedef struct ipg_iharm_model {
   void *fluid_header;          /* copy of the dump's /header group (for /fluid_header) */
   ipg_plugin plugin;           /* kind IPG_PLUGIN_IHARM, or a known-answer model (no fields) */
   double *trace_fields[3];     /* rho, u, beta per ghost-padded cell (trace output; NULL for plugins) */
+  double *bmag_code;           /* sqrt(b^2) per cell in code units, interior cells (batched instances; NULL for plugins) */
 } ipg_iharm_model;
 
 /* init_model: read the dump named in p->dump (an iharm v1 HDF5 dump, or the
@@ -144,6 +145,23 @@ typedef int (*ipg_tracer_fn)(void *user, const ipg_camera *cam, const int32_t *i
 int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const ipg_iharm_model *m, ipg_image *img,
                           void *log);
 void ipg_image_free(ipg_image *img);
+
+/* ---- batches of images (no counterpart in the reference, which renders
+ * one image per run) ----
+ * Upload the loaded dump's primitives for batches (ipg_upload_iharm_batch:
+ * rho and u with their ghost zones, the velocity and field primitives, and
+ * sqrt(b^2) in code units). */
+int ipg_upload_model_batch(ipg_ctx *ctx, const ipg_iharm_model *m);
+/* Render n images of the batch-uploaded dump in one ipg_render_batch call,
+ * image i with the parameters *ps[i] (modified as ipg_render_image modifies
+ * its parameters).  Each image equals the one ipg_render_image renders from
+ * the same dump loaded with ps[i]'s M_unit and electron keys, bit for bit.
+ * Instances share emission_type and -unpol; check mode, target_mdot,
+ * cooling_dynamical_times and a black-hole mass other than the model's
+ * return IPG_E_ARG.  imgs[0..n) are filled (free each with ipg_image_free,
+ * also after an error).  step_budget as for ipg_render_batch. */
+int ipg_render_batch_params(ipg_ctx *ctx, ipg_params *const *ps, size_t n, const ipg_iharm_model *m,
+                            ipg_image *imgs, uint64_t step_budget, void *log);
 
 /* print_image_stats (src/main.c:1001-1042) to `log` (a FILE*), same lines;
  * the "Ftot" line format is kept verbatim for scripts that scrape it. */

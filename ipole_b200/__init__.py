@@ -141,7 +141,8 @@ class _Model(C.Structure):
                 ("Mdot_dump", C.c_double), ("MdotEdd_dump", C.c_double), ("Ladv_dump", C.c_double),
                 ("t", C.c_double), ("DTd", C.c_double), ("electrons", C.c_int),
                 ("gam", C.c_double), ("game", C.c_double), ("gamp", C.c_double), ("fluid_header", C.c_void_p),
-                ("plugin", Plugin), ("trace_fields", C.POINTER(C.c_double) * 3)]
+                ("plugin", Plugin), ("trace_fields", C.POINTER(C.c_double) * 3),
+                ("bmag_code", C.POINTER(C.c_double))]
 
 
 class _Image(C.Structure):
@@ -215,6 +216,9 @@ def lib():
     L.ipg_print_image_stats.restype = None
     L.ipg_write_image.argtypes = [C.c_char_p, C.POINTER(_Image), C.POINTER(_Params), C.POINTER(_Model)]
     L.ipg_container_convert.argtypes = [C.c_char_p, C.c_char_p]
+    L.ipg_upload_model_batch.argtypes = [C.c_void_p, C.POINTER(_Model)]
+    L.ipg_render_batch_params.argtypes = [C.c_void_p, C.POINTER(C.POINTER(_Params)), C.c_size_t, C.POINTER(_Model),
+                                          C.POINTER(_Image), C.c_uint64, C.c_void_p]
     _lib = L
     return L
 
@@ -436,6 +440,16 @@ class Context:
         _check(lib().ipg_get_stats(self._h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
 
+    def upload_batch(self, model: Model):
+        """ipg_upload_model_batch: the dump's primitives for batched
+        instances (render_batch)."""
+        _check(lib().ipg_upload_model_batch(self._h, C.byref(model._m)), self._h)
+
+    def render_batch(self, params_list, model: Model, step_budget: int = 0):
+        """ipg_render_batch_params: one Image per Params, rendered in one
+        batch (instances with the same camera share their geodesics)."""
+        return _render_batch(self._h, params_list, model, step_budget)
+
     def render(self, params: Params, model: Model, log=False) -> Image:
         """Full image with adaptive refinement (main.c fast-light driver)."""
         p = params.copy()
@@ -449,6 +463,26 @@ class Context:
         finally:
             L.ipg_image_free(C.byref(im))
         return img
+
+
+def _render_batch(ctx_h, params_list, model: "Model", step_budget: int = 0):
+    n = len(params_list)
+    ps = [p.copy() for p in params_list]
+    arr = (C.POINTER(_Params) * n)(*[C.pointer(p._p) for p in ps])
+    ims = (_Image * n)()
+    L = lib()
+    rc = L.ipg_render_batch_params(ctx_h, arr, n, C.byref(model._m), ims, int(step_budget), None)
+    try:
+        _check(rc, ctx_h)
+        out = []
+        for k in range(n):
+            img = Image(ims[k], params_list[k])
+            img.params_after = ps[k]
+            out.append(img)
+    finally:
+        for k in range(n):
+            L.ipg_image_free(C.byref(ims[k]))
+    return out
 
 
 def render_with(tracer, params: Params, model: Model) -> Image:

@@ -36,15 +36,21 @@ static inline size_t IDX(const fluid_t *f, int i, int j, int k)
   return ((size_t)i * (f->n2 + 2) + j) * (f->n3 + 2) + k;
 }
 
+/* the mass-unit part of set_units: RHO_unit and B_unit of M_unit at L_unit */
+void ipg__units(double M_unit, double L_unit, double *RHO_unit, double *B_unit)
+{
+  *RHO_unit = M_unit / pow(L_unit, 3);
+  *B_unit = IPG_CL * sqrt(4. * M_PI * *RHO_unit);
+}
+
 /* set_units, model/iharm/model.c:595-608 */
 static void set_units(ipg_iharm_model *m, double MBH_solar, double *Mdotedd)
 {
   m->MBH = MBH_solar * IPG_MSUN;
   m->L_unit = IPG_GNEWT * m->MBH / (IPG_CL * IPG_CL);
   m->T_unit = m->L_unit / IPG_CL;
-  m->RHO_unit = m->M_unit / pow(m->L_unit, 3);
+  ipg__units(m->M_unit, m->L_unit, &m->RHO_unit, &m->B_unit);
   m->U_unit = m->RHO_unit * IPG_CL * IPG_CL;
-  m->B_unit = IPG_CL * sqrt(4. * M_PI * m->RHO_unit);
   *Mdotedd = 4. * M_PI * IPG_GNEWT * m->MBH * IPG_MP / IPG_CL / 0.1 / IPG_SIGMA_THOMSON;
   fprintf(stderr, "MBH: %g [Msun]\n", m->MBH / IPG_MSUN);
   fprintf(stderr, "L,T,M units: %g [cm] %g [s] %g [g]\n", m->L_unit, m->T_unit, m->M_unit);
@@ -106,6 +112,8 @@ void ipg_iharm_free(ipg_iharm_model *m)
     free(m->trace_fields[f]);
     m->trace_fields[f] = NULL;
   }
+  free(m->bmag_code);
+  m->bmag_code = NULL;
   if (m->fluid_header) {
     ipgc_free((ipgc_file *)m->fluid_header);
     free(m->fluid_header);
@@ -232,6 +240,9 @@ int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m)
   size_t ncell = (size_t)(N1 + 2) * (N2 + 2) * (N3 + 2);
   for (int l = 0; l < NPRIM_STORE; l++) f.p[l] = (double *)calloc(ncell, sizeof(double));
   f.b = (double *)calloc(ncell, sizeof(double));
+  /* sqrt(b^2) in code units, kept for batched instances, whose b field the
+   * device derives per mass unit (interior cells; ghost cells stay zero) */
+  m->bmag_code = (double *)calloc(ncell, sizeof(double));
   int n_prims = 0;
   const ipgc_entry *pe = ipgc_find(&file, "/prims");
   if (ipgc_get_i32(&file, "/header/n_prim", &n_prims) || !pe || pe->rank != 4 || pe->kind != IPGC_F64 ||
@@ -287,7 +298,9 @@ int ipg_iharm_load(const ipg_params *p, ipg_iharm_model *m)
         hc_flip_index(bcon, gcov, bcov);
         double bsq = 0.;
         for (int l = 0; l < NDIM; ++l) bsq += bcon[l] * bcov[l];
-        f.b[c] = sqrt(bsq) * m->B_unit;
+        const double bcode = sqrt(bsq);
+        m->bmag_code[c] = bcode;
+        f.b[c] = bcode * m->B_unit;
         if (i <= 21) dMact += gd * f.p[KRHO][c] * ucon[1];
         if (i <= 21) Ladv += gd * f.p[UU][c] * ucon[1] * ucov[0];
       }

@@ -161,13 +161,13 @@ int ipg_render_image_with(ipg_tracer_fn tracer, void *user, ipg_params *p, const
   return render(tracer, user, NULL, p, m, img, (FILE *)logp);
 }
 
-static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p, const ipg_iharm_model *m,
-                  ipg_image *img, FILE *log)
+/* The set-up of one image (main.c:102-168): the refinement geometry, the
+ * camera, the unit conversions of the parameters, and the image arrays
+ * (calloc'ed, internal size).  Fills ra with the image driver's sizes and
+ * keys.  Shared by the image driver and the batch driver. */
+static int image_setup(ipg_params *p, const ipg_iharm_model *m, ipg_image *img, ipg_refine_args *ra, FILE *log)
 {
-  if (!tracer || !p || !m || !img) return IPG_E_ARG;
-  tracer_t tr = {tracer, user};
   memset(img, 0, sizeof(*img));
-  if (p->perform_check && log) fprintf(log, "Running in check mode...\n");
   if (p->nx_min < 0) {
     p->nx_min = p->nx;
     p->ny_min = p->ny;
@@ -255,9 +255,41 @@ static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p,
   img->oddflag = (int32_t *)calloc(nx * ny, sizeof(int32_t));
   img->nstep = (int32_t *)calloc(nx * ny, sizeof(int32_t));
   if (!p->only_unpolarized) img->imageS = (double *)calloc(nx * ny * NIMG, sizeof(double));
+  if (!img->image || !img->taus || !img->interp_flag || !img->oddflag || !img->nstep ||
+      (!p->only_unpolarized && !img->imageS))
+    return IPG_E_NOMEM;
+  ra->nx = nx;
+  ra->ny = ny;
+  ra->nxmin = nxmin;
+  ra->nymin = nymin;
+  ra->refine_level = refine_level;
+  ra->params_nx = p->nx;
+  ra->params_ny = p->ny;
+  ra->f3 = pow(p->freqcgs, 3);
+  ra->only_unpolarized = p->only_unpolarized;
+  ra->qu_conv = p->qu_conv;
+  ra->nearest_neighbor = p->nearest_neighbor;
+  ra->refine_abs = p->refine_abs;
+  ra->refine_rel = p->refine_rel;
+  ra->refine_cut = p->refine_cut;
+  return IPG_OK;
+}
+
+static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p, const ipg_iharm_model *m,
+                  ipg_image *img, FILE *log)
+{
+  if (!tracer || !p || !m || !img) return IPG_E_ARG;
+  tracer_t tr = {tracer, user};
+  if (p->perform_check && log) fprintf(log, "Running in check mode...\n");
+  ipg_refine_args ra;
+  int rc = image_setup(p, m, img, &ra, log);
+  if (rc) return rc;
+  const size_t nx = ra.nx, ny = ra.ny, nxmin = ra.nxmin, nymin = ra.nymin;
+  const int refine_level = ra.refine_level;
+  ipg_camera *cam = &img->cam;
   int32_t *ij = (int32_t *)malloc(2 * nx * ny * sizeof(int32_t));
   ipg_pixel_out *out = (ipg_pixel_out *)malloc(nx * ny * sizeof(ipg_pixel_out));
-  if (!img->image || !img->taus || !img->interp_flag || !ij || !out || (!p->only_unpolarized && !img->imageS)) {
+  if (!ij || !out) {
     free(ij);
     free(out);
     return IPG_E_NOMEM;
@@ -300,21 +332,6 @@ static int render(ipg_tracer_fn tracer, void *user, ipg_ctx *dev, ipg_params *p,
   }
 
   if (dev) {
-    ipg_refine_args ra;
-    ra.nx = nx;
-    ra.ny = ny;
-    ra.nxmin = nxmin;
-    ra.nymin = nymin;
-    ra.refine_level = refine_level;
-    ra.params_nx = p->nx;
-    ra.params_ny = p->ny;
-    ra.f3 = pow(p->freqcgs, 3);
-    ra.only_unpolarized = p->only_unpolarized;
-    ra.qu_conv = p->qu_conv;
-    ra.nearest_neighbor = p->nearest_neighbor;
-    ra.refine_abs = p->refine_abs;
-    ra.refine_rel = p->refine_rel;
-    ra.refine_cut = p->refine_cut;
     free(ij);
     free(out);
     return ipg__render_levels_device(dev, cam, &ra, img, log);
@@ -448,6 +465,77 @@ done:
   free(prelim);
   free(ij);
   free(out);
+  return rc;
+}
+
+/* ---- batches (ipg_render_batch) ---- */
+int ipg_upload_model_batch(ipg_ctx *ctx, const ipg_iharm_model *m)
+{
+  if (!ctx || !m || m->plugin.kind != IPG_PLUGIN_IHARM || !m->bmag_code || !m->trace_fields[0] ||
+      !m->trace_fields[1])
+    return IPG_E_ARG;
+  const double *prims[IPG_NBPRIM] = {m->trace_fields[0],  m->trace_fields[1],  m->fields[IPG_F_U1],
+                                     m->fields[IPG_F_U2], m->fields[IPG_F_U3], m->fields[IPG_F_B1],
+                                     m->fields[IPG_F_B2], m->fields[IPG_F_B3], m->bmag_code};
+  return ipg_upload_iharm_batch(ctx, &m->grid, prims, m->gam, m->game, m->gamp);
+}
+
+int ipg_render_batch_params(ipg_ctx *ctx, ipg_params *const *ps, size_t n, const ipg_iharm_model *m,
+                            ipg_image *imgs, uint64_t step_budget, void *logp)
+{
+  FILE *log = (FILE *)logp;
+  if (!ctx || !ps || !m || !imgs || n == 0) return IPG_E_ARG;
+  for (size_t i = 0; i < n; i++) memset(&imgs[i], 0, sizeof(imgs[i]));
+  if (m->plugin.kind != IPG_PLUGIN_IHARM) return IPG_E_ARG;
+  ipg_instance *inst = (ipg_instance *)calloc(n, sizeof(ipg_instance));
+  ipg_instance_image *outs = (ipg_instance_image *)calloc(n, sizeof(ipg_instance_image));
+  int rc = (inst && outs) ? IPG_OK : IPG_E_NOMEM;
+  for (size_t i = 0; rc == IPG_OK && i < n; i++) {
+    ipg_params *p = ps[i];
+    /* the keys a batch does not serve: check mode, the accretion-rate
+     * rescaling of M_unit and the cooling cap of Theta_e; the black-hole
+     * mass fixes L_unit, which the dump's geometry carries */
+    const double L_unit = IPG_GNEWT * (p->MBH_solar * IPG_MSUN) / (IPG_CL * IPG_CL);
+    if (p->perform_check || p->target_mdot > 0 || p->cooling_dynamical_times > 1e-20 ||
+        L_unit != m->grid.L_unit) {
+      if (log)
+        fprintf(log, "batch instance %zu: check mode, target_mdot, cooling_dynamical_times and a black-hole "
+                     "mass other than the model's are not supported in a batch\n", i);
+      rc = IPG_E_ARG;
+      break;
+    }
+    ipg_refine_args ra;
+    rc = image_setup(p, m, &imgs[i], &ra, log);
+    if (rc) break;
+    ipg_instance *a = &inst[i];
+    a->cam = imgs[i].cam;
+    ipg__units(p->M_unit, m->grid.L_unit, &a->el.RHO_unit, &a->el.B_unit);
+    a->el.trat_large = p->trat_large;
+    a->el.trat_small = p->trat_small;
+    a->el.beta_crit = p->beta_crit;
+    a->nx = (int)ra.nx;
+    a->ny = (int)ra.ny;
+    a->nx_min = (int)ra.nxmin;
+    a->ny_min = (int)ra.nymin;
+    a->refine_level = ra.refine_level;
+    a->f3 = ra.f3;
+    a->qu_conv = ra.qu_conv;
+    a->nearest_neighbor = ra.nearest_neighbor;
+    a->refine_abs = ra.refine_abs;
+    a->refine_rel = ra.refine_rel;
+    a->refine_cut = ra.refine_cut;
+    outs[i].image = imgs[i].image;
+    outs[i].imageS = imgs[i].imageS;
+    outs[i].taus = imgs[i].taus;
+    outs[i].interp_flag = imgs[i].interp_flag;
+    outs[i].oddflag = imgs[i].oddflag;
+    outs[i].nstep = imgs[i].nstep;
+  }
+  if (rc == IPG_OK) rc = ipg_render_batch(ctx, inst, n, outs, step_budget);
+  if (rc == IPG_OK)
+    for (size_t i = 0; i < n; i++) imgs[i].traced = outs[i].traced;
+  free(inst);
+  free(outs);
   return rc;
 }
 

@@ -29,8 +29,37 @@ void ipg__set_error(ipg_ctx *ctx, const char *msg);
  * ipg__refine_release */
 void **ipg__refine_slot(ipg_ctx *ctx);
 
+/* the step arithmetic of the context (ipg_set_step_precision): 1 for FP32 */
+int ipg__step32(const ipg_ctx *ctx);
+/* per-context storage of the batch driver (ipg_refine.cu); ipg_destroy
+ * releases it with ipg__batch_arena_release */
+void **ipg__batch_arena_slot(ipg_ctx *ctx);
+/* set-up of a batch: one camera per camera group, the derived-field set of
+ * each (group, instance slot) as slot_set[g * G + k], the electron models */
+int ipg__batch_begin(ipg_ctx *ctx, const ipg_camera *grp_cam, int ngrp, const int *slot_set, int G,
+                     const ipg_electrons *sets, int nsets, int step32);
+/* the items of one traced level of a batch (device arrays) */
+typedef struct ipg_batch_items {
+  size_t n_geo;             /* geodesic items: one per (camera group, pixel) some instance traces */
+  const int32_t *geo_ij;    /* [2 n_geo] pixel */
+  const int32_t *geo_grp;   /* [n_geo] camera group */
+  const uint32_t *geo_mask; /* [n_geo] instance slots of the group that trace it */
+  size_t n_xf;              /* transfer items: one per (instance, traced pixel) */
+  const int32_t *xf_geo;    /* [n_xf] geodesic item */
+  const int32_t *xf_slot;   /* [n_xf] instance slot in its group */
+  ipg_pixel_out *xf_out;    /* [n_xf] get_pixel's outputs */
+} ipg_batch_items;
+/* trace one level; *steps_left (NULL: no budget) is the remaining step
+ * budget, decreased by the steps taken */
+int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *items, unsigned long long *steps_left);
+
+/* ---- provided by host/model_iharm.c ---- */
+/* RHO_unit and B_unit of a mass unit (set_units, model/iharm/model.c:595-608) */
+void ipg__units(double M_unit, double L_unit, double *RHO_unit, double *B_unit);
+
 /* ---- provided by ipg_refine.cu ---- */
 void ipg__refine_release(void *bufs);
+void ipg__batch_arena_release(void *arena);
 
 /* what the image driver needs beyond the camera: the sizes and keys of
  * src/main.c:102-123 and the save_pixel/refinement parameters */

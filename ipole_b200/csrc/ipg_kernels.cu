@@ -1326,8 +1326,11 @@ struct ipg_ctx {
   ipg_stats stats;
   void *refine; /* buffers of the on-device image driver (ipg_refine.cu) */
   double *d_trace_extra; /* rho, u, beta per cell for the trace output (ipg_upload_trace_fields) */
+  struct BatchState *batch; /* batch model and work arrays (ipg_batch.cuh) */
+  void *batch_arena;        /* buffers of the batch image driver (ipg_refine.cu) */
   char err[512];
 };
+static void batch_release(ipg_ctx *ctx);
 
 static int cuda_fail(ipg_ctx *ctx, cudaError_t e, const char *where)
 {
@@ -1404,6 +1407,8 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   ipg__refine_release(ctx->refine);
+  ipg__batch_arena_release(ctx->batch_arena);
+  batch_release(ctx);
   cudaFree(ctx->d_trace_extra);
   cudaFree(ctx->d_fields);
   cudaFree(ctx->d_pool);
@@ -2013,6 +2018,8 @@ extern "C" int ipg__trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_
 extern "C" void *ipg__stream(const ipg_ctx *ctx) { return (void *)ctx->stream; }
 extern "C" void ipg__set_error(ipg_ctx *ctx, const char *msg) { snprintf(ctx->err, sizeof(ctx->err), "%s", msg); }
 extern "C" void **ipg__refine_slot(ipg_ctx *ctx) { return &ctx->refine; }
+extern "C" void **ipg__batch_arena_slot(ipg_ctx *ctx) { return &ctx->batch_arena; }
+extern "C" int ipg__step32(const ipg_ctx *ctx) { return ctx->step32; }
 
 extern "C" int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n,
                                        ipg_pixel_out *d_out, void *stream)
@@ -2296,6 +2303,9 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
   NA_CK(cudaStreamSynchronize(stream));
   return n_maxn ? IPG_E_MAXNSTEP : IPG_OK;
 }
+
+/* batches of image instances */
+#include "ipg_batch.cuh"
 
 /* per-step trace of single rays (dump_var_along) */
 #include "ipg_trace.cuh"

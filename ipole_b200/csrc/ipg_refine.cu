@@ -587,3 +587,449 @@ extern "C" int ipg__render_levels_device(ipg_ctx *ctx, const ipg_camera *cam, co
   img->traced = traced;
   return IPG_OK;
 }
+
+/* ================================================================ batches */
+/* ipg_render_batch: the image driver above for many instances at once.  Per
+ * level, every instance decides which of its candidate pixels to trace
+ * exactly as a single image does (k_level with its own flux estimate and
+ * keys); the instances of a camera group share the candidates, so the union
+ * of their decisions is the group's list of geodesic items, each tagged with
+ * the mask of the instance slots that trace it, and every instance's own
+ * row-major list becomes its transfer items.  One ipg__batch_trace call
+ * traces the level of all groups; save_pixel, the checks and the flux
+ * estimate then run per instance on its share of the outputs. */
+
+__global__ void k_fill_i32(int32_t *a, int n, int v)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) a[t] = v;
+}
+
+/* mask[t]: bit k set when instance slot k of the group traces candidate t */
+__global__ void k_union(const int32_t *flags0, size_t stride, int G, int n, uint32_t *mask, int32_t *nz)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  uint32_t m = 0;
+  for (int k = 0; k < G; k++)
+    if (flags0[(size_t)k * stride + t]) m |= 1u << k;
+  mask[t] = m;
+  nz[t] = m != 0;
+}
+
+/* the group's geodesic items in candidate order, and each candidate's
+ * position among them */
+__global__ void __launch_bounds__(SCAN_TPB) k_union_scatter(const uint32_t *mask, const int32_t *nz, int n,
+                                                            const int32_t *block_sums, int nj, int nsx, int nsy,
+                                                            int g, int32_t *geo_ij, int32_t *geo_grp,
+                                                            uint32_t *geo_mask, int32_t *upos)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int f = t < n ? nz[t] : 0;
+  int e = block_exclusive_scan(f, NULL);
+  if (f) {
+    int pos = block_sums[blockIdx.x] + e;
+    geo_ij[2 * pos] = (t / nj) * nsx;
+    geo_ij[2 * pos + 1] = (t % nj) * nsy;
+    geo_grp[pos] = g;
+    geo_mask[pos] = mask[t];
+    upos[t] = pos;
+  }
+}
+
+/* an instance's traced pixels -> their geodesic items */
+__global__ void k_xf_map(const int32_t *ij, int n, int nj, int nsx, int nsy, const int32_t *upos, int geo_off,
+                         int slot, int32_t *xf_geo, int32_t *xf_slot)
+{
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  int t = (ij[2 * m] / nsx) * nj + ij[2 * m + 1] / nsy;
+  xf_geo[m] = geo_off + upos[t];
+  xf_slot[m] = slot;
+}
+
+namespace {
+/* bump allocation inside one device block (a first pass only sizes it) */
+struct Arena {
+  char *base = nullptr;
+  size_t off = 0;
+  template <class T>
+  T *take(size_t n)
+  {
+    size_t a = (off + 255) & ~(size_t)255;
+    off = a + n * sizeof(T);
+    return base ? reinterpret_cast<T *>(base + a) : nullptr;
+  }
+};
+
+struct BInst {
+  double *image, *taus, *imageS, *prelim;
+  int32_t *interp, *oddflag, *nstep, *flags, *bsums, *winner;
+  size_t npix, nprelim, traced;
+  int grp, slot, set;
+};
+
+struct BGrp {
+  int first, G; /* its instances are [first, first + G) in the internal order */
+  uint32_t *mask;
+  int32_t *nz, *bsums, *upos;
+  int sx, sy, nx, ny, nxmin, nymin, levels;
+};
+
+bool same_camera(const ipg_instance &a, const ipg_instance &b)
+{
+  const ipg_camera &x = a.cam, &y = b.cam;
+  return !memcmp(x.Xcam, y.Xcam, sizeof(x.Xcam)) && !memcmp(x.Econ, y.Econ, sizeof(x.Econ)) &&
+         !memcmp(x.Ecov, y.Ecov, sizeof(x.Ecov)) && x.fovx == y.fovx && x.fovy == y.fovy && x.rotcam == y.rotcam &&
+         x.xoff == y.xoff && x.yoff == y.yoff && x.freq == y.freq && x.eps == y.eps && x.nx == y.nx &&
+         x.ny == y.ny && x.maxnstep == y.maxnstep && x.only_unpolarized == y.only_unpolarized &&
+         x.emission_type == y.emission_type && x.stokes_floors == y.stokes_floors &&
+         x.target_nturns == y.target_nturns && x.subring_dtheta == y.subring_dtheta && x.counterjet == y.counterjet &&
+         a.nx == b.nx && a.ny == b.ny && a.nx_min == b.nx_min && a.ny_min == b.ny_min &&
+         a.refine_level == b.refine_level;
+}
+
+bool same_electrons(const ipg_electrons &a, const ipg_electrons &b)
+{
+  return a.RHO_unit == b.RHO_unit && a.B_unit == b.B_unit && a.trat_large == b.trat_large &&
+         a.trat_small == b.trat_small && a.beta_crit == b.beta_crit;
+}
+} // namespace
+
+struct BatchArena {
+  void *dev = nullptr;
+  size_t bytes = 0;
+};
+
+extern "C" void ipg__batch_arena_release(void *p)
+{
+  BatchArena *a = (BatchArena *)p;
+  if (!a) return;
+  cudaFree(a->dev);
+  delete a;
+}
+
+extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n, ipg_instance_image *outs,
+                                uint64_t step_budget)
+{
+  if (!ctx || !inst || !outs || n == 0) return IPG_E_ARG;
+  if (n > (size_t)IPG_BATCH_MAX_CAMERAS * IPG_BATCH_MAX_PER_CAMERA) return IPG_E_ARG;
+  cudaStream_t s = (cudaStream_t)ipg__stream(ctx);
+  /* camera groups and electron models */
+  std::vector<int> grp_of(n), set_of(n);
+  std::vector<int> grp_rep, set_rep;
+  for (size_t i = 0; i < n; i++) {
+    const ipg_instance &a = inst[i];
+    if (a.nx < 2 || a.ny < 2 || a.nx_min < 2 || a.ny_min < 2 || a.refine_level < 1 || !outs[i].image ||
+        !outs[i].taus || !outs[i].interp_flag || !outs[i].oddflag || !outs[i].nstep ||
+        (!a.cam.only_unpolarized && !outs[i].imageS) || (size_t)a.nx * a.ny >= (size_t)INT_MAX / 2)
+      return IPG_E_ARG;
+    int g = -1;
+    for (size_t q = 0; q < grp_rep.size(); q++)
+      if (same_camera(inst[grp_rep[q]], a)) g = (int)q;
+    if (g < 0) {
+      g = (int)grp_rep.size();
+      grp_rep.push_back((int)i);
+    }
+    grp_of[i] = g;
+    int e = -1;
+    for (size_t q = 0; q < set_rep.size(); q++)
+      if (same_electrons(inst[set_rep[q]].el, a.el)) e = (int)q;
+    if (e < 0) {
+      e = (int)set_rep.size();
+      set_rep.push_back((int)i);
+    }
+    set_of[i] = e;
+  }
+  const int ngrp = (int)grp_rep.size();
+  if (ngrp > IPG_BATCH_MAX_CAMERAS) {
+    ipg__set_error(ctx, "too many camera groups in one batch");
+    return IPG_E_ARG;
+  }
+  /* internal order: instances grouped by camera, slots in input order */
+  std::vector<int> order;
+  std::vector<BGrp> grps(ngrp);
+  int G = 1;
+  for (int g = 0; g < ngrp; g++) {
+    grps[g].first = (int)order.size();
+    for (size_t i = 0; i < n; i++)
+      if (grp_of[i] == g) order.push_back((int)i);
+    grps[g].G = (int)order.size() - grps[g].first;
+    if (grps[g].G > IPG_BATCH_MAX_PER_CAMERA) {
+      ipg__set_error(ctx, "more than IPG_BATCH_MAX_PER_CAMERA instances share one camera");
+      return IPG_E_ARG;
+    }
+    if (grps[g].G > G) G = grps[g].G;
+    const ipg_instance &r = inst[grp_rep[g]];
+    grps[g].nx = r.nx;
+    grps[g].ny = r.ny;
+    grps[g].nxmin = r.nx_min;
+    grps[g].nymin = r.ny_min;
+    grps[g].sx = (r.nx - 1) / (r.nx_min - 1);
+    grps[g].sy = (r.ny - 1) / (r.ny_min - 1);
+    grps[g].levels = r.refine_level;
+  }
+  std::vector<ipg_camera> gcam(ngrp);
+  std::vector<int> slot_set((size_t)ngrp * G, 0);
+  for (int g = 0; g < ngrp; g++) {
+    gcam[g] = inst[grp_rep[g]].cam;
+    for (int k = 0; k < grps[g].G; k++) slot_set[(size_t)g * G + k] = set_of[order[grps[g].first + k]];
+  }
+  std::vector<ipg_electrons> sets(set_rep.size());
+  for (size_t e = 0; e < set_rep.size(); e++) sets[e] = inst[set_rep[e]].el;
+  int rc = ipg__batch_begin(ctx, gcam.data(), ngrp, slot_set.data(), G, sets.data(), (int)sets.size(),
+                            ipg__step32(ctx));
+  if (rc) return rc;
+
+  /* device memory: per instance its image and level buffers, per group its
+   * union buffers, and the items of the largest level */
+  std::vector<BInst> bi(n);
+  size_t sum_pix = 0, sum_gpix = 0;
+  for (size_t q = 0; q < n; q++) {
+    const ipg_instance &a = inst[order[q]];
+    bi[q].npix = (size_t)a.nx * a.ny;
+    bi[q].nprelim = a.refine_level > 1 ? (size_t)a.nx_min * a.ny_min : 1;
+    bi[q].grp = grp_of[order[q]];
+    bi[q].slot = (int)q - grps[bi[q].grp].first;
+    bi[q].set = set_of[order[q]];
+    bi[q].traced = 0;
+    sum_pix += bi[q].npix;
+  }
+  for (int g = 0; g < ngrp; g++) sum_gpix += (size_t)grps[g].nx * grps[g].ny;
+  BatchArena **slot = (BatchArena **)ipg__batch_arena_slot(ctx);
+  if (!*slot) *slot = new BatchArena();
+  BatchArena *ar = *slot;
+  Arena A;
+  RefineStatus *st = nullptr, *gst = nullptr;
+  int32_t *ij_all = nullptr, *xf_geo = nullptr, *xf_slot = nullptr, *geo_ij = nullptr, *geo_grp = nullptr;
+  uint32_t *geo_mask = nullptr;
+  ipg_pixel_out *xf_out = nullptr;
+  std::vector<int32_t *> gflags(ngrp);
+  for (int pass = 0; pass < 2; pass++) {
+    A.base = pass ? (char *)ar->dev : nullptr;
+    A.off = 0;
+    for (size_t q = 0; q < n; q++) {
+      BInst &b = bi[q];
+      b.image = A.take<double>(b.npix);
+      b.taus = A.take<double>(b.npix);
+      b.imageS = gcam[b.grp].only_unpolarized ? nullptr : A.take<double>(b.npix * NIMG);
+      b.interp = A.take<int32_t>(b.npix);
+      b.oddflag = A.take<int32_t>(b.npix);
+      b.nstep = A.take<int32_t>(b.npix);
+      b.bsums = A.take<int32_t>(b.npix / SCAN_TPB + 2);
+      b.prelim = A.take<double>(b.nprelim);
+      b.winner = A.take<int32_t>(b.nprelim);
+    }
+    for (int g = 0; g < ngrp; g++) {
+      size_t gp = (size_t)grps[g].nx * grps[g].ny;
+      /* the candidate flags of the group's instances, one row each */
+      gflags[g] = A.take<int32_t>(gp * grps[g].G);
+      for (int k = 0; k < grps[g].G; k++) bi[grps[g].first + k].flags = gflags[g] ? gflags[g] + gp * k : nullptr;
+      grps[g].mask = A.take<uint32_t>(gp);
+      grps[g].nz = A.take<int32_t>(gp);
+      grps[g].bsums = A.take<int32_t>(gp / SCAN_TPB + 2);
+      grps[g].upos = A.take<int32_t>(gp);
+    }
+    st = A.take<RefineStatus>(n);
+    gst = A.take<RefineStatus>(ngrp);
+    ij_all = A.take<int32_t>(2 * sum_pix);
+    xf_geo = A.take<int32_t>(sum_pix);
+    xf_slot = A.take<int32_t>(sum_pix);
+    xf_out = A.take<ipg_pixel_out>(sum_pix);
+    geo_ij = A.take<int32_t>(2 * sum_gpix);
+    geo_grp = A.take<int32_t>(sum_gpix);
+    geo_mask = A.take<uint32_t>(sum_gpix);
+    if (pass == 0 && ar->bytes < A.off) {
+      cudaFree(ar->dev);
+      ar->dev = nullptr;
+      ar->bytes = 0;
+      CKR(cudaMalloc(&ar->dev, A.off));
+      ar->bytes = A.off;
+    }
+  }
+  for (size_t q = 0; q < n; q++) {
+    BInst &b = bi[q];
+    CKR(cudaMemsetAsync(b.image, 0, b.npix * sizeof(double), s));
+    CKR(cudaMemsetAsync(b.taus, 0, b.npix * sizeof(double), s));
+    if (b.imageS) CKR(cudaMemsetAsync(b.imageS, 0, b.npix * NIMG * sizeof(double), s));
+    CKR(cudaMemsetAsync(b.interp, 0, b.npix * sizeof(int32_t), s));
+    CKR(cudaMemsetAsync(b.oddflag, 0, b.npix * sizeof(int32_t), s));
+    CKR(cudaMemsetAsync(b.nstep, 0, b.npix * sizeof(int32_t), s));
+  }
+  {
+    std::vector<RefineStatus> z(n);
+    for (auto &x : z) {
+      memset(&x, 0, sizeof(x));
+      x.maxn_first = INT_MAX;
+    }
+    CKR(cudaMemcpyAsync(st, z.data(), n * sizeof(RefineStatus), cudaMemcpyHostToDevice, s));
+  }
+  unsigned long long steps_left = step_budget;
+  std::vector<RefineStatus> hst(n), hgst(ngrp);
+  std::vector<size_t> nlist(n), xoff(n), goff(ngrp), ucount(ngrp);
+  int maxlev = 0;
+  for (int g = 0; g < ngrp; g++) maxlev = grps[g].levels > maxlev ? grps[g].levels : maxlev;
+
+  for (int lvl = 0; lvl < maxlev; lvl++) {
+    std::vector<LevelArgs> L(ngrp);
+    std::vector<int> active(ngrp, 0);
+    for (int g = 0; g < ngrp; g++) {
+      BGrp &gr = grps[g];
+      if (lvl >= gr.levels) continue;
+      active[g] = 1;
+      LevelArgs &l = L[g];
+      memset(&l, 0, sizeof(l));
+      l.nx = gr.nx;
+      l.ny = gr.ny;
+      if (lvl == 0) {
+        l.nsx = gr.sx;
+        l.nsy = gr.sy;
+      } else {
+        l.nsx = (int)(gr.sx / pow(2, lvl));
+        l.nsy = (int)(gr.sy / pow(2, lvl));
+        if (l.nsx < 1 || l.nsy < 1) {
+          ipg__set_error(ctx, "refinement spacing below one pixel: nx_min/ny_min too small");
+          return IPG_E_ARG;
+        }
+      }
+      l.psx = 2 * l.nsx;
+      l.psy = 2 * l.nsy;
+      l.ni = (gr.nx - 1) / l.nsx + 1;
+      l.nj = (gr.ny - 1) / l.nsy + 1;
+    }
+    /* every instance's decisions and its own list count */
+    for (size_t q = 0; q < n; q++) {
+      BInst &b = bi[q];
+      if (!active[b.grp]) continue;
+      const ipg_instance &a = inst[order[q]];
+      LevelArgs l = L[b.grp];
+      l.unpol = a.cam.only_unpolarized;
+      l.nearest = a.nearest_neighbor;
+      l.refine_abs = a.refine_abs;
+      l.refine_rel = a.refine_rel;
+      l.refine_cut = a.refine_cut;
+      const int ncand = l.ni * l.nj, nb = grid_of(ncand, SCAN_TPB);
+      RefineStatus zz;
+      memset(&zz, 0, sizeof(zz));
+      zz.maxn_first = INT_MAX;
+      /* keep Iavg: the levels read it */
+      CKR(cudaMemcpyAsync(st + q, &zz, offsetof(RefineStatus, Iavg), cudaMemcpyHostToDevice, s));
+      ImgPtrs P = {b.image, b.taus, b.imageS, b.interp, b.oddflag, b.nstep, a.ny};
+      if (lvl == 0) k_fill_i32<<<grid_of(ncand, TPB), TPB, 0, s>>>(b.flags, ncand, 1);
+      else k_level<<<grid_of(ncand, TPB), TPB, 0, s>>>(l, P, st + q, b.flags, st + q);
+      k_scan_blocks<<<nb, SCAN_TPB, 0, s>>>(b.flags, ncand, b.bsums);
+      k_scan_top<<<1, SCAN_TPB, 0, s>>>(b.bsums, nb, st + q);
+    }
+    /* the groups' unions */
+    for (int g = 0; g < ngrp; g++) {
+      if (!active[g]) continue;
+      BGrp &gr = grps[g];
+      const int ncand = L[g].ni * L[g].nj, nb = grid_of(ncand, SCAN_TPB);
+      const size_t stride = (size_t)gr.nx * gr.ny;
+      k_union<<<grid_of(ncand, TPB), TPB, 0, s>>>(gflags[g], stride, gr.G, ncand, gr.mask, gr.nz);
+      k_scan_blocks<<<nb, SCAN_TPB, 0, s>>>(gr.nz, ncand, gr.bsums);
+      k_scan_top<<<1, SCAN_TPB, 0, s>>>(gr.bsums, nb, gst + g);
+    }
+    CKR(cudaGetLastError());
+    CKR(cudaMemcpyAsync(hst.data(), st, n * sizeof(RefineStatus), cudaMemcpyDeviceToHost, s));
+    CKR(cudaMemcpyAsync(hgst.data(), gst, ngrp * sizeof(RefineStatus), cudaMemcpyDeviceToHost, s));
+    CKR(cudaStreamSynchronize(s));
+    size_t n_geo = 0, n_xf = 0;
+    for (int g = 0; g < ngrp; g++) {
+      goff[g] = n_geo;
+      ucount[g] = active[g] ? (size_t)hgst[g].n : 0;
+      n_geo += ucount[g];
+    }
+    for (size_t q = 0; q < n; q++) {
+      nlist[q] = 0;
+      if (!active[bi[q].grp]) continue;
+      if (hst[q].nan) {
+        char m[128];
+        snprintf(m, sizeof(m), "NaN in the image of batch instance %d", order[q]);
+        ipg__set_error(ctx, m);
+        return IPG_E_NAN;
+      }
+      xoff[q] = n_xf;
+      nlist[q] = (size_t)hst[q].n;
+      n_xf += nlist[q];
+    }
+    if (n_geo == 0) continue;
+    for (int g = 0; g < ngrp; g++) {
+      if (!active[g] || !ucount[g]) continue;
+      const int ncand = L[g].ni * L[g].nj, nb = grid_of(ncand, SCAN_TPB);
+      k_union_scatter<<<nb, SCAN_TPB, 0, s>>>(grps[g].mask, grps[g].nz, ncand, grps[g].bsums, L[g].nj, L[g].nsx,
+                                               L[g].nsy, g, geo_ij + 2 * goff[g], geo_grp + goff[g],
+                                               geo_mask + goff[g], grps[g].upos);
+    }
+    for (size_t q = 0; q < n; q++) {
+      if (!nlist[q]) continue;
+      const BInst &b = bi[q];
+      const LevelArgs &l = L[b.grp];
+      const int ncand = l.ni * l.nj, nb = grid_of(ncand, SCAN_TPB);
+      k_scatter<<<nb, SCAN_TPB, 0, s>>>(b.flags, ncand, b.bsums, l.nj, l.nsx, l.nsy, ij_all + 2 * xoff[q]);
+      k_xf_map<<<grid_of((long long)nlist[q], TPB), TPB, 0, s>>>(ij_all + 2 * xoff[q], (int)nlist[q], l.nj, l.nsx,
+                                                                  l.nsy, grps[b.grp].upos, (int)goff[b.grp], b.slot,
+                                                                  xf_geo + xoff[q], xf_slot + xoff[q]);
+    }
+    CKR(cudaGetLastError());
+    ipg_batch_items items = {n_geo, geo_ij, geo_grp, geo_mask, n_xf, xf_geo, xf_slot, xf_out};
+    rc = ipg__batch_trace(ctx, &items, step_budget ? &steps_left : nullptr);
+    if (rc) return rc;
+    /* save_pixel, the checks and (base level) the flux estimate per instance */
+    for (size_t q = 0; q < n; q++) {
+      if (!nlist[q]) continue;
+      BInst &b = bi[q];
+      const ipg_instance &a = inst[order[q]];
+      const int nq = (int)nlist[q];
+      ImgPtrs P = {b.image, b.taus, b.imageS, b.interp, b.oddflag, b.nstep, a.ny};
+      k_check<<<grid_of(nq, TPB), TPB, 0, s>>>(xf_out + xoff[q], nq, a.cam.maxnstep, a.cam.only_unpolarized, st + q);
+      k_save<<<grid_of(nq, TPB), TPB, 0, s>>>(ij_all + 2 * xoff[q], xf_out + xoff[q], nq, P, a.f3,
+                                              a.cam.only_unpolarized, a.qu_conv, st + q);
+      if (lvl == 0 && a.refine_level > 1) {
+        const long long nslot = (long long)b.nprelim;
+        CKR(cudaMemsetAsync(b.prelim, 0, b.nprelim * sizeof(double), s));
+        CKR(cudaMemsetAsync(b.winner, 0xff, b.nprelim * sizeof(int32_t), s));
+        const BGrp &gr = grps[b.grp];
+        k_prelim_claim<<<grid_of(nq, TPB), TPB, 0, s>>>(ij_all + 2 * xoff[q], nq, a.nx, a.ny, a.ny_min, gr.sx,
+                                                        gr.sy, nslot, b.winner);
+        k_prelim_fill<<<grid_of(nq, TPB), TPB, 0, s>>>(ij_all + 2 * xoff[q], xf_out + xoff[q], nq, a.nx, a.ny,
+                                                       a.ny_min, gr.sx, gr.sy, nslot, b.winner, b.prelim);
+        k_prelim_sum<<<1, 32, 0, s>>>(b.prelim, nslot, a.f3, (double)b.npix, st + q);
+      }
+      b.traced += nlist[q];
+    }
+    CKR(cudaGetLastError());
+    CKR(cudaMemcpyAsync(hst.data(), st, n * sizeof(RefineStatus), cudaMemcpyDeviceToHost, s));
+    CKR(cudaStreamSynchronize(s));
+    for (size_t q = 0; q < n; q++) {
+      if (!nlist[q]) continue;
+      if (hst[q].maxn_first != INT_MAX) {
+        int32_t pij[2];
+        CKR(cudaMemcpy(pij, ij_all + 2 * (xoff[q] + (size_t)hst[q].maxn_first), sizeof(pij), cudaMemcpyDeviceToHost));
+        char m[160];
+        snprintf(m, sizeof(m), "MaxNStep exceeded in pixel %d %d of batch instance %d", pij[0], pij[1], order[q]);
+        ipg__set_error(ctx, m);
+        return IPG_E_MAXNSTEP;
+      }
+      if (hst[q].nan) {
+        char m[128];
+        snprintf(m, sizeof(m), "NaN in the image of batch instance %d", order[q]);
+        ipg__set_error(ctx, m);
+        return IPG_E_NAN;
+      }
+    }
+  }
+  for (size_t q = 0; q < n; q++) {
+    const BInst &b = bi[q];
+    ipg_instance_image &o = outs[order[q]];
+    CKR(cudaMemcpyAsync(o.image, b.image, b.npix * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CKR(cudaMemcpyAsync(o.taus, b.taus, b.npix * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (b.imageS) CKR(cudaMemcpyAsync(o.imageS, b.imageS, b.npix * NIMG * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CKR(cudaMemcpyAsync(o.interp_flag, b.interp, b.npix * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CKR(cudaMemcpyAsync(o.oddflag, b.oddflag, b.npix * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CKR(cudaMemcpyAsync(o.nstep, b.nstep, b.npix * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    o.traced = b.traced;
+  }
+  CKR(cudaStreamSynchronize(s));
+  return IPG_OK;
+}

@@ -1,0 +1,109 @@
+"""Batches of image instances (GPU): ipg_render_batch against one
+ipg_render_image call per instance.
+
+A batch shares the geodesics of instances with the same camera and derives
+each electron model's fields on the device; every instance's image must be
+the single-image path's image bit for bit (every array of the image,
+refinement decisions included).  The reference renders one image per run, so
+its pin is the single-image path's own parity with the reference's golden
+images, checked here again for the instance that repeats a golden case.
+"""
+import numpy as np
+import pytest
+
+import ipole_b200 as ip
+from tests import common
+
+pytestmark = pytest.mark.gpu
+
+BASE = ["--phicam=0", "--MBH=6.5e9", "--dsource=16.8e6", "--fov=160", "--trat_small=1"]
+
+# (camera, electrons) of each instance: three cameras (inclination,
+# frequency, rotation, size, refinement) and several electron models each
+CAMS = {
+    "A": ["--thetacam=163", "--rotcam=0", "--freqcgs=230.e9", "--nx=32", "--ny=32"],
+    "B": ["--thetacam=17", "--rotcam=30", "--qu_conv=1", "--freqcgs=345.e9", "--nx=32", "--ny=32", "--nx_min=8",
+          "--ny_min=8", "--refine_abs=2e-2", "--refine_rel=1e-2"],
+    "C": ["--thetacam=60", "--rotcam=0", "--freqcgs=86.e9", "--nx=33", "--ny=33", "--nx_min=9", "--ny_min=9"],
+}
+ELECTRONS = {
+    "A": [("3e27", "20"), ("3e27", "160"), ("9e27", "20"), ("1e26", "1")],
+    "B": [("3e27", "20"), ("3e27", "160"), ("1e27", "10")],
+    "C": [("3e27", "40")],
+}
+
+
+def _instances(dump):
+    out = []
+    for cam, els in ELECTRONS.items():
+        for mu, rh in els:
+            out.append(ip.Params.from_args([f"--dump={dump}", *BASE, *CAMS[cam], f"--M_unit={mu}",
+                                            f"--trat_large={rh}"]))
+    return out
+
+
+@pytest.fixture(scope="module")
+def c1_dump(dumps):
+    meta, _ = common.load_golden("c1_bright_32")
+    return dumps.get(meta)
+
+
+def _same(a, b):
+    for k in ("unpol", "tau", "pol", "interp_flag", "nstep", "oddflag"):
+        x, y = getattr(a, k), getattr(b, k)
+        assert x.shape == y.shape, k
+        assert np.array_equal(x.view(np.uint8), y.view(np.uint8)), k
+
+
+def test_batch_equals_single_images(c1_dump):
+    ps = _instances(c1_dump)
+    base = ip.Model.load(ps[0])
+    with ip.Context() as ctx:
+        ctx.upload_batch(base)
+        imgs = ctx.render_batch(ps, base)
+        st = ctx.stats()
+        assert st["ray_steps"] > 0 and st["waves"] >= 1
+        for p, img in zip(ps, imgs):
+            m = ip.Model.load(p)
+            ctx.upload(m)
+            ref = ctx.render(p, m)
+            _same(img, ref)
+            assert img.traced == ref.traced
+
+
+def test_batch_instance_matches_golden(c1_dump):
+    """c1_bright_32 as one instance of a batch against the reference's image"""
+    meta, arrs = common.load_golden("c1_bright_32")
+    ps = [common.params_for(meta, c1_dump)]
+    # a second instance on the same camera with another electron model
+    ps.append(common.params_for(meta, c1_dump, ["--trat_large=160"]))
+    m = ip.Model.load(ps[0])
+    with ip.Context() as ctx:
+        ctx.upload_batch(m)
+        img = ctx.render_batch(ps, m)[0]
+    e = common.image_errors(img, arrs)
+    for key in ("Ftot", "Ftot_unpol", "pix_I_max", "pix_unpol_max", "totQ", "totU", "totV", "EVPA_deg"):
+        assert e[key] <= common.tolerance(meta, key), (key, e[key])
+
+
+def test_batch_step_budget_times_out_and_context_recovers(c1_dump):
+    ps = _instances(c1_dump)[:3]
+    m = ip.Model.load(ps[0])
+    with ip.Context() as ctx:
+        ctx.upload_batch(m)
+        with pytest.raises(ip.IpgError) as e:
+            ctx.render_batch(ps, m, step_budget=2000)
+        assert e.value.code == ip.IPG_E_TIMEOUT
+        imgs = ctx.render_batch(ps, m)
+        assert all(np.isfinite(i.pol).all() and i.pol[..., 0].sum() > 0 for i in imgs)
+
+
+def test_batch_rejects_mixed_emission_types(c1_dump):
+    ps = _instances(c1_dump)[:2]
+    ps[1].set("emission_type", 1)
+    m = ip.Model.load(ps[0])
+    with ip.Context() as ctx:
+        ctx.upload_batch(m)
+        with pytest.raises(ip.IpgError) as e:
+            ctx.render_batch(ps, m)
+        assert e.value.code == ip.IPG_E_ARG
