@@ -260,6 +260,23 @@ typedef struct ipg_instance_image {
 int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n, ipg_instance_image *out,
                      uint64_t step_budget);
 
+/* ---- adjoint of the polarized image ----
+ * No counterpart in the reference, which only renders.  Given dL/d(I, Q,
+ * U, V) of the n pixels ij (the get_pixel outputs of ipg_pixel_out, before
+ * save_pixel's nu^3 and qu_conv sign), returns dL/dne, dL/dTheta_e and
+ * dL/d|B| for every ghost-padded cell of the uploaded iharm fields (the
+ * cell values the trilinear gather reads, layout of ipg_upload_iharm).  The
+ * call traces the pixels again (the forward outputs come back in out, when
+ * non-NULL), keeps N every ckpt_interval steps (16, 32 or 64) and walks each
+ * ray back to front, recomputing the coherency tensor between checkpoints
+ * and the fits with their derivatives at every radiating step.  Geodesics
+ * do not depend on the fluid and are not differentiated; neither are the
+ * sigma cut and the host's Theta_e floor (zero derivative almost
+ * everywhere).  Needs a polarized image without Stokes floors (IPG_E_ARG
+ * otherwise).  grad_* may be NULL. */
+int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *ij, size_t n, const double *dL_dIQUV,
+                int ckpt_interval, double *grad_ne, double *grad_thetae, double *grad_b, ipg_pixel_out *out);
+
 /* ---- per-step trace of one ray (dump_var_along, src/io.c:279-543) ----
  * Traces pixel (i, j) with the same kernels as the image and returns, for
  * steps s = 0..nstep, one row of IPG_TRACE_DOUBLES doubles: the quantities

@@ -163,6 +163,23 @@ int ipg_upload_model_batch(ipg_ctx *ctx, const ipg_iharm_model *m);
 int ipg_render_batch_params(ipg_ctx *ctx, ipg_params *const *ps, size_t n, const ipg_iharm_model *m,
                             ipg_image *imgs, uint64_t step_budget, void *log);
 
+/* ---- adjoint of an image (no counterpart in the reference) ----
+ * Gradients of a loss L of the polarized image rendered with *p (no
+ * refinement: every pixel is traced) from dL/dpol, the derivative with
+ * respect to the image's pol[nx][ny][0..3] (I, Q, U, V as the image file
+ * holds them).  Per cell: dL/dne, dL/dTheta_e, dL/d|B| of the model's fields
+ * (ipg_adjoint; dL/drho with Theta_e held is dL/dne RHO_unit / (MP + ME));
+ * and, through init_physical_quantities (model/iharm/model.c:610-717), the
+ * derivatives with respect to M_unit, R_high (trat_large) and R_low
+ * (trat_small).  The model must be loaded with p's electron keys.  pol_out
+ * (nx*ny*4, may be NULL) receives the image the adjoint traced. */
+typedef struct ipg_grad {
+  double *d_ne, *d_thetae, *d_b; /* per ghost-padded cell (caller-owned, may be NULL) */
+  double d_M_unit, d_R_high, d_R_low;
+} ipg_grad;
+int ipg_adjoint_params(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, const double *dL_dpol,
+                       int ckpt_interval, ipg_grad *g, double *pol_out);
+
 /* print_image_stats (src/main.c:1001-1042) to `log` (a FILE*), same lines;
  * the "Ftot" line format is kept verbatim for scripts that scrape it. */
 void ipg_print_image_stats(const ipg_image *img, const ipg_params *p, void *log);

@@ -153,6 +153,13 @@ class _Image(C.Structure):
                 ("oddflag", C.POINTER(C.c_int32)), ("nstep", C.POINTER(C.c_int32)), ("traced", C.c_size_t)]
 
 
+class Grad(C.Structure):
+    """ipg_grad: per-cell gradients and those of M_unit, R_high, R_low."""
+    _fields_ = [("d_ne", C.POINTER(C.c_double)), ("d_thetae", C.POINTER(C.c_double)),
+                ("d_b", C.POINTER(C.c_double)), ("d_M_unit", C.c_double), ("d_R_high", C.c_double),
+                ("d_R_low", C.c_double)]
+
+
 TRACER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(Camera), C.POINTER(C.c_int32), C.c_size_t,
                         C.POINTER(PixelOut))
 
@@ -217,6 +224,10 @@ def lib():
     L.ipg_write_image.argtypes = [C.c_char_p, C.POINTER(_Image), C.POINTER(_Params), C.POINTER(_Model)]
     L.ipg_container_convert.argtypes = [C.c_char_p, C.c_char_p]
     L.ipg_upload_model_batch.argtypes = [C.c_void_p, C.POINTER(_Model)]
+    L.ipg_adjoint.argtypes = [C.c_void_p, C.POINTER(Camera), C.c_void_p, C.c_size_t, C.c_void_p, C.c_int,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ipg_adjoint_params.argtypes = [C.c_void_p, C.POINTER(_Params), C.POINTER(_Model), C.c_void_p, C.c_int,
+                                     C.POINTER(Grad), C.c_void_p]
     L.ipg_render_batch_params.argtypes = [C.c_void_p, C.POINTER(C.POINTER(_Params)), C.c_size_t, C.POINTER(_Model),
                                           C.POINTER(_Image), C.c_uint64, C.c_void_p]
     _lib = L
@@ -449,6 +460,38 @@ class Context:
         """ipg_render_batch_params: one Image per Params, rendered in one
         batch (instances with the same camera share their geodesics)."""
         return _render_batch(self._h, params_list, model, step_budget)
+
+    def adjoint(self, cam: Camera, ij: np.ndarray, dL_dout: np.ndarray, ncell: int, ckpt: int = 16):
+        """ipg_adjoint: per-cell dL/dne, dL/dTheta_e, dL/d|B| (each (ncell,))
+        for dL_dout = dL/d(I, Q, U, V) of the pixels ij (get_pixel outputs),
+        and the forward outputs the call traced."""
+        ij = np.ascontiguousarray(ij, dtype=np.int32).reshape(-1, 2)
+        dL = np.ascontiguousarray(dL_dout, dtype=np.float64).reshape(len(ij), 4)
+        g = np.zeros((3, ncell))
+        out = np.zeros(len(ij), dtype=PIXEL_DTYPE)
+        _check(lib().ipg_adjoint(self._h, C.byref(cam), ij.ctypes.data, len(ij), dL.ctypes.data, int(ckpt),
+                                 g[0].ctypes.data, g[1].ctypes.data, g[2].ctypes.data, out.ctypes.data), self._h)
+        return g, out
+
+    def adjoint_image(self, params: Params, model: Model, dL_dpol: np.ndarray, ckpt: int = 16):
+        """ipg_adjoint_params: gradients of a loss of the (unrefined)
+        polarized image from dL/dpol (nx, ny, 4).  Returns a dict with the
+        per-cell gradients (ghost-padded (n1+2, n2+2, n3+2) arrays "ne",
+        "thetae", "b"), the scalars "M_unit", "R_high", "R_low" and the image
+        "pol" (nx, ny, 4) the adjoint traced."""
+        p = params.copy()
+        gr = model.grid
+        shape = (gr.n1 + 2, gr.n2 + 2, gr.n3 + 2)
+        ncell = shape[0] * shape[1] * shape[2]
+        dL = np.ascontiguousarray(dL_dpol, dtype=np.float64)
+        arrs = [np.zeros(ncell) for _ in range(3)]
+        g = Grad()
+        g.d_ne, g.d_thetae, g.d_b = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+        pol = np.zeros(dL.shape)
+        _check(lib().ipg_adjoint_params(self._h, C.byref(p._p), C.byref(model._m), dL.ctypes.data, int(ckpt),
+                                        C.byref(g), pol.ctypes.data), self._h)
+        return dict(ne=arrs[0].reshape(shape), thetae=arrs[1].reshape(shape), b=arrs[2].reshape(shape),
+                    M_unit=g.d_M_unit, R_high=g.d_R_high, R_low=g.d_R_low, pol=pol)
 
     def render(self, params: Params, model: Model, log=False) -> Image:
         """Full image with adaptive refinement (main.c fast-light driver)."""

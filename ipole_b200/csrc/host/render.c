@@ -539,6 +539,97 @@ int ipg_render_batch_params(ipg_ctx *ctx, ipg_params *const *ps, size_t n, const
   return rc;
 }
 
+/* ---- adjoint of an image ---- */
+int ipg_adjoint_params(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, const double *dL_dpol,
+                       int ckpt_interval, ipg_grad *g, double *pol_out)
+{
+  if (!ctx || !p || !m || !dL_dpol || !g) return IPG_E_ARG;
+  if (m->plugin.kind != IPG_PLUGIN_IHARM || !m->trace_fields[0] || !m->trace_fields[1] || !m->bmag_code ||
+      p->only_unpolarized || p->perform_check || p->target_mdot > 0 || p->cooling_dynamical_times > 1e-20)
+    return IPG_E_ARG;
+  ipg_image img;
+  ipg_refine_args ra;
+  int rc = image_setup(p, m, &img, &ra, NULL);
+  if (rc == IPG_OK && ra.refine_level != 1) rc = IPG_E_ARG; /* the adjoint traces every pixel */
+  const size_t nx = ra.nx, ny = ra.ny, npix = nx * ny;
+  const ipg_grid *gr = &m->grid;
+  const size_t ncell = (size_t)(gr->n1 + 2) * (gr->n2 + 2) * (gr->n3 + 2);
+  int32_t *ij = NULL;
+  double *dL = NULL, *gbuf = NULL;
+  ipg_pixel_out *out = NULL;
+  if (rc == IPG_OK) {
+    ij = (int32_t *)malloc(2 * npix * sizeof(int32_t));
+    dL = (double *)malloc(4 * npix * sizeof(double));
+    out = (ipg_pixel_out *)malloc(npix * sizeof(ipg_pixel_out));
+    gbuf = (double *)malloc(3 * ncell * sizeof(double));
+    if (!ij || !dL || !out || !gbuf) rc = IPG_E_NOMEM;
+  }
+  if (rc == IPG_OK) {
+    /* save_pixel (main.c:885-910): pol = (I, Q, U, V) nu^3, Q and U negated
+     * for qu_conv = 0 */
+    const double sq = p->qu_conv ? 1. : -1.;
+    for (size_t i = 0; i < nx; i++)
+      for (size_t j = 0; j < ny; j++) {
+        const size_t q = i * ny + j;
+        ij[2 * q] = (int32_t)i;
+        ij[2 * q + 1] = (int32_t)j;
+        dL[4 * q] = dL_dpol[4 * q] * ra.f3;
+        dL[4 * q + 1] = dL_dpol[4 * q + 1] * sq * ra.f3;
+        dL[4 * q + 2] = dL_dpol[4 * q + 2] * sq * ra.f3;
+        dL[4 * q + 3] = dL_dpol[4 * q + 3] * ra.f3;
+      }
+    rc = ipg_adjoint(ctx, &img.cam, ij, npix, dL, ckpt_interval, gbuf, gbuf + ncell, gbuf + 2 * ncell, out);
+  }
+  if (rc == IPG_OK) {
+    if (pol_out) {
+      const double sq = p->qu_conv ? 1. : -1.;
+      for (size_t q = 0; q < npix; q++) {
+        pol_out[4 * q] = out[q].I * ra.f3;
+        pol_out[4 * q + 1] = sq * out[q].Q * ra.f3;
+        pol_out[4 * q + 2] = sq * out[q].U * ra.f3;
+        pol_out[4 * q + 3] = out[q].V * ra.f3;
+      }
+    }
+    /* the electron model's parameters through init_physical_quantities
+     * (model/iharm/model.c:610-717): ne is proportional to M_unit and |B|
+     * to its square root; Theta_e = Th_u(trat) u / rho with
+     * trat = (R_high betasq + R_low) / (1 + betasq), floored at 1e-3 */
+    const double *ne = m->fields[IPG_F_NE], *th = m->fields[IPG_F_THETAE], *bb = m->fields[IPG_F_B];
+    const double *rho = m->trace_fields[0], *uu = m->trace_fields[1];
+    const double gam = m->gam, game = m->game, gamp = m->gamp;
+    const double gem1 = game - 1., gpm1 = gamp - 1.;
+    double dM = 0., dRh = 0., dRl = 0.;
+    for (size_t c = 0; c < ncell; c++) {
+      const double gn = gbuf[c], gt = gbuf[ncell + c], gb = gbuf[2 * ncell + c];
+      dM += gn * ne[c] + 0.5 * gb * bb[c];
+      if (gt == 0.) continue;
+      double bsq = bb[c] / m->B_unit;
+      bsq = bsq * bsq;
+      const double beta = uu[c] * (gam - 1.) / 0.5 / bsq;
+      const double betasq = beta * beta / p->beta_crit / p->beta_crit;
+      const double trat = p->trat_large * betasq / (1. + betasq) + p->trat_small / (1. + betasq);
+      const double den = gpm1 + gem1 * trat;
+      const double th_raw = (IPG_MP / IPG_ME) * gem1 * gpm1 / den * uu[c] / rho[c];
+      if (!(th_raw >= 1.e-3) || th[c] != th_raw) continue; /* floored */
+      const double dth_dtrat = -th_raw * gem1 / den;
+      dRh += gt * dth_dtrat * betasq / (1. + betasq);
+      dRl += gt * dth_dtrat / (1. + betasq);
+    }
+    g->d_M_unit = dM / m->M_unit;
+    g->d_R_high = dRh;
+    g->d_R_low = dRl;
+    if (g->d_ne) memcpy(g->d_ne, gbuf, ncell * sizeof(double));
+    if (g->d_thetae) memcpy(g->d_thetae, gbuf + ncell, ncell * sizeof(double));
+    if (g->d_b) memcpy(g->d_b, gbuf + 2 * ncell, ncell * sizeof(double));
+  }
+  free(ij);
+  free(dL);
+  free(out);
+  free(gbuf);
+  ipg_image_free(&img);
+  return rc;
+}
+
 void ipg_image_totals(const ipg_image *img, const ipg_params *p, double tot[5])
 {
   double Ftot = 0., Ftot_unpol = 0., Qtot = 0., Utot = 0., Vtot = 0.;

@@ -579,11 +579,17 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
  * step ending at s needs that does not depend on the radiation field.  The
  * record's geodesic block is overwritten by the coefficient block; dl and
  * nturns keep their slots. */
-template <int P, int EM = 0>
+/* ADJ (the adjoint's forward pass, iharm only): each radiating or last
+ * record also leaves an adjoint block of IPG_ADJ_DOUBLES in adj_side:
+ * X1 X2 X3, the fluid frequency, sin and cos of the k-B angle, the angle,
+ * and (along | in_domain << 1), from which the adjoint re-evaluates the fits
+ * with their derivatives. */
+#define IPG_ADJ_DOUBLES 8
+template <int P, int EM = 0, bool ADJ = false>
 __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     k_coeffs(double *__restrict__ pool, const int2 *__restrict__ chunk_meta,
              const unsigned long long *__restrict__ counters, long long n_chunks,
-             const RayRec *__restrict__ rays, const double *__restrict__ fields)
+             const RayRec *__restrict__ rays, const double *__restrict__ fields, double *__restrict__ adj_side)
 {
   const DevGrid &G = c_grid;
   const DevCam &C = c_cam;
@@ -624,6 +630,13 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
       model_point_t<P>(fields, X1, X2, X3, pg, &mp);
       int want_pol = pol && (flags & 1);
       coeffs_t<P>(mp, K, want_pol, EM ? EM : C.emission_type, &ju, &ku, &jar);
+      if constexpr (ADJ) {
+        JarGeo jg;
+        jar_geo(mp, K, EM ? EM : C.emission_type, &jg);
+        double *q = adj_side + ((size_t)c * IPG_CHUNK_STEPS + slot) * IPG_ADJ_DOUBLES;
+        store4(q, X1, X2, X3, jg.nu);
+        store4(q + 4, jg.sth, jg.cth, jg.theta, (double)(jg.along | (mp.in_domain << 1)));
+      }
       if (want_pol) {
         double Bcon[4] = {mp.Bcon[0], mp.Bcon[1], mp.Bcon[2], mp.Bcon[3]};
         double bsq = Bcon[0] * mp.Bcov[0] + Bcon[1] * mp.Bcov[1] + Bcon[2] * mp.Bcov[2] + Bcon[3] * mp.Bcov[3];
@@ -1143,11 +1156,14 @@ __device__ __forceinline__ void xfer_result(const DevCam &C, const Lane &L, int 
 
 /* RM: the step-record layout, 0 FP64, 1 compact, -1 from the camera (the
  * no-alloc path) */
-template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false, int RM = -1>
+/* CKK > 0 (the adjoint's forward pass): N of every step n with n % CKK == 0
+ * is kept in ckpt, at entry (chunk * 32 + n % 32) / min(CKK, 32), so that
+ * the adjoint recomputes N within a segment of CKK steps from its top. */
+template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false, int RM = -1, int CKK = 0>
 __global__ void __launch_bounds__(TPB, MINB)
     k_transfer(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
                const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays, ipg_pixel_out *__restrict__ out,
-               unsigned long long *__restrict__ counters)
+               unsigned long long *__restrict__ counters, double *__restrict__ ckpt)
 {
   const DevGrid &G = c_grid;
   const DevCam &C = c_cam;
@@ -1163,6 +1179,16 @@ __global__ void __launch_bounds__(TPB, MINB)
       atomicAdd(&counters[CNT_RAD], (unsigned long long)L.nrad);
       has = xfer_fetch<RM>(L, list, n_list, pool, chunk_prev, rays, out, counters);
       continue;
+    }
+    if constexpr (CKK > 0) {
+      if (L.n % CKK == 0) {
+        constexpr int KC = CKK < IPG_CHUNK_STEPS ? CKK : IPG_CHUNK_STEPS;
+        double *q = ckpt + (((size_t)L.chunk * IPG_CHUNK_STEPS + L.n % IPG_CHUNK_STEPS) / KC) * 16;
+        store4(q, L.N.r00, L.N.r01, L.N.r02, L.N.r03);
+        store4(q + 4, L.N.r11, L.N.r12, L.N.r13, L.N.r22);
+        store4(q + 8, L.N.r23, L.N.r33, L.N.s01, L.N.s02);
+        store4(q + 12, L.N.s03, L.N.s12, L.N.s13, L.N.s23);
+      }
     }
     /* step n -> n-1 of integrate_emission's loop, src/ipolarray.c:78-244 */
     int s = L.n - 1;
@@ -1690,15 +1716,16 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
     if (ctx->emission_type == 1) {
       int cb = grid_blocks(ctx, (const void *)k_coeffs<P, 1>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
       k_coeffs<P, 1><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays,
-                                                   ctx->d_fields);
+                                                   ctx->d_fields, nullptr);
     } else {
       int cb = grid_blocks(ctx, (const void *)k_coeffs<P, 4>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
       k_coeffs<P, 4><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays,
-                                                   ctx->d_fields);
+                                                   ctx->d_fields, nullptr);
     }
   } else {
     int cb = grid_blocks(ctx, (const void *)k_coeffs<P>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
-    k_coeffs<P><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields);
+    k_coeffs<P><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields,
+                                              nullptr);
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[2], b.stream));
@@ -1709,7 +1736,7 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
     int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM>, xthreads,    \
                          b.run);                                                                             \
     k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM><<<tb, xthreads, 0, b.stream>>>(                       \
-        b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);                                \
+        b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt, nullptr);                       \
   } while (0)
   if (ctx->step32) {
     if (ctx->rec_mixed) IPG_LAUNCH_XFER(true, 1);
@@ -2271,15 +2298,17 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
      * same bits for every ray */
     if (cam->emission_type == 1) {
       int cb = na_blocks(n_sm, (const void *)k_coeffs<IPG_PLUG_IHARM, 1>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
-      k_coeffs<IPG_PLUG_IHARM, 1><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
+      k_coeffs<IPG_PLUG_IHARM, 1><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields,
+                                                              nullptr);
     } else {
       int cb = na_blocks(n_sm, (const void *)k_coeffs<IPG_PLUG_IHARM, 4>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
-      k_coeffs<IPG_PLUG_IHARM, 4><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields);
+      k_coeffs<IPG_PLUG_IHARM, 4><<<cb, threads, 0, stream>>>(pool, chunk_meta, cnt_d, n_chunks, rays, d_fields,
+                                                              nullptr);
     }
     NA_CK(cudaGetLastError());
     int tb = na_blocks(n_sm, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0>, threads, run);
     k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0><<<tb, threads, 0, stream>>>(list, (int)run, pool, chunk_prev,
-                                                                                   rays, d_out, cnt_d);
+                                                                                   rays, d_out, cnt_d, nullptr);
     NA_CK(cudaGetLastError());
     unsigned long long cnt[CNT_N];
     NA_CK(cudaMemcpyAsync(cnt, cnt_d, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
@@ -2306,6 +2335,9 @@ extern "C" int ipg_trace_pixels_noalloc(const ipg_grid *g, const double *d_field
 
 /* batches of image instances */
 #include "ipg_batch.cuh"
+
+/* the adjoint of the polarized image */
+#include "ipg_adjoint.cuh"
 
 /* per-step trace of single rays (dump_var_along) */
 #include "ipg_trace.cuh"
