@@ -17,6 +17,7 @@ GOLDEN = os.path.join(HERE, "golden")
 PLUGIN_PREFIXES = ("analytic_", "sphere_")
 CHECK_PREFIX = "check_"
 TRACE_PREFIX = "trace_"
+ADJOINT_PREFIX = "adjoint_"  # finite differences of a loss (tests/test_gpu_adjoint.py), not images
 
 
 def golden_names(plugins=True, check=False, trace=False):
@@ -25,6 +26,7 @@ def golden_names(plugins=True, check=False, trace=False):
     check=True gives the check-mode cases instead (their arrays are the
     check/recheck blocks, not an image), trace=True the per-step traces."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    names = [n for n in names if not n.startswith(ADJOINT_PREFIX)]
     if check:
         return [n for n in names if n.startswith(CHECK_PREFIX)]
     if trace:
@@ -89,6 +91,12 @@ def oracle_tracer(orc, threads=8):
     return tracer
 
 
+def wrap180(d):
+    """|d| for an angle difference in degrees, taken modulo 180 (an EVPA and
+    its opposite direction are the same polarization)"""
+    return float(abs((d + 90.0) % 180.0 - 90.0))
+
+
 def image_errors(img, arrs):
     """Errors of a rendered image against golden arrays (relative to totals
     of I; per-pixel where I > 1e-6 max)."""
@@ -116,20 +124,29 @@ def image_errors(img, arrs):
             return np.hypot(Q, U) / It, V / It, 0.5 * np.arctan2(U, Q)
         lp, cp, ev = fr(p)
         lpg, cpg, evg = fr(pg)
+        e["LP_ref"] = float(lpg)
         e["LP_abs"] = float(abs(lp - lpg))
         e["CP_abs"] = float(abs(cp - cpg))
-        e["EVPA_deg"] = float(abs(np.degrees(ev - evg)))
+        e["EVPA_deg"] = wrap180(np.degrees(ev - evg))
     return e
 
 
 # Parity bound of the GPU tests: error <= max(base, FLOOR_FACTOR x the case's
 # reference noise floor: the largest deviation of the reference's other legal
-# builds (FMA contraction, -O2/-O3, AVX2/AVX-512) from its no-FMA build).
+# builds (FMA contraction, -O2/-O3, AVX2/AVX-512, a libm one ulp away) from its
+# no-FMA build).  The base tolerances are the target's: 1e-8 in total flux,
+# 1e-6 per pixel where I > 1e-6 max.
 BASE_TOL = dict(Ftot=1e-8, Ftot_unpol=1e-8, totQ=1e-7, totU=1e-7, totV=1e-7, pix_I_max=1e-6, pix_unpol_max=1e-6,
                 pix_QUV_over_I_max=1e-6, EVPA_deg=1e-5, LP_abs=1e-7, CP_abs=1e-7)
-FLOOR_FACTOR = 10.0
+FLOOR_FACTOR = 2.0
+# The flux-weighted EVPA is compared only where the image is polarized:
+# below a linear polarization fraction |sum Q + i sum U| / sum I of 1e-3 the
+# angle is set by rounding (the analytic models' nearly unpolarized images).
+EVPA_MIN_LP = 1e-3
 
 
 def tolerance(meta, key):
     floor = (meta.get("ref_noise_floor") or {}).get(key, 0.0)
+    if key == "EVPA_deg":
+        floor = wrap180(floor)  # floors recorded before the angle was wrapped
     return max(BASE_TOL[key], FLOOR_FACTOR * floor)

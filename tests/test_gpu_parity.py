@@ -11,11 +11,12 @@ last-bit differences of the metric by 1/(2 DEL), and the polarized step turns
 them into rotations through Faraday depths of ~1e3.  The GPU path (CUDA libm,
 FMA) sits on the same floor, so each metric must satisfy
 
-    error <= max(base tolerance, 10 x the case's reference noise floor)
+    error <= max(base tolerance, 2 x the case's reference noise floor)
 
 with base tolerances total I 1e-8, total Q/U/V 1e-7 of total I, per pixel
 (where I > 1e-6 max) 1e-6 for I and Q/U/V (relative to I), EVPA 1e-5 degree,
-LP/CP 1e-7.
+LP/CP 1e-7.  EVPA is compared where the reference image's linear
+polarization fraction is at least 1e-3 (common.EVPA_MIN_LP).
 """
 import numpy as np
 import pytest
@@ -46,7 +47,9 @@ def test_golden_image(case, dumps, ctx):
     print(case, {k: f"{v:.2e}" for k, v in e.items()})
     keys = ["Ftot_unpol", "pix_unpol_max"]
     if "pol" in arrs:
-        keys += ["Ftot", "totQ", "totU", "totV", "pix_I_max", "pix_QUV_over_I_max", "EVPA_deg", "LP_abs", "CP_abs"]
+        keys += ["Ftot", "totQ", "totU", "totV", "pix_I_max", "pix_QUV_over_I_max", "LP_abs", "CP_abs"]
+        if e["LP_ref"] >= common.EVPA_MIN_LP:
+            keys.append("EVPA_deg")
     bad = {k: (e[k], tolerance(meta, k)) for k in keys if not e[k] <= tolerance(meta, k)}
     assert not bad, bad
     assert np.all(img.oddflag == 0)
