@@ -364,6 +364,10 @@ def run_ours(args):
                          "EVPA_deg": abs(float(np.degrees(0.5 * (np.arctan2(U1, Q1) - np.arctan2(U0, Q0))))),
                          "pix_I_max_rel": float(np.max(np.abs(mo["I"][bright] / out["I"][bright] - 1)))}}
 
+    batched = bench_batched(ip, ctx, model, dump, args, world, stream, ms_max / args.steps)
+    adjoint = bench_adjoint(ip, ctx, model, p, args, world, stream)
+    ctx.upload(model)
+
     peak = ip.fp64_peak_tflops(local, 300.0)
     dom = max(kms, key=kms.get)
     fps = FLOPS_PER_STEP[dom]
@@ -393,7 +397,8 @@ def run_ours(args):
                        "l2": "inputs larger than L2: 392 MB field array + trajectory pool writes per step"},
             "ray_steps_per_s": total_steps / (ms_max / 1e3), "ray_steps_per_image": steps / args.steps,
             "radiating_fraction": rad / max(steps, 1), "Ftot_Jy": ftot, "e2e": e2e, "roofline": roofline,
-            "clocks": clk, "gpu_launches": launches, "mixed_records": mixed}
+            "clocks": clk, "gpu_launches": launches, "mixed_records": mixed, "batched": batched,
+            "adjoint": adjoint}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             cb = cpu_reference_sample(dump, args.m_unit)
@@ -409,6 +414,121 @@ def run_ours(args):
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+# Batches of instances (ipg_render_batch).  The headline batch is the bench
+# image's camera with the electron models of the batched workload: R_high
+# {1, 10, 40, 160} x M_unit {0.5, 2} x the bench's, 8 images of 400x400.  The
+# batched workload itself: {86, 230, 345} GHz x inclinations {17, 60, 120,
+# 163} x the same 8 electron models, 96 images; each of the 12 cameras has
+# its own resolution, 64, 160 or 320 pixels a side in turn, refined from a
+# quarter of it (refine_abs 2e-2, refine_rel 1e-2).
+BATCH_RHIGH = (1, 10, 40, 160)
+BATCH_MU = (0.5, 2.0)
+BATCH_FREQS = (86e9, 230e9, 345e9)
+BATCH_INCL = (17, 60, 120, 163)
+BATCH_RES = (64, 160, 320)
+
+
+def batch_params(ip, dump, m_unit, nx, incl=163, freq=230e9, refine=False):
+    out = []
+    for rh in BATCH_RHIGH:
+        for f in BATCH_MU:
+            a = [f"--dump={dump}", f"--freqcgs={freq:.6g}", f"--thetacam={incl}", "--phicam=0", "--rotcam=0",
+                 "--MBH=6.5e9", "--dsource=16.8e6", "--fov=160", "--trat_small=1", f"--trat_large={rh}",
+                 f"--M_unit={m_unit * f:g}", f"--nx={nx}", f"--ny={nx}"]
+            if refine:
+                a += [f"--nx_min={nx // 4}", f"--ny_min={nx // 4}", "--refine_abs=2e-2", "--refine_rel=1e-2"]
+            out.append(ip.Params.from_args(a))
+    return out
+
+
+def bench_batched(ip, ctx, model, dump, args, world, stream, single_ms):
+    """images/s of the batched forms, FP64 and with the FP32 polarized step,
+    beside the single-image FP64 rate of this run"""
+    import torch
+    nx = args.size
+    ctx.upload_batch(model)
+    res = {}
+    ps = batch_params(ip, dump, args.m_unit, nx)
+    for name, step32 in (("fp64", False), ("fp32_step", True)):
+        ctx.set_step_precision(ip.IPG_STEP_FP32 if step32 else ip.IPG_STEP_FP64)
+        ctx.render_batch(ps, model)
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(1, args.steps // 2)
+        e0.record(stream)
+        for _ in range(reps):
+            imgs = ctx.render_batch(ps, model)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world) / reps
+        st = ctx.stats()
+        res[name] = {"value": images_per_s(world, len(ps), ms), "unit": "images/s", "ms_per_batch": ms,
+                     "instances": len(ps), "vs_single_fp64": (len(ps) / ms) / (1.0 / single_ms),
+                     "geodesic_ms": st["geodesic_ms"], "coeffs_ms": st["coeffs_ms"],
+                     "transfer_ms": st["transfer_ms"], "waves": st["waves"]}
+        if step32:
+            ref = fp64_imgs
+            errs = []
+            for a, b in zip(imgs, ref):
+                I0, I1 = b.pol[..., 0].sum(), a.pol[..., 0].sum()
+                errs.append(abs(I1 / I0 - 1))
+            res[name]["vs_fp64_Ftot_rel_max"] = float(max(errs))
+        else:
+            fp64_imgs = imgs
+    ctx.set_step_precision(ip.IPG_STEP_FP64)
+    res["workload"] = (f"{len(ps)} instances of the bench image's camera ({nx}x{nx}, 230 GHz, thetacam 163): "
+                       f"R_high {list(BATCH_RHIGH)} x M_unit {list(BATCH_MU)} x {args.m_unit:g}")
+    if args.size == NX and not args.small:
+        # the batched workload: 96 instances of mixed resolution, refined
+        ps96 = []
+        for fi, fq in enumerate(BATCH_FREQS):
+            for ii, inc in enumerate(BATCH_INCL):
+                ps96 += batch_params(ip, dump, args.m_unit, BATCH_RES[(fi + ii) % 3], inc, fq, refine=True)
+        t = time.time()
+        imgs = ctx.render_batch(ps96, model)
+        torch.cuda.synchronize()
+        sec = time.time() - t
+        st = ctx.stats()
+        pix = sum(int(i.traced) for i in imgs)
+        res["workload_96"] = {"value": len(ps96) / sec, "unit": "images/s", "seconds": sec,
+                              "instances": len(ps96), "traced_pixels": pix, "ray_steps": st["ray_steps"],
+                              "pixels_per_s": pix / sec,
+                              "workload": "96 instances: {86,230,345} GHz x thetacam {17,60,120,163} x R_high "
+                                          "{1,10,40,160} x M_unit {0.5,2} x base; 64/160/320 pixels a side per "
+                                          "camera, refined from a quarter (refine_abs 2e-2, refine_rel 1e-2); "
+                                          "host-timed single call"}
+    return res
+
+
+def bench_adjoint(ip, ctx, model, p, args, world, stream):
+    """one adjoint image (ipg_adjoint_params: its own forward trace, then the
+    reverse walk) against one forward image of the same parameters"""
+    import numpy as np
+    import torch
+    ctx.upload(model)
+    img = ctx.render(p, model)
+    scale = float(np.abs(img.pol[..., 0]).max())
+    dL = img.pol[..., :4] / (scale * scale)  # the gradient of 0.5 sum (pol / scale)^2
+    res = {}
+    for K in (16, 64):
+        ctx.adjoint_image(p, model, dL, ckpt=K)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        r = ctx.adjoint_image(p, model, dL, ckpt=K)
+        torch.cuda.synchronize()
+        res[f"K{K}_ms"] = (time.time() - t0) * 1e3
+    t0 = time.time()
+    ctx.render(p, model)
+    torch.cuda.synchronize()
+    fwd_ms = (time.time() - t0) * 1e3
+    res.update({"forward_image_ms": fwd_ms, "cost_vs_forward_K16": res["K16_ms"] / fwd_ms,
+                "cost_vs_forward_K64": res["K64_ms"] / fwd_ms, "dL_dM_unit": r["M_unit"],
+                "note": "host-timed calls through ipg_adjoint_params and ipg_render_image (both include their "
+                        "host-side set-up and copies); the adjoint call includes its own forward trace"})
+    return res
 
 
 def run_one_ray(args):
