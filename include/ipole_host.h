@@ -223,6 +223,37 @@ int ipg_write_traces(ipg_ctx *ctx, const ipg_image *img, const ipg_params *p, co
  * B-tree, filters other than deflate and shuffle). */
 int ipg_container_convert(const char *src, const char *dst);
 
+/* ---- the reference's model plugin interface (src/model.h:9-44) ----
+ * The same names and signatures, over one library-global iharm model:
+ * try_set_model_parameter collects par keys (ipg_params_set on the
+ * interface's own parameters, ipg_model_params), init_model loads the dump
+ * they name (ipg_iharm_load) and sets the unit globals, the point queries
+ * read the loaded fields on the host.  Where the reference exits, init_model
+ * leaves no model loaded and ipg_model_status() returns the IPG_E_* code.
+ * update_data and update_data_until do nothing (one dump, fast light).  The
+ * image file's model header (the reference's output_hdf5) is written by
+ * ipg_write_image. */
+extern double M_unit, L_unit, T_unit, RHO_unit, U_unit, B_unit, Te_unit;
+void try_set_model_parameter(const char *word, const char *value);
+void init_model(double *tA, double *tB);
+int radiating_region(double X[4]);
+double get_model_thetae(double X[4]);
+double get_model_b(double X[4]);
+double get_model_sigma(double X[4]);
+double get_model_beta(double X[4]);
+double get_model_ne(double X[4]);
+void get_model_jar(double X[4], double Kcon[4], double *jI, double *jQ, double *jU, double *jV, double *aI,
+                   double *aQ, double *aU, double *aV, double *rQ, double *rU, double *rV);
+void get_model_fourv(double X[4], double Kcon[4], double Ucon[4], double Ucov[4], double Bcon[4], double Bcov[4]);
+void update_data(double *tA, double *tB);
+void update_data_until(double *tA, double *tB, double tgt);
+void get_model_primitives(double X[4], double *p);
+/* the interface's parameters, its loaded model (NULL before init_model) and
+ * the status of the last init_model */
+ipg_params *ipg_model_params(void);
+const ipg_iharm_model *ipg_model_loaded(void);
+int ipg_model_status(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,7 +29,8 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-v"]
 CC_FLAGS = ["-std=gnu99", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-result"]
 CU_EXTRA = ["ipg_refine.cu"]
-HOST_SRC = ["ipgc.c", "h5lite.c", "plugins.c", "trace.c", "coords.c", "par.c", "model_iharm.c", "camera.c", "render.c"]
+HOST_SRC = ["ipgc.c", "h5lite.c", "plugins.c", "trace.c", "coords.c", "par.c", "model_iharm.c", "camera.c", "render.c",
+            "model_api.c"]
 
 
 def _nvcc() -> str:
