@@ -42,15 +42,26 @@ METRIC = "IQUV 400² images/s & ray-steps/s, 1 B200: plain FP64 vs mixed+batched
 DUMP = dict(n1=288, n2=128, n3=128, seed=1)
 SMALL_DUMP = dict(n1=128, n2=64, n3=64, seed=1)
 NX = NY = 400
-M_UNIT = 7.5e27
+M_UNIT = 7.96e27  # total flux 0.6 Jy at R_high 160, thetacam 163 (tests/golden/tune_munit.py)
 BASE_ARGS = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
              "--fov=160", "--trat_large=160", "--trat_small=1"]
 CPU_SAMPLE = 64  # reference / oracle sample image size (pixels per side)
-# Work per ray-step of each kernel, from the ncu capture of a 200x200 image of
-# the 128x64x64 dump: FP64 flops (2 per DFMA, 1 per DADD/DMUL) and DRAM bytes
-# read + written.  k_coeffs works per step record
-# (ray-steps + one camera record per ray).
-FLOPS_PER_STEP = {"geodesic": 1831, "coeffs": 1535, "transfer": 913}
+# The reference algorithm's FP64 work, counted exactly by running the oracle's
+# restatement of it over a counting number type on the 128x128 image of the
+# 128x64x64 dump (oracle/opcount/count_ops.py -> counts_c1_128.json; each
+# transcendental call weighted 20 flops): per ray-step, the geodesic step
+# (push_photon, stepsize, stop test) and the two push_polar calls of
+# integrate_emission; per radiating step, the coefficients (point queries,
+# get_jkinv, jar_calc, plasma tetrad) and the transfer arithmetic (evolve_N).
+# These are the algorithmic flops of the roofline: the geodesic kernel does
+# the geodesic and the connections, the coefficient and transfer kernels the
+# rest.
+REF_FLOPS = {"geodesic_per_step": 24172.6, "push_per_step": 30454.0, "coeffs_per_radiating_step": 8942.3,
+             "transfer_per_radiating_step": 4751.9}
+# What the kernels execute per ray-step, from the ncu capture of a 200x200
+# image of the 128x64x64 dump: FP64 flops (2 per DFMA, 1 per DADD/DMUL) and
+# DRAM bytes read + written (k_coeffs works per step record).
+EXEC_FLOPS_PER_STEP = {"geodesic": 1831, "coeffs": 1535, "transfer": 913}
 DRAM_BYTES_PER_STEP = {"geodesic": 377, "coeffs": 412, "transfer": 537}
 
 
@@ -234,7 +245,8 @@ def run_reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "iharm FMKS 288x128x128 seed 1, 400x400 IQUV, 230 GHz, thetacam 163, "
-                                   "R_high 160", "M_unit": args.m_unit},
+                                   f"R_high 160, plain FP64 ({CPU_SAMPLE}² sample scaled to 400²)",
+                       "M_unit": args.m_unit},
             "cpu_baseline": {"value": v, "unit": "images/s", "cores": times[0]["cores"], "kind": times[0]["kind"],
                              "sample": times[0]["sample"]},
             "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -277,6 +289,7 @@ def run_ours(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     steps = rad = launches = 0
     kms = {"geodesic": 0.0, "coeffs": 0.0, "transfer": 0.0}
+    span = {"geodesic": 0.0, "coeffs": 0.0, "transfer": 0.0}
     pred_ms = wall_ms = 0.0
     torch.cuda.synchronize()
     e0.record(stream)
@@ -288,6 +301,7 @@ def run_ours(args):
         launches += s["launches"]
         for k in kms:
             kms[k] += s[f"{k}_ms"]
+            span[k] += s[f"{k}_span_ms"]
         pred_ms += s["predict_ms"]
         wall_ms += s["wall_ms"]
     e1.record(stream)
@@ -337,6 +351,7 @@ def run_ours(args):
     # kernels, timed like the headline, and its error against that image
     ctx.set_record_precision(ip.IPG_RECORDS_MIXED)
     ctx.set_step_precision(ip.IPG_STEP_FP32)
+    ctx.set_fit_precision(ip.IPG_FITS_FP32)
     ctx.trace_device(cam, d_ij.data_ptr(), n, d_out.data_ptr())
     torch.cuda.synchronize()
     barrier(world)
@@ -351,14 +366,16 @@ def run_ours(args):
     mo = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=ip.PIXEL_DTYPE)
     ctx.set_record_precision(ip.IPG_RECORDS_FP64)
     ctx.set_step_precision(ip.IPG_STEP_FP64)
+    ctx.set_fit_precision(ip.IPG_FITS_FP64)
     I0, Q0, U0, V0 = (float(out[k].sum()) for k in "IQUV")
     I1, Q1, U1, V1 = (float(mo[k].sum()) for k in "IQUV")
     bright = out["I"] > 1e-6 * out["I"].max()
     mixed = {"value": images_per_s(world, args.steps, mixed_ms), "unit": "images/s",
              "ms_per_step": mixed_ms / args.steps,
-             "form": "compact step records (transport matrices and tetrad rows in FP32) and the polarized "
-                     "step (Faraday rotation, absorption/emission) in FP32; geodesics, metric, tetrads, jar "
-                     "fits and the accumulation of N in FP64",
+             "form": "compact step records (transport matrices and tetrad rows in FP32), the polarized "
+                     "step (Faraday rotation, absorption/emission) in FP32 and the thermal fits' shapes in FP32 "
+                     "(prefactors and exponents FP64); geodesics, metric, tetrads and the accumulation of N in "
+                     "FP64",
              "vs_fp64": {"Ftot_rel": abs(I1 / I0 - 1), "Q_rel_to_I": abs(Q1 - Q0) / abs(I0),
                          "U_rel_to_I": abs(U1 - U0) / abs(I0), "V_rel_to_I": abs(V1 - V0) / abs(I0),
                          "EVPA_deg": abs(float(np.degrees(0.5 * (np.arctan2(U1, Q1) - np.arctan2(U0, Q0))))),
@@ -369,24 +386,43 @@ def run_ours(args):
     ctx.upload(model)
 
     peak = ip.fp64_peak_tflops(local, 300.0)
-    dom = max(kms, key=kms.get)
-    fps = FLOPS_PER_STEP[dom]
-    achieved = (fps * steps / (kms[dom] / 1e3) / 1e12) if fps else None
-    # launches of each main kernel per image: one per length class (a split
-    # wave adds 4 launches for the prediction and sort)
-    launches_dom = max(1, round((launches / args.steps - (4 if pred_ms > 0 else 0)) / 3))
-    traffic = DRAM_BYTES_PER_STEP[dom] * (steps / args.steps) / launches_dom
+    peak32 = ip.fp32_peak_tflops(local, 300.0)
+    # algorithmic flops (the reference algorithm's counted work) of each
+    # kernel over the timed images, against each kernel's wall span (first
+    # class start to last class end, per wave) and the whole pipeline against
+    # the image time
+    alg = {"geodesic": (REF_FLOPS["geodesic_per_step"] + REF_FLOPS["push_per_step"]) * steps,
+           "coeffs": REF_FLOPS["coeffs_per_radiating_step"] * rad,
+           "transfer": REF_FLOPS["transfer_per_radiating_step"] * rad}
+    dom = max(span, key=span.get)
+    kern = {k: {"span_ms_per_image": span[k] / args.steps, "summed_class_ms_per_image": kms[k] / args.steps,
+                "alg_tflops": alg[k] / (span[k] / 1e3) / 1e12 if span[k] > 0 else None,
+                "exec_tflops": EXEC_FLOPS_PER_STEP[k] * steps / (span[k] / 1e3) / 1e12 if span[k] > 0 else None}
+            for k in kms}
+    for k in kern:
+        a, x = kern[k]["alg_tflops"], kern[k]["exec_tflops"]
+        kern[k]["alg_frac"] = a / peak if a else None
+        kern[k]["exec_frac"] = x / peak if x else None
+    achieved = kern[dom]["alg_tflops"]
+    alg_total = sum(alg.values())
+    exec_total = sum(EXEC_FLOPS_PER_STEP.values()) * steps
+    traffic = DRAM_BYTES_PER_STEP[dom] * (steps / args.steps)
     roofline = {"bound": "fp64", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "traffic_note": "DRAM bytes per launch: ncu bytes per ray-step of the 200x200 small case "
-                                "times this image's ray-steps per launch",
-                "hbm_GBps_of_dominant": DRAM_BYTES_PER_STEP[dom] * steps / (kms[dom] / 1e3) / 1e9,
+                "traffic_note": "DRAM bytes per image (all class launches of the kernel): ncu bytes per ray-step "
+                                "of the 200x200 small case times this image's ray-steps",
+                "frac_pipeline": alg_total / (ms / 1e3) / 1e12 / peak,
+                "frac_pipeline_executed": exec_total / (ms / 1e3) / 1e12 / peak,
+                "alg_flops_per_ray_step": alg_total / max(steps, 1),
+                "exec_flops_per_ray_step": exec_total / max(steps, 1),
+                "alg_note": "algorithmic = the reference algorithm's FP64 operations counted with a counting "
+                            "number type (transcendentals 20 flops); the kernels execute ~15x fewer (analytic "
+                            "connection and metric instead of finite differences of gcov with LU inversions), "
+                            "so the algorithmic fractions can exceed 1; *_executed uses ncu's executed FP64 flops",
+                "kernels": kern, "hbm_GBps_of_dominant": traffic * args.steps / (span[dom] / 1e3) / 1e9,
                 "peak_source": "measured in this run: FP64 FMA loop (ipg_measure_fp64_peak); MEASURED_PEAKS.json "
                                "has no FP64 figure",
-                "flops_per_ray_step": fps, "kernel_ms_per_image": kms[dom] / args.steps,
-                **{f"{k}_ms_per_image": v / args.steps for k, v in kms.items()},
-                "predict_ms_per_image": pred_ms / args.steps,
-                "note": "per-kernel times are summed over the concurrent length classes of an image"}
+                "fp32_peak_tflops": peak32, "predict_ms_per_image": pred_ms / args.steps}
     line = {"metric": METRIC, "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -444,15 +480,17 @@ def batch_params(ip, dump, m_unit, nx, incl=163, freq=230e9, refine=False):
 
 
 def bench_batched(ip, ctx, model, dump, args, world, stream, single_ms):
-    """images/s of the batched forms, FP64 and with the FP32 polarized step,
-    beside the single-image FP64 rate of this run"""
+    """images/s of the batched forms: FP64, with the FP32 polarized step, and
+    the mixed tier (FP32 step and FP32 fit shapes), beside the single-image
+    FP64 rate of this run"""
     import torch
     nx = args.size
     ctx.upload_batch(model)
     res = {}
     ps = batch_params(ip, dump, args.m_unit, nx)
-    for name, step32 in (("fp64", False), ("fp32_step", True)):
+    for name, step32, fits32 in (("fp64", False, False), ("fp32_step", True, False), ("mixed", True, True)):
         ctx.set_step_precision(ip.IPG_STEP_FP32 if step32 else ip.IPG_STEP_FP64)
+        ctx.set_fit_precision(ip.IPG_FITS_FP32 if fits32 else ip.IPG_FITS_FP64)
         ctx.render_batch(ps, model)
         torch.cuda.synchronize()
         barrier(world)
@@ -479,6 +517,7 @@ def bench_batched(ip, ctx, model, dump, args, world, stream, single_ms):
         else:
             fp64_imgs = imgs
     ctx.set_step_precision(ip.IPG_STEP_FP64)
+    ctx.set_fit_precision(ip.IPG_FITS_FP64)
     res["workload"] = (f"{len(ps)} instances of the bench image's camera ({nx}x{nx}, 230 GHz, thetacam 163): "
                        f"R_high {list(BATCH_RHIGH)} x M_unit {list(BATCH_MU)} x {args.m_unit:g}")
     if args.size == NX and not args.small:

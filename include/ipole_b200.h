@@ -340,6 +340,12 @@ typedef struct ipg_stats {
   double coeffs_ms;
   double predict_ms;
   double wall_ms;
+  /* each kernel's wall time per wave: from the first length class's start
+   * of that kernel to the last class's end (the *_ms above sum the classes'
+   * concurrent launches) */
+  double geodesic_span_ms;
+  double coeffs_span_ms;
+  double transfer_span_ms;
 } ipg_stats;
 int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 
@@ -368,6 +374,29 @@ int ipg_set_record_precision(ipg_ctx *ctx, int precision);
 #define IPG_STEP_FP32 1
 int ipg_set_step_precision(ipg_ctx *ctx, int precision);
 
+/* Arithmetic of the thermal synchrotron fits (no counterpart in the
+ * reference).  IPG_FITS_FP64 (the default) evaluates get_jkinv and jar_calc
+ * (src/model_radiation.c:145-332) in FP64.  IPG_FITS_FP32 evaluates the
+ * shape of each fit (its transcendental functions and the Bessel functions
+ * K_n(1/Theta_e), kept as mantissa and exponent) in FP32 and the
+ * prefactors and exponents in FP64, so that no coefficient leaves FP32's
+ * range; the coefficients keep FP64 storage.  Applies to ipg_render_* and
+ * ipg_render_batch; ipg_trace_ray, ipg_trace_pixels_noalloc and ipg_adjoint
+ * always use the FP64 fits.  The test of this mode states its errors.
+ * Returns IPG_E_ARG for another value. */
+#define IPG_FITS_FP64 0
+#define IPG_FITS_FP32 1
+int ipg_set_fit_precision(ipg_ctx *ctx, int precision);
+
+/* The thermal fits at given plasma parameters (the fits of jar_calc,
+ * src/model_radiation.c:182-332, for emission_type 4 or 1, without the
+ * model lookup): in[5n] = (nu, Ne, Thetae, B, theta) per point, host memory;
+ * out[12n] = (j_I/nu^2 and a_I of get_jkinv, then jI jQ jU jV aI aQ aU aV rQ
+ * rV of jar_calc) per point, zeros where Ne <= 0.  precision is
+ * IPG_FITS_FP64 or IPG_FITS_FP32 (the kernels' two forms). */
+int ipg_thermal_coefficients(ipg_ctx *ctx, const double *in, size_t n, int emission_type, int precision,
+                             double *out);
+
 /* The context's CUDA stream (a cudaStream_t), on which every kernel of the
  * context is launched; lets a caller bracket calls with its own events. */
 int ipg_get_stream(const ipg_ctx *ctx, void **stream);
@@ -387,6 +416,8 @@ int ipg_camera_setup(const ipg_grid *grid, double rcam, double thetacam_deg, dou
 /* Peak FP64 FMA throughput of the device in TFLOP/s (2 flops per FMA),
  * measured with a register-resident FMA loop for `ms` milliseconds. */
 int ipg_measure_fp64_peak(int device, double ms, double *tflops);
+/* The same probe with FP32 FMA chains: the FP32 CUDA-core peak. */
+int ipg_measure_fp32_peak(int device, double ms, double *tflops);
 
 #ifdef __cplusplus
 }

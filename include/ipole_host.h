@@ -73,6 +73,10 @@ typedef struct ipg_params {
   /* "fp32_step" (no reference counterpart): 1 evaluates the polarized step
    * in FP32 (ipg_set_step_precision, IPG_STEP_FP32); 0, the default, FP64 */
   int fp32_step;
+  /* "fp32_fits" (no reference counterpart): 1 evaluates the thermal fits
+   * with FP32 shapes (ipg_set_fit_precision, IPG_FITS_FP32); 0, the default,
+   * FP64 */
+  int fp32_fits;
 } ipg_params;
 
 /* Defaults of load_par_from_argv (src/par.c:48-100) and the model/radiation

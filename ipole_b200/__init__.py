@@ -25,7 +25,8 @@ import numpy as np
 from . import build as _build
 
 __all__ = ["lib", "Params", "Model", "Context", "Image", "Camera", "PixelOut", "Grid", "IpgError",
-           "PIXEL_DTYPE", "trace_pixels", "fp64_peak_tflops", "convert_container"]
+           "PIXEL_DTYPE", "trace_pixels", "fp64_peak_tflops", "fp32_peak_tflops",
+           "convert_container"]
 
 IPG_OK, IPG_E_ARG, IPG_E_CUDA, IPG_E_MAXNSTEP, IPG_E_NAN, IPG_E_TIMEOUT, IPG_E_NOMEM, IPG_E_IO, IPG_E_STATE, \
     IPG_E_FORMAT = range(10)
@@ -35,6 +36,8 @@ STRLEN = 2048
 IPG_RECORDS_FP64, IPG_RECORDS_MIXED = 0, 1
 # arithmetic of the polarized step (ipg_set_step_precision)
 IPG_STEP_FP64, IPG_STEP_FP32 = 0, 1
+# arithmetic of the thermal fits (ipg_set_fit_precision)
+IPG_FITS_FP64, IPG_FITS_FP32 = 0, 1
 # per-step trace columns (include/ipole_b200.h, IPG_TRACE_*)
 TRACE_DOUBLES = 127
 TRACE_COLS = {"b": (0, 1), "ne": (1, 1), "thetae": (2, 1), "nu": (3, 1), "b_k_angle": (4, 1), "sigma": (5, 1),
@@ -88,7 +91,8 @@ assert PIXEL_DTYPE.itemsize == C.sizeof(PixelOut)
 class Stats(C.Structure):
     _fields_ = [("ray_steps", C.c_uint64), ("radiating_steps", C.c_uint64), ("launches", C.c_int32),
                 ("waves", C.c_int32), ("geodesic_ms", C.c_double), ("transfer_ms", C.c_double),
-                ("coeffs_ms", C.c_double), ("predict_ms", C.c_double), ("wall_ms", C.c_double)]
+                ("coeffs_ms", C.c_double), ("predict_ms", C.c_double), ("wall_ms", C.c_double),
+                ("geodesic_span_ms", C.c_double), ("coeffs_span_ms", C.c_double), ("transfer_span_ms", C.c_double)]
 
 
 class _Params(C.Structure):
@@ -122,7 +126,7 @@ class _Params(C.Structure):
                 ("plugin", C.c_char * STRLEN), ("MBH_set", C.c_int), ("analytic_model", C.c_int),
                 ("rho_unit", C.c_double), ("sphere_Thetae0", C.c_double), ("sphere_R0", C.c_double),
                 ("sphere_tau0", C.c_double), ("sphere_beta0", C.c_double), ("sphere_gam", C.c_double),
-                ("mixed_records", C.c_int), ("fp32_step", C.c_int)]
+                ("mixed_records", C.c_int), ("fp32_step", C.c_int), ("fp32_fits", C.c_int)]
 
 
 class Plugin(C.Structure):
@@ -198,11 +202,14 @@ def lib():
     L.ipg_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.ipg_set_record_precision.argtypes = [C.c_void_p, C.c_int]
     L.ipg_set_step_precision.argtypes = [C.c_void_p, C.c_int]
+    L.ipg_set_fit_precision.argtypes = [C.c_void_p, C.c_int]
+    L.ipg_thermal_coefficients.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p]
     L.ipg_camera_setup.argtypes = [C.POINTER(Grid)] + [C.c_double] * 9 + [C.c_int, C.c_int, C.c_double, C.c_int,
                                                                           C.POINTER(Camera), C.POINTER(C.c_double),
                                                                           C.POINTER(C.c_double),
                                                                           C.POINTER(C.c_double)]
     L.ipg_measure_fp64_peak.argtypes = [C.c_int, C.c_double, C.POINTER(C.c_double)]
+    L.ipg_measure_fp32_peak.argtypes = [C.c_int, C.c_double, C.POINTER(C.c_double)]
     L.ipg_params_default.argtypes = [C.POINTER(_Params)]
     L.ipg_params_default.restype = None
     L.ipg_params_set.argtypes = [C.POINTER(_Params), C.c_char_p, C.c_char_p]
@@ -440,6 +447,22 @@ class Context:
         FP32)."""
         _check(lib().ipg_set_step_precision(self._h, int(precision)), self._h)
 
+    def set_fit_precision(self, precision: int):
+        """ipg_set_fit_precision: IPG_FITS_FP64 (default) or IPG_FITS_FP32
+        (the thermal fits' shapes in FP32, prefactors and exponents in
+        FP64)."""
+        _check(lib().ipg_set_fit_precision(self._h, int(precision)), self._h)
+
+    def thermal_coefficients(self, points, emission_type: int = 4, precision: int = IPG_FITS_FP64):
+        """ipg_thermal_coefficients: points (n, 5) = (nu, Ne, Thetae, B,
+        theta) -> (n, 12) = (jI/nu^2, aI of get_jkinv; jI jQ jU jV aI aQ aU
+        aV rQ rV of jar_calc)."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 5)
+        out = np.zeros((len(pts), 12))
+        _check(lib().ipg_thermal_coefficients(self._h, pts.ctypes.data, len(pts), int(emission_type),
+                                              int(precision), out.ctypes.data), self._h)
+        return out
+
     def stream(self) -> int:
         """The context's cudaStream_t as an integer handle."""
         s = C.c_void_p()
@@ -574,4 +597,10 @@ def convert_container(src: str, dst: str) -> None:
 def fp64_peak_tflops(device: int = 0, ms: float = 200.0) -> float:
     v = C.c_double()
     _check(lib().ipg_measure_fp64_peak(int(device), float(ms), C.byref(v)))
+    return v.value
+
+
+def fp32_peak_tflops(device: int = 0, ms: float = 200.0) -> float:
+    v = C.c_double()
+    _check(lib().ipg_measure_fp32_peak(int(device), float(ms), C.byref(v)))
     return v.value

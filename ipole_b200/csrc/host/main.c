@@ -54,6 +54,7 @@ int main(int argc, char *argv[])
   }
   if (p.mixed_records) rc = ipg_set_record_precision(ctx, IPG_RECORDS_MIXED);
   if (!rc && p.fp32_step) rc = ipg_set_step_precision(ctx, IPG_STEP_FP32);
+  if (!rc && p.fp32_fits) rc = ipg_set_fit_precision(ctx, IPG_FITS_FP32);
   if (!rc) rc = ipg_upload_model(ctx, &m);
   if (rc) {
     fprintf(stderr, "model upload failed: %s (%s)\n", ipg_strerror(rc), ipg_last_error(ctx));

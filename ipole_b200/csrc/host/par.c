@@ -208,6 +208,7 @@ void ipg_params_set(ipg_params *p, const char *word, const char *value)
   set_by_word_val(word, value, "trace_outf", p->trace_outf, TYPE_STR);
   set_by_word_val(word, value, "mixed_records", &p->mixed_records, TYPE_INT);
   set_by_word_val(word, value, "fp32_step", &p->fp32_step, TYPE_INT);
+  set_by_word_val(word, value, "fp32_fits", &p->fp32_fits, TYPE_INT);
   set_by_word_val(word, value, "histo", &p->histo, TYPE_INT);
   set_by_word_val(word, value, "histo_polar", &p->histo_polar, TYPE_INT);
   set_by_word_val(word, value, "histo_outf", p->histo_outf, TYPE_STR);

@@ -148,7 +148,7 @@ __global__ void k_derive(const double *__restrict__ rho, const double *__restric
  * shared part goes into the record in place (flags, tetrad rows; dl and
  * nturns keep their slots), the instances' coefficients into their blocks
  * of the side pool: side[((chunk * 32 + slot) * G + k) * IPG_BCOEF]. */
-template <int EM>
+template <int EM, bool F32 = false>
 __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     k_coef_batch(double *__restrict__ pool, double *__restrict__ side, int G, const int2 *__restrict__ chunk_meta,
                  const unsigned long long *__restrict__ counters, long long n_chunks, const RayRec *__restrict__ rays,
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
       }
       double ju = 0., ku = 0.;
       Jar jar;
-      coeffs_t<IPG_PLUG_IHARM>(mp, K, want_pol, EM, &ju, &ku, &jar);
+      coeffs_t<IPG_PLUG_IHARM, F32>(mp, K, want_pol, EM, &ju, &ku, &jar);
       double2 *q2 = reinterpret_cast<double2 *>(q0 + (size_t)k * IPG_BCOEF);
       q2[0] = make_double2(ju, ku);
       q2[1] = make_double2(jar.jI, jar.jQ);
@@ -461,6 +461,12 @@ struct BatchState {
   int G; /* instance slots per group of the current batch */
   int emission_type, step32, unpol;
   int xfer_threads; /* transfer block size (128 or 256) */
+  /* the transfer block size is tuned per batch shape (slots per group,
+   * groups): the first call of a shape runs 128 threads, the second 256,
+   * and later calls keep the one whose transfer took less time per
+   * transfer item (the images do not depend on it: one lane per item) */
+  int tune_G, tune_ngrp, tune_calls;
+  double tune_ms[2], tune_items[2], call_xfer_ms, call_items;
 };
 
 static void batch_ws_free(BatchWs *w)
@@ -604,7 +610,25 @@ extern "C" int ipg__batch_begin(ipg_ctx *ctx, const ipg_camera *grp_cam, int ngr
   B->emission_type = em;
   B->unpol = unpol;
   B->step32 = step32;
-  if (!B->xfer_threads) B->xfer_threads = 128;
+  /* block-size tuning: close the previous call's sample, pick this call's */
+  if (B->tune_calls > 0 && B->tune_calls <= 2 && B->call_items > 0) {
+    B->tune_ms[B->tune_calls - 1] = B->call_xfer_ms;
+    B->tune_items[B->tune_calls - 1] = B->call_items;
+  }
+  if (G != B->tune_G || ngrp != B->tune_ngrp) {
+    B->tune_G = G;
+    B->tune_ngrp = ngrp;
+    B->tune_calls = 0;
+  }
+  if (B->tune_calls < 2) {
+    B->xfer_threads = B->tune_calls == 0 ? 128 : 256;
+  } else if (B->tune_calls == 2) {
+    const double r128 = B->tune_ms[0] / fmax(B->tune_items[0], 1.), r256 = B->tune_ms[1] / fmax(B->tune_items[1], 1.);
+    B->xfer_threads = r256 < r128 ? 256 : 128;
+  }
+  if (B->tune_calls <= 2) B->tune_calls++;
+  B->call_xfer_ms = 0.;
+  B->call_items = 0.;
   memset(&ctx->stats, 0, sizeof(ctx->stats));
   return IPG_OK;
 }
@@ -691,15 +715,25 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
         it->geo_grp);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], st));
+#define IPG_LAUNCH_BCOEF(EMT, F)                                                                              \
+  do {                                                                                                       \
+    int cb = grid_blocks(ctx, (const void *)k_coef_batch<EMT, F>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS); \
+    k_coef_batch<EMT, F><<<cb, threads, 0, st>>>(pool, side, G, ctx->d_chunk_meta, W.cnt, n_chunks, W.rays,  \
+                                                 it->geo_grp, it->geo_mask, B->m.fourv, B->m.sets,          \
+                                                 (long long)B->m.ncell);                                      \
+  } while (0)
     if (B->emission_type == 1) {
-      int cb = grid_blocks(ctx, (const void *)k_coef_batch<1>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
-      k_coef_batch<1><<<cb, threads, 0, st>>>(pool, side, G, ctx->d_chunk_meta, W.cnt, n_chunks, W.rays, it->geo_grp,
-                                              it->geo_mask, B->m.fourv, B->m.sets, (long long)B->m.ncell);
+      if (ctx->fits32)
+        IPG_LAUNCH_BCOEF(1, true);
+      else
+        IPG_LAUNCH_BCOEF(1, false);
     } else {
-      int cb = grid_blocks(ctx, (const void *)k_coef_batch<4>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
-      k_coef_batch<4><<<cb, threads, 0, st>>>(pool, side, G, ctx->d_chunk_meta, W.cnt, n_chunks, W.rays, it->geo_grp,
-                                              it->geo_mask, B->m.fourv, B->m.sets, (long long)B->m.ncell);
+      if (ctx->fits32)
+        IPG_LAUNCH_BCOEF(4, true);
+      else
+        IPG_LAUNCH_BCOEF(4, false);
     }
+#undef IPG_LAUNCH_BCOEF
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[2], st));
     if (B->step32) {
@@ -722,6 +756,8 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
     ctx->stats.coeffs_ms += b;
     ctx->stats.transfer_ms += c;
     ctx->stats.wall_ms += a + b + c;
+    B->call_xfer_ms += c;
+    B->call_items += (double)pend_x;
     ctx->stats.ray_steps += h[CNT_STEPS];
     ctx->stats.radiating_steps += h[CNT_RAD];
     ctx->stats.launches += 3;

@@ -31,6 +31,7 @@ void **ipg__refine_slot(ipg_ctx *ctx);
 
 /* the step arithmetic of the context (ipg_set_step_precision): 1 for FP32 */
 int ipg__step32(const ipg_ctx *ctx);
+int ipg__fits32(const ipg_ctx *ctx);
 /* per-context storage of the batch driver (ipg_refine.cu); ipg_destroy
  * releases it with ipg__batch_arena_release */
 void **ipg__batch_arena_slot(ipg_ctx *ctx);

@@ -34,9 +34,11 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "ipg_device.cuh"
+#include "ipg_fits_f32.cuh"
 #include "ipg_internal.h"
 #include "ipg_plugins.cuh"
 #include "ipole_b200.h"
@@ -583,9 +585,10 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
  * record also leaves an adjoint block of IPG_ADJ_DOUBLES in adj_side:
  * X1 X2 X3, the fluid frequency, sin and cos of the k-B angle, the angle,
  * and (along | in_domain << 1), from which the adjoint re-evaluates the fits
- * with their derivatives. */
+ * with their derivatives.  F32: the thermal fits with FP32 shapes
+ * (jar_both_f32). */
 #define IPG_ADJ_DOUBLES 8
-template <int P, int EM = 0, bool ADJ = false>
+template <int P, int EM = 0, bool ADJ = false, bool F32 = false>
 __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     k_coeffs(double *__restrict__ pool, const int2 *__restrict__ chunk_meta,
              const unsigned long long *__restrict__ counters, long long n_chunks,
@@ -629,7 +632,7 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
       ModelPt mp;
       model_point_t<P>(fields, X1, X2, X3, pg, &mp);
       int want_pol = pol && (flags & 1);
-      coeffs_t<P>(mp, K, want_pol, EM ? EM : C.emission_type, &ju, &ku, &jar);
+      coeffs_t<P, F32>(mp, K, want_pol, EM ? EM : C.emission_type, &ju, &ku, &jar);
       if constexpr (ADJ) {
         JarGeo jg;
         jar_geo(mp, K, EM ? EM : C.emission_type, &jg);
@@ -1277,13 +1280,15 @@ __global__ void k_len_scatter(const int32_t *__restrict__ list, const int32_t *_
 }
 
 /* ===================================================================== */
-/* FP64 peak probe                                                        */
+/* FP64 / FP32 peak probes                                                */
 /* ===================================================================== */
-__global__ void k_fma_peak(double *out, int iters, double seed)
+/* 8 independent FMA chains per thread, 16 x 8 FMAs per iteration */
+template <class T>
+__global__ void k_fma_peak(T *out, int iters, T seed)
 {
-  double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
-         a7 = a0 + 7;
-  const double m = 0.999999, c = 1e-7;
+  T a0 = seed + (T)threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+    a7 = a0 + 7;
+  const T m = (T)0.999999, c = (T)1e-7;
   for (int i = 0; i < iters; i++) {
 #pragma unroll
     for (int u = 0; u < 16; u++) {
@@ -1291,8 +1296,8 @@ __global__ void k_fma_peak(double *out, int iters, double seed)
       a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
     }
   }
-  double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
-  if (s == 12345.678) out[0] = s;
+  T s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == (T)12345.678) out[0] = s;
 }
 
 /* ===================================================================== */
@@ -1345,6 +1350,7 @@ struct ipg_ctx {
   int emission_type; /* of the camera being traced */
   int rec_mixed;     /* IPG_RECORDS_MIXED: compact step records */
   int step32;        /* IPG_STEP_FP32: the polarized step in FP32 */
+  int fits32;        /* IPG_FITS_FP32: the thermal fits with FP32 shapes */
   int32_t *d_ij;
   ipg_pixel_out *d_out;
   size_t cap;
@@ -1712,16 +1718,26 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
    * family the camera selects (Dexter, type 4, or Pandya, type 1): 88.6 KB
    * of code for iharm with Dexter's fits instead of 99.7 KB, and a 400x400
    * image 1% faster, since instruction fetch is this kernel's largest stall */
+#define IPG_LAUNCH_COEF(EMT, F)                                                                                 \
+  do {                                                                                                         \
+    int cb = grid_blocks(ctx, (const void *)k_coeffs<P, EMT, false, F>, threads,                              \
+                         (size_t)b.n_chunks * IPG_CHUNK_STEPS);                                                \
+    k_coeffs<P, EMT, false, F><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks,         \
+                                                             ctx->d_rays, ctx->d_fields, nullptr);             \
+  } while (0)
   if constexpr (P != IPG_PLUG_ANALYTIC && IPG_COEF_EM_SPECIALIZE) {
     if (ctx->emission_type == 1) {
-      int cb = grid_blocks(ctx, (const void *)k_coeffs<P, 1>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
-      k_coeffs<P, 1><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays,
-                                                   ctx->d_fields, nullptr);
+      if (ctx->fits32)
+        IPG_LAUNCH_COEF(1, true);
+      else
+        IPG_LAUNCH_COEF(1, false);
     } else {
-      int cb = grid_blocks(ctx, (const void *)k_coeffs<P, 4>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
-      k_coeffs<P, 4><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays,
-                                                   ctx->d_fields, nullptr);
+      if (ctx->fits32)
+        IPG_LAUNCH_COEF(4, true);
+      else
+        IPG_LAUNCH_COEF(4, false);
     }
+#undef IPG_LAUNCH_COEF
   } else {
     int cb = grid_blocks(ctx, (const void *)k_coeffs<P>, threads, (size_t)b.n_chunks * IPG_CHUNK_STEPS);
     k_coeffs<P><<<cb, threads, 0, b.stream>>>(b.pool, b.chunk_meta, b.cnt, b.n_chunks, ctx->d_rays, ctx->d_fields,
@@ -1961,12 +1977,26 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
       float pms = 0.f, wms = 0.f;
       cudaEventElapsedTime(&pms, ctx->ev_pred[0], ctx->ev_pred[1]);
       ctx->stats.predict_ms += pms;
+      /* each kernel's wall span over the concurrent classes: first start
+       * to last end, from the fork */
+      float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {0.f, 0.f, 0.f};
       for (int b = 0; b < nb; b++) {
         float w = 0.f;
         cudaEventElapsedTime(&w, ctx->ev_fork, ctx->ev_join[b]);
         if (w > wms) wms = w;
         add_batch_stats(ctx, bt[b].ev, cnt + b * CNT_N);
+        const int st[3] = {0, 4, 2}, en[3] = {1, 2, 3};
+        for (int k = 0; k < 3; k++) {
+          float t0 = 0.f, t1 = 0.f;
+          cudaEventElapsedTime(&t0, ctx->ev_fork, bt[b].ev[st[k]]);
+          cudaEventElapsedTime(&t1, ctx->ev_fork, bt[b].ev[en[k]]);
+          lo[k] = fminf(lo[k], t0);
+          hi[k] = fmaxf(hi[k], t1);
+        }
       }
+      ctx->stats.geodesic_span_ms += hi[0] - lo[0];
+      ctx->stats.coeffs_span_ms += hi[1] - lo[1];
+      ctx->stats.transfer_span_ms += hi[2] - lo[2];
       ctx->stats.wall_ms += wms + pms;
       ctx->stats.waves += 1;
 #ifdef IPG_DEBUG_TIMING
@@ -2018,6 +2048,15 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
       cudaEventElapsedTime(&wms, ctx->ev[0], ctx->ev[3]);
       ctx->stats.wall_ms += wms;
       add_batch_stats(ctx, ctx->ev, cnt);
+      {
+        float a = 0, b2 = 0, c = 0;
+        cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&b2, ctx->ev[4], ctx->ev[2]);
+        cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]);
+        ctx->stats.geodesic_span_ms += a;
+        ctx->stats.coeffs_span_ms += b2;
+        ctx->stats.transfer_span_ms += c;
+      }
       ctx->stats.waves += 1;
       deferred = (size_t)cnt[CNT_DEFER];
       if (deferred == pending) {
@@ -2047,6 +2086,7 @@ extern "C" void ipg__set_error(ipg_ctx *ctx, const char *msg) { snprintf(ctx->er
 extern "C" void **ipg__refine_slot(ipg_ctx *ctx) { return &ctx->refine; }
 extern "C" void **ipg__batch_arena_slot(ipg_ctx *ctx) { return &ctx->batch_arena; }
 extern "C" int ipg__step32(const ipg_ctx *ctx) { return ctx->step32; }
+extern "C" int ipg__fits32(const ipg_ctx *ctx) { return ctx->fits32; }
 
 extern "C" int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n,
                                        ipg_pixel_out *d_out, void *stream)
@@ -2111,6 +2151,74 @@ extern "C" int ipg_set_step_precision(ipg_ctx *ctx, int precision)
   return IPG_OK;
 }
 
+extern "C" int ipg_set_fit_precision(ipg_ctx *ctx, int precision)
+{
+  if (!ctx || (precision != IPG_FITS_FP64 && precision != IPG_FITS_FP32)) return IPG_E_ARG;
+  ctx->fits32 = precision == IPG_FITS_FP32;
+  return IPG_OK;
+}
+
+/* The fits at given plasma parameters, one thread per point: the geometry
+ * of jar_geo from the angle itself (sin and cos of theta; along the field
+ * for theta <= 0 or >= pi, as get_bk_angle's callers test it) */
+template <bool F32>
+__global__ void k_thermal_coefficients(const double *__restrict__ in, long long n, int emission_type,
+                                       double *__restrict__ out)
+{
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double *q = in + 5 * i;
+    double *o = out + 12 * i;
+    double ju = 0., ku = 0.;
+    Jar jr = {0., 0., 0., 0., 0., 0., 0., 0., 0., 0., 0.};
+    if (q[1] > 0.) {
+      JarGeo jg;
+      jg.nu = q[0];
+      jg.inusq = 1. / (q[0] * q[0]);
+      jg.theta = q[4];
+      jg.along = (q[4] <= 0. || q[4] >= IPG_PI);
+      sincos(q[4], &jg.sth, &jg.cth);
+      if constexpr (F32)
+        jar_fits_f32(q[1], q[2], q[3], jg, 1, emission_type, &ju, &ku, &jr);
+      else
+        jar_fits(q[1], q[2], q[3], jg, 1, emission_type, &ju, &ku, &jr);
+    }
+    const double v[12] = {ju, ku, jr.jI, jr.jQ, jr.jU, jr.jV, jr.aI, jr.aQ, jr.aU, jr.aV, jr.rQ, jr.rV};
+#pragma unroll
+    for (int k = 0; k < 12; k++) o[k] = v[k];
+  }
+}
+
+extern "C" int ipg_thermal_coefficients(ipg_ctx *ctx, const double *in, size_t n, int emission_type, int precision,
+                                        double *out)
+{
+  if (!ctx || (n && (!in || !out)) || (emission_type != 1 && emission_type != 4) ||
+      (precision != IPG_FITS_FP64 && precision != IPG_FITS_FP32))
+    return IPG_E_ARG;
+  if (!n) return IPG_OK;
+  CK(cudaSetDevice(ctx->device));
+  double *d = nullptr;
+  CK(cudaMalloc(&d, n * 17 * sizeof(double)));
+  int rc = IPG_OK;
+  cudaError_t e = cudaMemcpyAsync(d, in, n * 5 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    const int blocks = (int)std::min<size_t>((n + 127) / 128, (size_t)ctx->n_sm * 8);
+    if (precision == IPG_FITS_FP32)
+      k_thermal_coefficients<true><<<blocks, 128, 0, ctx->stream>>>(d, (long long)n, emission_type, d + n * 5);
+    else
+      k_thermal_coefficients<false><<<blocks, 128, 0, ctx->stream>>>(d, (long long)n, emission_type, d + n * 5);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, d + n * 5, n * 12 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    snprintf(ctx->err, sizeof(ctx->err), "%s", cudaGetErrorString(e));
+    rc = IPG_E_CUDA;
+  }
+  cudaFree(d);
+  return rc;
+}
+
 extern "C" int ipg_get_stream(const ipg_ctx *ctx, void **stream)
 {
   if (!ctx || !stream) return IPG_E_ARG;
@@ -2118,15 +2226,16 @@ extern "C" int ipg_get_stream(const ipg_ctx *ctx, void **stream)
   return IPG_OK;
 }
 
-extern "C" int ipg_measure_fp64_peak(int device, double ms, double *tflops)
+template <class T>
+static int measure_fma_peak(int device, double ms, double *tflops)
 {
   ipg_ctx *ctx = NULL;
   if (!tflops) return IPG_E_ARG;
   CK(cudaSetDevice(device));
   int nsm = 0;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-  double *d = NULL;
-  CK(cudaMalloc(&d, sizeof(double)));
+  T *d = NULL;
+  CK(cudaMalloc(&d, sizeof(T)));
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
@@ -2135,7 +2244,7 @@ extern "C" int ipg_measure_fp64_peak(int device, double ms, double *tflops)
   float t = 0;
   for (int rep = 0; rep < 12; rep++) {
     CK(cudaEventRecord(a));
-    k_fma_peak<<<blocks, threads>>>(d, iters, 1.0);
+    k_fma_peak<T><<<blocks, threads>>>(d, iters, (T)1);
     CK(cudaEventRecord(b));
     CK(cudaEventSynchronize(b));
     CK(cudaEventElapsedTime(&t, a, b));
@@ -2148,6 +2257,16 @@ extern "C" int ipg_measure_fp64_peak(int device, double ms, double *tflops)
   cudaEventDestroy(b);
   cudaFree(d);
   return IPG_OK;
+}
+
+extern "C" int ipg_measure_fp64_peak(int device, double ms, double *tflops)
+{
+  return measure_fma_peak<double>(device, ms, tflops);
+}
+
+extern "C" int ipg_measure_fp32_peak(int device, double ms, double *tflops)
+{
+  return measure_fma_peak<float>(device, ms, tflops);
 }
 
 /* ===================================================================== */

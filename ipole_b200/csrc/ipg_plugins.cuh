@@ -160,9 +160,9 @@ __device__ __forceinline__ void model_point_t(const double *__restrict__ fields,
 }
 
 /* get_jkinv and jar_calc at a point (src/model_radiation.c:104-169): the
- * thermal fits, or the model's own coefficients for emission_type 10
- * (E_CUSTOM), here those of model/analytic/model.c:204-240 */
-template <int P>
+ * thermal fits (with FP32 shapes when F32), or the model's own coefficients
+ * for emission_type 10 (E_CUSTOM), here those of model/analytic/model.c:204-240 */
+template <int P, bool F32 = false>
 __device__ __forceinline__ void coeffs_t(const ModelPt &mp, const double K[4], int want_pol, int emission_type,
                                          double *ju, double *ku, Jar *jr)
 {
@@ -183,6 +183,8 @@ __device__ __forceinline__ void coeffs_t(const ModelPt &mp, const double K[4], i
       jr->jI = j;
       jr->aI = k;
     }
+  } else if constexpr (F32) {
+    jar_both_f32(mp, K, want_pol, emission_type, ju, ku, jr);
   } else {
     jar_both(mp, K, want_pol, emission_type, ju, ku, jr);
   }

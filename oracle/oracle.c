@@ -715,6 +715,9 @@ static double rho_V(const fitp *p, int dexter)
   return 2. * S_PI * p->nu / S_CL * eps12;
 }
 
+static void jar_fits_at(const fitp *pp, int dist, int pol, double *jI, double *jQ, double *jU, double *jV,
+                        double *aI, double *aQ, double *aU, double *aV, double *rQ, double *rU, double *rV);
+
 /* jar_calc_dist, src/model_radiation.c:145-332 (thermal types 1, 4) */
 static void jar_calc_dist(const orc_model *m, int dist, int pol, const double X[NDIM], const double Kcon[NDIM],
                           double *jI, double *jQ, double *jU, double *jV, double *aI, double *aQ, double *aU,
@@ -730,9 +733,19 @@ static void jar_calc_dist(const orc_model *m, int dist, int pol, const double X[
   double Ucon[NDIM], Ucov[NDIM], Bcon[NDIM], Bcov[NDIM];
   get_model_fourv(m, X, Ucon, Ucov, Bcon, Bcov);
   double nu = get_fluid_nu(Kcon, Ucov);
-  double nusq = nu * nu;
   double theta = get_bk_angle(Kcon, Ucov, Bcon, Bcov);
   fitp p = {nu, get_model_b(m, X), Ne, theta, get_model_thetae(m, X)};
+  jar_fits_at(&p, dist, pol, jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV);
+}
+
+/* the thermal fits of jar_calc_dist at given (nu, B, Ne, theta, Thetae),
+ * Ne > 0: src/model_radiation.c:182-332 after the model lookup */
+static void jar_fits_at(const fitp *pp, int dist, int pol, double *jI, double *jQ, double *jU, double *jV,
+                        double *aI, double *aQ, double *aU, double *aV, double *rQ, double *rU, double *rV)
+{
+  fitp p = *pp;
+  double nu = p.nu, theta = p.theta;
+  double nusq = nu * nu;
   if (theta <= 0.0 || theta >= M_PI) {
     *jI = 0.0; *jQ = 0.0; *jU = 0.0; *jV = 0.0;
     *aI = 0.0; *aQ = 0.0; *aU = 0.0; *aV = 0.0;
@@ -789,6 +802,24 @@ static void get_jkinv(const orc_model *m, const orc_camera *c, const double X[ND
 {
   double a, b, d, e, f, g, h, q, r;
   jar_calc_dist(m, c->emission_type, 0, X, K, j, &a, &b, &d, k, &e, &f, &g, &h, &q, &r);
+}
+
+/* Both calls of jar_calc_dist at given plasma parameters: in = (nu, Ne,
+ * Thetae, B, theta) per point, out = (jI/nu^2 and aI of pol = 0, then jI jQ
+ * jU jV aI aQ aU aV rQ rV of pol = 1) per point; zeros where Ne <= 0. */
+void orc_thermal_coefficients(const double *in, int n, int dist, double *out)
+{
+  for (int i = 0; i < n; i++) {
+    const double *q = in + 5 * (size_t)i;
+    double *o = out + 12 * (size_t)i;
+    for (int k = 0; k < 12; k++) o[k] = 0.;
+    if (q[1] <= 0.) continue;
+    fitp p = {q[0], q[3], q[1], q[4], q[2]};
+    double a, b, d, e, f, g, h, r, t;
+    jar_fits_at(&p, dist, 0, &o[0], &a, &b, &d, &o[1], &e, &f, &g, &h, &r, &t);
+    double rU;
+    jar_fits_at(&p, dist, 1, &o[2], &o[3], &o[4], &o[5], &o[6], &o[7], &o[8], &o[9], &o[10], &rU, &o[11]);
+  }
 }
 
 /* ---------------- ipolarray.c ---------------- */

@@ -45,5 +45,9 @@ double orc_camera_setup(const orc_model *m, double rcam, double thetacam, double
                         double fov_muas, double dsource_pc, int nx, int ny, double freqcgs, orc_camera *c);
 /* sum of nstep over pixels from the last orc_trace_pixels call */
 long long orc_last_steps(void);
+/* the thermal fits of jar_calc_dist at given plasma parameters: in[5n] =
+ * (nu, Ne, Thetae, B, theta), out[12n] = (jI/nu^2 and aI of pol = 0, then
+ * jI jQ jU jV aI aQ aU aV rQ rV of pol = 1), zeros where Ne <= 0 */
+void orc_thermal_coefficients(const double *in, int n, int dist, double *out);
 
 #endif

@@ -69,8 +69,19 @@ def lib():
                                                                                    C.POINTER(OrcCamera)]
         L.orc_camera_setup.restype = C.c_double
         L.orc_last_steps.restype = C.c_longlong
+        L.orc_thermal_coefficients.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.orc_thermal_coefficients.restype = None
         _lib = L
     return _lib
+
+
+def thermal_coefficients(points, emission_type):
+    """orc_thermal_coefficients: points (n, 5) = (nu, Ne, Thetae, B, theta)
+    -> (n, 12) = (jI/nu^2, aI of pol = 0; jI jQ jU jV aI aQ aU aV rQ rV)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 5)
+    out = np.zeros((len(pts), 12))
+    lib().orc_thermal_coefficients(pts.ctypes.data, len(pts), int(emission_type), out.ctypes.data)
+    return out
 
 
 class Oracle:

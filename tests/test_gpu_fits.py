@@ -1,0 +1,98 @@
+"""The thermal fits at points on the GPU (ipg_thermal_coefficients).
+
+FP64 (the kernels' default form): against the coefficients the reference
+wrote in its per-step traces, and against the oracle's fits over a seeded
+sample of plasma parameters far wider than the flows' (both emission
+types).  FP32 shapes (IPG_FITS_FP32): the same points, with the error
+distribution printed.
+
+Errors are taken relative to the coefficient's own family at the point:
+|d - r| / (|r| + 1e-9 s), s = the magnitude of j_I (emissivities), a_I
+(absorptivities) or sqrt(rho_Q^2 + rho_V^2) (rotativities), so that a
+coefficient crossing zero (rho_Q's fit changes sign) is measured against
+the size of its family.
+"""
+import numpy as np
+import pytest
+
+import ipole_b200 as ip
+from oracle import oracle as O
+from tests import fits_points
+
+pytestmark = pytest.mark.gpu
+
+COL = fits_points.COLUMNS
+
+
+def family_scale(r):
+    s = np.zeros_like(r)
+    s[:, 0] = np.abs(r[:, 0])
+    s[:, 1] = np.abs(r[:, 1])
+    for k in (2, 3, 4, 5):
+        s[:, k] = np.abs(r[:, 2])
+    for k in (6, 7, 8, 9):
+        s[:, k] = np.abs(r[:, 6])
+    s[:, 10] = s[:, 11] = np.hypot(r[:, 10], r[:, 11])
+    return s
+
+
+def rel_err(d, r):
+    s = family_scale(r)
+    den = np.abs(r) + 1e-9 * s
+    e = np.where(den > 0, np.abs(d - r) / np.where(den > 0, den, 1.), np.where(d == r, 0., np.inf))
+    return e
+
+
+def summary(e):
+    return {COL[k]: f"{e[:, k].max():.1e}/{np.quantile(e[:, k], 0.999):.1e}" for k in range(12)}
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    with ip.Context() as c:
+        yield c
+
+
+def test_fp64_fits_against_reference_trace(ctx):
+    pts, ref = fits_points.trace_points()
+    d = ctx.thermal_coefficients(pts, 4, ip.IPG_FITS_FP64)
+    e = rel_err(d, ref)
+    print("fp64 vs reference trace (max/p99.9):", summary(e))
+    assert e.max() <= 1e-12
+
+
+@pytest.mark.parametrize("em", [4, 1])
+def test_fp64_fits_against_oracle_wide(ctx, em):
+    pts = fits_points.grid_points()
+    ref = O.thermal_coefficients(pts, em)
+    d = ctx.thermal_coefficients(pts, em, ip.IPG_FITS_FP64)
+    finite = np.isfinite(ref).all(1)
+    assert np.array_equal(np.isfinite(d).all(1), finite)
+    e = rel_err(d[finite], ref[finite])
+    print(f"fp64 vs oracle, emission {em} (max/p99.9):", summary(e))
+    assert e.max() <= 1e-10
+
+
+@pytest.mark.parametrize("em", [4, 1])
+def test_fp32_fits_error_distribution(ctx, em):
+    pts = np.concatenate([fits_points.trace_points()[0], fits_points.grid_points()])
+    ref = ctx.thermal_coefficients(pts, em, ip.IPG_FITS_FP64)
+    d = ctx.thermal_coefficients(pts, em, ip.IPG_FITS_FP32)
+    finite = np.isfinite(ref).all(1)
+    e = rel_err(d[finite], ref[finite])
+    print(f"fp32 vs fp64 fits, emission {em} (max/p99.9):", summary(e))
+    # the flows' own points (the traces) and the wide sample
+    ntr = len(fits_points.trace_points()[0])
+    print("  trace points max:", f"{e[:ntr].max():.2e}", " wide sample p99:", f"{np.quantile(e[ntr:], 0.99):.2e}")
+    assert np.quantile(e, 0.99) <= 1e-4
+    assert e[:ntr].max() <= 1e-4
+
+
+def test_fits_arguments(ctx):
+    with pytest.raises(ip.IpgError) as err:
+        ctx.thermal_coefficients(np.ones((1, 5)), 7)
+    assert err.value.code == ip.IPG_E_ARG
+    with pytest.raises(ip.IpgError) as err:
+        ctx.thermal_coefficients(np.ones((1, 5)), 4, 5)
+    assert err.value.code == ip.IPG_E_ARG
+    assert ctx.thermal_coefficients(np.zeros((0, 5))).shape == (0, 12)

@@ -102,3 +102,36 @@ def test_fp32_step_against_fp64(case, dumps):
         assert np.array_equal(img.nstep, full.nstep)
         bad = {k: v for k, v in e.items() if k in BOUNDS and not v <= BOUNDS[k]}
         assert not bad, (tag, bad)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fp32_fits_against_fp64(case, dumps):
+    """ipg_set_fit_precision(IPG_FITS_FP32): the thermal fits with FP32
+    shapes, alone and with the FP32 step and compact records (the whole
+    mixed tier), against the FP64 image and against the reference's golden
+    image."""
+    meta, arrs = common.load_golden(case)
+    p = common.params_for(meta, dumps.get(meta))
+    m = ip.Model.load(p)
+    with ip.Context() as c:
+        c.upload(m)
+        full = c.render(p, m)
+        c.set_fit_precision(ip.IPG_FITS_FP32)
+        fits = c.render(p, m)
+        c.set_step_precision(ip.IPG_STEP_FP32)
+        c.set_record_precision(ip.IPG_RECORDS_MIXED)
+        tier = c.render(p, m)
+        c.set_fit_precision(ip.IPG_FITS_FP64)
+        c.set_step_precision(ip.IPG_STEP_FP64)
+        c.set_record_precision(ip.IPG_RECORDS_FP64)
+        again = c.render(p, m)
+    assert again.unpol.tobytes() == full.unpol.tobytes()
+    ref = {"unpol": full.unpol, **({"pol": full.pol} if full.pol is not None else {})}
+    for tag, img in (("fp32 fits", fits), ("mixed tier", tier)):
+        e = common.image_errors(img, ref)
+        g = common.image_errors(img, arrs)
+        print(case, tag, "vs fp64:", {k: f"{v:.2e}" for k, v in e.items()})
+        print(case, tag, "vs reference:", {k: f"{v:.2e}" for k, v in g.items()})
+        assert np.array_equal(img.nstep, full.nstep)
+        bad = {k: v for k, v in e.items() if k in BOUNDS and not v <= BOUNDS[k]}
+        assert not bad, (tag, bad)
