@@ -31,6 +31,9 @@ __all__ = ["lib", "Params", "Model", "Context", "Image", "Camera", "PixelOut", "
 IPG_OK, IPG_E_ARG, IPG_E_CUDA, IPG_E_MAXNSTEP, IPG_E_NAN, IPG_E_TIMEOUT, IPG_E_NOMEM, IPG_E_IO, IPG_E_STATE, \
     IPG_E_FORMAT = range(10)
 NFIELD = 10
+# field order of ipg_upload_iharm (enum IPG_F_*)
+(IPG_F_U1, IPG_F_U2, IPG_F_U3, IPG_F_B1, IPG_F_B2, IPG_F_B3, IPG_F_NE, IPG_F_THETAE, IPG_F_B,
+ IPG_F_SIGMA) = range(NFIELD)
 STRLEN = 2048
 # step-record storage precision (ipg_set_record_precision)
 IPG_RECORDS_FP64, IPG_RECORDS_MIXED = 0, 1

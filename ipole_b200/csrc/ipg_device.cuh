@@ -931,7 +931,6 @@ __device__ __forceinline__ void rho_QV(R Ne, double nu, R Thetae, R B, double st
   double tpn = 2. * pi * nu;
   double itpn = 1. / tpn;
   R x = Thetae * sqrt(1.4142135623730951 * sth * (1.e3 * omega0 * itpn));
-  R ik2 = (k2 > 0.) ? 1. / k2 : NumT<R>::c(0.);
   if (want_q) {
     R lx = log(x);
     R l16 = (val(x) + 1.e-16 == val(x)) ? lx : log(x + 1.e-16);
@@ -940,7 +939,9 @@ __device__ __forceinline__ void rho_QV(R Ne, double nu, R Thetae, R B, double st
                   (0.5 + 0.5 * tanh((lx - 4.78749174278204599425) * 10.));
     R jffunc = 2.011 * exp(exp(1.035 * lx) * (-1. / 4.7)) - cos(0.5 * x) * exp(exp(1.2 * lx) * (-1. / 2.73)) -
                .011 * e472 + extraterm;
-    R k_ratio = (k2 > 0.) ? k1 * ik2 : NumT<R>::c(1.);
+    /* K1/K2 by division, as the reference: for Theta_e < 1/708 both are
+     * subnormal and a reciprocal of K2 overflows */
+    R k_ratio = (k2 > 0.) ? k1 / k2 : NumT<R>::c(1.);
     double itpn2 = itpn * itpn;
     R eps11m22 = jffunc * wp2 * (omega0 * omega0) * (itpn2 * itpn2) * (k_ratio + 6. * Thetae) * (sth * sth);
     *rQ = tpn * (0.5 / IPG_CL) * eps11m22 * nu;
@@ -948,9 +949,9 @@ __device__ __forceinline__ void rho_QV(R Ne, double nu, R Thetae, R B, double st
   R fit_factor;
   if (dexter_v && k2 > 0.) {
     R shgmfunc = 0.43793091 * log(1. + 0.00185777 * pow(x, 1.50316886));
-    fit_factor = (k0 - shgmfunc) * ik2;
+    fit_factor = (k0 - shgmfunc) / k2;
   } else {
-    R k_ratio = (k2 > 0.) ? k0 * ik2 : NumT<R>::c(1.);
+    R k_ratio = (k2 > 0.) ? k0 / k2 : NumT<R>::c(1.);
     R shgmfunc = 1 - 0.11 * log(1 + 0.035 * x);
     fit_factor = k_ratio * shgmfunc;
   }

@@ -188,8 +188,10 @@ __device__ __forceinline__ void jar_fits_f32(double Ne, double Thetae, double B,
       float f = sqrtf(X) + 1.8877486253633868f * sqrtf(cx); /* 2^(11/12) X^(1/6) */
       f = f * f;
       const double lnK2 = fmax(lnk2, -92.103403719761836); /* ln SMALL */
-      j = ((1.4142135623730951 * pi * IPG_EE * IPG_EE / (3. * IPG_CL)) * Ne * nus) * (double)f *
-          exp_split(-(double)cx - lnK2);
+      /* e^-X^(1/3) underflows to 0 in the FP64 fit beyond 745.13 */
+      if (cx <= 745.13f)
+        j = ((1.4142135623730951 * pi * IPG_EE * IPG_EE / (3. * IPG_CL)) * Ne * nus) * (double)f *
+            exp_split(-(double)cx - lnK2);
     }
     *ju = j * inusq;
     *ku = *ju * bnu;

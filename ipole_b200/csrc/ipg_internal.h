@@ -49,6 +49,7 @@ typedef struct ipg_batch_items {
   const int32_t *xf_geo;    /* [n_xf] geodesic item */
   const int32_t *xf_slot;   /* [n_xf] instance slot in its group */
   ipg_pixel_out *xf_out;    /* [n_xf] get_pixel's outputs */
+  const int32_t *xf_order;  /* [n_xf] the order in which the transfer takes the items (NULL: 0..n_xf-1) */
 } ipg_batch_items;
 /* trace one level; *steps_left (NULL: no budget) is the remaining step
  * budget, decreased by the steps taken */

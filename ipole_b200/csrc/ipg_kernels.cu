@@ -1149,8 +1149,11 @@ __device__ __forceinline__ void xfer_result(const DevCam &C, const Lane &L, int 
     hn_stokes(L.N, C.Ecov[1], C.Ecov[2], &T11, &T22, &T12r, &T21i);
     double Q = (T11 - T22) / 2, U = T12r;
     o->I = (T11 + T22) / 2;
-    o->Q = Q * C.cproj - U * C.sproj;
-    o->U = Q * C.sproj + U * C.cproj;
+    /* the rotation by -2 rotcam with its roundings spelled out, so that
+     * every kernel that inlines this (the image, the batch, the adjoint's
+     * forward pass) gives the same bits whatever it contracts */
+    o->Q = fma(Q, C.cproj, -__dmul_rn(U, C.sproj));
+    o->U = fma(Q, C.sproj, __dmul_rn(U, C.cproj));
     o->V = T21i;
   }
   o->nstep = nstep;

@@ -648,6 +648,34 @@ __global__ void k_xf_map(const int32_t *ij, int n, int nj, int nsx, int nsy, con
   xf_slot[m] = slot;
 }
 
+/* The transfer order: items grouped by geodesic item, by slot within it, so
+ * that the instances that trace one pixel sit in adjacent lanes and walk its
+ * records in step (one load of the shared record serves them all, and their
+ * coefficient blocks are contiguous).  cnt[g] = instances tracing item g;
+ * off = its exclusive scan; order[off[g] + rank of the slot] = item. */
+__global__ void k_geo_count(const uint32_t *mask, int n, int32_t *cnt)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) cnt[t] = __popc(mask[t]);
+}
+
+__global__ void __launch_bounds__(SCAN_TPB) k_geo_offsets(const int32_t *cnt, int n, const int32_t *block_sums,
+                                                          int32_t *off)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int e = block_exclusive_scan(t < n ? cnt[t] : 0, NULL);
+  if (t < n) off[t] = block_sums[blockIdx.x] + e;
+}
+
+__global__ void k_xf_order(const int32_t *xf_geo, const int32_t *xf_slot, const uint32_t *mask, const int32_t *off,
+                           int n, int32_t *order)
+{
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const int g = xf_geo[m], k = xf_slot[m];
+  order[off[g] + __popc(mask[g] & ((1u << k) - 1u))] = m;
+}
+
 namespace {
 /* bump allocation inside one device block (a first pass only sizes it) */
 struct Arena {
@@ -803,6 +831,8 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
   RefineStatus *st = nullptr, *gst = nullptr;
   int32_t *ij_all = nullptr, *xf_geo = nullptr, *xf_slot = nullptr, *geo_ij = nullptr, *geo_grp = nullptr;
   uint32_t *geo_mask = nullptr;
+  int32_t *geo_cnt = nullptr, *geo_bsums = nullptr, *geo_off = nullptr, *xf_order = nullptr;
+  RefineStatus *ord_st = nullptr;
   ipg_pixel_out *xf_out = nullptr;
   std::vector<int32_t *> gflags(ngrp);
   for (int pass = 0; pass < 2; pass++) {
@@ -839,6 +869,11 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
     geo_ij = A.take<int32_t>(2 * sum_gpix);
     geo_grp = A.take<int32_t>(sum_gpix);
     geo_mask = A.take<uint32_t>(sum_gpix);
+    geo_cnt = A.take<int32_t>(sum_gpix);
+    geo_bsums = A.take<int32_t>(sum_gpix / SCAN_TPB + 2);
+    geo_off = A.take<int32_t>(sum_gpix);
+    xf_order = A.take<int32_t>(sum_pix);
+    ord_st = A.take<RefineStatus>(1);
     if (pass == 0 && ar->bytes < A.off) {
       cudaFree(ar->dev);
       ar->dev = nullptr;
@@ -971,8 +1006,17 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
                                                                   l.nsy, grps[b.grp].upos, (int)goff[b.grp], b.slot,
                                                                   xf_geo + xoff[q], xf_slot + xoff[q]);
     }
+    {
+      const int ng = (int)n_geo, nb = grid_of(ng, SCAN_TPB);
+      k_geo_count<<<grid_of(ng, TPB), TPB, 0, s>>>(geo_mask, ng, geo_cnt);
+      k_scan_blocks<<<nb, SCAN_TPB, 0, s>>>(geo_cnt, ng, geo_bsums);
+      k_scan_top<<<1, SCAN_TPB, 0, s>>>(geo_bsums, nb, ord_st);
+      k_geo_offsets<<<nb, SCAN_TPB, 0, s>>>(geo_cnt, ng, geo_bsums, geo_off);
+      if (n_xf) k_xf_order<<<grid_of((long long)n_xf, TPB), TPB, 0, s>>>(xf_geo, xf_slot, geo_mask, geo_off, (int)n_xf,
+                                                                      xf_order);
+    }
     CKR(cudaGetLastError());
-    ipg_batch_items items = {n_geo, geo_ij, geo_grp, geo_mask, n_xf, xf_geo, xf_slot, xf_out};
+    ipg_batch_items items = {n_geo, geo_ij, geo_grp, geo_mask, n_xf, xf_geo, xf_slot, xf_out, xf_order};
     rc = ipg__batch_trace(ctx, &items, step_budget ? &steps_left : nullptr);
     if (rc) return rc;
     /* save_pixel, the checks and (base level) the flux estimate per instance */

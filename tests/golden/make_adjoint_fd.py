@@ -6,8 +6,12 @@ image (16x16, 230 GHz, inclination 163 deg, the seeded 128x64x64 dump) and a
 target rendered at M_unit x 1.3 and R_high 25, normalized by the target's
 largest intensity.  Every image here comes from the reference build
 oracle/_ref/ipole_nofma: the target, and the images at each parameter
-moved by a relative +-1e-4, whose central differences are stored in
-tests/golden/adjoint_fd_c1_16.npz with the target image.
+moved by a relative +-eps, whose central differences are stored in
+tests/golden/adjoint_fd_c1_16.npz with the target image: "fd" at eps =
+1e-6, and "fd_eps" at 1e-4, 1e-5 and 1e-6.  The loss turns fast with the
+Faraday rotation of this optically and Faraday-thick image, so the central
+difference at 1e-4 is still 1.7% (M_unit) from its limit; at 1e-6 it has
+converged to ~1e-6 while FP64 rounding stays far below.
 
     python tests/golden/make_adjoint_fd.py
 
@@ -29,7 +33,8 @@ sys.path.insert(0, ROOT)
 
 from ipole_b200 import ipgc, synthdump  # noqa: E402
 
-EPS = 1e-4
+EPS = 1e-6
+EPS_ALL = (1e-4, 1e-5, 1e-6)
 DUMP = (128, 64, 64, 1)
 BASE = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
         "--fov=160", "--trat_small=1", "--nx=16", "--ny=16"]
@@ -63,14 +68,17 @@ def main():
             return float((r * r).sum())
 
         L0 = loss(render(binary, dump, td))
-        fd = {}
-        for key in PARAMS:
-            x = PARAMS[key]
-            lp = loss(render(binary, dump, td, **{key: x * (1 + EPS)}))
-            lm = loss(render(binary, dump, td, **{key: x * (1 - EPS)}))
-            fd[key] = (lp - lm) / (2 * EPS * x)
+        fd_eps = {}
+        for e in EPS_ALL:
+            fd_eps[repr(e)] = {}
+            for key in PARAMS:
+                x = PARAMS[key]
+                lp = loss(render(binary, dump, td, **{key: x * (1 + e)}))
+                lm = loss(render(binary, dump, td, **{key: x * (1 - e)}))
+                fd_eps[repr(e)][key] = (lp - lm) / (2 * e * x)
+        fd = fd_eps[repr(EPS)]
     meta = {"dump_shape_seed": DUMP, "dump_sha256": h, "args": BASE, "params": PARAMS, "target_params": TARGET,
-            "eps": EPS, "loss": L0, "scale": scale, "fd": fd,
+            "eps": EPS, "loss": L0, "scale": scale, "fd": fd, "fd_eps": fd_eps,
             "generator": "oracle/_ref/ipole_nofma (reference sources, -O2 -ffp-contract=off)"}
     np.savez_compressed(os.path.join(HERE, "adjoint_fd_c1_16.npz"), meta=json.dumps(meta), target=target)
     print(json.dumps(meta, indent=1))

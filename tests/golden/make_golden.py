@@ -12,9 +12,14 @@ tests/golden/<case>.npz together with the command-line arguments and the
 sha256 of the dump's primitives (the dump is regenerated on demand from its
 seed, so the tests check the hash before comparing) and the reference's own
 noise floor: how far its other legal builds (oracle/Makefile targets ref and
-noise) land from this one, per test metric.
+noise) land from this one, per test metric.  The other builds are sampled
+as NOISE_RUNS lists them: the makefile's -O3 build, -O2 with FMA
+contraction, -O3 for AVX-512, and three independent "other libms" (the ulp
+shim with IPG_ULP_SALT 0, 1, 2), each without and with FMA contraction.
 
     python tests/golden/make_golden.py [case ...]
+    python tests/golden/make_golden.py --floor [case ...]   # floors only: runs
+        the realizations a stored golden's floor lacks and merges them in
 
 Needs the reference builds (``make -C oracle ref noise REF=<checkout>``), i.e. the reference tree.
 """
@@ -114,39 +119,62 @@ TRACE_CASES = {
 CASES.update(TRACE_CASES)
 
 
-def make_trace_case(case, binary, tmpdir, dumps):
+# the realizations of the reference's noise floor: (name recorded in the
+# golden, binary in oracle/_ref, IPG_ULP_SALT or None)
+NOISE_RUNS = [("ipole", "ipole", None), ("ipole_o2fma", "ipole_o2fma", None), ("ipole_v4", "ipole_v4", None),
+              ("ipole_ulp", "ipole_ulp", None), ("ipole_ulpfma", "ipole_ulpfma", None),
+              ("ipole_ulp:1", "ipole_ulp", "1"), ("ipole_ulpfma:1", "ipole_ulpfma", "1"),
+              ("ipole_ulp:2", "ipole_ulp", "2"), ("ipole_ulpfma:2", "ipole_ulpfma", "2")]
+
+
+def run_env(salt):
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "8"))
+    env.pop("IPG_ULP_SALT", None)
+    if salt is not None:
+        env["IPG_ULP_SALT"] = salt
+    return env
+
+
+def make_trace_case(case, binary, tmpdir, dumps, skip=()):
     dname, extra = CASES[case]
     dpath, dhash = dumps[dname]
     env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "8"))
 
-    def run(bin_name):
-        tr = os.path.join(tmpdir, f"{case}_{bin_name}_trace.ipgc")
-        out = os.path.join(tmpdir, f"{case}_{bin_name}.ipgc")
+    def run(bin_name, salt=None):
+        tr = os.path.join(tmpdir, f"{case}_{bin_name}_{salt}_trace.ipgc")
+        out = os.path.join(tmpdir, f"{case}_{bin_name}_{salt}.ipgc")
         if os.path.exists(tr):
             os.remove(tr)
         r = subprocess.run([os.path.join(os.path.dirname(binary), bin_name), f"--dump={dpath}", *BASE, *extra,
-                            f"--trace_outf={tr}", f"--outfile={out}"], capture_output=True, text=True, env=env)
+                            f"--trace_outf={tr}", f"--outfile={out}"], capture_output=True, text=True,
+                           env=run_env(salt))
         if r.returncode != 0:
             raise RuntimeError(f"{case}: {bin_name} exited {r.returncode}\n{r.stderr[-2000:]}")
         t = ipgc.read(tr)
         n = int(t["/nstep"][0, 0])
         return n, {k[1:]: v[0, 0, :n + 1] for k, v in t.items() if isinstance(v, np.ndarray) and v.ndim >= 3}
 
-    n, rec = run("ipole_nofma")
+    if skip:
+        # floors only: the stored golden is the no-FMA build's output
+        meta0, rec = load_stored(case)
+        n = meta0["nstep"]
+        floor, used = dict(meta0["ref_noise_floor"]), list(meta0["ref_noise_builds"])
+    else:
+        n, rec = run("ipole_nofma")
+        floor, used = {}, []
     # per dataset: the largest deviation of the other builds, relative to the
     # dataset's largest magnitude along the ray
-    floor, used = {}, []
-    for other in ("ipole", "ipole_o2fma", "ipole_v4", "ipole_ulp"):
-        if not os.path.exists(os.path.join(os.path.dirname(binary), other)):
+    for name, other, salt in NOISE_RUNS:
+        if name in used or not os.path.exists(os.path.join(os.path.dirname(binary), other)):
             continue
-        n2, rec2 = run(other)
+        n2, rec2 = run(other, salt)
         if n2 != n:
             floor["nstep_differs"] = 1.0
             continue
         for k, v in rec.items():
             sc = float(np.max(np.abs(v))) or 1.0
             floor[k] = max(floor.get(k, 0.0), float(np.max(np.abs(rec2[k] - v))) / sc)
-        used.append(other)
+        used.append(name)
     meta = {"case": case, "dump": dname, "dump_shape_seed": DUMPS[dname], "dump_sha256": dhash,
             "args": [*BASE, *extra], "nstep": n, "trace": True,
             "generator": "oracle/_ref/ipole_nofma (reference sources, -O2 -ffp-contract=off)",
@@ -170,53 +198,66 @@ def dump_path(name: str, tmpdir: str) -> tuple[str, str]:
     return path, h
 
 
-def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
+def load_stored(case):
+    z = np.load(os.path.join(HERE, f"{case}.npz"))
+    return json.loads(str(z["meta"])), {k: z[k] for k in z.files if k != "meta"}
+
+
+def make_case(case: str, binary: str, tmpdir: str, dumps: dict, floor_only: bool = False) -> None:
     dname, extra = CASES[case]
     out = os.path.join(tmpdir, f"{case}.ipgc")
     if dname in PLUGINS:
         binary = os.path.join(os.path.dirname(binary), f"ipole_{dname}")
-        base, dhash, others = [], None, (f"ipole_{dname}_fma",)
+        base, dhash, others = [], None, [(f"ipole_{dname}_fma", f"ipole_{dname}_fma", None)]
         args = [*extra, f"--outfile={out}"]
     else:
         dpath, dhash = dumps[dname]
-        base, others = BASE, ("ipole", "ipole_o2fma", "ipole_v4", "ipole_ulp")
+        base, others = BASE, NOISE_RUNS
         args = [f"--dump={dpath}", *BASE, *extra, f"--outfile={out}"]
-    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "8"))
+    env = run_env(None)
     check = case in CHECK_CASES
-    r = run_checked(binary, args, out, env) if check else subprocess.run([binary, *args], capture_output=True,
-                                                                          text=True, env=env)
-    if r.returncode != 0:
-        raise RuntimeError(f"{case}: reference exited {r.returncode}\n{r.stderr[-2000:]}")
-    img = ipgc.read(out)
-    if check:
-        # the check block is compared like an image; the recheck block rides along
-        img = {**img, "/unpol": img["/unpol_check"], "/tau": img["/tau_check"],
-               **({"/pol": img["/pol_check"]} if "/pol_check" in img else {})}
-    rec = {"unpol": img["/unpol"], "tau": img["/tau"]}
-    if "/pol" in img:
-        rec["pol"] = img["/pol"]
-    if case in SLIM:
-        del rec["tau"]
-        rec["pol"] = np.ascontiguousarray(rec["pol"][..., :4])
-    if check:
-        for k in CHECK_KEYS:
-            if f"/{k}_recheck" in img:
-                rec[f"{k}_recheck"] = img[f"/{k}_recheck"]
+    if floor_only:
+        # the stored golden is the no-FMA build's output; only the missing
+        # realizations of the floor run
+        meta0, rec = load_stored(case)
+        img = None
+    else:
+        r = run_checked(binary, args, out, env) if check else subprocess.run([binary, *args], capture_output=True,
+                                                                              text=True, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"{case}: reference exited {r.returncode}\n{r.stderr[-2000:]}")
+        img = ipgc.read(out)
+        if check:
+            # the check block is compared like an image; the recheck block rides along
+            img = {**img, "/unpol": img["/unpol_check"], "/tau": img["/tau_check"],
+                   **({"/pol": img["/pol_check"]} if "/pol_check" in img else {})}
+        rec = {"unpol": img["/unpol"], "tau": img["/tau"]}
+        if "/pol" in img:
+            rec["pol"] = img["/pol"]
+        if case in SLIM:
+            del rec["tau"]
+            rec["pol"] = np.ascontiguousarray(rec["pol"][..., :4])
+        if check:
+            for k in CHECK_KEYS:
+                if f"/{k}_recheck" in img:
+                    rec[f"{k}_recheck"] = img[f"/{k}_recheck"]
     # the reference's own noise floor: the largest deviation from this
     # -ffp-contract=off build among the other legal builds of the same sources
-    # (the makefile's -O3 FMA build, -O2 with FMA contraction, -O3 for
-    # AVX-512, and the no-FMA build with a libm one ulp away; oracle/Makefile
-    # targets ref and noise), in the metrics the tests use
+    # (NOISE_RUNS; oracle/Makefile targets ref and noise), in the metrics the
+    # tests use
     from tests.common import image_errors
     floor, used = None, []
-    for other_bin in others:
+    if floor_only:
+        floor, used = dict(meta0["ref_noise_floor"]), list(meta0["ref_noise_builds"])
+    for name, other_bin, salt in others:
         path = os.path.join(os.path.dirname(binary), other_bin)
-        if not os.path.exists(path):
+        if name in used or not os.path.exists(path):
             continue
-        out2 = os.path.join(tmpdir, f"{case}_{other_bin}.ipgc")
+        out2 = os.path.join(tmpdir, f"{case}_{other_bin}_{salt}.ipgc")
         oargs = [*args[:-1], f"--outfile={out2}"]
-        r = run_checked(path, oargs, out2, env) if check else subprocess.run([path, *oargs], capture_output=True,
-                                                                             text=True, env=env)
+        oenv = run_env(salt)
+        r = run_checked(path, oargs, out2, oenv) if check else subprocess.run([path, *oargs], capture_output=True,
+                                                                              text=True, env=oenv)
         if r.returncode != 0:
             continue
         other = ipgc.read(out2)
@@ -227,8 +268,15 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
             unpol = other["/unpol"]
             pol = other.get("/pol")
         e = image_errors(_Img, rec)
-        floor = e if floor is None else {k: max(floor[k], e[k]) for k in e}
-        used.append(other_bin)
+        floor = e if floor is None else {k: max(floor.get(k, 0.0), e[k]) for k in e}
+        used.append(name)
+        print(f"  {case} {name}: " + " ".join(f"{k} {e[k]:.1e}" for k in ("Ftot", "totQ", "EVPA_deg") if k in e),
+              flush=True)
+    if floor_only:
+        meta0.update(ref_noise_floor=floor, ref_noise_builds=used)
+        np.savez_compressed(os.path.join(HERE, f"{case}.npz"), meta=json.dumps(meta0), **rec)
+        print(case, "floor updated from", len(used), "builds")
+        return
     meta = {"case": case, "dump": dname, "dump_shape_seed": DUMPS.get(dname), "dump_sha256": dhash,
             "args": [*base, *extra], "Ftot_unpol": float(img["/Ftot_unpol"]),
             "Ftot": float(img["/Ftot"]) if "/Ftot" in img else None, "scale": float(img["/header/scale"]),
@@ -239,7 +287,7 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict) -> None:
     print(case, "Ftot", meta["Ftot"], "Ftot_unpol", meta["Ftot_unpol"])
 
 
-def main(cases):
+def main(cases, floor_only=False):
     binary = os.path.join(ROOT, "oracle", "_ref", "ipole_nofma")
     if not os.path.exists(binary):
         raise SystemExit("build the reference first: make -C oracle ref REF=<reference checkout>")
@@ -250,10 +298,13 @@ def main(cases):
             if d not in dumps and d not in PLUGINS:
                 dumps[d] = dump_path(d, td)
             if c in TRACE_CASES:
-                make_trace_case(c, binary, td, dumps)
+                make_trace_case(c, binary, td, dumps, skip=floor_only)
             else:
-                make_case(c, binary, td, dumps)
+                make_case(c, binary, td, dumps, floor_only=floor_only)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or list(CASES))
+    argv = sys.argv[1:]
+    fo = "--floor" in argv
+    argv = [a for a in argv if a != "--floor"]
+    main(argv or list(CASES), floor_only=fo)

@@ -5,8 +5,12 @@ image the adjoint traces.
 
 The loss is the L2 distance between the image and a target image rendered at
 perturbed parameters (M_unit x 1.3, R_high 20 -> 25), normalized by the
-target's largest intensity.  Finite differences are central with a relative
-step of 1e-4, and the adjoint must match them to 1e-4 relative.
+target's largest intensity.  Finite differences are central; the adjoint
+must match them to 1e-4 relative.  The loss turns fast with the Faraday
+rotation of this image: the central difference with a relative step of 1e-4
+is still 1.7% from its limit for M_unit (1e-5: 0.02%, 1e-6: 2e-6, measured
+on the oracle), so the checks take steps of 1e-6 (FP64 rounding of the
+loss stays ~1e-9 of the difference there) and show the convergence.
 """
 import json
 import os
@@ -19,7 +23,7 @@ from tests import common
 
 pytestmark = pytest.mark.gpu
 
-EPS = 1e-4
+EPS = 1e-6
 TOL = 1e-4
 BASE = ["--freqcgs=230.e9", "--thetacam=163", "--phicam=0", "--rotcam=0", "--MBH=6.5e9", "--dsource=16.8e6",
         "--fov=160", "--trat_small=1", "--nx=16", "--ny=16"]
@@ -69,13 +73,65 @@ def test_adjoint_scalars_match_finite_differences(setup):
     res = s["ctx"].adjoint_image(p, m, dL, ckpt=16)
     # the adjoint's own forward pass is the image's, bit for bit
     assert np.array_equal(res["pol"], img.pol[..., :4])
+    bad = {}
     for key, name in (("M_unit", "M_unit"), ("trat_large", "R_high"), ("trat_small", "R_low")):
         x = PARAMS[key]
-        lp = _loss_at(s, **{key: x * (1 + EPS)})
-        lm = _loss_at(s, **{key: x * (1 - EPS)})
-        fd = (lp - lm) / (2 * EPS * x)
         ad = res[name]
-        assert abs(ad - fd) <= TOL * abs(fd), (name, ad, fd)
+        errs = []
+        for e in (1e-4, 1e-5, EPS):
+            lp = _loss_at(s, **{key: x * (1 + e)})
+            lm = _loss_at(s, **{key: x * (1 - e)})
+            fd = (lp - lm) / (2 * e * x)
+            errs.append(abs(ad / fd - 1))
+            print(f"{name}: adjoint {ad:.8e} finite difference (eps {e:g}) {fd:.8e} relative {errs[-1]:.2e}")
+        if not errs[-1] <= TOL:
+            bad[name] = (ad, fd)
+        # the differences converge on the adjoint as the step shrinks
+        assert errs[-1] <= errs[0] or errs[0] <= TOL, (name, errs)
+    assert not bad, bad
+
+
+def _field_loss(s, m, fields, p):
+    """the loss of the image traced from the given field arrays"""
+    ctx = s["ctx"]
+    ctx.upload_arrays(m.grid, fields)
+    cam = ip.camera_for(p, m.grid)
+    ij = np.array([(i, j) for i in range(16) for j in range(16)], np.int32)
+    o = ctx.trace(cam, ij)
+    f3 = p.freqcgs ** 3
+    pol = np.zeros((16, 16, 4))
+    pol[ij[:, 0], ij[:, 1], 0] = o["I"] * f3
+    pol[ij[:, 0], ij[:, 1], 1] = -o["Q"] * f3
+    pol[ij[:, 0], ij[:, 1], 2] = -o["U"] * f3
+    pol[ij[:, 0], ij[:, 1], 3] = o["V"] * f3
+    return _loss(pol, s)[0]
+
+
+def test_adjoint_field_scalings_match_finite_differences(setup):
+    """Directional derivatives along each whole field: scaling every cell's
+    ne (Theta_e, |B|) by 1 +- 1e-4 against sum_c dL/dx_c x_c"""
+    s = setup
+    p = _params(s["dump"])
+    m = ip.Model.load(p)
+    ctx = s["ctx"]
+    ctx.upload(m)
+    img = ctx.render(p, m)
+    _, dL = _loss(img.pol, s)
+    res = ctx.adjoint_image(p, m, dL, ckpt=16)
+    fields = [np.array(m.field(q)) for q in range(ip.NFIELD)]
+    bad = {}
+    for name, fi in (("ne", ip.IPG_F_NE), ("thetae", ip.IPG_F_THETAE), ("b", ip.IPG_F_B)):
+        fp = [f.copy() for f in fields]
+        fm = [f.copy() for f in fields]
+        fp[fi] = fields[fi] * (1 + EPS)
+        fm[fi] = fields[fi] * (1 - EPS)
+        fd = (_field_loss(s, m, fp, p) - _field_loss(s, m, fm, p)) / (2 * EPS)
+        ad = float(np.sum(res[name] * fields[fi]))
+        print(f"field {name}: adjoint {ad:.8e} finite difference {fd:.8e} relative {abs(ad / fd - 1):.2e}")
+        if not abs(ad - fd) <= TOL * abs(fd):
+            bad[name] = (ad, fd)
+    ctx.upload(m)
+    assert not bad, bad
 
 
 def test_adjoint_cells_match_finite_differences(setup):
@@ -122,7 +178,9 @@ def test_adjoint_cells_match_finite_differences(setup):
 
 def test_checkpoint_interval_leaves_gradients_unchanged(setup):
     """The segments are recomputed with the forward's own arithmetic, so the
-    interval changes memory and time, not a bit of the result"""
+    interval changes memory and time; the per-point gradients are the same
+    bits, and only the order of the FP64 atomic scatter-adds into a cell
+    varies from run to run (a few ulps of the cell's sum)"""
     s = setup
     p = _params(s["dump"])
     m = ip.Model.load(p)
@@ -132,8 +190,11 @@ def test_checkpoint_interval_leaves_gradients_unchanged(setup):
     r16 = s["ctx"].adjoint_image(p, m, dL, ckpt=16)
     r64 = s["ctx"].adjoint_image(p, m, dL, ckpt=64)
     for k in ("ne", "thetae", "b"):
-        assert np.array_equal(r16[k], r64[k]), k
-    assert (r16["M_unit"], r16["R_high"], r16["R_low"]) == (r64["M_unit"], r64["R_high"], r64["R_low"])
+        a, b = r16[k], r64[k]
+        assert np.array_equal(a != 0, b != 0), k
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(a)), k
+    for k in ("M_unit", "R_high", "R_low"):
+        assert abs(r16[k] - r64[k]) <= 1e-12 * abs(r16[k]), k
 
 
 def test_autograd_wrapper_chains_to_the_electron_parameters(setup):
