@@ -146,12 +146,13 @@ __device__ __forceinline__ void rho_QV_f32(double Ne, double nu, double Thetae, 
   }
   double fit_factor;
   if (dexter_v && k2pos) {
-    /* (K_0 - shgm) / K_2 */
-    const float shgm = 0.43793091f * logf(1.f + 0.00185777f * powf(x, 1.50316886f));
+    /* (K_0 - shgm) / K_2; log1p keeps the small shgm that 1/K_2 (up to
+     * e^744) magnifies, which log(1 + y) loses in FP32 below y ~ 1e-7 */
+    const float shgm = 0.43793091f * log1pf(0.00185777f * powf(x, 1.50316886f));
     fit_factor = (double)kr0 - (double)shgm * exp_split(-lnk2);
   } else {
     const float k_ratio = k2pos ? kr0 : 1.f;
-    fit_factor = (double)(k_ratio * (1.f - 0.11f * logf(1.f + 0.035f * x)));
+    fit_factor = (double)(k_ratio * (1.f - 0.11f * log1pf(0.035f * x)));
   }
   const double eps12 = wp2 * omega0 * (itpn * itpn * itpn) * fit_factor * cth;
   *rV = tpn * (1. / IPG_CL) * eps12 * nu;

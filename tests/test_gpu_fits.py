@@ -56,6 +56,17 @@ def subnormal_k2(pts):
     return pts[:, 2] < 1. / 708.
 
 
+def subnormal_tolerance(pts):
+    """relative tolerance of a ratio K_n/K_2 whose terms are subnormal: four
+    spacings of the subnormal range (4.94e-324) over the smallest term"""
+    from scipy.special import kve
+    a = 1. / pts[:, 2]
+    with np.errstate(all="ignore"):
+        k = np.minimum(kve(1, a), kve(2, a)) * np.exp(-a)
+        tol = np.where(k > 0, 4 * 4.94e-324 / np.where(k > 0, k, 1.), np.inf)
+    return np.maximum(tol, 1e-10)
+
+
 def summary(e):
     return {COL[k]: f"{e[:, k].max():.1e}/{np.quantile(e[:, k], 0.999):.1e}" for k in range(12)}
 
@@ -90,9 +101,11 @@ def test_fp64_fits_against_oracle_wide(ctx, em):
     e = rel_err(d[finite & ~sub], ref[finite & ~sub])
     es = rel_err(d[finite & sub], ref[finite & sub])
     print(f"fp64 vs oracle, emission {em} (max/p99.9):", summary(e))
-    print(f"  Theta_e < 1/708 ({int(sub.sum())} points): max {es.max() if es.size else 0.:.2e}")
+    tol = subnormal_tolerance(pts[finite & sub])[:, None]
+    print(f"  Theta_e < 1/708 ({int(sub.sum())} points): max {es.max() if es.size else 0.:.2e}, "
+          f"max over its bound {(es / tol).max() if es.size else 0.:.2e}")
     assert e.max() <= 1e-10
-    assert es.size == 0 or es.max() <= 1e-2
+    assert es.size == 0 or (es <= tol).all()
 
 
 @pytest.mark.parametrize("em", [4, 1])
