@@ -559,6 +559,11 @@ def bench_adjoint(ip, ctx, model, p, args, world, stream):
         r = ctx.adjoint_image(p, model, dL, ckpt=K)
         torch.cuda.synchronize()
         res[f"K{K}_ms"] = (time.time() - t0) * 1e3
+        st = ctx.stats()
+        res[f"K{K}_device_ms"] = {k: st[f"{k}_ms"] for k in ("geodesic", "coeffs", "transfer", "adjoint", "adj_scatter",
+                                                             "wall")}
+        res[f"K{K}_waves"] = st["waves"]
+        res[f"K{K}_nonfinite_cells"] = int(sum((~np.isfinite(r[k])).sum() for k in ("ne", "thetae", "b")))
     t0 = time.time()
     ctx.render(p, model)
     torch.cuda.synchronize()

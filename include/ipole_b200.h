@@ -346,6 +346,11 @@ typedef struct ipg_stats {
   double geodesic_span_ms;
   double coeffs_span_ms;
   double transfer_span_ms;
+  /* ipg_adjoint: the reverse walk (link pass and adjoint kernel) and the
+   * scatter of the cells' gradients; its forward pass is in geodesic_ms,
+   * coeffs_ms and transfer_ms */
+  double adjoint_ms;
+  double adj_scatter_ms;
 } ipg_stats;
 int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 

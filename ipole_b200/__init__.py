@@ -95,7 +95,8 @@ class Stats(C.Structure):
     _fields_ = [("ray_steps", C.c_uint64), ("radiating_steps", C.c_uint64), ("launches", C.c_int32),
                 ("waves", C.c_int32), ("geodesic_ms", C.c_double), ("transfer_ms", C.c_double),
                 ("coeffs_ms", C.c_double), ("predict_ms", C.c_double), ("wall_ms", C.c_double),
-                ("geodesic_span_ms", C.c_double), ("coeffs_span_ms", C.c_double), ("transfer_span_ms", C.c_double)]
+                ("geodesic_span_ms", C.c_double), ("coeffs_span_ms", C.c_double), ("transfer_span_ms", C.c_double),
+                ("adjoint_ms", C.c_double), ("adj_scatter_ms", C.c_double)]
 
 
 class _Params(C.Structure):

@@ -20,10 +20,15 @@
  * |B|) at the point and scatter-adds that to the eight cells of the
  * trilinear gather (src/grid.c:15-44), with their weights.
  *
- *   - The N_n it needs are recomputed, not stored: the forward pass keeps
+ *   - The N it needs are recomputed, not stored: the forward pass keeps
  *     N every K steps (k_transfer with CKK = K), and the adjoint
- *     recomputes the K values of a segment from its top, with the forward's
- *     own functions, so they are the forward's bits.
+ *     recomputes a segment from its top with the forward's own functions,
+ *     so they are the forward's bits; it keeps, per step of the segment,
+ *     N after the step's two pushes (the state evolve_N was applied to).
+ *   - The walk (k_adjoint, one lane per ray) leaves dL/d(coefficients) at
+ *     each radiating record; k_adj_scatter, one thread per record, turns
+ *     them into dL/d(ne, Theta_e, |B|) and scatter-adds those to the cells,
+ *     off the walk's critical path.
  *   - The coefficients' derivatives come from re-evaluating the fits
  *     (jar_fits) in forward-mode dual numbers along ne, Theta_e, |B|
  *     (ipg_dual.cuh), and the step's from re-evaluating the Faraday and
@@ -239,8 +244,10 @@ __global__ void k_adj_link(const int *__restrict__ prev, const int2 *__restrict_
   }
 }
 
-/* one forward step n -> n-1 of N (the polarized part of xfer_step) */
-__device__ __forceinline__ void fwd_N(const DevCam &C, const double *rec_n, const double *rec_m, HermN *N)
+/* one forward step n -> n-1 of N (the polarized part of xfer_step);
+ * *Np receives N after the two pushes, before evolve_N */
+__device__ __forceinline__ void fwd_N(const DevCam &C, const double *rec_n, const double *rec_m, HermN *N,
+                                      HermN *Np)
 {
   const DevGrid &G = c_grid;
   const double dl = rec_n[REC_DL];
@@ -250,6 +257,7 @@ __device__ __forceinline__ void fwd_N(const DevCam &C, const double *rec_n, cons
   hn_push(*N, *N, A, (0.5 * dl) * G.inv_dlfac, &Nh);
   load_A(rec_n + REC_A2, A);
   hn_push(*N, Nh, A, dl * G.inv_dlfac, &Nn);
+  *Np = Nn;
   CoefBlock cb;
   load_coef(rec_m, cb);
   const int flags = (int)cb.flags;
@@ -314,7 +322,7 @@ __device__ __forceinline__ void fluid_scatter(const double *__restrict__ fields,
 /* One lane per ray of the wave: the adjoint walk, camera to source. */
 template <int K>
 __global__ void __launch_bounds__(128, 1)
-    k_adjoint(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
+    k_adjoint(const int32_t *__restrict__ list, int n_list, double *__restrict__ pool,
               const double *__restrict__ adj_side, const double *__restrict__ ckpt, const int *__restrict__ prev,
               const int *__restrict__ next, const int *__restrict__ first, const RayRec *__restrict__ rays,
               const double *__restrict__ dL_dout, const double *__restrict__ fields, double *__restrict__ g_ne,
@@ -353,19 +361,19 @@ __global__ void __launch_bounds__(128, 1)
         N.r23 = q[8]; N.r33 = q[9]; N.s01 = q[10]; N.s02 = q[11];
         N.s03 = q[12]; N.s12 = q[13]; N.s13 = q[14]; N.s23 = q[15];
       }
-      /* N_n for n = hi .. lo+1, the forward's values */
-      Nbuf[0] = N;
-      for (int n = hi; n > lo + 1; n--) {
+      /* for n = hi .. lo+1, N_n after the two pushes of step n (the
+       * state evolve_N was applied to), the forward's values */
+      for (int n = hi; n > lo; n--) {
         const double *rn = walk_rec(w, n, pool, prev, next);
         const double *rm = walk_rec(w, n - 1, pool, prev, next);
-        fwd_N(C, rn, rm, &N);
-        Nbuf[hi - n + 1] = N;
+        HermN Np;
+        fwd_N(C, rn, rm, &N, &Np);
+        Nbuf[hi - n] = Np;
       }
       /* the adjoint of steps n = lo+1 .. hi */
       for (int n = lo + 1; n <= hi; n++) {
         const double *rn = walk_rec(w, n, pool, prev, next);
-        const double *rm = walk_rec(w, n - 1, pool, prev, next);
-        const HermN Nn_in = Nbuf[hi - n];
+        double *rm = const_cast<double *>(walk_rec(w, n - 1, pool, prev, next));
         const double dl = rn[REC_DL];
         const double dlfull = dl * Gd.inv_dlfac, dlhalf = (0.5 * dl) * Gd.inv_dlfac;
         double A1[4][4], A2[4][4];
@@ -375,15 +383,15 @@ __global__ void __launch_bounds__(128, 1)
         load_coef(rm, cb);
         const int flags = (int)cb.flags;
         if (flags & 1) {
-          HermN Nh, Np;
-          hn_push(Nn_in, Nn_in, A1, dlhalf, &Nh);
-          hn_push(Nn_in, Nh, A2, dlfull, &Np);
           int zero_emission = (flags & 2) ? 1 : 0;
           if (C.target_nturns >= 0 && (int)rn[REC_NTURNS] != C.target_nturns) zero_emission = 1;
           double gc[8];
-          evolve_adj(cb, dl, zero_emission, Np, &G, gc);
-          const double *sd = adj_side + (size_t)(rm - pool) / IPG_STEP_DOUBLES * IPG_ADJ_DOUBLES;
-          fluid_scatter(fields, sd, C.emission_type, gc, g_ne, g_th, g_b);
+          evolve_adj(cb, dl, zero_emission, Nbuf[hi - n], &G, gc);
+          /* dL/d(coefficients) of the record of step n-1, in place of its
+           * A1, which this walk read for the last time at step n-1;
+           * k_adj_scatter turns them into the cells' gradients */
+          store4(rm + REC_A1, gc[0], gc[1], gc[2], gc[3]);
+          store4(rm + REC_A1 + 4, gc[4], gc[5], gc[6], gc[7]);
         }
         /* push_polar twice, transposed: G_Nh = -dlfull (A2^T G + G A2),
          * G_N = G + G_Nh - dlhalf (A1^T G_Nh + G_Nh A1) */
@@ -398,6 +406,39 @@ __global__ void __launch_bounds__(128, 1)
         G.s03 += Gs.s03; G.s12 += Gs.s12; G.s13 += Gs.s13; G.s23 += Gs.s23;
       }
     }
+  }
+}
+
+/* One thread per step record of the wave: the coefficient gradients the
+ * walk left at each radiating record (steps 0 .. nstep-1 of a traced ray)
+ * become dL/d(ne, Theta_e, |B|) at its point and are scattered to the
+ * cells of its gather (fluid_scatter).  Parallel over records, where the
+ * walk is one lane per ray. */
+__global__ void __launch_bounds__(128, 3)
+    k_adj_scatter(const double *__restrict__ pool, const int2 *__restrict__ chunk_meta,
+                  const unsigned long long *__restrict__ counters, long long n_chunks,
+                  const RayRec *__restrict__ rays, const double *__restrict__ adj_side,
+                  const double *__restrict__ fields, double *__restrict__ g_ne, double *__restrict__ g_th,
+                  double *__restrict__ g_b)
+{
+  const DevCam &C = c_cam;
+  long long used = (long long)counters[CNT_POOL];
+  if (used > n_chunks) used = n_chunks;
+  const long long total = used * IPG_CHUNK_STEPS;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / IPG_CHUNK_STEPS), slot = (int)(t % IPG_CHUNK_STEPS);
+    const int2 meta = chunk_meta[c];
+    const RayRec rec = rays[meta.x];
+    const int s = meta.y + slot;
+    if (rec.status != IPG_RAY_OK || s >= rec.nstep) continue;
+    const double *p = step_ptr(const_cast<double *>(pool), c, slot);
+    if (!((int)p[REC_FLAGS] & 1)) continue;
+    double gc[8];
+    load4(p + REC_A1, gc);
+    load4(p + REC_A1 + 4, gc + 4);
+    fluid_scatter(fields, adj_side + ((size_t)c * IPG_CHUNK_STEPS + slot) * IPG_ADJ_DOUBLES, C.emission_type, gc,
+                  g_ne, g_th, g_b);
   }
 }
 
@@ -417,6 +458,7 @@ static int adjoint_wave(ipg_ctx *ctx, int em, const int32_t *d_ij, const int32_t
                                                                         ctx->d_chunk_meta, n_chunks, cnt, ctx->d_rays,
                                                                         deferred, nullptr);
   CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev[2], st)); /* stage boundaries, read by ipg_adjoint */
   if (em == 1) {
     int cb = grid_blocks(ctx, (const void *)k_coeffs<IPG_PLUG_IHARM, 1, true>, threads, (size_t)n_chunks * 32);
     k_coeffs<IPG_PLUG_IHARM, 1, true><<<cb, threads, 0, st>>>(pool, ctx->d_chunk_meta, cnt, n_chunks, ctx->d_rays,
@@ -427,15 +469,22 @@ static int adjoint_wave(ipg_ctx *ctx, int em, const int32_t *d_ij, const int32_t
                                                               ctx->d_fields, side);
   }
   CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev[3], st));
   int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0, K>, threads, run);
   k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0, K><<<tb, threads, 0, st>>>(
       list, (int)run, pool, ctx->d_chunk_prev, ctx->d_rays, d_out, cnt, ckpt);
   CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev[4], st));
   k_adj_link<<<4 * ctx->n_sm, 256, 0, st>>>(ctx->d_chunk_prev, ctx->d_chunk_meta, cnt, n_chunks, next, first);
   CK(cudaGetLastError());
   int ab = grid_blocks(ctx, (const void *)k_adjoint<K>, threads, run);
   k_adjoint<K><<<ab, threads, 0, st>>>(list, (int)run, pool, side, ckpt, ctx->d_chunk_prev, next, first, ctx->d_rays,
                                        dL, ctx->d_fields, g, g + ncell, g + 2 * ncell, cnt + CNT_N);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev_pred[0], st));
+  int sb = grid_blocks(ctx, (const void *)k_adj_scatter, threads, (size_t)n_chunks * IPG_CHUNK_STEPS);
+  k_adj_scatter<<<sb, threads, 0, st>>>(pool, ctx->d_chunk_meta, cnt, n_chunks, ctx->d_rays, side, ctx->d_fields, g,
+                                        g + ncell, g + 2 * ncell);
   CK(cudaGetLastError());
   return IPG_OK;
 }
@@ -505,9 +554,15 @@ extern "C" int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *i
   CKA(cudaMemcpyAsync(dL, dL_dout, 4 * n * sizeof(double), cudaMemcpyHostToDevice, st));
   CKA(cudaMemsetAsync(g, 0, 3 * ncell * sizeof(double), st));
   memset(&ctx->stats, 0, sizeof(ctx->stats));
-  /* waves as in the image trace (unsplit): rays that find the pool full
-   * go to the next wave, after this wave's adjoint is done */
-  const int32_t *list = NULL;
+  /* waves as in the image trace (unsplit, longest predicted rays first):
+   * rays that find the pool full go to the next wave, after this wave's
+   * adjoint is done */
+  rc = sort_by_length(ctx, ctx->d_ij, n, cam);
+  if (rc) {
+    release();
+    return rc;
+  }
+  const int32_t *list = ctx->d_sorted;
   size_t pending = n, wave = n;
   int cur = 0;
   while (pending > 0) {
@@ -538,9 +593,19 @@ extern "C" int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *i
     unsigned long long h[CNT_N];
     CKA(cudaMemcpyAsync(h, ctx->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
     CKA(cudaStreamSynchronize(st));
-    float ms = 0.f;
+    float ms = 0.f, t[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&t[0], ctx->ev[0], ctx->ev[2]);
+    cudaEventElapsedTime(&t[1], ctx->ev[2], ctx->ev[3]);
+    cudaEventElapsedTime(&t[2], ctx->ev[3], ctx->ev[4]);
+    cudaEventElapsedTime(&t[3], ctx->ev[4], ctx->ev_pred[0]);
+    cudaEventElapsedTime(&t[4], ctx->ev_pred[0], ctx->ev[1]);
     ctx->stats.wall_ms += ms;
+    ctx->stats.geodesic_ms += t[0];
+    ctx->stats.coeffs_ms += t[1];
+    ctx->stats.transfer_ms += t[2];
+    ctx->stats.adjoint_ms += t[3];
+    ctx->stats.adj_scatter_ms += t[4];
     ctx->stats.ray_steps += h[CNT_STEPS];
     ctx->stats.radiating_steps += h[CNT_RAD];
     ctx->stats.launches += 5;

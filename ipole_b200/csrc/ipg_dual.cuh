@@ -81,14 +81,15 @@ __device__ __forceinline__ Dual<D> operator*(const Dual<D> &a, const Dual<D> &b)
   for (int k = 0; k < D; k++) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
   return r;
 }
+/* by division, not by a reciprocal: 1/b overflows for a subnormal b (the
+ * Bessel functions of cold electrons), a/b does not */
 template <int D>
 __device__ __forceinline__ Dual<D> operator/(const Dual<D> &a, const Dual<D> &b)
 {
   Dual<D> r;
-  const double ib = 1. / b.v;
   r.v = a.v / b.v;
 #pragma unroll
-  for (int k = 0; k < D; k++) r.d[k] = (a.d[k] - r.v * b.d[k]) * ib;
+  for (int k = 0; k < D; k++) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v;
   return r;
 }
 template <int D>
@@ -213,11 +214,15 @@ __device__ __forceinline__ Dual<D> log(const Dual<D> &x)
 {
   return dchain(x, log(x.v), 1. / x.v);
 }
+/* At a zero argument (the k-B angle's sine along the field) the functions
+ * below with an infinite slope there take the derivative 0: the argument is
+ * then identically zero in every direction that occurs (sin theta = 0 does
+ * not move with ne, Theta_e or |B|), and inf * 0 would poison the result. */
 template <int D>
 __device__ __forceinline__ Dual<D> sqrt(const Dual<D> &x)
 {
   const double s = sqrt(x.v);
-  return dchain(x, s, 0.5 / s);
+  return dchain(x, s, x.v == 0. ? 0. : 0.5 / s);
 }
 template <int D>
 __device__ __forceinline__ Dual<D> rsqrt(const Dual<D> &x)
@@ -229,13 +234,13 @@ template <int D>
 __device__ __forceinline__ Dual<D> cbrt(const Dual<D> &x)
 {
   const double c = cbrt(x.v);
-  return dchain(x, c, c / (3. * x.v));
+  return dchain(x, c, x.v == 0. ? 0. : c / (3. * x.v));
 }
 template <int D>
 __device__ __forceinline__ Dual<D> pow(const Dual<D> &x, double p)
 {
   const double v = pow(x.v, p);
-  return dchain(x, v, p * v / x.v);
+  return dchain(x, v, x.v == 0. ? 0. : p * v / x.v);
 }
 template <int D>
 __device__ __forceinline__ Dual<D> tanh(const Dual<D> &x)

@@ -1877,6 +1877,32 @@ static int plan_split(ipg_ctx *ctx, const int32_t *d_ij, const int32_t *list, si
   return IPG_OK;
 }
 
+/* The rays 0..n-1 in ctx->d_sorted, longest predicted first (the length
+ * prediction of plan_split without the classes): a lane-persistent kernel
+ * that takes them in this order starts its longest rays first, so that their
+ * tails overlap the rest of the wave. */
+static int sort_by_length(ipg_ctx *ctx, const int32_t *d_ij, size_t n, const ipg_camera *cam)
+{
+  const int threads = 128;
+  unsigned long long *cnt = ctx->d_cnt;
+  CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
+  int cap = (int)(cam->maxnstep / PRED_EPS_SCALE) + 1;
+  if (cap > LEN_BUCKETS - 1) cap = LEN_BUCKETS - 1;
+  switch (ctx->plug) {
+    case IPG_PLUG_ANALYTIC: launch_count_t<IPG_PLUG_ANALYTIC>(ctx, threads, d_ij, NULL, n, cap, cnt + CNT_NEXT_G); break;
+    case IPG_PLUG_SPHERE: launch_count_t<IPG_PLUG_SPHERE>(ctx, threads, d_ij, NULL, n, cap, cnt + CNT_NEXT_G); break;
+    default: launch_count_t<IPG_PLUG_IHARM>(ctx, threads, d_ij, NULL, n, cap, cnt + CNT_NEXT_G);
+  }
+  CK(cudaMemsetAsync(ctx->d_len_hist, 0, LEN_BUCKETS * sizeof(int), ctx->stream));
+  int sb = (int)((n + 255) / 256);
+  if (sb > 4 * ctx->n_sm) sb = 4 * ctx->n_sm;
+  k_len_hist<<<sb, 256, 0, ctx->stream>>>(ctx->d_pred, (int)n, 0, ctx->d_len_hist);
+  k_len_scan<<<1, LEN_SCAN_THREADS, 0, ctx->stream>>>(ctx->d_len_hist);
+  k_len_scatter<<<sb, 256, 0, ctx->stream>>>(NULL, ctx->d_pred, (int)n, 0, ctx->d_len_hist, ctx->d_sorted);
+  CK(cudaGetLastError());
+  return IPG_OK;
+}
+
 /* device-resident core: d_ij/d_out on the device, enqueued on ctx->stream */
 static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, size_t n, ipg_pixel_out *d_out)
 {

@@ -113,6 +113,10 @@ def image_errors(img, arrs):
         e["Ftot"] = abs(p[..., 0].sum() / Itot - 1)
         for c, n in ((1, "Q"), (2, "U"), (3, "V")):
             e["tot" + n] = abs(p[..., c].sum() - pg[..., c].sum()) / abs(Itot)
+        # the deviation of the linear-polarization vector (sum Q, sum U): the
+        # same for any orientation of the camera frame (rotcam, qu_conv),
+        # which only redistributes it between Q and U
+        e["totQU"] = float(np.hypot(p[..., 1].sum() - pg[..., 1].sum(), p[..., 2].sum() - pg[..., 2].sum())) / abs(Itot)
         m = I > 1e-6 * I.max()
         rel = np.abs(p[..., 0][m] / I[m] - 1)
         e["pix_I_max"] = float(rel.max())
@@ -146,7 +150,18 @@ EVPA_MIN_LP = 1e-3
 
 
 def tolerance(meta, key):
-    floor = (meta.get("ref_noise_floor") or {}).get(key, 0.0)
+    """The bound of one metric.  Q and U are the components of one vector in
+    the camera's frame; which of the two a build's deviation falls into is
+    a matter of that frame, so their floors are the largest deviation of the
+    vector itself (totQU), and the EVPA's floor is also at least the angle
+    such a vector deviation subtends at the image's linear polarization."""
+    fl = meta.get("ref_noise_floor") or {}
+    floor = fl.get(key, 0.0)
+    if key in ("totQ", "totU") and "totQU" in fl:
+        floor = max(floor, fl["totQU"])
     if key == "EVPA_deg":
         floor = wrap180(floor)  # floors recorded before the angle was wrapped
+        lp = fl.get("LP_ref", 0.0)
+        if "totQU" in fl and lp > 0:
+            floor = max(floor, float(np.degrees(fl["totQU"] / (2. * lp))))
     return max(BASE_TOL[key], FLOOR_FACTOR * floor)

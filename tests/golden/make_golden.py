@@ -20,6 +20,8 @@ shim with IPG_ULP_SALT 0, 1, 2), each without and with FMA contraction.
     python tests/golden/make_golden.py [case ...]
     python tests/golden/make_golden.py --floor [case ...]   # floors only: runs
         the realizations a stored golden's floor lacks and merges them in
+    python tests/golden/make_golden.py --refloor [case ...]  # floors only,
+        every realization again (after a change of the metrics)
 
 Needs the reference builds (``make -C oracle ref noise REF=<checkout>``), i.e. the reference tree.
 """
@@ -135,6 +137,9 @@ def run_env(salt):
     return env
 
 
+REDO = False  # --refloor: recompute floors from every realization
+
+
 def make_trace_case(case, binary, tmpdir, dumps, skip=()):
     dname, extra = CASES[case]
     dpath, dhash = dumps[dname]
@@ -247,7 +252,7 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict, floor_only: bool
     # tests use
     from tests.common import image_errors
     floor, used = None, []
-    if floor_only:
+    if floor_only and not REDO:
         floor, used = dict(meta0["ref_noise_floor"]), list(meta0["ref_noise_builds"])
     for name, other_bin, salt in others:
         path = os.path.join(os.path.dirname(binary), other_bin)
@@ -273,6 +278,9 @@ def make_case(case: str, binary: str, tmpdir: str, dumps: dict, floor_only: bool
         print(f"  {case} {name}: " + " ".join(f"{k} {e[k]:.1e}" for k in ("Ftot", "totQ", "EVPA_deg") if k in e),
               flush=True)
     if floor_only:
+        if not used:
+            print(case, "no other build available: floor unchanged")
+            return
         meta0.update(ref_noise_floor=floor, ref_noise_builds=used)
         np.savez_compressed(os.path.join(HERE, f"{case}.npz"), meta=json.dumps(meta0), **rec)
         print(case, "floor updated from", len(used), "builds")
@@ -305,6 +313,7 @@ def main(cases, floor_only=False):
 
 if __name__ == "__main__":
     argv = sys.argv[1:]
-    fo = "--floor" in argv
-    argv = [a for a in argv if a != "--floor"]
+    fo = "--floor" in argv or "--refloor" in argv
+    REDO = "--refloor" in argv
+    argv = [a for a in argv if a not in ("--floor", "--refloor")]
     main(argv or list(CASES), floor_only=fo)

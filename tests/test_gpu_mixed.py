@@ -19,8 +19,20 @@ pytestmark = pytest.mark.gpu
 
 CASES = ["c1_bright_32", "c1_faraday_24", "c1_thick_24", "c1_incl17_rot_24", "c2_rhigh160_incl163_24",
          "c2_rhigh1_incl17_24", "c1_unpol_24", "c1_refine_32", "analytic_m2_32", "sphere_f223_i30_32"]
-BOUNDS = {"Ftot": 1e-3, "Ftot_unpol": 1e-3, "EVPA_deg": 0.5, "LP_abs": 1e-3, "CP_abs": 1e-3,
-          "pix_I_max": 1e-2, "pix_unpol_max": 1e-2}
+# The mixed tier's end targets (total flux 1e-3, flux-weighted EVPA 0.5
+# degree against the FP64 images) are far above what these forms measure,
+# so the bounds here are about ten times the largest error measured on the
+# ten cases, per form: a regression shows long before a target is missed.
+# The compact records alone (FP32 storage of order-one values; measured
+# worst: total flux 3.1e-8, EVPA 8.1e-5 deg, LP 2.0e-7, CP 1.8e-9, per pixel
+# 2.1e-6, the unpolarized image unchanged):
+RECORD_BOUNDS = {"Ftot": 3e-7, "Ftot_unpol": 0., "EVPA_deg": 1e-3, "LP_abs": 2e-6, "CP_abs": 2e-8,
+                 "pix_I_max": 2e-5, "pix_unpol_max": 0.}
+# with the FP32 step and the FP32 fit shapes (measured worst: total flux
+# 6.5e-6, EVPA 1.8e-2 deg on the optically thick case, LP 5.5e-6, CP 4.1e-7,
+# per pixel 2.9e-5):
+BOUNDS = {"Ftot": 7e-5, "Ftot_unpol": 7e-5, "EVPA_deg": 0.2, "LP_abs": 6e-5, "CP_abs": 5e-6,
+          "pix_I_max": 3e-4, "pix_unpol_max": 3e-4}
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -42,7 +54,7 @@ def test_mixed_records_against_fp64(case, dumps):
     e = common.image_errors(mixed, ref)
     print(case, {k: f"{v:.2e}" for k, v in e.items()})
     assert np.array_equal(mixed.nstep, full.nstep)  # the geodesics are the same
-    bad = {k: v for k, v in e.items() if k in BOUNDS and not v <= BOUNDS[k]}
+    bad = {k: v for k, v in e.items() if k in RECORD_BOUNDS and not v <= RECORD_BOUNDS[k]}
     assert not bad, bad
 
 
