@@ -245,3 +245,57 @@ def test_dense_groups_are_refused(tmp_path):
     with pytest.raises(ip.IpgError) as e:
         ip.convert_container(str(p), str(tmp_path / "x.ipgc"))
     assert e.value.code == ip.IPG_E_FORMAT
+
+
+def _spec_same(ent, dec):
+    """an entry dict given to ipgc.write against the independent decoder's"""
+    assert sorted(ent) == sorted(dec), (sorted(ent), sorted(dec))
+    for k, v in ent.items():
+        d = dec[k]
+        if v is None:
+            assert d is None, k
+        elif isinstance(v, str):
+            assert d.rstrip(b"\0").decode() == v, k
+        else:
+            v = np.asarray(v)
+            assert d.dtype == v.dtype and d.shape == v.shape and np.array_equal(d, v), k
+
+
+def test_writer_output_decodes_with_an_independent_reader(tmp_path):
+    """The HDF5 files the library writes, decoded by tests/h5_spec_reader.py
+    (a second implementation, in Python, of the specification's superblock
+    v0, v1 object headers, symbol-table groups and messages): every entry
+    kind, a group spread over several symbol-table nodes, a large array,
+    and the image schema of ipole's output."""
+    from tests import h5_spec_reader
+    ent = {"/g/a": np.arange(24.).reshape(2, 3, 4), "/g/n": np.int32(-7), "/s": "FMKS",
+           "/g/h/x": np.float64(1.5), "/e": None, "/g/a@units": "cm", "/@githash": "abc123",
+           "/g@k": np.int32(3), "/m": np.arange(6, dtype=np.int32).reshape(3, 2),
+           "/g/a@scale": np.array([1.5, -2.5]), "/empty": np.zeros((0, 3)), "/g": None, "/g/h": None}
+    ent.update({f"/many/d{i:03d}": np.float64(i) for i in range(150)})
+    ent["/many"] = None
+    ent["/big"] = np.random.default_rng(1).standard_normal((64, 64, 64))
+    src, h5 = str(tmp_path / "x.ipgc"), str(tmp_path / "x.h5")
+    ipgc.write(src, {k: v for k, v in ent.items() if v is not None or k == "/e"}, strlen={"/s": 20})
+    ip.convert_container(src, h5)
+    _spec_same(ent, h5_spec_reader.read(h5))
+
+
+def test_image_file_decodes_with_an_independent_reader(tmp_path):
+    """an ipole image as ipg_write_image lays it out (io.c:140-273 schema),
+    converted to HDF5 by the library, read back by the independent decoder"""
+    from tests import h5_spec_reader
+    rng = np.random.default_rng(3)
+    ent = {"/pol": rng.random((8, 6, 5)), "/unpol": rng.random((8, 6)), "/tau": rng.random((8, 6)),
+           "/Ftot": np.float64(0.6), "/Ftot_unpol": np.float64(0.61), "/nuLnu": np.float64(1e34),
+           "/header/camera/nx": np.int32(8), "/header/camera/ny": np.int32(6), "/header/freqcgs": np.float64(2.3e11),
+           "/header/version": "1.0", "/header/scale": np.float64(58.7), "/header/units/M_unit": np.float64(7.96e27),
+           "/fluid_header/geom/mmks/a": np.float64(0.9375)}
+    src, h5 = str(tmp_path / "img.ipgc"), str(tmp_path / "img.h5")
+    ipgc.write(src, ent, strlen={"/header/version": 8})
+    ip.convert_container(src, h5)
+    dec = h5_spec_reader.read(h5)
+    groups = {k for k in dec if dec[k] is None}
+    assert groups == {"/header", "/header/camera", "/header/units", "/fluid_header", "/fluid_header/geom",
+                      "/fluid_header/geom/mmks"}
+    _spec_same(ent, {k: v for k, v in dec.items() if k not in groups})
