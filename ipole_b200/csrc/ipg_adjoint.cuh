@@ -45,6 +45,8 @@
  * Included by ipg_kernels.cu.
  */
 
+#include "ipg_step_vjp.cuh"
+
 /* gradient of a Hermitian N: g.r[ij] = dL/dRe N[i][j] = dL/dRe N[j][i],
  * g.s[ij] = dL/dIm N[i][j] = -dL/dIm N[j][i] (the same layout as HermN) */
 typedef HermN GradN;
@@ -193,15 +195,8 @@ __device__ __forceinline__ void evolve_adj(const CoefBlock &cb, double dlam, int
   const double u[4] = {g11 + g22, g11 - g22, g12, g21};
   double cv[8];
   coef_values(cb, zero_emission, cv);
-  double gS[4], gA[4], gB[4];
-  step_vjp_pass(S0, cv, dlam, u, 0, gS);
-  step_vjp_pass(S0, cv, dlam, u, 4, gA);
-  step_vjp_pass(S0, cv, dlam, u, 8, gB);
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    gc[k] = gA[k];
-    gc[4 + k] = gB[k];
-  }
+  double gS[4];
+  stokes_step_vjp(cv, dlam, S0, u, gS, gc);
   if (zero_emission) gc[0] = gc[1] = gc[2] = 0.;
   /* d/dT: directly (-d) and through S = (T11+T22, T11-T22)/2, T12r, T21i */
   const double t11 = -g11 + 0.5 * (gS[0] + gS[1]);
@@ -440,6 +435,120 @@ __global__ void __launch_bounds__(128, 3)
     fluid_scatter(fields, adj_side + ((size_t)c * IPG_CHUNK_STEPS + slot) * IPG_ADJ_DOUBLES, C.emission_type, gc,
                   g_ne, g_th, g_b);
   }
+}
+
+/* Self-check of stokes_step_vjp against the forward-mode dual numbers
+ * (step_vjp_pass, three passes of four directions) on seeded coefficients
+ * and Stokes vectors in four regimes: 0 no polarized absorption
+ * (approximate_solve), 1 no Faraday rotation, 2 both, 3 optically thin
+ * steps (tau ~ 1e-7: absorb_emit's small-tau series).  err[i] = the largest
+ * difference over the twelve gradients, each relative to its own size plus
+ * 1e-9 of the largest gradient of its group (Stokes inputs, emissivities,
+ * absorptivities, rotativities).  In regime 3 absorb_emit divides by
+ * a_P^2 ~ 1e-17, and both forms carry the cancellation that follows. */
+__device__ __forceinline__ double vjp_rand(unsigned long long seed, int i, int k)
+{
+  unsigned long long z = seed * 0x9e3779b97f4a7c15ULL + (unsigned long long)i * 0xbf58476d1ce4e5b9ULL + (unsigned)k;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1. / 9007199254740992.); /* [0, 1) */
+}
+
+__global__ void k_check_step_vjp(int n, unsigned long long seed, double *__restrict__ err, double *__restrict__ info)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = pow(10., -3. + 4. * vjp_rand(seed, i, 0));
+  const double aI = pow(10., -5. + 6. * vjp_rand(seed, i, 1));
+  const int regime = (int)(vjp_rand(seed, i, 2) * 4.);
+  double fq = 2. * vjp_rand(seed, i, 3) - 1., fv = 2. * vjp_rand(seed, i, 4) - 1.;
+  const double nf = sqrt(fq * fq + fv * fv) + 1e-300;
+  const double pf = 0.98 * vjp_rand(seed, i, 5); /* |a_P| < a_I */
+  double aQ = regime == 0 ? 0. : aI * pf * fq / nf, aV = regime == 0 ? 0. : aI * pf * fv / nf;
+  const double jI = pow(10., -3. + 4. * vjp_rand(seed, i, 6));
+  const double jQ = jI * (2. * vjp_rand(seed, i, 7) - 1.) * 0.7, jV = jI * (2. * vjp_rand(seed, i, 8) - 1.) * 0.3;
+  double rQ = pow(10., -4. + 6. * vjp_rand(seed, i, 9)) * (vjp_rand(seed, i, 10) < 0.5 ? -1. : 1.);
+  double rV = pow(10., -4. + 6. * vjp_rand(seed, i, 11)) * (vjp_rand(seed, i, 12) < 0.5 ? -1. : 1.);
+  if (regime == 1) rQ = rV = 0.;
+  if (regime == 3) { /* small optical depths: the series */
+    const double s = 1e-7 / (aI * x);
+    aQ *= s;
+    aV *= s;
+  }
+  const double aIx = regime == 3 ? 1e-7 / x : aI;
+  const double cv[8] = {jI, jQ, jV, aIx, aQ, aV, rQ, rV};
+  const double SI = pow(10., -2. + 3. * vjp_rand(seed, i, 13));
+  const double S0[4] = {SI, SI * (2. * vjp_rand(seed, i, 14) - 1.) * 0.5, SI * (2. * vjp_rand(seed, i, 15) - 1.) * 0.5,
+                        SI * (2. * vjp_rand(seed, i, 16) - 1.) * 0.3};
+  const double u[4] = {2. * vjp_rand(seed, i, 17) - 1., 2. * vjp_rand(seed, i, 18) - 1.,
+                       2. * vjp_rand(seed, i, 19) - 1., 2. * vjp_rand(seed, i, 20) - 1.};
+  double gS[4], gc[8], dS[4], dA[4], dB[4];
+  stokes_step_vjp(cv, x, S0, u, gS, gc);
+  step_vjp_pass(S0, cv, x, u, 0, dS);
+  step_vjp_pass(S0, cv, x, u, 4, dA);
+  step_vjp_pass(S0, cv, x, u, 8, dB);
+  const double a[12] = {gS[0], gS[1], gS[2], gS[3], gc[0], gc[1], gc[2], gc[3], gc[4], gc[5], gc[6], gc[7]};
+  const double b[12] = {dS[0], dS[1], dS[2], dS[3], dA[0], dA[1], dA[2], dA[3], dB[0], dB[1], dB[2], dB[3]};
+  /* each gradient against its own size and the scale of its group (the
+   * Stokes inputs, the emissivities, the absorptivities, the rotativities) */
+  const int grp[12] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3};
+  double sc[4] = {0., 0., 0., 0.};
+  for (int k = 0; k < 12; k++) sc[grp[k]] = fmax(sc[grp[k]], fabs(b[k]));
+  double e = 0.;
+  int kw = 0;
+  for (int k = 0; k < 12; k++) {
+    const double d = fabs(a[k] - b[k]), den = fabs(b[k]) + 1e-9 * sc[grp[k]] + 1e-300;
+    const double r = (d != d) ? 1e300 : d / den;
+    if (r > e) {
+      e = r;
+      kw = k;
+    }
+  }
+  err[i] = e;
+  /* the case itself: gradient index, both values, regime, x, the eight
+   * coefficients and the Stokes vector */
+  double *q = info + (size_t)i * 24;
+  q[0] = kw;
+  q[1] = a[kw];
+  q[2] = b[kw];
+  q[3] = regime;
+  q[4] = x;
+  for (int k = 0; k < 8; k++) q[5 + k] = cv[k];
+  for (int k = 0; k < 4; k++) q[13 + k] = S0[k];
+  q[17] = sc[grp[kw]];
+  q[18] = u[0];
+  q[19] = u[1];
+  q[20] = u[2];
+  q[21] = u[3];
+}
+
+extern "C" int ipg__check_step_vjp(int device, int n, unsigned long long seed, double max_err[4], double worst[96])
+{
+  ipg_ctx *ctx = NULL;
+  if (n <= 0 || !max_err) return IPG_E_ARG;
+  CK(cudaSetDevice(device));
+  double *d = NULL;
+  CK(cudaMalloc(&d, (size_t)n * 25 * sizeof(double)));
+  k_check_step_vjp<<<(n + 127) / 128, 128>>>(n, seed, d, d + n);
+  cudaError_t e = cudaGetLastError();
+  std::vector<double> h((size_t)n * 25);
+  if (e == cudaSuccess) e = cudaMemcpy(h.data(), d, (size_t)n * 25 * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return IPG_E_CUDA;
+  int im[4] = {0, 0, 0, 0};
+  for (int r = 0; r < 4; r++) max_err[r] = -1.;
+  for (int i = 0; i < n; i++) {
+    const int r = (int)h[n + (size_t)i * 24 + 3];
+    if (r >= 0 && r < 4 && h[i] > max_err[r]) {
+      max_err[r] = h[i];
+      im[r] = i;
+    }
+  }
+  if (worst)
+    for (int r = 0; r < 4; r++)
+      for (int k = 0; k < 24; k++) worst[24 * r + k] = h[n + (size_t)im[r] * 24 + k];
+  return IPG_OK;
 }
 
 /* ===================================================================== */

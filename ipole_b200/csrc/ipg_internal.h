@@ -32,6 +32,9 @@ void **ipg__refine_slot(ipg_ctx *ctx);
 /* the step arithmetic of the context (ipg_set_step_precision): 1 for FP32 */
 int ipg__step32(const ipg_ctx *ctx);
 int ipg__fits32(const ipg_ctx *ctx);
+/* self-check of the adjoint's reverse-mode transfer step against forward
+ * dual numbers on n seeded cases; *max_err the largest relative difference */
+int ipg__check_step_vjp(int device, int n, unsigned long long seed, double max_err[4], double worst[96]);
 /* per-context storage of the batch driver (ipg_refine.cu); ipg_destroy
  * releases it with ipg__batch_arena_release */
 void **ipg__batch_arena_slot(ipg_ctx *ctx);
