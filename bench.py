@@ -575,6 +575,31 @@ def bench_adjoint(ip, ctx, model, p, args, world, stream):
     return res
 
 
+def run_leg(args):
+    """One call of the batched or the adjoint leg at --size (a profiling case;
+    no timing is printed)."""
+    import numpy as np
+
+    import ipole_b200 as ip
+    dump = ensure_dump(SMALL_DUMP if args.small else DUMP)
+    n = args.size
+    p = ip.Params.from_args(workload_args(dump, n, n, args.m_unit))
+    model = ip.Model.load(p)
+    with ip.Context(0, pool_bytes=int(args.pool_gb * (1 << 30))) as ctx:
+        if args.leg == "batched":
+            ps = batch_params(ip, dump, args.m_unit, n)
+            ctx.upload_batch(model)
+            ctx.render_batch(ps, model)
+        else:
+            ctx.upload(model)
+            img = ctx.render(p, model)
+            scale = float(np.abs(img.pol[..., 0]).max())
+            ctx.adjoint_image(p, model, img.pol[..., :4] / (scale * scale), ckpt=16)
+        st = ctx.stats()
+        print(json.dumps({"leg": args.leg, "size": n, "ray_steps": st["ray_steps"], "waves": st["waves"]}))
+    return 0
+
+
 def run_one_ray(args):
     """One ray alone on the GPU: the geodesic and transfer kernels' device time
     divided by its steps is the step latency of a lone lane, which bounds the
@@ -622,11 +647,16 @@ def main():
                     help="step-record storage between the kernels (ipg_set_record_precision); with --quick only")
     ap.add_argument("--step", default="fp64", choices=["fp64", "fp32"],
                     help="arithmetic of the polarized step (ipg_set_step_precision); with --quick only")
+    ap.add_argument("--leg", default="", choices=["", "batched", "adjoint"],
+                    help="run one call of that leg at --size and nothing else (profiling case): the batch of 8 "
+                         "instances of the bench camera, or one adjoint image")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.ray:
         return run_one_ray(args)
+    if args.leg:
+        return run_leg(args)
     return run_ours(args)
 
 

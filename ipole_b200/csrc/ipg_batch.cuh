@@ -689,7 +689,7 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
   cudaStream_t st = ctx->stream;
   const int threads = 128;
   size_t pend_g = it->n_geo, pend_x = it->n_xf, wave = it->n_geo;
-  const int32_t *gl = NULL, *xl = it->xf_order;
+  const int32_t *gl = it->geo_order, *xl = it->xf_order;
   int cur = 0;
   while (pend_g > 0 || pend_x > 0) {
     size_t run = pend_g < wave ? pend_g : wave;

@@ -53,7 +53,11 @@ typedef struct ipg_batch_items {
   const int32_t *xf_slot;   /* [n_xf] instance slot in its group */
   ipg_pixel_out *xf_out;    /* [n_xf] get_pixel's outputs */
   const int32_t *xf_order;  /* [n_xf] the order in which the transfer takes the items (NULL: 0..n_xf-1) */
+  const int32_t *geo_order; /* [n_geo] the order in which the geodesics start (NULL: 0..n_geo-1) */
 } ipg_batch_items;
+/* the geodesic items in *sorted, longest predicted first (pred: n scratch) */
+int ipg__batch_sort_geo(ipg_ctx *ctx, const int32_t *geo_ij, const int32_t *geo_grp, size_t n, int maxnstep,
+                        int32_t *pred, int32_t *sorted);
 /* trace one level; *steps_left (NULL: no budget) is the remaining step
  * budget, decreased by the steps taken */
 int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *items, unsigned long long *steps_left);

@@ -512,15 +512,15 @@ __global__ void __launch_bounds__(TPB, MINB)
  * storing anything: a cheap prediction of the ray lengths, so that the full
  * trace can start the longest rays first.  pred[t] is the count of list
  * entry t; a ray whose position turns non-finite, or that passes step_cap,
- * stops there. */
-template <int P>
+ * stops there.  CS, ray_grp: the camera of each ray, as in k_geodesic. */
+template <int P, class CS = CamOne>
 __global__ void __launch_bounds__(128, IPG_GEO_MINB)
     k_geodesic_count(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list, double eps_scale,
-                     int step_cap, int32_t *__restrict__ pred, unsigned long long *__restrict__ counter)
+                     int step_cap, int32_t *__restrict__ pred, unsigned long long *__restrict__ counter,
+                     const int32_t *__restrict__ ray_grp)
 {
   const DevGrid &G = c_grid;
-  const DevCam &C = c_cam;
-  const double eps = C.eps * eps_scale;
+  double eps = 0.;
   double X[4], K[4], Xh[4], Kh[4], h = 0.;
   int t = -1, nstep = 0, phase = 0;
   bool has = false, drained = false;
@@ -532,7 +532,9 @@ __global__ void __launch_bounds__(128, IPG_GEO_MINB)
       if (has) {
         t = (int)q;
         int ray = list ? list[t] : t;
+        const DevCam &C = CS::get(ray_grp ? ray_grp[ray] : 0);
         init_ray(C, ij[2 * ray], ij[2 * ray + 1], X, K);
+        eps = C.eps * eps_scale;
         nstep = 0;
         phase = 0;
       }
@@ -1811,7 +1813,7 @@ static void launch_count_t(ipg_ctx *ctx, int threads, const int32_t *d_ij, const
 {
   int gb = grid_blocks(ctx, (const void *)k_geodesic_count<P>, threads, run);
   k_geodesic_count<P><<<gb, threads, 0, ctx->stream>>>(d_ij, list, (int)run, PRED_EPS_SCALE, cap, ctx->d_pred,
-                                                       counter);
+                                                       counter, nullptr);
 }
 #define SPLIT_MIN_RAYS 4096
 
@@ -1899,6 +1901,31 @@ static int sort_by_length(ipg_ctx *ctx, const int32_t *d_ij, size_t n, const ipg
   k_len_hist<<<sb, 256, 0, ctx->stream>>>(ctx->d_pred, (int)n, 0, ctx->d_len_hist);
   k_len_scan<<<1, LEN_SCAN_THREADS, 0, ctx->stream>>>(ctx->d_len_hist);
   k_len_scatter<<<sb, 256, 0, ctx->stream>>>(NULL, ctx->d_pred, (int)n, 0, ctx->d_len_hist, ctx->d_sorted);
+  CK(cudaGetLastError());
+  return IPG_OK;
+}
+
+/* The geodesic items of a batch level in *sorted, longest predicted first
+ * (k_geodesic_count with the batch's camera table; pred: n scratch ints).
+ * Enqueued on the context's stream after ipg__batch_begin. */
+extern "C" int ipg__batch_sort_geo(ipg_ctx *ctx, const int32_t *geo_ij, const int32_t *geo_grp, size_t n,
+                                   int maxnstep, int32_t *pred, int32_t *sorted)
+{
+  if (!n) return IPG_OK;
+  const int threads = 128;
+  unsigned long long *cnt = ctx->d_cnt;
+  CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * CNT_N, ctx->stream));
+  int cap = (int)(maxnstep / PRED_EPS_SCALE) + 1;
+  if (cap > LEN_BUCKETS - 1) cap = LEN_BUCKETS - 1;
+  int gb = grid_blocks(ctx, (const void *)k_geodesic_count<IPG_PLUG_IHARM, CamTable>, threads, n);
+  k_geodesic_count<IPG_PLUG_IHARM, CamTable><<<gb, threads, 0, ctx->stream>>>(
+      geo_ij, NULL, (int)n, PRED_EPS_SCALE, cap, pred, cnt + CNT_NEXT_G, geo_grp);
+  CK(cudaMemsetAsync(ctx->d_len_hist, 0, LEN_BUCKETS * sizeof(int), ctx->stream));
+  int sb = (int)((n + 255) / 256);
+  if (sb > 4 * ctx->n_sm) sb = 4 * ctx->n_sm;
+  k_len_hist<<<sb, 256, 0, ctx->stream>>>(pred, (int)n, 0, ctx->d_len_hist);
+  k_len_scan<<<1, LEN_SCAN_THREADS, 0, ctx->stream>>>(ctx->d_len_hist);
+  k_len_scatter<<<sb, 256, 0, ctx->stream>>>(NULL, pred, (int)n, 0, ctx->d_len_hist, sorted);
   CK(cudaGetLastError());
   return IPG_OK;
 }

@@ -651,12 +651,18 @@ __global__ void k_xf_map(const int32_t *ij, int n, int nj, int nsx, int nsy, con
 /* The transfer order: items grouped by geodesic item, by slot within it, so
  * that the instances that trace one pixel sit in adjacent lanes and walk its
  * records in step (one load of the shared record serves them all, and their
- * coefficient blocks are contiguous).  cnt[g] = instances tracing item g;
- * off = its exclusive scan; order[off[g] + rank of the slot] = item. */
-__global__ void k_geo_count(const uint32_t *mask, int n, int32_t *cnt)
+ * coefficient blocks are contiguous); the geodesic items in the order their
+ * geodesics start (longest predicted first).  cnt[r] = instances tracing the
+ * r-th item of that order; off = its exclusive scan; order[off[rank of g] +
+ * rank of the slot] = item. */
+__global__ void k_geo_count(const uint32_t *mask, const int32_t *sorted, int n, int32_t *cnt, int32_t *rank)
 {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) cnt[t] = __popc(mask[t]);
+  if (t < n) {
+    const int g = sorted[t];
+    cnt[t] = __popc(mask[g]);
+    rank[g] = t;
+  }
 }
 
 __global__ void __launch_bounds__(SCAN_TPB) k_geo_offsets(const int32_t *cnt, int n, const int32_t *block_sums,
@@ -668,12 +674,12 @@ __global__ void __launch_bounds__(SCAN_TPB) k_geo_offsets(const int32_t *cnt, in
 }
 
 __global__ void k_xf_order(const int32_t *xf_geo, const int32_t *xf_slot, const uint32_t *mask, const int32_t *off,
-                           int n, int32_t *order)
+                           const int32_t *rank, int n, int32_t *order)
 {
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
   const int g = xf_geo[m], k = xf_slot[m];
-  order[off[g] + __popc(mask[g] & ((1u << k) - 1u))] = m;
+  order[off[rank[g]] + __popc(mask[g] & ((1u << k) - 1u))] = m;
 }
 
 namespace {
@@ -746,8 +752,10 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
   /* camera groups and electron models */
   std::vector<int> grp_of(n), set_of(n);
   std::vector<int> grp_rep, set_rep;
+  int maxnstep_all = 2; /* the step cap of the length prediction */
   for (size_t i = 0; i < n; i++) {
     const ipg_instance &a = inst[i];
+    if (a.cam.maxnstep > maxnstep_all) maxnstep_all = a.cam.maxnstep;
     if (a.nx < 2 || a.ny < 2 || a.nx_min < 2 || a.ny_min < 2 || a.refine_level < 1 || !outs[i].image ||
         !outs[i].taus || !outs[i].interp_flag || !outs[i].oddflag || !outs[i].nstep ||
         (!a.cam.only_unpolarized && !outs[i].imageS) || (size_t)a.nx * a.ny >= (size_t)INT_MAX / 2)
@@ -832,6 +840,7 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
   int32_t *ij_all = nullptr, *xf_geo = nullptr, *xf_slot = nullptr, *geo_ij = nullptr, *geo_grp = nullptr;
   uint32_t *geo_mask = nullptr;
   int32_t *geo_cnt = nullptr, *geo_bsums = nullptr, *geo_off = nullptr, *xf_order = nullptr;
+  int32_t *geo_sorted = nullptr, *geo_rank = nullptr, *geo_pred = nullptr;
   RefineStatus *ord_st = nullptr;
   ipg_pixel_out *xf_out = nullptr;
   std::vector<int32_t *> gflags(ngrp);
@@ -874,6 +883,9 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
     geo_off = A.take<int32_t>(sum_gpix);
     xf_order = A.take<int32_t>(sum_pix);
     ord_st = A.take<RefineStatus>(1);
+    geo_sorted = A.take<int32_t>(sum_gpix);
+    geo_rank = A.take<int32_t>(sum_gpix);
+    geo_pred = A.take<int32_t>(sum_gpix);
     if (pass == 0 && ar->bytes < A.off) {
       cudaFree(ar->dev);
       ar->dev = nullptr;
@@ -1008,15 +1020,16 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
     }
     {
       const int ng = (int)n_geo, nb = grid_of(ng, SCAN_TPB);
-      k_geo_count<<<grid_of(ng, TPB), TPB, 0, s>>>(geo_mask, ng, geo_cnt);
+      if ((rc = ipg__batch_sort_geo(ctx, geo_ij, geo_grp, n_geo, maxnstep_all, geo_pred, geo_sorted))) return rc;
+      k_geo_count<<<grid_of(ng, TPB), TPB, 0, s>>>(geo_mask, geo_sorted, ng, geo_cnt, geo_rank);
       k_scan_blocks<<<nb, SCAN_TPB, 0, s>>>(geo_cnt, ng, geo_bsums);
       k_scan_top<<<1, SCAN_TPB, 0, s>>>(geo_bsums, nb, ord_st);
       k_geo_offsets<<<nb, SCAN_TPB, 0, s>>>(geo_cnt, ng, geo_bsums, geo_off);
-      if (n_xf) k_xf_order<<<grid_of((long long)n_xf, TPB), TPB, 0, s>>>(xf_geo, xf_slot, geo_mask, geo_off, (int)n_xf,
-                                                                      xf_order);
+      if (n_xf) k_xf_order<<<grid_of((long long)n_xf, TPB), TPB, 0, s>>>(xf_geo, xf_slot, geo_mask, geo_off, geo_rank,
+                                                                      (int)n_xf, xf_order);
     }
     CKR(cudaGetLastError());
-    ipg_batch_items items = {n_geo, geo_ij, geo_grp, geo_mask, n_xf, xf_geo, xf_slot, xf_out, xf_order};
+    ipg_batch_items items = {n_geo, geo_ij, geo_grp, geo_mask, n_xf, xf_geo, xf_slot, xf_out, xf_order, geo_sorted};
     rc = ipg__batch_trace(ctx, &items, step_budget ? &steps_left : nullptr);
     if (rc) return rc;
     /* save_pixel, the checks and (base level) the flux estimate per instance */
