@@ -491,6 +491,7 @@ def bench_batched(ip, ctx, model, dump, args, world, stream, single_ms):
     for name, step32, fits32 in (("fp64", False, False), ("fp32_step", True, False), ("mixed", True, True)):
         ctx.set_step_precision(ip.IPG_STEP_FP32 if step32 else ip.IPG_STEP_FP64)
         ctx.set_fit_precision(ip.IPG_FITS_FP32 if fits32 else ip.IPG_FITS_FP64)
+        ctx.set_record_precision(ip.IPG_RECORDS_MIXED if fits32 else ip.IPG_RECORDS_FP64)
         ctx.render_batch(ps, model)
         torch.cuda.synchronize()
         barrier(world)
@@ -518,6 +519,7 @@ def bench_batched(ip, ctx, model, dump, args, world, stream, single_ms):
             fp64_imgs = imgs
     ctx.set_step_precision(ip.IPG_STEP_FP64)
     ctx.set_fit_precision(ip.IPG_FITS_FP64)
+    ctx.set_record_precision(ip.IPG_RECORDS_FP64)
     res["workload"] = (f"{len(ps)} instances of the bench image's camera ({nx}x{nx}, 230 GHz, thetacam 163): "
                        f"R_high {list(BATCH_RHIGH)} x M_unit {list(BATCH_MU)} x {args.m_unit:g}")
     if args.size == NX and not args.small:

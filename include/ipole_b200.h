@@ -362,7 +362,9 @@ int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
  * rotation coefficients in FP64; all arithmetic stays FP64, and the walk back
  * reads 320 bytes per step instead of 512.  Its images differ from the FP64
  * records' by the FP32 rounding of those values (the test of this mode states
- * the errors); ipg_trace_ray and ipg_trace_pixels_noalloc always use FP64.
+ * the errors).  Batches (ipg_render_batch) store their shared records in the
+ * same compact layout, the instances' coefficient blocks in FP64;
+ * ipg_trace_ray, ipg_trace_pixels_noalloc and ipg_adjoint always use FP64.
  * Returns IPG_E_ARG for another value. */
 #define IPG_RECORDS_FP64 0
 #define IPG_RECORDS_MIXED 1

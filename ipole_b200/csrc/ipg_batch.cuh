@@ -148,7 +148,25 @@ __global__ void k_derive(const double *__restrict__ rho, const double *__restric
  * shared part goes into the record in place (flags, tetrad rows; dl and
  * nturns keep their slots), the instances' coefficients into their blocks
  * of the side pool: side[((chunk * 32 + slot) * G + k) * IPG_BCOEF]. */
-template <int EM, bool F32 = false>
+/* the shared part of a record in the compact layout (IPG_RECORDS_MIXED):
+ * flags, dl and nturns in the coefficient block, the tetrad rows in FP32
+ * over the geodesic state (read before) */
+__device__ __forceinline__ void store_shared_m(double *p, int flags, double dl, double nturns, const double e1[4],
+                                               const double e2[4], const double a[4], const double b[4])
+{
+  double *q = p + RECM_COEF;
+  store4(q, (double)flags, 0., 0., dl);
+  store4(q + 4, 0., 0., 0., 0.);
+  store4(q + 8, 0., 0., nturns, 0.);
+  store4(q + 12, 0., 0., 0., 0.);
+  float4 *t = reinterpret_cast<float4 *>(reinterpret_cast<float *>(p) + RECM_TETF);
+  t[0] = make_float4((float)e1[0], (float)e1[1], (float)e1[2], (float)e1[3]);
+  t[1] = make_float4((float)e2[0], (float)e2[1], (float)e2[2], (float)e2[3]);
+  t[2] = make_float4((float)a[0], (float)a[1], (float)a[2], (float)a[3]);
+  t[3] = make_float4((float)b[0], (float)b[1], (float)b[2], (float)b[3]);
+}
+
+template <int EM, bool F32 = false, bool RM = false>
 __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     k_coef_batch(double *__restrict__ pool, double *__restrict__ side, int G, const int2 *__restrict__ chunk_meta,
                  const unsigned long long *__restrict__ counters, long long n_chunks, const RayRec *__restrict__ rays,
@@ -173,6 +191,9 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     double X1 = p[REC_X1], X2 = p[REC_X2], X3 = p[REC_X3];
     double K[4];
     load4(p + REC_K, K);
+    /* RM: dl and nturns move out of the geodesic state, which the compact
+     * tetrad rows overwrite */
+    const double dl_rec = RM ? p[REC_DL] : 0., nturns_rec = RM ? p[REC_NTURNS] : 0.;
     PointGeo pg;
     point_geo<IPG_MET_FMKS>(X1, X2, &pg);
     int flags = radiating_t<IPG_PLUG_IHARM>(pg) ? 1 : 0;
@@ -184,6 +205,11 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     }
     if (!((flags & 1) || s == rec.nstep)) {
       /* no coefficients here: the transfer reads only the flags */
+      if constexpr (RM) {
+        const double z[4] = {0., 0., 0., 0.};
+        store_shared_m(p, flags, dl_rec, nturns_rec, z, z, z, z);
+        continue;
+      }
       p[REC_FLAGS] = (double)flags;
       store4(p + REC_E1COV, 0., 0., 0., 0.);
       store4(p + REC_E2COV, 0., 0., 0., 0.);
@@ -223,11 +249,15 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
         flags |= tf << 2;
       }
       /* the shared part first: the tetrad is dead before the slot loop */
-      p[REC_FLAGS] = (double)flags;
-      store4(p + REC_E1COV, e1[0], e1[1], e1[2], e1[3]);
-      store4(p + REC_E2COV, e2[0], e2[1], e2[2], e2[3]);
-      store4(p + REC_E1CON, Econ[1][0], Econ[1][1], Econ[1][2], Econ[1][3]);
-      store4(p + REC_E2CON, Econ[2][0], Econ[2][1], Econ[2][2], Econ[2][3]);
+      if constexpr (RM) {
+        store_shared_m(p, flags, dl_rec, nturns_rec, e1, e2, Econ[1], Econ[2]);
+      } else {
+        p[REC_FLAGS] = (double)flags;
+        store4(p + REC_E1COV, e1[0], e1[1], e1[2], e1[3]);
+        store4(p + REC_E2COV, e2[0], e2[1], e2[2], e2[3]);
+        store4(p + REC_E1CON, Econ[1][0], Econ[1][1], Econ[1][2], Econ[1][3]);
+        store4(p + REC_E2CON, Econ[2][0], Econ[2][1], Econ[2][2], Econ[2][3]);
+      }
     }
     double *q0 = side + ((size_t)c * IPG_CHUNK_STEPS + slot) * G * IPG_BCOEF;
     for (uint32_t m = geo_mask[meta.x]; m; m &= m - 1) {
@@ -291,6 +321,38 @@ __device__ __forceinline__ void load_coef_b(const double *__restrict__ p, const 
 static_assert(REC_FLAGS % 2 == 0 && REC_DL == REC_FLAGS + 3 && REC_E1COV % 2 == 0 && REC_E2CON == REC_E1COV + 12,
               "load_coef_b follows the record layout");
 
+/* the same from a compact shared record (store_shared_m) */
+__device__ __forceinline__ void load_coef_bm(const double *__restrict__ p, const double *__restrict__ q, CoefBlock &c)
+{
+  const double2 *r = reinterpret_cast<const double2 *>(p + RECM_COEF);
+  const double2 h0 = r[0], h1 = r[1], h5 = r[5];
+  c.flags = h0.x;
+  c.dl = h1.y;
+  c.nturns = h5.x;
+  const float4 *t = reinterpret_cast<const float4 *>(reinterpret_cast<const float *>(p) + RECM_TETF);
+  float4 w[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) w[k] = t[k];
+  c.e1[0] = w[0].x; c.e1[1] = w[0].y; c.e1[2] = w[0].z; c.e1[3] = w[0].w;
+  c.e2[0] = w[1].x; c.e2[1] = w[1].y; c.e2[2] = w[1].z; c.e2[3] = w[1].w;
+  c.a[0] = w[2].x; c.a[1] = w[2].y; c.a[2] = w[2].z; c.a[3] = w[2].w;
+  c.b[0] = w[3].x; c.b[1] = w[3].y; c.b[2] = w[3].z; c.b[3] = w[3].w;
+  const double2 *b2 = reinterpret_cast<const double2 *>(q);
+  double2 v[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) v[k] = b2[k];
+  c.ju = v[0].x;
+  c.ku = v[0].y;
+  c.jI = v[1].x;
+  c.jQ = v[1].y;
+  c.jV = v[2].x;
+  c.aI = v[2].y;
+  c.aQ = v[3].x;
+  c.aV = v[3].y;
+  c.rQ = v[4].x;
+  c.rV = v[4].y;
+}
+
 struct XbLane {
   HermN N;
   const double *rec_i;
@@ -307,6 +369,7 @@ __device__ __forceinline__ const double *side_ptr(const double *side, int G, int
 /* next (instance, ray) item whose geodesic is complete; items whose
  * geodesic was deferred go to the next wave's list; after the step budget
  * is spent no new item starts */
+template <bool RM>
 __device__ __forceinline__ bool xb_fetch(XbLane &L, const int32_t *__restrict__ list, int n_list,
                                          const double *__restrict__ pool, const double *__restrict__ side, int G,
                                          const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays,
@@ -347,13 +410,13 @@ __device__ __forceinline__ bool xb_fetch(XbLane &L, const int32_t *__restrict__ 
     L.chunk = rec.last_chunk;
     L.rec_i = step_ptr(const_cast<double *>(pool), L.chunk, L.n % IPG_CHUNK_STEPS);
     L.cprev = chunk_prev[L.chunk];
-    prefetch_rec<0>(L.rec_i);
+    prefetch_rec<RM>(L.rec_i);
     /* get_jkinv at the far end of the ray, src/ipolarray.c:74 */
     const double *q = side_ptr(side, G, L.chunk, L.n % IPG_CHUNK_STEPS, L.kslot);
     L.js = q[0];
     L.ks = q[1];
-    L.dl_i = L.rec_i[REC_DL];
-    L.nturns_i = L.rec_i[REC_NTURNS];
+    L.dl_i = L.rec_i[RM ? RECM_COEF + 3 : REC_DL];
+    L.nturns_i = L.rec_i[RM ? RECM_COEF + 10 : REC_NTURNS];
     L.I = L.tau = L.tauF = 0.;
     hn_zero(&L.N);
     L.flag = 0;
@@ -362,7 +425,7 @@ __device__ __forceinline__ bool xb_fetch(XbLane &L, const int32_t *__restrict__ 
   }
 }
 
-template <int TPB, bool S32>
+template <int TPB, bool S32, bool RM = false>
 __global__ void __launch_bounds__(TPB, 1)
     k_xfer_batch(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
                  const double *__restrict__ side, int G, const int *__restrict__ chunk_prev,
@@ -372,7 +435,7 @@ __global__ void __launch_bounds__(TPB, 1)
                  int32_t *__restrict__ xdeferred)
 {
   XbLane L;
-  bool has = xb_fetch(L, list, n_list, pool, side, G, chunk_prev, rays, xf_geo, xf_slot, geo_grp, out, counters,
+  bool has = xb_fetch<RM>(L, list, n_list, pool, side, G, chunk_prev, rays, xf_geo, xf_slot, geo_grp, out, counters,
                       xdeferred);
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
@@ -385,7 +448,7 @@ __global__ void __launch_bounds__(TPB, 1)
       out[L.item] = o;
       atomicAdd(&counters[CNT_RAD], (unsigned long long)L.nrad);
       atomicAdd(&counters[CNT_XSTEPS], (unsigned long long)nstep);
-      has = xb_fetch(L, list, n_list, pool, side, G, chunk_prev, rays, xf_geo, xf_slot, geo_grp, out, counters,
+      has = xb_fetch<RM>(L, list, n_list, pool, side, G, chunk_prev, rays, xf_geo, xf_slot, geo_grp, out, counters,
                      xdeferred);
       continue;
     }
@@ -397,12 +460,15 @@ __global__ void __launch_bounds__(TPB, 1)
     }
     const double *rec_f = step_ptr(const_cast<double *>(pool), L.chunk, s % IPG_CHUNK_STEPS);
     if (s >= 1) {
-      if ((s - 1) % IPG_CHUNK_STEPS != IPG_CHUNK_STEPS - 1) prefetch_rec<0>(rec_f - IPG_STEP_DOUBLES);
-      else if (L.cprev >= 0) prefetch_rec<0>(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
+      if ((s - 1) % IPG_CHUNK_STEPS != IPG_CHUNK_STEPS - 1) prefetch_rec<RM>(rec_f - IPG_STEP_DOUBLES);
+      else if (L.cprev >= 0) prefetch_rec<RM>(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
     }
     CoefBlock cb;
-    load_coef_b(rec_f, side_ptr(side, G, L.chunk, s % IPG_CHUNK_STEPS, L.kslot), cb);
-    xfer_step<S32, 0>(C, L, cb, unpol);
+    if constexpr (RM)
+      load_coef_bm(rec_f, side_ptr(side, G, L.chunk, s % IPG_CHUNK_STEPS, L.kslot), cb);
+    else
+      load_coef_b(rec_f, side_ptr(side, G, L.chunk, s % IPG_CHUNK_STEPS, L.kslot), cb);
+    xfer_step<S32, RM ? 1 : 0>(C, L, cb, unpol);
     L.dl_i = cb.dl;
     L.nturns_i = cb.nturns;
     L.rec_i = rec_f;
@@ -459,7 +525,7 @@ struct BatchState {
   BatchModel m;
   BatchWs w;
   int G; /* instance slots per group of the current batch */
-  int emission_type, step32, unpol;
+  int emission_type, step32, unpol, rec_mixed;
   int xfer_threads; /* transfer block size (128 or 256) */
   /* the transfer block size is tuned per batch shape (slots per group,
    * groups): the first call of a shape runs 128 threads, the second 256,
@@ -575,7 +641,7 @@ extern "C" int ipg__batch_begin(ipg_ctx *ctx, const ipg_camera *grp_cam, int ngr
     }
     if (grp_cam[g].maxnstep < 2 || grp_cam[g].nx <= 0 || grp_cam[g].ny <= 0) return IPG_E_ARG;
     make_devcam(&grp_cam[g], &dcs[g]);
-    dcs[g].mixed = 0;
+    dcs[g].mixed = ctx->rec_mixed; /* the shared records' layout (the coefficient blocks stay FP64) */
   }
   int rc = ensure_pool(ctx);
   if (rc) return rc;
@@ -610,6 +676,7 @@ extern "C" int ipg__batch_begin(ipg_ctx *ctx, const ipg_camera *grp_cam, int ngr
   B->emission_type = em;
   B->unpol = unpol;
   B->step32 = step32;
+  B->rec_mixed = ctx->rec_mixed;
   /* block-size tuning: close the previous call's sample, pick this call's */
   if (B->tune_calls > 0 && B->tune_calls <= 2 && B->call_items > 0) {
     B->tune_ms[B->tune_calls - 1] = B->call_xfer_ms;
@@ -657,10 +724,10 @@ static int batch_ws_reserve(ipg_ctx *ctx, BatchWs &w, size_t n_geo, size_t n_xf)
   return IPG_OK;
 }
 
-#define IPG_LAUNCH_XB(TPB, S32)                                                                                  \
+#define IPG_LAUNCH_XB(TPB, S32, RMC)                                                                                  \
   do {                                                                                                          \
-    int tb = grid_blocks(ctx, (const void *)k_xfer_batch<TPB, S32>, TPB, pend_x);                               \
-    k_xfer_batch<TPB, S32><<<tb, TPB, 0, st>>>(xl, (int)pend_x, pool, side, G, ctx->d_chunk_prev, W.rays,      \
+    int tb = grid_blocks(ctx, (const void *)k_xfer_batch<TPB, S32, RMC>, TPB, pend_x);                               \
+    k_xfer_batch<TPB, S32, RMC><<<tb, TPB, 0, st>>>(xl, (int)pend_x, pool, side, G, ctx->d_chunk_prev, W.rays,      \
                                                 it->xf_geo, it->xf_slot, it->geo_grp, it->xf_out, W.cnt, xnext); \
   } while (0)
 
@@ -715,33 +782,47 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
         it->geo_grp);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], st));
-#define IPG_LAUNCH_BCOEF(EMT, F)                                                                              \
+#define IPG_LAUNCH_BCOEF(EMT, F, RMC)                                                                              \
   do {                                                                                                       \
-    int cb = grid_blocks(ctx, (const void *)k_coef_batch<EMT, F>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS); \
-    k_coef_batch<EMT, F><<<cb, threads, 0, st>>>(pool, side, G, ctx->d_chunk_meta, W.cnt, n_chunks, W.rays,  \
+    int cb = grid_blocks(ctx, (const void *)k_coef_batch<EMT, F, RMC>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS); \
+    k_coef_batch<EMT, F, RMC><<<cb, threads, 0, st>>>(pool, side, G, ctx->d_chunk_meta, W.cnt, n_chunks, W.rays,  \
                                                  it->geo_grp, it->geo_mask, B->m.fourv, B->m.sets,          \
                                                  (long long)B->m.ncell);                                      \
   } while (0)
     if (B->emission_type == 1) {
-      if (ctx->fits32)
-        IPG_LAUNCH_BCOEF(1, true);
-      else
-        IPG_LAUNCH_BCOEF(1, false);
+      if (ctx->fits32) {
+        if (B->rec_mixed) IPG_LAUNCH_BCOEF(1, true, true);
+        else IPG_LAUNCH_BCOEF(1, true, false);
+      } else {
+        if (B->rec_mixed) IPG_LAUNCH_BCOEF(1, false, true);
+        else IPG_LAUNCH_BCOEF(1, false, false);
+      }
     } else {
-      if (ctx->fits32)
-        IPG_LAUNCH_BCOEF(4, true);
-      else
-        IPG_LAUNCH_BCOEF(4, false);
+      if (ctx->fits32) {
+        if (B->rec_mixed) IPG_LAUNCH_BCOEF(4, true, true);
+        else IPG_LAUNCH_BCOEF(4, true, false);
+      } else {
+        if (B->rec_mixed) IPG_LAUNCH_BCOEF(4, false, true);
+        else IPG_LAUNCH_BCOEF(4, false, false);
+      }
     }
 #undef IPG_LAUNCH_BCOEF
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[2], st));
-    if (B->step32) {
-      if (B->xfer_threads == 256) IPG_LAUNCH_XB(256, true);
-      else IPG_LAUNCH_XB(128, true);
+    if (B->rec_mixed) {
+      if (B->step32) {
+        if (B->xfer_threads == 256) IPG_LAUNCH_XB(256, true, true);
+        else IPG_LAUNCH_XB(128, true, true);
+      } else {
+        if (B->xfer_threads == 256) IPG_LAUNCH_XB(256, false, true);
+        else IPG_LAUNCH_XB(128, false, true);
+      }
+    } else if (B->step32) {
+      if (B->xfer_threads == 256) IPG_LAUNCH_XB(256, true, false);
+      else IPG_LAUNCH_XB(128, true, false);
     } else {
-      if (B->xfer_threads == 256) IPG_LAUNCH_XB(256, false);
-      else IPG_LAUNCH_XB(128, false);
+      if (B->xfer_threads == 256) IPG_LAUNCH_XB(256, false, false);
+      else IPG_LAUNCH_XB(128, false, false);
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[3], st));

@@ -118,3 +118,28 @@ def test_batch_rejects_mixed_emission_types(c1_dump):
         with pytest.raises(ip.IpgError) as e:
             ctx.render_batch(ps, m)
         assert e.value.code == ip.IPG_E_ARG
+
+
+def test_mixed_tier_batch_equals_single_images(c1_dump):
+    """With compact step records, the FP32 step and the FP32 fit shapes set on
+    the context, every instance of a batch is the single image rendered with
+    the same settings, bit for bit (the shared records in the compact
+    layout, the instances' coefficient blocks in FP64)."""
+    ps = _instances(c1_dump)
+    base = ip.Model.load(ps[0])
+    with ip.Context() as ctx:
+        ctx.set_record_precision(ip.IPG_RECORDS_MIXED)
+        ctx.set_step_precision(ip.IPG_STEP_FP32)
+        ctx.set_fit_precision(ip.IPG_FITS_FP32)
+        ctx.upload_batch(base)
+        imgs = ctx.render_batch(ps, base)
+        bad = {}
+        for q, (p, img) in enumerate(zip(ps, imgs)):
+            m = ip.Model.load(p)
+            ctx.upload(m)
+            ref = ctx.render(p, m)
+            d = _diff(img, ref)
+            if d or img.traced != ref.traced:
+                bad[q] = (d, img.traced, ref.traced)
+        print("mixed tier: instances that differ from their single image:", bad)
+        assert not bad, bad
