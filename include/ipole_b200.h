@@ -181,11 +181,11 @@ int ipg_trace_pixels_device(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *
  * ipg_trace_pixels_device.
  *
  * The first call on a device sets the call up: it looks up the device address
- * of the scratch array, which may load the library's device code, so make
- * that first call before any stream capture begins.  The address is kept for
- * the life of the process, so resetting the device (cudaDeviceReset) between
- * calls is not supported.  Every call synchronises `stream` and copies a few
- * status words back to the host before it returns.  All calls share the
+ * of the scratch array, which may load the library's device code.  The
+ * address is kept for the life of the process, so resetting the device
+ * (cudaDeviceReset) between calls is not supported.  Every call synchronises
+ * `stream` and copies a few status words back to the host before it returns,
+ * so no call can be captured into a CUDA graph.  All calls share the
  * scratch array and the kernels' constant parameters, which keep what the last
  * call wrote: calls whose work overlaps on the GPU (from other streams or host
  * threads, or a context's ipg_trace_pixels* calls) race and give wrong
