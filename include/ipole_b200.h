@@ -351,6 +351,9 @@ typedef struct ipg_stats {
    * coeffs_ms and transfer_ms */
   double adjoint_ms;
   double adj_scatter_ms;
+  /* ipg_render_batch: geodesic items of the longest predicted class traced
+   * beside the waves (batches that take more than one wave) */
+  uint64_t long_class_items;
 } ipg_stats;
 int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 

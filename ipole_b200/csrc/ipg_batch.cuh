@@ -171,16 +171,18 @@ __global__ void __launch_bounds__(128, IPG_COEF_MINB)
     k_coef_batch(double *__restrict__ pool, double *__restrict__ side, int G, const int2 *__restrict__ chunk_meta,
                  const unsigned long long *__restrict__ counters, long long n_chunks, const RayRec *__restrict__ rays,
                  const int32_t *__restrict__ geo_grp, const uint32_t *__restrict__ geo_mask,
-                 const double *__restrict__ fourv, const double *__restrict__ sets, long long ncell)
+                 const double *__restrict__ fourv, const double *__restrict__ sets, long long ncell,
+                 long long c_first)
 {
   const DevGrid &Gd = c_grid;
   long long used = (long long)counters[CNT_POOL];
   if (used > n_chunks) used = n_chunks;
   const long long total = used * IPG_CHUNK_STEPS;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+  for (long long t = c_first * IPG_CHUNK_STEPS + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     int c = (int)(t / IPG_CHUNK_STEPS), slot = (int)(t % IPG_CHUNK_STEPS);
     int2 meta = chunk_meta[c];
+    if (meta.x < 0) continue;
     RayRec rec = rays[meta.x];
     int s = meta.y + slot;
     if (rec.status != IPG_RAY_OK || s > rec.nstep) continue;
@@ -493,6 +495,23 @@ __global__ void k_iota(int32_t *list, int n, int first)
   if (t < n) list[t] = first + t;
 }
 
+/* chunks [0, n) of the pool have no owner: the coefficient pass skips them
+ * (the longest class's range, of which its geodesics use a part) */
+__global__ void k_meta_clear(int2 *__restrict__ chunk_meta, long long n)
+{
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    chunk_meta[c] = make_int2(-1, 0);
+}
+
+/* the longest class's geodesic records become visible to the coefficient
+ * and transfer passes */
+__global__ void k_rider_merge(const int32_t *__restrict__ items, int n, const RayRec *__restrict__ from,
+                              RayRec *__restrict__ to)
+{
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) to[items[t]] = from[items[t]];
+}
+
 /* ===================================================================== */
 /* host side                                                              */
 /* ===================================================================== */
@@ -519,6 +538,11 @@ struct BatchWs {
   int32_t *glist[2]; /* wave lists of geodesic items */
   int32_t *xlist[2]; /* wave lists of transfer items */
   unsigned long long *cnt;
+  /* the longest class's own queue and counters (first wave) and its
+   * deferred items */
+  unsigned long long *cnt_long;
+  int32_t *gdef_long;
+  RayRec *rays_long; /* per geodesic item, written by the longest class's geodesics */
 };
 
 struct BatchState {
@@ -543,6 +567,9 @@ static void batch_ws_free(BatchWs *w)
   cudaFree(w->xlist[0]);
   cudaFree(w->xlist[1]);
   cudaFree(w->cnt);
+  cudaFree(w->cnt_long);
+  cudaFree(w->gdef_long);
+  cudaFree(w->rays_long);
   memset(w, 0, sizeof(*w));
 }
 
@@ -703,14 +730,21 @@ extern "C" int ipg__batch_begin(ipg_ctx *ctx, const ipg_camera *grp_cam, int ngr
 static int batch_ws_reserve(ipg_ctx *ctx, BatchWs &w, size_t n_geo, size_t n_xf)
 {
   if (!w.cnt) CK(cudaMalloc(&w.cnt, CNT_NB * sizeof(unsigned long long)));
+  if (!w.cnt_long) CK(cudaMalloc(&w.cnt_long, CNT_NB * sizeof(unsigned long long)));
   if (w.cap_geo < n_geo) {
     cudaFree(w.rays);
     cudaFree(w.glist[0]);
     cudaFree(w.glist[1]);
+    cudaFree(w.gdef_long);
+    cudaFree(w.rays_long);
+    w.gdef_long = nullptr;
+    w.rays_long = nullptr;
     w.cap_geo = 0;
     CK(cudaMalloc(&w.rays, n_geo * sizeof(RayRec)));
     CK(cudaMalloc(&w.glist[0], n_geo * sizeof(int32_t)));
     CK(cudaMalloc(&w.glist[1], n_geo * sizeof(int32_t)));
+    CK(cudaMalloc(&w.gdef_long, n_geo * sizeof(int32_t)));
+    CK(cudaMalloc(&w.rays_long, n_geo * sizeof(RayRec)));
     w.cap_geo = n_geo;
   }
   if (w.cap_xf < n_xf) {
@@ -736,16 +770,30 @@ static int batch_ws_reserve(ipg_ctx *ctx, BatchWs &w, size_t n_geo, size_t n_xf)
  * (instance, ray) transfer item.  Waves as in the single-image trace: items
  * whose geodesic finds the pool full are deferred with their transfer
  * items.  The pool is shared out per chunk of 32 steps as the 32 shared
- * records (512 B each) and the G instance blocks of each (80 B each). */
-extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigned long long *steps_left)
+ * records (512 B each) and the G instance blocks of each (80 B each).
+ *
+ * The longest predicted class (items->n_long, the head of the sorted order)
+ * rides beside the waves.  Started in a wave with the others, its rays, in
+ * flight the longest, are the ones the full pool defers, and their walks,
+ * at a lone ray's step latency, then set the last wave's geodesic time.
+ * Instead its geodesics start at once on the context's stream, in a pool
+ * range [0, cl) reserved for them and in blocks of 256 lanes (their
+ * registers fill an SM, so these rays get SMs of their own).  The waves run
+ * the other items on a second stream, allocating from cl up.  The class
+ * joins the first wave that starts after its geodesics end (or the wave that
+ * has no other geodesics left, which waits for them): that wave's
+ * coefficient pass covers the range too, and its transfer takes the class's
+ * transfer items, which read as deferred until then. */
+struct BatchRider {
+  size_t nl;     /* items in the class (0: none) */
+  long long cl;  /* its pool range [0, cl) */
+  bool launched, merged;
+};
+
+static int batch_waves(ipg_ctx *ctx, const ipg_batch_items *it, unsigned long long *steps_left, BatchRider &R)
 {
   BatchState *B = ctx->batch;
-  if (!B || !B->m.have || !B->G) return IPG_E_STATE;
-  if (it->n_geo == 0) return IPG_OK;
-  if (it->n_geo > 0x7fffffff || it->n_xf > 0x7fffffff) return IPG_E_ARG;
   BatchWs &W = B->w;
-  int rc = batch_ws_reserve(ctx, W, it->n_geo, it->n_xf);
-  if (rc) return rc;
   const int G = B->G;
   const size_t rec_bytes = (size_t)IPG_CHUNK_STEPS * IPG_STEP_DOUBLES * sizeof(double);
   const size_t side_bytes = (size_t)IPG_CHUNK_STEPS * G * IPG_BCOEF * sizeof(double);
@@ -753,18 +801,88 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
   if (n_chunks < 16) return IPG_E_NOMEM;
   double *pool = ctx->d_pool;
   double *side = ctx->d_pool + (size_t)n_chunks * IPG_CHUNK_STEPS * IPG_STEP_DOUBLES;
-  cudaStream_t st = ctx->stream;
   const int threads = 128;
-  size_t pend_g = it->n_geo, pend_x = it->n_xf, wave = it->n_geo;
+  const void *geo_fn = (const void *)k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB, false, CamTable>;
+  cudaStream_t st = ctx->stream; /* the waves */
+  size_t pend_g = it->n_geo, pend_x = it->n_xf;
   const int32_t *gl = it->geo_order, *xl = it->xf_order;
+  /* only where the items take more than one wave: in a wave that holds them
+   * all, the class's transfer overlaps the others' instead of following it */
+  if (ctx->split && it->geo_order && it->n_long > 0 && it->n_long < it->n_geo &&
+      it->pred_steps > (double)n_chunks * IPG_CHUNK_STEPS) {
+    /* its predicted steps with the single image's 15% margin */
+    const long long cl = (long long)(it->long_steps * 1.15 / IPG_CHUNK_STEPS) + (long long)it->n_long + 16;
+    if (cl <= n_chunks / 2) {
+      R.nl = it->n_long;
+      R.cl = cl;
+    }
+  }
+  if (R.nl) {
+    cudaStream_t sr = ctx->stream;
+    const int nl = (int)R.nl;
+    unsigned long long hl0[CNT_NB];
+    memset(hl0, 0, sizeof(hl0));
+    hl0[CNT_BUDGET] = steps_left ? *steps_left : 0;
+    CK(cudaMemcpyAsync(W.cnt_long, hl0, sizeof(hl0), cudaMemcpyHostToDevice, sr));
+    k_meta_clear<<<4 * ctx->n_sm, 256, 0, sr>>>(ctx->d_chunk_meta, R.cl);
+    k_mark_pending<<<(nl + 255) / 256, 256, 0, sr>>>(it->geo_order, nl, W.rays);
+    k_mark_pending<<<(nl + 255) / 256, 256, 0, sr>>>(it->geo_order, nl, W.rays_long);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->bev[0][2], sr));
+    const int lb = grid_blocks(ctx, geo_fn, 256, R.nl);
+    k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB, false, CamTable><<<lb, 256, 0, sr>>>(
+        it->geo_ij, it->geo_order, nl, pool, ctx->d_chunk_prev, ctx->d_chunk_meta, R.cl, W.cnt_long, W.rays_long,
+        W.gdef_long, it->geo_grp);
+    CK(cudaGetLastError());
+    R.launched = true;
+    CK(cudaEventRecord(ctx->ev_join[0], sr)); /* the class's geodesics are done */
+    st = ctx->bstream[0];
+    CK(cudaStreamWaitEvent(st, ctx->bev[0][2], 0));
+    gl = it->geo_order + R.nl;
+    pend_g -= R.nl;
+  }
+  const long long c0 = R.cl; /* the waves allocate from here */
+  size_t wave = pend_g;
   int cur = 0;
+  bool first = true;
   while (pend_g > 0 || pend_x > 0) {
+    /* the class joins this wave: its records and its rays that found its
+     * range full (continued as ordinary items) */
+    long long c_first = c0;
+    if (R.launched && !R.merged && !first && (pend_g == 0 || cudaEventQuery(ctx->ev_join[0]) == cudaSuccess)) {
+      CK(cudaStreamWaitEvent(st, ctx->ev_join[0], 0));
+      k_rider_merge<<<(int)((R.nl + 255) / 256), 256, 0, st>>>(it->geo_order, (int)R.nl, W.rays_long, W.rays);
+      CK(cudaGetLastError());
+      unsigned long long hl[CNT_NB];
+      CK(cudaMemcpyAsync(hl, W.cnt_long, sizeof(hl), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      R.merged = true;
+      ctx->stats.ray_steps += hl[CNT_STEPS];
+      ctx->stats.long_class_items += R.nl;
+      if (steps_left) *steps_left = hl[CNT_STEPS] >= *steps_left ? 0 : *steps_left - hl[CNT_STEPS];
+      if (hl[CNT_TIMEOUT]) {
+        snprintf(ctx->err, sizeof(ctx->err), "the batch's step budget ran out");
+        return IPG_E_TIMEOUT;
+      }
+      if (hl[CNT_DEFER]) {
+        CK(cudaMemcpyAsync(W.glist[cur] + pend_g, W.gdef_long, hl[CNT_DEFER] * sizeof(int32_t),
+                           cudaMemcpyDeviceToDevice, st));
+        pend_g += (size_t)hl[CNT_DEFER];
+        gl = W.glist[cur];
+      }
+      c_first = 0;
+#ifdef IPG_DEBUG_TIMING
+      fprintf(stderr, "batch: the longest class (%zu items, range %lld, used %llu, deferred %llu) joins wave %d\n",
+              R.nl, R.cl, hl[CNT_POOL], hl[CNT_DEFER], ctx->stats.waves + 1);
+#endif
+    }
     size_t run = pend_g < wave ? pend_g : wave;
     size_t carry = pend_g - run;
     int32_t *gnext = W.glist[cur ^ 1], *xnext = W.xlist[cur ^ 1];
     if (steps_left && *steps_left == 0) return IPG_E_TIMEOUT;
     unsigned long long h0[CNT_NB];
     memset(h0, 0, sizeof(h0));
+    h0[CNT_POOL] = (unsigned long long)c0;
     h0[CNT_DEFER] = carry;
     h0[CNT_BUDGET] = steps_left ? *steps_left : 0;
     CK(cudaMemcpyAsync(W.cnt, h0, sizeof(h0), cudaMemcpyHostToDevice, st));
@@ -775,8 +893,7 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[0], st));
-    int gb = grid_blocks(ctx, (const void *)k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB, false, CamTable>, threads,
-                         run);
+    int gb = grid_blocks(ctx, geo_fn, threads, run);
     k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB, false, CamTable><<<gb, threads, 0, st>>>(
         it->geo_ij, gl, (int)run, pool, ctx->d_chunk_prev, ctx->d_chunk_meta, n_chunks, W.cnt, W.rays, gnext,
         it->geo_grp);
@@ -787,7 +904,7 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
     int cb = grid_blocks(ctx, (const void *)k_coef_batch<EMT, F, RMC>, threads, (size_t)n_chunks * IPG_CHUNK_STEPS); \
     k_coef_batch<EMT, F, RMC><<<cb, threads, 0, st>>>(pool, side, G, ctx->d_chunk_meta, W.cnt, n_chunks, W.rays,  \
                                                  it->geo_grp, it->geo_mask, B->m.fourv, B->m.sets,          \
-                                                 (long long)B->m.ncell);                                      \
+                                                 (long long)B->m.ncell, c_first);                             \
   } while (0)
     if (B->emission_type == 1) {
       if (ctx->fits32) {
@@ -851,6 +968,10 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
       snprintf(ctx->err, sizeof(ctx->err), "the batch's step budget ran out");
       return IPG_E_TIMEOUT;
     }
+#ifdef IPG_DEBUG_TIMING
+    fprintf(stderr, "batch wave: run %zu used %llu deferred %llu; geo %.1f coef %.1f xfer %.1f ms\n", run,
+            h[CNT_POOL] - (unsigned long long)c0, h[CNT_DEFER], a, b, c);
+#endif
     const size_t dg = (size_t)h[CNT_DEFER], dx = (size_t)h[CNT_XDEFER];
     if (dg == pend_g && pend_g > 0) {
       /* nothing fitted: fewer rays share the pool next time */
@@ -863,10 +984,31 @@ extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigne
     }
     pend_g = dg;
     pend_x = dx;
+    first = false;
     cur ^= 1;
     gl = W.glist[cur];
     xl = W.xlist[cur];
   }
   return IPG_OK;
+}
+
+extern "C" int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *it, unsigned long long *steps_left)
+{
+  BatchState *B = ctx->batch;
+  if (!B || !B->m.have || !B->G) return IPG_E_STATE;
+  if (it->n_geo == 0) return IPG_OK;
+  if (it->n_geo > 0x7fffffff || it->n_xf > 0x7fffffff) return IPG_E_ARG;
+  int rc = batch_ws_reserve(ctx, B->w, it->n_geo, it->n_xf);
+  if (rc) return rc;
+  BatchRider R = {0, 0, false, false};
+  rc = batch_waves(ctx, it, steps_left, R);
+  if (R.launched) {
+    /* the context's stream continues after the waves; on an early return
+     * the class's geodesics, which write into the pool, end before it */
+    cudaEventRecord(ctx->ev_join[1], ctx->bstream[0]);
+    cudaStreamWaitEvent(ctx->stream, ctx->ev_join[1], 0);
+    if (rc || !R.merged) cudaStreamSynchronize(ctx->stream);
+  }
+  return rc;
 }
 #undef IPG_LAUNCH_XB

@@ -54,10 +54,16 @@ typedef struct ipg_batch_items {
   ipg_pixel_out *xf_out;    /* [n_xf] get_pixel's outputs */
   const int32_t *xf_order;  /* [n_xf] the order in which the transfer takes the items (NULL: 0..n_xf-1) */
   const int32_t *geo_order; /* [n_geo] the order in which the geodesics start (NULL: 0..n_geo-1) */
+  size_t n_long;            /* the first n_long of geo_order are the longest class (0: none) */
+  double long_steps;        /* their predicted steps at the full step size */
+  double pred_steps;        /* the predicted steps of all the items */
 } ipg_batch_items;
-/* the geodesic items in *sorted, longest predicted first (pred: n scratch) */
+/* the geodesic items in *sorted, longest predicted first (pred: n scratch);
+ * *n_long of them, with *long_steps predicted steps, form the longest length
+ * class (predicted at least the single image's first class factor times the
+ * mean); *pred_steps is the predicted steps of all n */
 int ipg__batch_sort_geo(ipg_ctx *ctx, const int32_t *geo_ij, const int32_t *geo_grp, size_t n, int maxnstep,
-                        int32_t *pred, int32_t *sorted);
+                        int32_t *pred, int32_t *sorted, size_t *n_long, double *long_steps, double *pred_steps);
 /* trace one level; *steps_left (NULL: no budget) is the remaining step
  * budget, decreased by the steps taken */
 int ipg__batch_trace(ipg_ctx *ctx, const ipg_batch_items *items, unsigned long long *steps_left);

@@ -1909,8 +1909,12 @@ static int sort_by_length(ipg_ctx *ctx, const int32_t *d_ij, size_t n, const ipg
  * (k_geodesic_count with the batch's camera table; pred: n scratch ints).
  * Enqueued on the context's stream after ipg__batch_begin. */
 extern "C" int ipg__batch_sort_geo(ipg_ctx *ctx, const int32_t *geo_ij, const int32_t *geo_grp, size_t n,
-                                   int maxnstep, int32_t *pred, int32_t *sorted)
+                                   int maxnstep, int32_t *pred, int32_t *sorted, size_t *n_long, double *long_steps,
+                                   double *pred_steps)
 {
+  *n_long = 0;
+  *long_steps = 0.;
+  *pred_steps = 0.;
   if (!n) return IPG_OK;
   const int threads = 128;
   unsigned long long *cnt = ctx->d_cnt;
@@ -1924,6 +1928,27 @@ extern "C" int ipg__batch_sort_geo(ipg_ctx *ctx, const int32_t *geo_ij, const in
   int sb = (int)((n + 255) / 256);
   if (sb > 4 * ctx->n_sm) sb = 4 * ctx->n_sm;
   k_len_hist<<<sb, 256, 0, ctx->stream>>>(pred, (int)n, 0, ctx->d_len_hist);
+  CK(cudaGetLastError());
+  /* the longest class, as plan_split draws it for a single image */
+  std::vector<int> hist(LEN_BUCKETS);
+  CK(cudaMemcpyAsync(hist.data(), ctx->d_len_hist, LEN_BUCKETS * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double total = 0.;
+  for (int b = 0; b < LEN_BUCKETS; b++) total += (double)b * hist[b];
+  *pred_steps = total * PRED_EPS_SCALE;
+  if (total > 0. && n >= SPLIT_MIN_RAYS) {
+    const int thr = (int)(k_class_facs[0] * total / (double)n) + 1;
+    size_t c = 0;
+    double st = 0.;
+    for (int b = thr; b < LEN_BUCKETS; b++) {
+      c += (size_t)hist[b];
+      st += (double)b * hist[b];
+    }
+    if (c < n) {
+      *n_long = c;
+      *long_steps = st * PRED_EPS_SCALE;
+    }
+  }
   k_len_scan<<<1, LEN_SCAN_THREADS, 0, ctx->stream>>>(ctx->d_len_hist);
   k_len_scatter<<<sb, 256, 0, ctx->stream>>>(NULL, pred, (int)n, 0, ctx->d_len_hist, sorted);
   CK(cudaGetLastError());

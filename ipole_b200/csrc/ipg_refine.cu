@@ -1018,9 +1018,13 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
                                                                   l.nsy, grps[b.grp].upos, (int)goff[b.grp], b.slot,
                                                                   xf_geo + xoff[q], xf_slot + xoff[q]);
     }
+    size_t n_long = 0;
+    double long_steps = 0., pred_steps = 0.;
     {
       const int ng = (int)n_geo, nb = grid_of(ng, SCAN_TPB);
-      if ((rc = ipg__batch_sort_geo(ctx, geo_ij, geo_grp, n_geo, maxnstep_all, geo_pred, geo_sorted))) return rc;
+      if ((rc = ipg__batch_sort_geo(ctx, geo_ij, geo_grp, n_geo, maxnstep_all, geo_pred, geo_sorted, &n_long,
+                                    &long_steps, &pred_steps)))
+        return rc;
       k_geo_count<<<grid_of(ng, TPB), TPB, 0, s>>>(geo_mask, geo_sorted, ng, geo_cnt, geo_rank);
       k_scan_blocks<<<nb, SCAN_TPB, 0, s>>>(geo_cnt, ng, geo_bsums);
       k_scan_top<<<1, SCAN_TPB, 0, s>>>(geo_bsums, nb, ord_st);
@@ -1029,7 +1033,8 @@ extern "C" int ipg_render_batch(ipg_ctx *ctx, const ipg_instance *inst, size_t n
                                                                       (int)n_xf, xf_order);
     }
     CKR(cudaGetLastError());
-    ipg_batch_items items = {n_geo, geo_ij, geo_grp, geo_mask, n_xf, xf_geo, xf_slot, xf_out, xf_order, geo_sorted};
+    ipg_batch_items items = {n_geo,   geo_ij, geo_grp,  geo_mask,   n_xf,   xf_geo,
+                             xf_slot, xf_out, xf_order, geo_sorted, n_long, long_steps, pred_steps};
     rc = ipg__batch_trace(ctx, &items, step_budget ? &steps_left : nullptr);
     if (rc) return rc;
     /* save_pixel, the checks and (base level) the flux estimate per instance */

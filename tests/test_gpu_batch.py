@@ -82,6 +82,36 @@ def test_batch_equals_single_images(c1_dump):
         assert not bad, bad
 
 
+def test_batch_longest_class_beside_the_waves(c1_dump):
+    """A batch that takes several waves of the trajectory pool traces its
+    longest predicted class beside them (blocks that fill an SM, a pool range
+    of its own, joining a later wave's coefficient and transfer passes).
+    Every instance is still its single image bit for bit, and a step budget
+    that runs out while that class is in flight leaves the context usable."""
+    ps = [ip.Params.from_args([f"--dump={c1_dump}", *BASE, *CAMS["A"][:3], "--nx=64", "--ny=64", f"--M_unit={mu}",
+                               f"--trat_large={rh}"]) for mu, rh in (("3e27", "20"), ("3e27", "160"), ("9e27", "20"))]
+    base = ip.Model.load(ps[0])
+    with ip.Context(pool_bytes=2 << 30) as ctx:
+        ctx.upload_batch(base)
+        with pytest.raises(ip.IpgError) as e:
+            ctx.render_batch(ps, base, step_budget=200000)
+        assert e.value.code == ip.IPG_E_TIMEOUT
+        imgs = ctx.render_batch(ps, base)
+        st = ctx.stats()
+        print("waves", st["waves"], "longest class items", st["long_class_items"])
+        assert st["waves"] >= 2 and st["long_class_items"] > 0, st
+        bad = {}
+        for q, (p, img) in enumerate(zip(ps, imgs)):
+            m = ip.Model.load(p)
+            ctx.upload(m)
+            ref = ctx.render(p, m)
+            d = _diff(img, ref)
+            if d or img.traced != ref.traced:
+                bad[q] = (d, img.traced, ref.traced)
+        print("longest class beside the waves: instances that differ from their single image:", bad)
+        assert not bad, bad
+
+
 def test_batch_instance_matches_golden(c1_dump):
     """c1_bright_32 as one instance of a batch against the reference's image"""
     meta, arrs = common.load_golden("c1_bright_32")
