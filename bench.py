@@ -507,7 +507,8 @@ def bench_batched(ip, ctx, model, dump, args, world, stream, single_ms):
         res[name] = {"value": images_per_s(world, len(ps), ms), "unit": "images/s", "ms_per_batch": ms,
                      "instances": len(ps), "vs_single_fp64": (len(ps) / ms) / (1.0 / single_ms),
                      "geodesic_ms": st["geodesic_ms"], "coeffs_ms": st["coeffs_ms"],
-                     "transfer_ms": st["transfer_ms"], "waves": st["waves"]}
+                     "transfer_ms": st["transfer_ms"], "waves": st["waves"],
+                     "long_class_items": st["long_class_items"]}
         if step32:
             ref = fp64_imgs
             errs = []
