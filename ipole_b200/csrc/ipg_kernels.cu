@@ -1094,29 +1094,35 @@ __device__ __forceinline__ bool xfer_fetch(XferLane &L, const int32_t *__restric
  * for a lane whose record of step n is L.rec_i and whose coefficients of
  * step n-1 are cb: push_polar twice, then the unpolarized and polarized
  * transfer steps at radiating points. */
+/* push_polar twice (src/ipolarray.c:85-89) with the transport matrices of
+ * record rec and that record's step length dl */
 template <bool S32, int RM, class Lane>
-__device__ __forceinline__ void xfer_step(const DevCam &C, Lane &L, const CoefBlock &cb, int unpol)
+__device__ __forceinline__ void xfer_push(Lane &L, const double *rec, double dl)
 {
   const DevGrid &G = c_grid;
-  double dl = L.dl_i;
-  if (!unpol) {
-    /* push_polar twice, src/ipolarray.c:85-89 */
-    double dlfull = dl * G.inv_dlfac;
-    double dlhalf = (0.5 * dl) * G.inv_dlfac;
-    double A[4][4];
-    HermN Nh, Nn;
-    load_A_rec<RM>(L.rec_i, 0, A);
-    if constexpr (S32 && IPG_S32_PUSH) {
-      hn_push_f32(L.N, L.N, A, dlhalf, &Nh);
-      load_A_rec<RM>(L.rec_i, 1, A);
-      hn_push_f32(L.N, Nh, A, dlfull, &Nn);
-    } else {
-      hn_push(L.N, L.N, A, dlhalf, &Nh);
-      load_A_rec<RM>(L.rec_i, 1, A);
-      hn_push(L.N, Nh, A, dlfull, &Nn);
-    }
-    L.N = Nn;
+  double dlfull = dl * G.inv_dlfac;
+  double dlhalf = (0.5 * dl) * G.inv_dlfac;
+  double A[4][4];
+  HermN Nh, Nn;
+  load_A_rec<RM>(rec, 0, A);
+  if constexpr (S32 && IPG_S32_PUSH) {
+    hn_push_f32(L.N, L.N, A, dlhalf, &Nh);
+    load_A_rec<RM>(rec, 1, A);
+    hn_push_f32(L.N, Nh, A, dlfull, &Nn);
+  } else {
+    hn_push(L.N, L.N, A, dlhalf, &Nh);
+    load_A_rec<RM>(rec, 1, A);
+    hn_push(L.N, Nh, A, dlfull, &Nn);
   }
+  L.N = Nn;
+}
+
+/* the unpolarized and polarized transfer steps at a radiating point, with
+ * the coefficient block cb of the step's end and the step length dl of its
+ * start (src/ipolarray.c:91-244) */
+template <bool S32, class Lane>
+__device__ __forceinline__ void xfer_evolve(const DevCam &C, Lane &L, const CoefBlock &cb, double dl, int unpol)
+{
   int flags = (int)cb.flags;
   if (flags & 1) {
     L.nrad++;
@@ -1134,6 +1140,14 @@ __device__ __forceinline__ void xfer_step(const DevCam &C, Lane &L, const CoefBl
       else L.flag |= evolve_N_coef(cb, dl, zero_emission, &L.N, &L.tauF, C.stokes_floors);
     }
   }
+}
+
+template <bool S32, int RM, class Lane>
+__device__ __forceinline__ void xfer_step(const DevCam &C, Lane &L, const CoefBlock &cb, int unpol)
+{
+  double dl = L.dl_i;
+  if (!unpol) xfer_push<S32, RM>(L, L.rec_i, dl);
+  xfer_evolve<S32>(C, L, cb, dl, unpol);
 }
 
 /* get_pixel's outputs at the end of a lane's walk: project_N
@@ -1219,6 +1233,162 @@ __global__ void __launch_bounds__(TPB, MINB)
     L.rec_i = rec_f;
     L.n--;
   }
+}
+
+/* ===================================================================== */
+/* k_transfer with its step records staged in shared memory               */
+/* ===================================================================== */
+/* k_transfer loads a step's record when the step starts, so each step
+ * waits for a round trip to L2 or DRAM (long_scoreboard is its largest
+ * stall).  Here every lane copies its next record into its own slots of
+ * shared memory with cp.async while it computes the current one.
+ *
+ * One iteration consumes one record k: the transfer step k+1 -> k with k's
+ * coefficient block (and record k+1's step length), then the push of N for
+ * the step k -> k-1 with k's transport matrices (and k's step length).
+ * That is k_transfer's sequence of operations, regrouped by record, so the
+ * images are bit-identical.
+ *
+ * A record is copied in two parts, each issued as soon as the previous
+ * record's part has been read from its slot: the coefficient block with the
+ * tetrad rows (P1) and the transport matrices (P2).  A part's copy then
+ * overlaps the other part's arithmetic.  With NBC = 2 the P1 part has two
+ * slots and its copy is issued a whole iteration ahead.  Each lane's slots
+ * are NBC P1 + P2 + 16 bytes apart: the 16-byte skew puts the lanes of a
+ * quarter-warp in different banks. */
+template <int RM, int NBC>
+struct XStage {
+  static constexpr int P1_OFF = RM ? 128 : 256; /* byte offset of the coefficient block in the record */
+  static constexpr int P1 = RM ? 192 : 256;     /* coefficient block + tetrad rows */
+  static constexpr int P2 = RM ? 128 : 256;     /* transport matrices A1, A2 (from byte 0) */
+  static constexpr int LANE = NBC * P1 + P2 + 16; /* bytes of shared memory per lane */
+  static_assert(NBC == 1 || NBC == 2, "one or two coefficient slots");
+  static_assert(LANE % 16 == 0 && LANE % 128 == 16, "16-byte copies; quarter-warp lanes in distinct banks");
+  static_assert(IPG_XFER_WIDE * LANE <= 227 * 1024, "a wide block's slots fit an SM's shared memory");
+};
+/* slots per layout: FP64 records take one coefficient slot (528 bytes per
+ * lane: three 128-lane blocks per SM, as many as the registers allow), the
+ * compact records two (528 bytes as well) */
+template <int RM>
+struct XStageOf {
+  static constexpr int NBC = RM ? 2 : 1;
+  using T = XStage<RM, NBC>;
+};
+
+/* .ca: through L1, so the second 16 bytes of a 32-byte sector come from L1
+ * instead of a second L2 request (with .cg the walk ran 30% slower) */
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_bytes(unsigned char *dst, const unsigned char *src)
+{
+#pragma unroll
+  for (int o = 0; o < BYTES; o += 16) cp_async16(dst + o, src + o);
+}
+
+template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false, int RM = 0>
+__global__ void __launch_bounds__(TPB, MINB)
+    k_transfer_staged(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
+                      const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays,
+                      ipg_pixel_out *__restrict__ out, unsigned long long *__restrict__ counters)
+{
+  static_assert(RM == 0 || RM == 1, "the staged walk is compiled per record layout");
+  using X = typename XStageOf<RM>::T;
+  constexpr int NBC = XStageOf<RM>::NBC;
+  extern __shared__ __align__(16) unsigned char xsm[];
+  unsigned char *slot_c = xsm + (size_t)threadIdx.x * X::LANE; /* NBC P1 slots */
+  unsigned char *slot_a = slot_c + NBC * X::P1;                /* one P2 slot */
+  const double *view_a = reinterpret_cast<const double *>(slot_a);
+  const DevCam &C = c_cam;
+  const int unpol = C.unpol;
+  XferLane L;
+  int n0 = 0;
+  /* a new ray: its top record's coefficients were read by xfer_fetch, so
+   * the first group is empty; the second copies the top record's matrices.
+   * In flight at the top of the iteration for record k, oldest first: k's
+   * P1 group, k's P2 group (NBC = 1: nothing else). */
+  auto start = [&]() {
+    n0 = L.n;
+    cp_async_commit();
+    if (!unpol && L.n > 0) cp_async_bytes<X::P2>(slot_a, reinterpret_cast<const unsigned char *>(L.rec_i));
+    cp_async_commit();
+  };
+  bool has = xfer_fetch<RM>(L, list, n_list, pool, chunk_prev, rays, out, counters);
+  if (has) start();
+  while (__any_sync(0xffffffffu, has)) {
+    if (!has) continue;
+    const int k = L.n;
+    const double *rec_f = nullptr; /* record k-1 */
+    if (k >= 1) {
+      const int s = k - 1;
+      if (s % IPG_CHUNK_STEPS == IPG_CHUNK_STEPS - 1) {
+        L.chunk = L.cprev;
+        L.cprev = chunk_prev[L.chunk];
+      }
+      rec_f = step_ptr(const_cast<double *>(pool), L.chunk, s % IPG_CHUNK_STEPS);
+      /* the record after it, into L2 */
+      if (s >= 1) {
+        if ((s - 1) % IPG_CHUNK_STEPS != IPG_CHUNK_STEPS - 1) prefetch_rec<RM>(rec_f - IPG_STEP_DOUBLES);
+        else if (L.cprev >= 0) prefetch_rec<RM>(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
+      }
+    }
+    const unsigned char *src_c = reinterpret_cast<const unsigned char *>(rec_f) + X::P1_OFF;
+    if constexpr (NBC == 2) {
+      if (k >= 1) cp_async_bytes<X::P1>(slot_c + ((k - 1) & 1) * X::P1, src_c);
+      cp_async_commit();
+    }
+    /* the transfer step k+1 -> k (integrate_emission's loop,
+     * src/ipolarray.c:91-244) with record k's coefficients */
+    if (k < n0) {
+      if constexpr (NBC == 2) cp_async_wait<2>();
+      else cp_async_wait<1>();
+      CoefBlock cb;
+      const double *view_c = reinterpret_cast<const double *>(slot_c + (NBC == 2 ? (k & 1) : 0) * X::P1 - X::P1_OFF);
+      if constexpr (RM) load_coef_m(view_c, cb);
+      else load_coef(view_c, cb);
+      xfer_evolve<S32>(C, L, cb, L.dl_i, unpol);
+      L.dl_i = cb.dl;
+      L.nturns_i = cb.nturns;
+    }
+    if (k == 0) {
+      if constexpr (NBC == 1) cp_async_commit();
+      cp_async_commit();
+      ipg_pixel_out o;
+      xfer_result(C, L, unpol, rays[L.ray].nstep, &o);
+      out[L.ray] = o;
+      atomicAdd(&counters[CNT_RAD], (unsigned long long)L.nrad);
+      has = xfer_fetch<RM>(L, list, n_list, pool, chunk_prev, rays, out, counters);
+      if (has) start();
+      continue;
+    }
+    if constexpr (NBC == 1) {
+      cp_async_bytes<X::P1>(slot_c, src_c); /* the slot was read by the load above */
+      cp_async_commit();
+    }
+    /* push_polar for the step k -> k-1 with record k's matrices, then the
+     * copy of record k-1's matrices into the slot the push has read */
+    if (!unpol) {
+      cp_async_wait<1>();
+      xfer_push<S32, RM>(L, view_a, L.dl_i);
+      if (k >= 2) cp_async_bytes<X::P2>(slot_a, reinterpret_cast<const unsigned char *>(rec_f));
+    }
+    cp_async_commit();
+    L.rec_i = rec_f;
+    L.n = k - 1;
+  }
+  cp_async_wait<0>();
 }
 
 /* ===================================================================== */
@@ -1352,6 +1522,7 @@ struct ipg_ctx {
   int32_t *d_pred;   /* predicted step counts (list positions), also staging */
   int *d_len_hist;   /* LEN_BUCKETS counters of the sort */
   int split;         /* 1: split waves into long and short batches */
+  int xstage;        /* 1: the transfer walk stages its records in shared memory */
   int emission_type; /* of the camera being traced */
   int rec_mixed;     /* IPG_RECORDS_MIXED: compact step records */
   int step32;        /* IPG_STEP_FP32: the polarized step in FP32 */
@@ -1429,6 +1600,24 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_cnt, (NB_MAX + 1) * CNT_N * sizeof(unsigned long long));
   ctx->split = 1;
   if (getenv("IPG_NO_SPLIT")) ctx->split = 0;
+  /* the transfer walk with its records staged in shared memory (default);
+   * IPG_XFER_STAGE=0 selects the walk that loads them from global memory */
+  {
+    const char *xs = getenv("IPG_XFER_STAGE");
+    ctx->xstage = (xs && xs[0] == '0') ? 0 : 1;
+  }
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void *)k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<0>::T::LANE);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void *)k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, true, 0>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<0>::T::LANE);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void *)k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, false, 1>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<1>::T::LANE);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void *)k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, true, 1>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<1>::T::LANE);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_len_hist, LEN_BUCKETS * sizeof(int));
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) {
@@ -1669,10 +1858,10 @@ static void make_devcam(const ipg_camera *c, DevCam *d)
 
 /* persistent grid: the resident blocks of the kernel on every SM, no more
  * than the work needs */
-static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n)
+static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n, size_t smem = 0)
 {
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   if (per_sm < 1) per_sm = 1;
   size_t full = (size_t)ctx->n_sm * per_sm;
   size_t need = (n + threads - 1) / threads;
@@ -1754,10 +1943,18 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
    * holding only its own paths */
 #define IPG_LAUNCH_XFER(S32, RM)                                                                              \
   do {                                                                                                       \
-    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM>, xthreads,    \
-                         b.run);                                                                             \
-    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM><<<tb, xthreads, 0, b.stream>>>(                       \
-        b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt, nullptr);                       \
+    if (ctx->xstage) {                                                                                       \
+      size_t sm = (size_t)xthreads * XStageOf<RM>::T::LANE;                                                       \
+      int tb = grid_blocks(ctx, (const void *)k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM>,      \
+                           xthreads, b.run, sm);                                                             \
+      k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM><<<tb, xthreads, sm, b.stream>>>(             \
+          b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);                              \
+    } else {                                                                                                 \
+      int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM>, xthreads,  \
+                           b.run);                                                                           \
+      k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM><<<tb, xthreads, 0, b.stream>>>(                     \
+          b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt, nullptr);                     \
+    }                                                                                                        \
   } while (0)
   if (ctx->step32) {
     if (ctx->rec_mixed) IPG_LAUNCH_XFER(true, 1);
