@@ -354,6 +354,9 @@ typedef struct ipg_stats {
   /* ipg_render_batch: geodesic items of the longest predicted class traced
    * beside the waves (batches that take more than one wave) */
   uint64_t long_class_items;
+  /* waves whose longest length class's blocks did not all report resident
+   * within the host's bounded wait before the other classes were launched */
+  uint64_t start_waits_timed_out;
 } ipg_stats;
 int ipg_get_stats(const ipg_ctx *ctx, ipg_stats *stats);
 

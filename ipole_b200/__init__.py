@@ -97,7 +97,7 @@ class Stats(C.Structure):
                 ("coeffs_ms", C.c_double), ("predict_ms", C.c_double), ("wall_ms", C.c_double),
                 ("geodesic_span_ms", C.c_double), ("coeffs_span_ms", C.c_double), ("transfer_span_ms", C.c_double),
                 ("adjoint_ms", C.c_double), ("adj_scatter_ms", C.c_double),
-                ("long_class_items", C.c_uint64)]
+                ("long_class_items", C.c_uint64), ("start_waits_timed_out", C.c_uint64)]
 
 
 class _Params(C.Structure):

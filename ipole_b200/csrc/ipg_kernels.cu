@@ -35,6 +35,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <vector>
 
 #include "ipg_device.cuh"
@@ -337,9 +338,16 @@ __global__ void __launch_bounds__(TPB, MINB)
     k_geodesic(const int32_t *__restrict__ ij, const int32_t *__restrict__ list, int n_list,
                double *__restrict__ pool, int *__restrict__ chunk_prev, int2 *__restrict__ chunk_meta,
                long long n_chunks, unsigned long long *__restrict__ counters, RayRec *__restrict__ rays,
-               int32_t *__restrict__ deferred, const int32_t *__restrict__ ray_grp)
+               int32_t *__restrict__ deferred, const int32_t *__restrict__ ray_grp, int *started = nullptr)
 {
   const DevGrid &G = c_grid;
+  /* a block marks its start in host memory when asked (the host waits for
+   * the longest class's blocks to be resident before it launches the other
+   * classes) */
+  if (started && threadIdx.x == 0) {
+    *(volatile int *)(started + blockIdx.x) = 1;
+    __threadfence_system();
+  }
   GeoLane L;
   bool has = geo_fetch<CS>(L, ij, list, n_list, pool, chunk_prev, chunk_meta, n_chunks, counters, rays, deferred, ray_grp);
   if constexpr (FULL) {
@@ -1496,6 +1504,8 @@ static void devgrid_derived(DevGrid *d)
 #endif
 static const double k_class_facs[] = {PRED_CLASS_FACS};
 #define NB_MAX ((int)(sizeof(k_class_facs) / sizeof(k_class_facs[0])) + 1)
+#define IPG_STARTED_MAX 1024   /* geodesic blocks of the longest class that can mark their start */
+#define IPG_STARTED_WAIT_US 2000 /* the host's wait for them */
 
 struct ipg_ctx {
   int device;
@@ -1504,6 +1514,7 @@ struct ipg_ctx {
   cudaStream_t bstream[NB_MAX]; /* the length classes of a split wave */
   cudaEvent_t bev[NB_MAX][5];   /* per class: geodesic, coeffs, transfer boundaries (and coeffs start) */
   cudaEvent_t ev_fork, ev_join[NB_MAX], ev_pred[2];
+  int *h_started, *d_started; /* mapped host flags: the longest class's geodesic blocks mark their start */
   double *d_fields;
   size_t ncell;
   int have_model;
@@ -1597,6 +1608,8 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
   }
   for (int i = 0; e == cudaSuccess && i < 2; i++) e = cudaEventCreate(&ctx->ev_pred[i]);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_fork);
+  if (e == cudaSuccess) e = cudaHostAlloc((void **)&ctx->h_started, IPG_STARTED_MAX * sizeof(int), cudaHostAllocMapped);
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&ctx->d_started, ctx->h_started, 0);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_cnt, (NB_MAX + 1) * CNT_N * sizeof(unsigned long long));
   ctx->split = 1;
   if (getenv("IPG_NO_SPLIT")) ctx->split = 0;
@@ -1657,6 +1670,7 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   }
   for (int i = 0; i < 2; i++) cudaEventDestroy(ctx->ev_pred[i]);
   cudaEventDestroy(ctx->ev_fork);
+  cudaFreeHost(ctx->h_started);
   cudaStreamDestroy(ctx->stream);
   free(ctx);
 }
@@ -1869,6 +1883,28 @@ static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n, 
   return (int)(need < full ? need : full);
 }
 
+/* The host waits (at most IPG_STARTED_WAIT_US) until the first n blocks of
+ * a launch have marked their start.  Launched first but placed behind the
+ * shorter classes' blocks, the longest class's SM-filling blocks wait for
+ * whole SMs to drain, and its geodesics (the image's critical path) then end
+ * 30-40 ms later.  No kernel waits here: if the marks do not come in time
+ * the launches go on. */
+static void wait_started(ipg_ctx *ctx, int n)
+{
+  const volatile int *f = ctx->h_started;
+  auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    int k = 0;
+    while (k < n && f[k]) k++;
+    if (k == n) return;
+    auto us = std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
+    if (us > IPG_STARTED_WAIT_US) {
+      ctx->stats.start_waits_timed_out++;
+      return;
+    }
+  }
+}
+
 /* One batch of a wave: a slice of a ray list, a slice of the trajectory pool
  * and its own counters, run as geodesic -> coefficients -> transfer on one
  * stream.  wide = 1 launches the two sequential kernels in 256-thread blocks,
@@ -1888,6 +1924,8 @@ struct Batch {
   cudaEvent_t *ev;
   int wide;
   cudaEvent_t coef_after; /* k_coeffs waits for this event (or none) */
+  int *started;           /* device view of host flags: the geodesic's blocks mark their start (or none) */
+  mutable int geo_blocks; /* the geodesic's grid, as launched */
 };
 
 template <int P>
@@ -1901,9 +1939,11 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
   const int gthreads = b.wide ? 256 : threads, xthreads = b.wide ? IPG_XFER_WIDE : threads;
   CK(cudaEventRecord(b.ev[0], b.stream));
   int gb = grid_blocks(ctx, (const void *)k_geodesic<P, 256, IPG_GEO_MINB>, gthreads, b.run);
+  if (b.started && gb > IPG_STARTED_MAX) gb = IPG_STARTED_MAX;
+  b.geo_blocks = gb;
   k_geodesic<P, 256, IPG_GEO_MINB><<<gb, gthreads, 0, b.stream>>>(d_ij, b.list, (int)b.run, b.pool, b.chunk_prev,
                                                                   b.chunk_meta, b.n_chunks, b.cnt, ctx->d_rays,
-                                                                  b.deferred, nullptr);
+                                                                  b.deferred, nullptr, b.started);
   CK(cudaGetLastError());
   CK(cudaEventRecord(b.ev[1], b.stream));
   if (b.coef_after) CK(cudaStreamWaitEvent(b.stream, b.coef_after, 0));
@@ -2232,6 +2272,8 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
         bt[b].ev = ctx->bev[b];
         bt[b].wide = wide[b];
         bt[b].coef_after = nullptr;
+        bt[b].started = (b == 0 && wide[0] && nb > 1) ? ctx->d_started : nullptr;
+        bt[b].geo_blocks = 0;
         /* the shorter classes' coefficient passes wait for the longest
          * class's geodesics: run beside them, they slow the longest rays'
          * steps four- to eightfold (those rays' SMs hold no other block) */
@@ -2239,12 +2281,18 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
         c0 += ncb;
         r0 += sizes[b];
       }
+      /* the classes' counters are cleared before the fork, so that each
+       * class stream starts with its geodesic launch and the longest class's
+       * SM-filling blocks, launched first, are placed first: placed behind
+       * the shorter classes' blocks, they wait for whole SMs to drain */
+      CK(cudaMemsetAsync(ctx->d_cnt + CNT_N, 0, sizeof(unsigned long long) * CNT_N * nb, ctx->stream));
       CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+      if (bt[0].started) memset(ctx->h_started, 0, IPG_STARTED_MAX * sizeof(int));
       for (int b = 0; b < nb; b++) {
         CK(cudaStreamWaitEvent(bt[b].stream, ctx->ev_fork, 0));
-        CK(cudaMemsetAsync(bt[b].cnt, 0, sizeof(unsigned long long) * CNT_N, bt[b].stream));
         rc = launch_batch(ctx, bt[b], d_ij, d_out);
         if (rc) return rc;
+        if (bt[b].started) wait_started(ctx, bt[b].geo_blocks);
         CK(cudaEventRecord(ctx->ev_join[b], bt[b].stream));
         CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join[b], 0));
       }
