@@ -512,7 +512,7 @@ class Context:
         shape = (gr.n1 + 2, gr.n2 + 2, gr.n3 + 2)
         ncell = shape[0] * shape[1] * shape[2]
         dL = np.ascontiguousarray(dL_dpol, dtype=np.float64)
-        arrs = [np.zeros(ncell) for _ in range(3)]
+        arrs = [np.empty(ncell) for _ in range(3)]  # every cell is written
         g = Grad()
         g.d_ne, g.d_thetae, g.d_b = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
         pol = np.zeros(dL.shape)

@@ -556,13 +556,20 @@ int ipg_adjoint_params(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, co
   const size_t ncell = (size_t)(gr->n1 + 2) * (gr->n2 + 2) * (gr->n3 + 2);
   int32_t *ij = NULL;
   double *dL = NULL, *gbuf = NULL;
+  double *gne = g->d_ne, *gth = g->d_thetae, *gb = g->d_b; /* the cells' gradients land in the caller's arrays */
   ipg_pixel_out *out = NULL;
   if (rc == IPG_OK) {
     ij = (int32_t *)malloc(2 * npix * sizeof(int32_t));
     dL = (double *)malloc(4 * npix * sizeof(double));
     out = (ipg_pixel_out *)malloc(npix * sizeof(ipg_pixel_out));
-    gbuf = (double *)malloc(3 * ncell * sizeof(double));
-    if (!ij || !dL || !out || !gbuf) rc = IPG_E_NOMEM;
+    /* scratch only for the arrays the caller does not take */
+    const size_t nmiss = (gne ? 0 : 1) + (gth ? 0 : 1) + (gb ? 0 : 1);
+    if (nmiss) gbuf = (double *)malloc(nmiss * ncell * sizeof(double));
+    if (!ij || !dL || !out || (nmiss && !gbuf)) rc = IPG_E_NOMEM;
+    double *q = gbuf;
+    if (!gne) gne = q, q += ncell;
+    if (!gth) gth = q, q += ncell;
+    if (!gb) gb = q;
   }
   if (rc == IPG_OK) {
     /* save_pixel (main.c:885-910): pol = (I, Q, U, V) nu^3, Q and U negated
@@ -578,7 +585,7 @@ int ipg_adjoint_params(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, co
         dL[4 * q + 2] = dL_dpol[4 * q + 2] * sq * ra.f3;
         dL[4 * q + 3] = dL_dpol[4 * q + 3] * ra.f3;
       }
-    rc = ipg_adjoint(ctx, &img.cam, ij, npix, dL, ckpt_interval, gbuf, gbuf + ncell, gbuf + 2 * ncell, out);
+    rc = ipg_adjoint(ctx, &img.cam, ij, npix, dL, ckpt_interval, gne, gth, gb, out);
   }
   if (rc == IPG_OK) {
     if (pol_out) {
@@ -600,8 +607,8 @@ int ipg_adjoint_params(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, co
     const double gem1 = game - 1., gpm1 = gamp - 1.;
     double dM = 0., dRh = 0., dRl = 0.;
     for (size_t c = 0; c < ncell; c++) {
-      const double gn = gbuf[c], gt = gbuf[ncell + c], gb = gbuf[2 * ncell + c];
-      dM += gn * ne[c] + 0.5 * gb * bb[c];
+      const double gn = gne[c], gt = gth[c], gbc = gb[c];
+      dM += gn * ne[c] + 0.5 * gbc * bb[c];
       if (gt == 0.) continue;
       double bsq = bb[c] / m->B_unit;
       bsq = bsq * bsq;
@@ -618,9 +625,6 @@ int ipg_adjoint_params(ipg_ctx *ctx, ipg_params *p, const ipg_iharm_model *m, co
     g->d_M_unit = dM / m->M_unit;
     g->d_R_high = dRh;
     g->d_R_low = dRl;
-    if (g->d_ne) memcpy(g->d_ne, gbuf, ncell * sizeof(double));
-    if (g->d_thetae) memcpy(g->d_thetae, gbuf + ncell, ncell * sizeof(double));
-    if (g->d_b) memcpy(g->d_b, gbuf + 2 * ncell, ncell * sizeof(double));
   }
   free(ij);
   free(dL);

@@ -640,26 +640,29 @@ extern "C" int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *i
   double *pool = ctx->d_pool;
   double *side = pool + (size_t)n_chunks * IPG_CHUNK_STEPS * IPG_STEP_DOUBLES;
   double *ckpt = side + (size_t)n_chunks * IPG_CHUNK_STEPS * IPG_ADJ_DOUBLES;
-  double *dL = nullptr, *g = nullptr;
-  int *next = nullptr, *first = nullptr;
-  auto release = [&]() {
-    cudaFree(dL);
-    cudaFree(g);
-    cudaFree(next);
-    cudaFree(first);
+  /* scratch kept in the context between calls (grow-only) */
+  auto grow = [](void **ptr, size_t *cap, size_t bytes) -> cudaError_t {
+    if (*cap >= bytes) return cudaSuccess;
+    cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e == cudaSuccess) *cap = bytes;
+    return e;
   };
 #define CKA(call)                       \
   do {                                  \
     cudaError_t e_ = (call);            \
     if (e_ != cudaSuccess) {            \
-      release();                        \
       return cuda_fail(ctx, e_, #call); \
     }                                   \
   } while (0)
-  CKA(cudaMalloc(&dL, 4 * n * sizeof(double)));
-  CKA(cudaMalloc(&g, 3 * ncell * sizeof(double)));
-  CKA(cudaMalloc(&next, (size_t)n_chunks * sizeof(int)));
-  CKA(cudaMalloc(&first, n * sizeof(int)));
+  CKA(grow((void **)&ctx->d_adj_dl, &ctx->adj_dl_cap, 4 * n * sizeof(double)));
+  CKA(grow((void **)&ctx->d_adj_g, &ctx->adj_g_cap, 3 * ncell * sizeof(double)));
+  CKA(grow((void **)&ctx->d_adj_next, &ctx->adj_next_cap, (size_t)n_chunks * sizeof(int)));
+  CKA(grow((void **)&ctx->d_adj_first, &ctx->adj_first_cap, n * sizeof(int)));
+  double *dL = ctx->d_adj_dl, *g = ctx->d_adj_g;
+  int *next = ctx->d_adj_next, *first = ctx->d_adj_first;
   CKA(cudaMemcpyAsync(dL, dL_dout, 4 * n * sizeof(double), cudaMemcpyHostToDevice, st));
   CKA(cudaMemsetAsync(g, 0, 3 * ncell * sizeof(double), st));
   memset(&ctx->stats, 0, sizeof(ctx->stats));
@@ -667,10 +670,7 @@ extern "C" int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *i
    * rays that find the pool full go to the next wave, after this wave's
    * adjoint is done */
   rc = sort_by_length(ctx, ctx->d_ij, n, cam);
-  if (rc) {
-    release();
-    return rc;
-  }
+  if (rc) return rc;
   const int32_t *list = ctx->d_sorted;
   size_t pending = n, wave = n;
   int cur = 0;
@@ -694,10 +694,7 @@ extern "C" int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *i
                                             dL, ctx->d_out, g, ncell, nextl);
     else rc = adjoint_wave<64>(ctx, em, ctx->d_ij, list, run, pool, side, ckpt, n_chunks, next, first, dL,
                                ctx->d_out, g, ncell, nextl);
-    if (rc) {
-      release();
-      return rc;
-    }
+    if (rc) return rc;
     CKA(cudaEventRecord(ctx->ev[1], st));
     unsigned long long h[CNT_N];
     CKA(cudaMemcpyAsync(h, ctx->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
@@ -722,7 +719,6 @@ extern "C" int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *i
     size_t deferred = (size_t)h[CNT_DEFER];
     if (deferred == pending) {
       if (run == 1) {
-        release();
         snprintf(ctx->err, sizeof(ctx->err), "trajectory pool too small for a single ray");
         return IPG_E_NOMEM;
       }
@@ -740,7 +736,6 @@ extern "C" int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *i
   CKA(cudaMemcpyAsync(o, ctx->d_out, n * sizeof(ipg_pixel_out), cudaMemcpyDeviceToHost, st));
   CKA(cudaStreamSynchronize(st));
 #undef CKA
-  release();
   for (size_t m = 0; m < n; m++)
     if (o[m].nstep >= cam->maxnstep - 1) {
       snprintf(ctx->err, sizeof(ctx->err), "MaxNStep exceeded in pixel %d %d", ij[2 * m], ij[2 * m + 1]);

@@ -829,11 +829,16 @@ static int batch_waves(ipg_ctx *ctx, const ipg_batch_items *it, unsigned long lo
     k_mark_pending<<<(nl + 255) / 256, 256, 0, sr>>>(it->geo_order, nl, W.rays_long);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->bev[0][2], sr));
-    const int lb = grid_blocks(ctx, geo_fn, 256, R.nl);
+    int lb = grid_blocks(ctx, geo_fn, 256, R.nl);
+    if (lb > IPG_STARTED_MAX) lb = IPG_STARTED_MAX;
+    memset(ctx->h_started, 0, IPG_STARTED_MAX * sizeof(int));
     k_geodesic<IPG_PLUG_IHARM, 256, IPG_GEO_MINB, false, CamTable><<<lb, 256, 0, sr>>>(
         it->geo_ij, it->geo_order, nl, pool, ctx->d_chunk_prev, ctx->d_chunk_meta, R.cl, W.cnt_long, W.rays_long,
-        W.gdef_long, it->geo_grp);
+        W.gdef_long, it->geo_grp, ctx->d_started);
     CK(cudaGetLastError());
+    /* the waves' blocks are launched once the class's SM-filling blocks are
+     * resident (bounded host wait), so these find whole SMs */
+    wait_started(ctx, lb);
     R.launched = true;
     CK(cudaEventRecord(ctx->ev_join[0], sr)); /* the class's geodesics are done */
     st = ctx->bstream[0];

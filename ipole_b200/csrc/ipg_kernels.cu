@@ -1545,6 +1545,11 @@ struct ipg_ctx {
   ipg_stats stats;
   void *refine; /* buffers of the on-device image driver (ipg_refine.cu) */
   double *d_trace_extra; /* rho, u, beta per cell for the trace output (ipg_upload_trace_fields) */
+  /* the adjoint's scratch, kept between calls (grow-only): dL/dout per
+   * pixel, the cells' gradients, the walk's links */
+  double *d_adj_dl, *d_adj_g;
+  int *d_adj_next, *d_adj_first;
+  size_t adj_dl_cap, adj_g_cap, adj_next_cap, adj_first_cap;
   struct BatchState *batch; /* batch model and work arrays (ipg_batch.cuh) */
   void *batch_arena;        /* buffers of the batch image driver (ipg_refine.cu) */
   char err[512];
@@ -1649,6 +1654,10 @@ extern "C" void ipg_destroy(ipg_ctx *ctx)
   ipg__batch_arena_release(ctx->batch_arena);
   batch_release(ctx);
   cudaFree(ctx->d_trace_extra);
+  cudaFree(ctx->d_adj_dl);
+  cudaFree(ctx->d_adj_g);
+  cudaFree(ctx->d_adj_next);
+  cudaFree(ctx->d_adj_first);
   cudaFree(ctx->d_fields);
   cudaFree(ctx->d_pool);
   cudaFree(ctx->d_chunk_prev);
