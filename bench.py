@@ -407,7 +407,9 @@ def run_ours(args):
     alg_total = sum(alg.values())
     exec_total = sum(EXEC_FLOPS_PER_STEP.values()) * steps
     traffic = DRAM_BYTES_PER_STEP[dom] * (steps / args.steps)
-    roofline = {"bound": "fp64", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+    # the transfer walk stages its records in shared memory unless IPG_XFER_STAGE=0
+    kname = "k_transfer_staged" if dom == "transfer" and os.environ.get("IPG_XFER_STAGE", "1") != "0" else f"k_{dom}"
+    roofline = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "traffic_note": "DRAM bytes per image (all class launches of the kernel): ncu bytes per ray-step "
                                 "of the 200x200 small case times this image's ray-steps",
