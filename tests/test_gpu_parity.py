@@ -69,19 +69,28 @@ def test_rays_against_oracle(dumps, ctx):
     gpu = ctx.trace(cam, ij)
     orc = Oracle(m.grid, [m.field(q) for q in range(10)])
     ref = common.oracle_tracer(orc)(cam, ij)
+    # Bounds at about ten times the measured worst case of these 96 rays
+    # (every ray with the oracle's step count; I 8.0e-8, Q and U 2.9e-5 of I,
+    # V 1.4e-7 of I): the rounding differences of the contracted (FMA)
+    # kernels against the oracle's unfused arithmetic, grown along the ray;
+    # Q and U carry them through the Faraday rotation angle.
     same = gpu["nstep"] == ref["nstep"]
-    assert same.mean() >= 0.97, (gpu["nstep"][~same], ref["nstep"][~same])
+    print("rays with the oracle's step count:", same.sum(), "of", len(same))
+    assert same.all(), (gpu["nstep"][~same], ref["nstep"][~same])
     assert np.array_equal(gpu["flag"], ref["flag"])
     for k in ("I_unpol", "I"):
         g, r = gpu[k][same], ref[k][same]
         assert np.array_equal(g == 0, r == 0), k  # rays that miss all emission agree exactly
         nz = r != 0
         rel = np.abs(g[nz] / r[nz] - 1)
-        assert rel.max() < 2e-5, (k, rel.max())
+        print(k, "max rel", rel.max(), "median", np.median(rel))
+        assert rel.max() < 1e-6, (k, rel.max())
     I = ref["I"][same]
     nz = I > 0
     for k in ("Q", "U", "V"):
-        assert np.max(np.abs(gpu[k][same][nz] - ref[k][same][nz]) / I[nz]) < 2e-4, k
+        d = np.abs(gpu[k][same][nz] - ref[k][same][nz]) / I[nz]
+        print(k, "max of I", d.max(), "median", np.median(d))
+        assert d.max() < (2e-6 if k == "V" else 3e-4), (k, d.max())
     np.testing.assert_allclose(gpu["tau"][same], ref["tau"][same], rtol=1e-5, atol=1e-12)
 
 
@@ -148,9 +157,12 @@ def test_near_polar_camera_against_oracle(dumps):
         g = c.trace(cam, ij)
     r = common.oracle_tracer(Oracle(m.grid, [m.field(q) for q in range(10)]))(cam, ij)
     same = g["nstep"] == r["nstep"]
-    assert same.mean() > 0.9
+    print("near-polar rays with the oracle's step count:", same.sum(), "of", len(same))
+    # measured: every ray with the oracle's step count, I within 4.6e-8
+    assert same.all(), (g["nstep"][~same], r["nstep"][~same])
     rel = np.abs(g["I"][same] - r["I"][same]) / np.maximum(np.abs(r["I"][same]), 1e-300)
-    assert rel.max() < 1e-4
+    print("near-polar I max rel", rel.max(), "median", np.median(rel))
+    assert rel.max() < 1e-6
 
 
 def test_device_pointer_entry(dumps):
