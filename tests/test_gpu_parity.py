@@ -69,7 +69,7 @@ def test_rays_against_oracle(dumps, ctx):
     gpu = ctx.trace(cam, ij)
     orc = Oracle(m.grid, [m.field(q) for q in range(10)])
     ref = common.oracle_tracer(orc)(cam, ij)
-    # Bounds at about ten times the measured worst case of these 96 rays
+    # Bounds at seven to fifteen times the measured worst case of these 96 rays
     # (every ray with the oracle's step count; I 8.0e-8, Q and U 2.9e-5 of I,
     # V 1.4e-7 of I): the rounding differences of the contracted (FMA)
     # kernels against the oracle's unfused arithmetic, grown along the ray;
@@ -90,7 +90,7 @@ def test_rays_against_oracle(dumps, ctx):
     for k in ("Q", "U", "V"):
         d = np.abs(gpu[k][same][nz] - ref[k][same][nz]) / I[nz]
         print(k, "max of I", d.max(), "median", np.median(d))
-        assert d.max() < (2e-6 if k == "V" else 3e-4), (k, d.max())
+        assert d.max() < (2e-6 if k == "V" else 2e-4), (k, d.max())
     np.testing.assert_allclose(gpu["tau"][same], ref["tau"][same], rtol=1e-5, atol=1e-12)
 
 
