@@ -531,19 +531,32 @@ def bench_batched(ip, ctx, model, dump, args, world, stream, single_ms):
         for fi, fq in enumerate(BATCH_FREQS):
             for ii, inc in enumerate(BATCH_INCL):
                 ps96 += batch_params(ip, dump, args.m_unit, BATCH_RES[(fi + ii) % 3], inc, fq, refine=True)
-        t = time.time()
-        imgs = ctx.render_batch(ps96, model)
-        torch.cuda.synchronize()
-        sec = time.time() - t
-        st = ctx.stats()
-        pix = sum(int(i.traced) for i in imgs)
-        res["workload_96"] = {"value": len(ps96) / sec, "unit": "images/s", "seconds": sec,
-                              "instances": len(ps96), "traced_pixels": pix, "ray_steps": st["ray_steps"],
-                              "pixels_per_s": pix / sec,
-                              "workload": "96 instances: {86,230,345} GHz x thetacam {17,60,120,163} x R_high "
-                                          "{1,10,40,160} x M_unit {0.5,2} x base; 64/160/320 pixels a side per "
-                                          "camera, refined from a quarter (refine_abs 2e-2, refine_rel 1e-2); "
-                                          "host-timed single call"}
+        # FP64, then the mixed tier (FP32 step, FP32 fit shapes, compact
+        # records); each timed on its second call (the first tunes the
+        # transfer's block size for the batch's shape)
+        for tag, mixed in (("workload_96", False), ("workload_96_mixed", True)):
+            ctx.set_step_precision(ip.IPG_STEP_FP32 if mixed else ip.IPG_STEP_FP64)
+            ctx.set_fit_precision(ip.IPG_FITS_FP32 if mixed else ip.IPG_FITS_FP64)
+            ctx.set_record_precision(ip.IPG_RECORDS_MIXED if mixed else ip.IPG_RECORDS_FP64)
+            ctx.render_batch(ps96, model)
+            torch.cuda.synchronize()
+            t = time.time()
+            imgs = ctx.render_batch(ps96, model)
+            torch.cuda.synchronize()
+            sec = time.time() - t
+            st = ctx.stats()
+            pix = sum(int(i.traced) for i in imgs)
+            res[tag] = {"value": len(ps96) / sec, "unit": "images/s", "seconds": sec,
+                        "instances": len(ps96), "traced_pixels": pix, "ray_steps": st["ray_steps"],
+                        "pixels_per_s": pix / sec,
+                        "workload": "96 instances: {86,230,345} GHz x thetacam {17,60,120,163} x R_high "
+                                    "{1,10,40,160} x M_unit {0.5,2} x base; 64/160/320 pixels a side per "
+                                    "camera, refined from a quarter (refine_abs 2e-2, refine_rel 1e-2); "
+                                    "host-timed call after one untimed call"
+                                    + ("; mixed tier" if mixed else "; FP64")}
+        ctx.set_step_precision(ip.IPG_STEP_FP64)
+        ctx.set_fit_precision(ip.IPG_FITS_FP64)
+        ctx.set_record_precision(ip.IPG_RECORDS_FP64)
     return res
 
 
