@@ -407,8 +407,10 @@ def run_ours(args):
     alg_total = sum(alg.values())
     exec_total = sum(EXEC_FLOPS_PER_STEP.values()) * steps
     traffic = DRAM_BYTES_PER_STEP[dom] * (steps / args.steps)
-    # the transfer walk stages its records in shared memory unless IPG_XFER_STAGE=0
-    kname = "k_transfer_staged" if dom == "transfer" and os.environ.get("IPG_XFER_STAGE", "1") != "0" else f"k_{dom}"
+    # the walk of FP64 records fetches them by bulk copies into shared memory
+    # unless IPG_XFER_STAGE selects 16-byte copies (1) or global loads (0)
+    walk = {"0": "k_transfer", "1": "k_transfer_staged"}.get(os.environ.get("IPG_XFER_STAGE", ""), "k_transfer_bulk")
+    kname = walk if dom == "transfer" else f"k_{dom}"
     roofline = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "traffic_note": "DRAM bytes per image (all class launches of the kernel): ncu bytes per ray-step "

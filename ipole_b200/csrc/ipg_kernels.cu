@@ -51,7 +51,7 @@ struct RayRec {
   int pad;
 };
 
-enum { CNT_POOL = 0, CNT_STEPS = 1, CNT_RAD = 2, CNT_DEFER = 3, CNT_NEXT_G = 4, CNT_NEXT_T = 5, CNT_N = 6 };
+enum { CNT_POOL = 0, CNT_STEPS = 1, CNT_RAD = 2, CNT_DEFER = 3, CNT_NEXT_G = 4, CNT_NEXT_T = 5, CNT_STALL = 6, CNT_N = 7 };
 /* the counters of a batch wave (ipg_batch.cuh) continue the list: transfer
  * items deferred, the wave's step budget (0: none), the budget-spent flag,
  * transfer steps done */
@@ -1399,6 +1399,165 @@ __global__ void __launch_bounds__(TPB, MINB)
   cp_async_wait<0>();
 }
 
+/* The same walk with each record part fetched by one bulk copy of the
+ * tensor-memory-access unit (cp.async.bulk, completion on an mbarrier of the
+ * lane's slot) instead of 16-byte copies through the load/store pipe: the
+ * staged walk's largest stall is the shared-memory instruction queue (mio
+ * throttle), which its 32 copies per step fill.  A slot's barrier flips its
+ * phase when its copy has landed; before a slot is refilled, a proxy fence
+ * orders the lane's reads of it before the copy's writes.  Every wait is
+ * bounded: a copy that has not landed after IPG_XFER_BULK_SPINS polls sets
+ * CNT_STALL and ends the lane, and the host reports the call as failed. */
+#ifndef IPG_XFER_BULK_SPINS
+#define IPG_XFER_BULK_SPINS (1u << 20)
+#endif
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bulk_fetch(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+/* waits for the barrier's phase `parity` to complete; false if it did not
+ * within the bound */
+__device__ __forceinline__ bool bulk_wait(unsigned long long *bar, unsigned parity)
+{
+  for (unsigned it = 0; it < IPG_XFER_BULK_SPINS; it++) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_slot_refill() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false, int RM = 0>
+__global__ void __launch_bounds__(TPB, MINB)
+    k_transfer_bulk(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
+                    const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays,
+                    ipg_pixel_out *__restrict__ out, unsigned long long *__restrict__ counters)
+{
+  static_assert(RM == 0 || RM == 1, "the staged walk is compiled per record layout");
+  using X = typename XStageOf<RM>::T;
+  constexpr int NBC = XStageOf<RM>::NBC;
+  extern __shared__ __align__(16) unsigned char xsm[];
+  __shared__ __align__(8) unsigned long long xbar[TPB][NBC + 1]; /* per lane: coefficient slot(s), matrices slot */
+  unsigned char *slot_c = xsm + (size_t)threadIdx.x * X::LANE;
+  unsigned char *slot_a = slot_c + NBC * X::P1;
+  const double *view_a = reinterpret_cast<const double *>(slot_a);
+  unsigned long long *bar = xbar[threadIdx.x];
+#pragma unroll
+  for (int j = 0; j <= NBC; j++)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + j)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  unsigned ph = 0;   /* phase parity of each barrier */
+  unsigned pend = 0; /* barriers with a copy issued and not yet waited for */
+  const DevCam &C = c_cam;
+  const int unpol = C.unpol;
+  XferLane L;
+  int n0 = 0;
+  bool has = xfer_fetch<RM>(L, list, n_list, pool, chunk_prev, rays, out, counters);
+  auto fetch = [&](void *dst, const void *src, unsigned bytes, int j) {
+    bulk_fetch(dst, src, bytes, bar + j);
+    pend |= 1u << j;
+  };
+  auto wait = [&](int j) {
+    bool ok = bulk_wait(bar + j, (ph >> j) & 1);
+    ph ^= 1u << j;
+    pend &= ~(1u << j);
+    return ok;
+  };
+  auto start = [&]() {
+    n0 = L.n;
+    if (!unpol && L.n > 0) fetch(slot_a, L.rec_i, X::P2, NBC);
+  };
+  /* a copy that did not land: flag it, give the lane's other copies in
+   * flight their bounded wait, and end the lane */
+  auto stall = [&]() {
+    atomicAdd(&counters[CNT_STALL], 1ULL);
+    for (int j = 0; j <= NBC; j++)
+      if (pend & (1u << j)) wait(j);
+    has = false;
+  };
+  if (has) start();
+  while (__any_sync(0xffffffffu, has)) {
+    if (!has) continue;
+    const int k = L.n;
+    const double *rec_f = nullptr; /* record k-1 */
+    if (k >= 1) {
+      const int s = k - 1;
+      if (s % IPG_CHUNK_STEPS == IPG_CHUNK_STEPS - 1) {
+        L.chunk = L.cprev;
+        L.cprev = chunk_prev[L.chunk];
+      }
+      rec_f = step_ptr(const_cast<double *>(pool), L.chunk, s % IPG_CHUNK_STEPS);
+      if (s >= 1) {
+        if ((s - 1) % IPG_CHUNK_STEPS != IPG_CHUNK_STEPS - 1) prefetch_rec<RM>(rec_f - IPG_STEP_DOUBLES);
+        else if (L.cprev >= 0) prefetch_rec<RM>(step_ptr(const_cast<double *>(pool), L.cprev, IPG_CHUNK_STEPS - 1));
+      }
+    }
+    const unsigned char *src_c = reinterpret_cast<const unsigned char *>(rec_f) + X::P1_OFF;
+    if constexpr (NBC == 2) {
+      if (k >= 1) {
+        fence_slot_refill();
+        fetch(slot_c + ((k - 1) & 1) * X::P1, src_c, X::P1, (k - 1) & 1);
+      }
+    }
+    /* the transfer step k+1 -> k with record k's coefficients */
+    if (k < n0) {
+      const int j = NBC == 2 ? (k & 1) : 0;
+      if (!wait(j)) {
+        stall();
+        continue;
+      }
+      CoefBlock cb;
+      const double *view_c = reinterpret_cast<const double *>(slot_c + j * X::P1 - X::P1_OFF);
+      if constexpr (RM) load_coef_m(view_c, cb);
+      else load_coef(view_c, cb);
+      xfer_evolve<S32>(C, L, cb, L.dl_i, unpol);
+      L.dl_i = cb.dl;
+      L.nturns_i = cb.nturns;
+    }
+    if (k == 0) {
+      ipg_pixel_out o;
+      xfer_result(C, L, unpol, rays[L.ray].nstep, &o);
+      out[L.ray] = o;
+      atomicAdd(&counters[CNT_RAD], (unsigned long long)L.nrad);
+      has = xfer_fetch<RM>(L, list, n_list, pool, chunk_prev, rays, out, counters);
+      if (has) start();
+      continue;
+    }
+    if constexpr (NBC == 1) {
+      fence_slot_refill(); /* the slot was read by the load above */
+      fetch(slot_c, src_c, X::P1, 0);
+    }
+    /* push_polar for the step k -> k-1 with record k's matrices, then the
+     * fetch of record k-1's matrices into the slot the push has read */
+    if (!unpol) {
+      if (!wait(NBC)) {
+        stall();
+        continue;
+      }
+      xfer_push<S32, RM>(L, view_a, L.dl_i);
+      if (k >= 2) {
+        fence_slot_refill();
+        fetch(slot_a, rec_f, X::P2, NBC);
+      }
+    }
+    L.rec_i = rec_f;
+    L.n = k - 1;
+  }
+}
+
 /* ===================================================================== */
 /* longest-first order                                                    */
 /* ===================================================================== */
@@ -1504,6 +1663,9 @@ static void devgrid_derived(DevGrid *d)
 #endif
 static const double k_class_facs[] = {PRED_CLASS_FACS};
 #define NB_MAX ((int)(sizeof(k_class_facs) / sizeof(k_class_facs[0])) + 1)
+#ifndef IPG_COEF_WAIT_LONGEST
+#define IPG_COEF_WAIT_LONGEST 1 /* the shorter classes' coefficient passes wait for the longest class's geodesics */
+#endif
 #define IPG_STARTED_MAX 1024   /* geodesic blocks of the longest class that can mark their start */
 #define IPG_STARTED_WAIT_US 2000 /* the host's wait for them */
 
@@ -1533,7 +1695,7 @@ struct ipg_ctx {
   int32_t *d_pred;   /* predicted step counts (list positions), also staging */
   int *d_len_hist;   /* LEN_BUCKETS counters of the sort */
   int split;         /* 1: split waves into long and short batches */
-  int xstage;        /* 1: the transfer walk stages its records in shared memory */
+  int xstage;        /* records of the walk: 0 global loads, 1 16-byte copies, 2 bulk copies, -1 per layout */
   int emission_type; /* of the camera being traced */
   int rec_mixed;     /* IPG_RECORDS_MIXED: compact step records */
   int step32;        /* IPG_STEP_FP32: the polarized step in FP32 */
@@ -1618,11 +1780,14 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_cnt, (NB_MAX + 1) * CNT_N * sizeof(unsigned long long));
   ctx->split = 1;
   if (getenv("IPG_NO_SPLIT")) ctx->split = 0;
-  /* the transfer walk with its records staged in shared memory (default);
-   * IPG_XFER_STAGE=0 selects the walk that loads them from global memory */
+  /* how the transfer walk reads its step records: by default staged in
+   * shared memory, by one bulk copy per record part for FP64 records and by
+   * 16-byte copies for compact records (the faster of the two for each
+   * layout on the 400x400 image); IPG_XFER_STAGE=0 loads them from global
+   * memory, =1 and =2 select the 16-byte and the bulk copies for both */
   {
     const char *xs = getenv("IPG_XFER_STAGE");
-    ctx->xstage = (xs && xs[0] == '0') ? 0 : 1;
+    ctx->xstage = (xs && xs[0] >= '0' && xs[0] <= '2') ? xs[0] - '0' : -1;
   }
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void *)k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0>,
@@ -1635,6 +1800,18 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
                              cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<1>::T::LANE);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void *)k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, true, 1>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<1>::T::LANE);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void *)k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<0>::T::LANE);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void *)k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, true, 0>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<0>::T::LANE);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void *)k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, false, 1>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<1>::T::LANE);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void *)k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, true, 1>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, IPG_XFER_WIDE * XStageOf<1>::T::LANE);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_len_hist, LEN_BUCKETS * sizeof(int));
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device);
@@ -1892,6 +2069,14 @@ static int grid_blocks(ipg_ctx *ctx, const void *kernel, int threads, size_t n, 
   return (int)(need < full ? need : full);
 }
 
+/* a bulk copy of the transfer walk that did not land within its bounded
+ * wait (no such copy has been seen: its source is the pool, in bounds) */
+static int stall_fail(ipg_ctx *ctx)
+{
+  snprintf(ctx->err, sizeof(ctx->err), "a step record's copy into shared memory did not complete");
+  return IPG_E_CUDA;
+}
+
 /* The host waits (at most IPG_STARTED_WAIT_US) until the first n blocks of
  * a launch have marked their start.  Launched first but placed behind the
  * shorter classes' blocks, the longest class's SM-filling blocks wait for
@@ -1992,7 +2177,14 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
    * holding only its own paths */
 #define IPG_LAUNCH_XFER(S32, RM)                                                                              \
   do {                                                                                                       \
-    if (ctx->xstage) {                                                                                       \
+    const int xmode = ctx->xstage >= 0 ? ctx->xstage : (RM ? 1 : 2);                                         \
+    if (xmode == 2) {                                                                                        \
+      size_t sm = (size_t)xthreads * XStageOf<RM>::T::LANE;                                                  \
+      int tb = grid_blocks(ctx, (const void *)k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM>,        \
+                           xthreads, b.run, sm);                                                             \
+      k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM><<<tb, xthreads, sm, b.stream>>>(               \
+          b.list, (int)b.run, b.pool, b.chunk_prev, ctx->d_rays, d_out, b.cnt);                              \
+    } else if (xmode == 1) {                                                                                 \
       size_t sm = (size_t)xthreads * XStageOf<RM>::T::LANE;                                                       \
       int tb = grid_blocks(ctx, (const void *)k_transfer_staged<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM>,      \
                            xthreads, b.run, sm);                                                             \
@@ -2286,7 +2478,7 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
         /* the shorter classes' coefficient passes wait for the longest
          * class's geodesics: run beside them, they slow the longest rays'
          * steps four- to eightfold (those rays' SMs hold no other block) */
-        if (b > 0 && wide[0]) bt[b].coef_after = ctx->bev[0][1];
+        if (IPG_COEF_WAIT_LONGEST && b > 0 && wide[0]) bt[b].coef_after = ctx->bev[0][1];
         c0 += ncb;
         r0 += sizes[b];
       }
@@ -2309,6 +2501,8 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
       CK(cudaMemcpyAsync(cnt, ctx->d_cnt + CNT_N, nb * CNT_N * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                          ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
+      for (int b = 0; b < nb; b++)
+        if (cnt[b * CNT_N + CNT_STALL]) return stall_fail(ctx);
       float pms = 0.f, wms = 0.f;
       cudaEventElapsedTime(&pms, ctx->ev_pred[0], ctx->ev_pred[1]);
       ctx->stats.predict_ms += pms;
@@ -2379,6 +2573,7 @@ static int trace_core(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *d_ij, 
       unsigned long long cnt[CNT_N];
       CK(cudaMemcpyAsync(cnt, cnt_d, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
+      if (cnt[CNT_STALL]) return stall_fail(ctx);
       float wms = 0.f;
       cudaEventElapsedTime(&wms, ctx->ev[0], ctx->ev[3]);
       ctx->stats.wall_ms += wms;

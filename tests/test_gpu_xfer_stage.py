@@ -1,11 +1,13 @@
-"""The transfer walk with its step records staged in shared memory
-(k_transfer_staged, the default) against the walk that loads them from
-global memory (k_transfer, IPG_XFER_STAGE=0).
+"""The transfer walks with their step records staged in shared memory, by
+16-byte copies (k_transfer_staged, IPG_XFER_STAGE=1; the default for
+compact records) and by one bulk copy per record part (k_transfer_bulk,
+IPG_XFER_STAGE=2; the default for FP64 records), against the walk that loads
+them from global memory (k_transfer, IPG_XFER_STAGE=0).
 
-Both run the operations of integrate_emission's loop (src/ipolarray.c:78-244)
-in the same order; the staged walk only regroups them by record (the
+All run the operations of integrate_emission's loop (src/ipolarray.c:78-244)
+in the same order; the staged walks only regroup them by record (the
 transfer step with record k's coefficients, then the push with record k's
-transport matrices) and reads the records from shared memory.  So every
+transport matrices) and read the records from shared memory.  So every
 image, in every step arithmetic and record layout, must be bit-identical.
 """
 import os
@@ -26,7 +28,7 @@ FORMS = [(ip.IPG_RECORDS_FP64, ip.IPG_STEP_FP64), (ip.IPG_RECORDS_MIXED, ip.IPG_
 
 def _render(p, m, stage, rec, step):
     old = os.environ.get("IPG_XFER_STAGE")
-    os.environ["IPG_XFER_STAGE"] = "1" if stage else "0"
+    os.environ["IPG_XFER_STAGE"] = str(stage)
     try:
         with ip.Context() as c:  # the setting is read when a context is created
             c.upload(m)
@@ -46,9 +48,10 @@ def test_staged_walk_bit_identical(case, dumps):
     p = common.params_for(meta, dumps.get(meta))
     m = ip.Model.load(p)
     for rec, step in FORMS:
-        a = _render(p, m, False, rec, step)
-        b = _render(p, m, True, rec, step)
-        assert np.array_equal(a.nstep, b.nstep)
-        assert a.unpol.tobytes() == b.unpol.tobytes(), (case, rec, step)
-        if a.pol is not None:
-            assert a.pol.tobytes() == b.pol.tobytes(), (case, rec, step)
+        a = _render(p, m, 0, rec, step)
+        for stage in (1, 2):  # 16-byte copies, bulk copies
+            b = _render(p, m, stage, rec, step)
+            assert np.array_equal(a.nstep, b.nstep)
+            assert a.unpol.tobytes() == b.unpol.tobytes(), (case, rec, step, stage)
+            if a.pol is not None:
+                assert a.pol.tobytes() == b.pol.tobytes(), (case, rec, step, stage)
