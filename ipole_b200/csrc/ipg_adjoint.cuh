@@ -579,9 +579,20 @@ static int adjoint_wave(ipg_ctx *ctx, int em, const int32_t *d_ij, const int32_t
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[3], st));
-  int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0, K>, threads, run);
-  k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0, K><<<tb, threads, 0, st>>>(
-      list, (int)run, pool, ctx->d_chunk_prev, ctx->d_rays, d_out, cnt, ckpt);
+  if (ctx->xstage < 0 || ctx->xstage == 2) {
+    /* the walk of FP64 records with bulk copies into shared memory, as the
+     * image's (bit-identical to the walk that loads from global memory) */
+    const void *fn = (const void *)k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0, K>;
+    const size_t sm = (size_t)threads * XStageOf<0>::T::LANE;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int tb = grid_blocks(ctx, fn, threads, run, sm);
+    k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0, K><<<tb, threads, sm, st>>>(
+        list, (int)run, pool, ctx->d_chunk_prev, ctx->d_rays, d_out, cnt, ckpt);
+  } else {
+    int tb = grid_blocks(ctx, (const void *)k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0, K>, threads, run);
+    k_transfer<IPG_XFER_WIDE, IPG_XFER_MINB, false, 0, K><<<tb, threads, 0, st>>>(
+        list, (int)run, pool, ctx->d_chunk_prev, ctx->d_rays, d_out, cnt, ckpt);
+  }
   CK(cudaGetLastError());
   CK(cudaEventRecord(ctx->ev[4], st));
   k_adj_link<<<4 * ctx->n_sm, 256, 0, st>>>(ctx->d_chunk_prev, ctx->d_chunk_meta, cnt, n_chunks, next, first);
@@ -699,6 +710,7 @@ extern "C" int ipg_adjoint(ipg_ctx *ctx, const ipg_camera *cam, const int32_t *i
     unsigned long long h[CNT_N];
     CKA(cudaMemcpyAsync(h, ctx->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
     CKA(cudaStreamSynchronize(st));
+    if (h[CNT_STALL]) return stall_fail(ctx);
     float ms = 0.f, t[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     cudaEventElapsedTime(&t[0], ctx->ev[0], ctx->ev[2]);

@@ -1440,11 +1440,14 @@ __device__ __forceinline__ bool bulk_wait(unsigned long long *bar, unsigned pari
 
 __device__ __forceinline__ void fence_slot_refill() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false, int RM = 0>
+/* CKK > 0 (the adjoint's forward pass): N at every record k with
+ * k % CKK == 0, before the push k -> k-1, is kept in ckpt as by k_transfer */
+template <int TPB = IPG_XFER_WIDE, int MINB = IPG_XFER_MINB, bool S32 = false, int RM = 0, int CKK = 0>
 __global__ void __launch_bounds__(TPB, MINB)
     k_transfer_bulk(const int32_t *__restrict__ list, int n_list, const double *__restrict__ pool,
                     const int *__restrict__ chunk_prev, const RayRec *__restrict__ rays,
-                    ipg_pixel_out *__restrict__ out, unsigned long long *__restrict__ counters)
+                    ipg_pixel_out *__restrict__ out, unsigned long long *__restrict__ counters,
+                    double *__restrict__ ckpt = nullptr)
 {
   static_assert(RM == 0 || RM == 1, "the staged walk is compiled per record layout");
   using X = typename XStageOf<RM>::T;
@@ -1492,6 +1495,7 @@ __global__ void __launch_bounds__(TPB, MINB)
   while (__any_sync(0xffffffffu, has)) {
     if (!has) continue;
     const int k = L.n;
+    const int chunk_k = L.chunk; /* record k's chunk */
     const double *rec_f = nullptr; /* record k-1 */
     if (k >= 1) {
       const int s = k - 1;
@@ -1539,6 +1543,16 @@ __global__ void __launch_bounds__(TPB, MINB)
     if constexpr (NBC == 1) {
       fence_slot_refill(); /* the slot was read by the load above */
       fetch(slot_c, src_c, X::P1, 0);
+    }
+    if constexpr (CKK > 0) {
+      if (k % CKK == 0) {
+        constexpr int KC = CKK < IPG_CHUNK_STEPS ? CKK : IPG_CHUNK_STEPS;
+        double *q = ckpt + (((size_t)chunk_k * IPG_CHUNK_STEPS + k % IPG_CHUNK_STEPS) / KC) * 16;
+        store4(q, L.N.r00, L.N.r01, L.N.r02, L.N.r03);
+        store4(q + 4, L.N.r11, L.N.r12, L.N.r13, L.N.r22);
+        store4(q + 8, L.N.r23, L.N.r33, L.N.s01, L.N.s02);
+        store4(q + 12, L.N.s03, L.N.s12, L.N.s13, L.N.s23);
+      }
     }
     /* push_polar for the step k -> k-1 with record k's matrices, then the
      * fetch of record k-1's matrices into the slot the push has read */
