@@ -408,8 +408,10 @@ def run_ours(args):
     exec_total = sum(EXEC_FLOPS_PER_STEP.values()) * steps
     traffic = DRAM_BYTES_PER_STEP[dom] * (steps / args.steps)
     # the walk of FP64 records fetches them by bulk copies into shared memory
-    # unless IPG_XFER_STAGE selects 16-byte copies (1) or global loads (0)
-    walk = {"0": "k_transfer", "1": "k_transfer_staged"}.get(os.environ.get("IPG_XFER_STAGE", ""), "k_transfer_bulk")
+    # (16-byte copies in the longest length class) unless IPG_XFER_STAGE
+    # selects 16-byte copies (1) or global loads (0) for every class
+    walk = {"0": "k_transfer", "1": "k_transfer_staged"}.get(os.environ.get("IPG_XFER_STAGE", ""),
+                                                           "k_transfer_bulk (k_transfer_staged for the longest class)")
     kname = walk if dom == "transfer" else f"k_{dom}"
     roofline = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,

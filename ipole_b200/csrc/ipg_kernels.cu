@@ -1795,10 +1795,14 @@ extern "C" int ipg_create(ipg_ctx **out, int device, size_t pool_bytes)
   ctx->split = 1;
   if (getenv("IPG_NO_SPLIT")) ctx->split = 0;
   /* how the transfer walk reads its step records: by default staged in
-   * shared memory, by one bulk copy per record part for FP64 records and by
-   * 16-byte copies for compact records (the faster of the two for each
-   * layout on the 400x400 image); IPG_XFER_STAGE=0 loads them from global
-   * memory, =1 and =2 select the 16-byte and the bulk copies for both */
+   * shared memory; for FP64 records by 16-byte copies in the longest length
+   * class (lower latency per step: its walk alone takes 50 ms against 65 ms
+   * with bulk copies) and by one bulk copy per record part in the others
+   * (higher throughput: the bulk class's walk alone 29 ms against 50 ms),
+   * for compact records by 16-byte copies in every class (measured a little
+   * faster on the 400x400 image); IPG_XFER_STAGE=0 loads them from global
+   * memory, =1 and =2 select the 16-byte and the bulk copies for every
+   * class */
   {
     const char *xs = getenv("IPG_XFER_STAGE");
     ctx->xstage = (xs && xs[0] >= '0' && xs[0] <= '2') ? xs[0] - '0' : -1;
@@ -2191,7 +2195,7 @@ static int launch_batch_t(ipg_ctx *ctx, const Batch &b, const int32_t *d_ij, ipg
    * holding only its own paths */
 #define IPG_LAUNCH_XFER(S32, RM)                                                                              \
   do {                                                                                                       \
-    const int xmode = ctx->xstage >= 0 ? ctx->xstage : (RM ? 1 : 2);                                         \
+    const int xmode = ctx->xstage >= 0 ? ctx->xstage : ((RM || b.wide) ? 1 : 2);                             \
     if (xmode == 2) {                                                                                        \
       size_t sm = (size_t)xthreads * XStageOf<RM>::T::LANE;                                                  \
       int tb = grid_blocks(ctx, (const void *)k_transfer_bulk<IPG_XFER_WIDE, IPG_XFER_MINB, S32, RM>,        \
