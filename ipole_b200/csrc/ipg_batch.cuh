@@ -166,8 +166,11 @@ __device__ __forceinline__ void store_shared_m(double *p, int flags, double dl, 
   t[3] = make_float4((float)b[0], (float)b[1], (float)b[2], (float)b[3]);
 }
 
+#ifndef IPG_BCOEF_MINB
+#define IPG_BCOEF_MINB IPG_COEF_MINB /* blocks of 128 per SM the batch's coefficient pass is compiled for */
+#endif
 template <int EM, bool F32 = false, bool RM = false>
-__global__ void __launch_bounds__(128, IPG_COEF_MINB)
+__global__ void __launch_bounds__(128, IPG_BCOEF_MINB)
     k_coef_batch(double *__restrict__ pool, double *__restrict__ side, int G, const int2 *__restrict__ chunk_meta,
                  const unsigned long long *__restrict__ counters, long long n_chunks, const RayRec *__restrict__ rays,
                  const int32_t *__restrict__ geo_grp, const uint32_t *__restrict__ geo_mask,
