@@ -1,8 +1,10 @@
 """The transfer walks with their step records staged in shared memory, by
-16-byte copies (k_transfer_staged, IPG_XFER_STAGE=1; the default for
-compact records) and by one bulk copy per record part (k_transfer_bulk,
-IPG_XFER_STAGE=2; the default for FP64 records), against the walk that loads
-them from global memory (k_transfer, IPG_XFER_STAGE=0).
+16-byte copies (k_transfer_staged, IPG_XFER_STAGE=1) and by one bulk copy
+per record part (k_transfer_bulk, IPG_XFER_STAGE=2), and the default mixture
+(IPG_XFER_STAGE unset: bulk copies for FP64 records except in the longest
+length class, 16-byte copies otherwise; the 128x128 case is split into
+length classes), against the walk that loads them from global memory
+(k_transfer, IPG_XFER_STAGE=0).
 
 All run the operations of integrate_emission's loop (src/ipolarray.c:78-244)
 in the same order; the staged walks only regroup them by record (the
@@ -28,7 +30,10 @@ FORMS = [(ip.IPG_RECORDS_FP64, ip.IPG_STEP_FP64), (ip.IPG_RECORDS_MIXED, ip.IPG_
 
 def _render(p, m, stage, rec, step):
     old = os.environ.get("IPG_XFER_STAGE")
-    os.environ["IPG_XFER_STAGE"] = str(stage)
+    if stage is None:
+        os.environ.pop("IPG_XFER_STAGE", None)
+    else:
+        os.environ["IPG_XFER_STAGE"] = str(stage)
     try:
         with ip.Context() as c:  # the setting is read when a context is created
             c.upload(m)
@@ -37,7 +42,7 @@ def _render(p, m, stage, rec, step):
             return c.render(p, m)
     finally:
         if old is None:
-            del os.environ["IPG_XFER_STAGE"]
+            os.environ.pop("IPG_XFER_STAGE", None)
         else:
             os.environ["IPG_XFER_STAGE"] = old
 
@@ -49,7 +54,7 @@ def test_staged_walk_bit_identical(case, dumps):
     m = ip.Model.load(p)
     for rec, step in FORMS:
         a = _render(p, m, 0, rec, step)
-        for stage in (1, 2):  # 16-byte copies, bulk copies
+        for stage in (1, 2, None):  # 16-byte copies, bulk copies, the default
             b = _render(p, m, stage, rec, step)
             assert np.array_equal(a.nstep, b.nstep)
             assert a.unpol.tobytes() == b.unpol.tobytes(), (case, rec, step, stage)
