@@ -27,7 +27,7 @@ CLI = os.path.join(BIN, "ipole_b200")
 
 NVCC_FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-v"]
-CC_FLAGS = ["-std=gnu99", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-result"]
+CC_FLAGS = ["-std=gnu99", "-O2", "-fPIC", "-ffp-contract=off", "-fopenmp", "-Wall", "-Wno-unused-result"]
 CU_EXTRA = ["ipg_refine.cu"]
 HOST_SRC = ["ipgc.c", "h5lite.c", "plugins.c", "trace.c", "coords.c", "par.c", "model_iharm.c", "camera.c", "render.c",
             "model_api.c"]
@@ -100,7 +100,7 @@ def build(force: bool = False, verbose: bool = False, defines=(), out_dir: str |
             _run([_cc(), *CC_FLAGS, "-I", INC, "-c", os.path.join(HOST, s), "-o", o], log)
             objs.append(o)
         tmp = lib + ".tmp"
-        _run([_nvcc(), "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-lz", "-lm"], log)
+        _run([_nvcc(), "-shared", "-Xcompiler", "-fPIC,-fopenmp", "-o", tmp, *objs, "-lz", "-lm"], log)
         os.replace(tmp, lib)
         if not out_dir:
             _run([_cc(), *CC_FLAGS, "-I", INC, os.path.join(HOST, "main.c"), "-o", CLI, "-L", BUILD,
