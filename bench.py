@@ -60,9 +60,12 @@ REF_FLOPS = {"geodesic_per_step": 24172.6, "push_per_step": 30454.0, "coeffs_per
              "transfer_per_radiating_step": 4751.9}
 # What the kernels execute per ray-step, from the ncu capture of a 200x200
 # image of the 128x64x64 dump: FP64 flops (2 per DFMA, 1 per DADD/DMUL) and
-# DRAM bytes read + written (k_coeffs works per step record).
+# DRAM bytes read + written (k_coeffs works per step record); the walk's
+# bytes are those of its bulk-copy form (the image's walk outside the
+# longest class) on an unsplit 256x256 wave of the same dump, 618 per step
+# against 539 for its 16-byte-copy form.
 EXEC_FLOPS_PER_STEP = {"geodesic": 1831, "coeffs": 1535, "transfer": 913}
-DRAM_BYTES_PER_STEP = {"geodesic": 377, "coeffs": 412, "transfer": 537}
+DRAM_BYTES_PER_STEP = {"geodesic": 377, "coeffs": 412, "transfer": 619}
 
 
 def data_dir():
