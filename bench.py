@@ -419,7 +419,8 @@ def run_ours(args):
     roofline = {"bound": "fp64", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "traffic_note": "DRAM bytes per image (all class launches of the kernel): ncu bytes per ray-step "
-                                "of the 200x200 small case times this image's ray-steps",
+                                "of a small case of the 128x64x64 dump (the walk: its bulk-copy form on an "
+                                "unsplit 256x256 wave) times this image's ray-steps",
                 "frac_pipeline": alg_total / (ms / 1e3) / 1e12 / peak,
                 "frac_pipeline_executed": exec_total / (ms / 1e3) / 1e12 / peak,
                 "alg_flops_per_ray_step": alg_total / max(steps, 1),
